@@ -1,0 +1,362 @@
+#!/usr/bin/env python3
+"""Benchmark of the grid-integration Fock build (XC build of (H2O)_n, PBE).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nkx|reference]
+                    [--waters 64] [--precision auto|fp64|mixed]
+
+A step is one Fock build (one SCF iteration's XC work: collocation, density,
+functional, V_xc = Phi Z^T) over the whole synthetic (H2O)_n grid
+(Treutler-Ahlrichs 75 radial x Lebedev 302 per atom, Becke, 256-point
+batches, screening 1e-10), with the orbital coefficients already resident in
+HBM.  `e2e` is the same build through the public API with host buffers
+(C copied in, V and E copied out inside the timed region).  One JSON line is
+printed by rank 0.  With N > 1 the grid is split by atoms across ranks (one
+process per GPU) and the partial V_xc and E_xc are summed with an NCCL
+all-reduce inside the timed region (strong scaling).
+
+--impl reference times the CPU restatement of the reference's dense
+algorithm (the oracle) on a bounded, seeded sample of the same grid on all
+host cores, on the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Fock-build ms/SCF-iter and grid pts/s: mixed vs FP64 on B200 at dE_xc<=1e-6 Eh"
+UNIT = "grid_pts/s"
+FUNCS = ("GGA_X_PBE", "GGA_C_PBE")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="nkx", choices=["nkx", "reference"])
+    ap.add_argument("--waters", type=int, default=64)
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--cpu-sample", type=int, default=8192, help="points in the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n):
+    from nukexc_b200 import molecules as M
+    c, Z = M.water_cluster(n, seed=0)
+    funcs = M.sto_basis(c, Z)
+    C = M.random_orbitals(len(funcs), 5 * n, seed=0)
+    return c, Z, funcs, C
+
+
+def config(args, extra=None):
+    cfg = {"workload": f"(H2O)_{args.waters} PBE XC Fock build", "waters": args.waters,
+           "basis": "even-tempered STO zeta_k=0.5*2.2^k, O 6s4p2d, H 4s2p",
+           "grid": "Treutler-Ahlrichs M4 75 x Lebedev 302 per atom, Becke (Laqua clamp), w>1e-15",
+           "batch_points": 256, "screen_tol": 1e-10, "nocc": 5 * args.waters, "occ": 1.0,
+           "l2": "inputs larger than L2 (per-chunk workspace of several GB streamed each step)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ------------------------------------------------------- CPU baseline ----
+def cpu_sample(c, Z, funcs, C, npts):
+    """Seeded sample of the workload's grid: unpartitioned atom grids from
+    the oracle, every k-th point, Becke-partitioned by the oracle."""
+    from oracle import oracle as O
+    nr = np.full(len(Z), 75, np.int32)
+    Rs = np.array([O.radial_scale(z, "ta") for z in Z])
+    L = O._lib()
+    tot = L.orc_atom_grids(len(Z), np.ascontiguousarray(c).reshape(-1), nr, Rs, 1, 0.6, 29, None, None, None)
+    pts = np.zeros((tot, 3))
+    w = np.zeros(tot)
+    own = np.zeros(tot, np.int32)
+    L.orc_atom_grids(len(Z), np.ascontiguousarray(c).reshape(-1), nr, Rs, 1, 0.6, 29,
+                     O._ptr(pts), O._ptr(w), O._ptr(own))
+    idx = np.random.default_rng(0).choice(tot, size=min(npts, tot), replace=False)
+    idx.sort()
+    wp = O.becke(c, pts[idx], own[idx], w[idx])
+    keep = wp > 1e-15
+    return pts[idx][keep], wp[keep], tot
+
+
+def cpu_baseline(c, Z, funcs, C, npts, reps=1):
+    from oracle import oracle as O
+    pts, w, tot = cpu_sample(c, Z, funcs, C, npts)
+    ob = O.make_manual_basis(funcs)
+    occ = np.ones(C.shape[1])
+    O.xc_build(ob, pts[:256], w[:256], [101, 130], [C], [occ])  # warm-up
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.xc_build(ob, pts, w, [101, 130], [C], [occ])
+        times.append(time.perf_counter() - t0)
+    t = min(times)
+    cores = os.cpu_count()
+    return {"value": len(pts) / t, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{len(pts)} of {tot} grid points (seeded uniform sample, Becke-partitioned), "
+                      f"full dense XC build on them, {t:.2f} s, OMP threads={cores}"}
+
+
+# ------------------------------------------------------------- clocks ----
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) > 8 for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def fp64_gemm_peak(torch):
+    """cuBLAS DGEMM throughput (TFLOP/s), the FP64 denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e30
+    for _ in range(3):
+        e0.record()
+        a @ b
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return json.load(open(p)), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# ---------------------------------------------------------- reference ----
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    c, Z, funcs, C = workload(args.waters)
+    npts = max(256, args.cpu_sample)
+    for _ in range(args.warmup):
+        cpu_baseline(c, Z, funcs, C, 512)
+    vals = []
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(c, Z, funcs, C, npts)["value"])
+    cb = cpu_baseline(c, Z, funcs, C, npts)
+    v = float(np.median(vals))
+    cb["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config(args, {"precision": "fp64 (CPU oracle port of the reference dense algorithm)"}),
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- nkx ----
+def vgemm_flops(info_pairs_per_batch, nz=1):
+    """Algorithmic FLOPs of the V = Phi Z^T contraction: sum_b 2 n_b^2 256."""
+    nb = np.asarray(info_pairs_per_batch, dtype=np.float64) * 128.0
+    return float(nz * (2.0 * nb * nb * 256.0).sum())
+
+
+def run_nkx(args):
+    import torch
+    from nukexc_b200 import api as A
+    from nukexc_b200 import molecules as M  # noqa: F401
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    c, Z, funcs, Cm = workload(args.waters)
+    g = A.make_flat_grid(c, Z, 75, 29, weight_threshold=1e-15, radial="ta")
+    # strong scaling: rank r integrates the points of its share of atoms
+    lo, hi = (len(Z) * rank) // world, (len(Z) * (rank + 1)) // world
+    sel = (g.point_owner >= lo) & (g.point_owner < hi)
+    pts, w = g.quad_points[sel], g.weights[sel]
+    b = A.make_manual_basis(funcs)
+    t0 = time.perf_counter()
+    fb = A.FockBuilder(c, Z, b, (pts, w), func_ids=FUNCS)
+    setup_s = time.perf_counter() - t0
+    info = fb.info()
+    nbf = len(funcs)
+    occ = np.ones(Cm.shape[1])
+    Cd = torch.as_tensor(Cm, device="cuda")
+    od = torch.as_tensor(occ, device="cuda")
+    stream = torch.cuda.current_stream()
+    prec = args.precision
+    if prec == "auto":
+        try:
+            fb.build([Cd], [od], precision="mixed", stream=stream.cuda_stream)
+            prec = "mixed"
+        except Exception:
+            prec = "fp64"
+
+    def step(host=False):
+        if host:
+            E, V, _ = fb.build([Cm], [occ], precision=prec, stream=stream.cuda_stream)
+            V = torch.as_tensor(V[0], device="cuda")
+        else:
+            E, V, _ = fb.build([Cd], [od], precision=prec, stream=stream.cuda_stream)
+            V = V[0]
+        if dist is not None:
+            buf = torch.cat([V.reshape(-1), torch.tensor([E], dtype=torch.float64, device="cuda")])
+            dist.all_reduce(buf)
+            E = buf[-1].item()
+        return E
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    stage = {}
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+            t = fb.timing()
+            launches += t["launches"]
+            for k, v in t.items():
+                stage[k] = stage.get(k, 0.0) + v
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = tt.item()
+        dist.barrier()
+    total_pts = len(g.weights)
+    value = total_pts / (ms * 1e-3)
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        for _ in range(2):
+            step(host=True)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step(host=True)
+        torch.cuda.synchronize()
+        em = (time.perf_counter() - t0) * 1e3 / args.steps
+        if dist is not None:
+            tt = torch.tensor([em], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            em = tt.item()
+        e2e = {"value": total_pts / (em * 1e-3), "unit": UNIT, "ms_per_step": em,
+               "h2d_bytes_per_step": int(Cm.nbytes + occ.nbytes), "d2h_bytes_per_step": int(nbf * nbf * 8 + 8)}
+
+    if rank == 0:
+        flops = vgemm_flops(fb.batch_blocks())
+        vg_ms = stage["vgemm_ms"] / args.steps
+        peaks, src = measured_peaks()
+        if prec == "fp64":
+            peak = fp64_gemm_peak(torch)
+            peak_note = f"cuBLAS DGEMM 8192^3 measured in this run ({src} peaks file has no FP64 figure)"
+        else:
+            peak = peaks["bf16_tflops_sustained"]
+            peak_note = f"bf16 dense sustained, {src}"
+        # per launch: flops/nchunks over vg_ms/nchunks (one vgemm launch per chunk)
+        ach = flops / (vg_ms * 1e-3) / 1e12
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == "fp64" else "tf32x3/f32acc+f64", "data": "synthetic",
+            "config": config(args, {"precision": prec, "npoints": total_pts, "nbf": nbf,
+                                    "nbatches": info["nbatches"], "npairs": info["npairs"],
+                                    "nchunks": info["nchunks"], "plan_setup_s": setup_s,
+                                    "parallelism": f"grid split by atoms over {world} GPU(s)"}),
+            "stage_ms_per_step": {k: v / args.steps for k, v in stage.items() if k.endswith("_ms")},
+            "roofline": {"bound": "tensor", "kernel": "vgemm (V = Phi Z^T)", "achieved": ach, "peak": peak,
+                         "unit": "TFLOP/s", "frac": ach / peak, "traffic": None, "peak_source": peak_note,
+                         "algorithmic_flops_per_step": flops},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "e2e": e2e,
+        }
+        if os.environ.get("NKX_BENCH_NO_CPU") is None and world == 1:
+            line["cpu_baseline"] = cpu_baseline(c, Z, funcs, Cm, args.cpu_sample)
+        print(json.dumps(line), flush=True)
+    fb.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_nkx(args)
+
+
+if __name__ == "__main__":
+    main()

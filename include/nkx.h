@@ -1,0 +1,235 @@
+/*
+ * nkx.h -- C ABI of the B200-native grid-integration Fock build.
+ *
+ * Plain pointers and sizes only.  Every function returns an nkx_status and
+ * never throws across the boundary.  "Device" pointers are CUDA device
+ * pointers of the current device; "stream" is a cudaStream_t passed as
+ * void* (NULL = legacy default stream).  Matrices are column-major
+ * (Kokkos LayoutLeft in the reference): element (i, j) of an R x C matrix
+ * is at i + j*R.
+ *
+ * Each entry point names the NuKEXC interface it replaces (paths relative
+ * to the NuKEXC project root).
+ */
+#ifndef NKX_H
+#define NKX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define NKX_API __declspec(dllexport)
+#else
+#define NKX_API __attribute__((visibility("default")))
+#endif
+
+typedef int nkx_status;
+enum {
+  NKX_OK = 0,
+  NKX_ERR_ARG = 1,         /* invalid argument (reference: std::runtime_error) */
+  NKX_ERR_ALLOC = 2,       /* device or host allocation failed */
+  NKX_ERR_CUDA = 3,        /* a CUDA runtime / library call failed */
+  NKX_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+  NKX_ERR_NUMERIC = 5,     /* non-positive metric, negative grid weight, NaN */
+  NKX_ERR_UNSUPPORTED = 6  /* functional id, angular momentum or size not supported */
+};
+
+/* Precision of the dense contractions (the density and the V = Phi Z^T
+ * contraction).  FP64: plain FP64 kernels.  MIXED: tcgen05 tensor-core
+ * TF32 products of split operands (hi + lo) with FP32 accumulation per grid
+ * batch and FP64 accumulation across batches. */
+enum { NKX_PREC_FP64 = 0, NKX_PREC_MIXED = 1 };
+
+/* Radial quadratures (IntegratorXX Becke / TreutlerAhlrichs, nukexc/grid.hpp:172-305) */
+enum { NKX_RADIAL_BECKE = 0, NKX_RADIAL_TA = 1 };
+/* Per-element radial sizing (nukexc/grid.hpp:129-148) */
+enum { NKX_SIZING_UNIFORM = 0, NKX_SIZING_PYSCF = 1 };
+
+/* libxc functional ids supported on the device (libxc numbering) */
+enum {
+  NKX_XC_LDA_X = 1,
+  NKX_XC_LDA_C_VWN = 7, /* VWN5 */
+  NKX_XC_GGA_X_PBE = 101,
+  NKX_XC_GGA_C_PBE = 130
+};
+
+/* Memory space of the caller's buffers for nkx_fock_build */
+enum { NKX_MEM_DEVICE = 0, NKX_MEM_HOST = 1 };
+
+/* Molecule (nukexc/molecule.hpp:50-93): natoms centres in bohr, xyz[3*natoms] */
+typedef struct {
+  int natoms;
+  const double *xyz;
+  const int *Z;
+} nkx_molecule;
+
+/* STO basis in SoA form (STOBasisSet, nukexc/stobasis.hpp:54-64): one entry
+ * per function; center[3*nbf] in bohr.  The normalisation
+ * N = (2 zeta)^(n+1/2) / sqrt((2n)!) and the cutoff radius at cutoff_tol
+ * are computed by the library (make_manual_basis, stobasis.hpp:175-225). */
+typedef struct {
+  int nbf;
+  const int *n, *l, *m;
+  const double *zeta;
+  const double *center;
+  double cutoff_tol; /* reference default 1e-10 */
+} nkx_basis;
+
+/* make_flat_grid parameters (nukexc/grid.hpp:172-181) */
+typedef struct {
+  int radial_scheme;       /* NKX_RADIAL_* */
+  int nrad;                /* radial points (H/He count for PySCF sizing) */
+  int nang_order;          /* Lebedev algebraic order requested (next available is used) */
+  double weight_threshold; /* drop points with w <= threshold after Becke */
+  double ta_alpha;         /* Treutler-Ahlrichs exponent (0.6 = M4) */
+  int sizing;              /* NKX_SIZING_* */
+  double becke_clamp;      /* Laqua clamp of R_ij in bohr (5.0); <= 0: original Becke */
+} nkx_grid_spec;
+
+/* Plan options */
+typedef struct {
+  int batch_points;        /* points per grid batch; 256 */
+  double screen_tol;       /* basis cutoff tolerance for batch screening (1e-10) */
+  int nfunc;               /* number of functional ids summed (1..4) */
+  int func_ids[4];         /* NKX_XC_* */
+  double dens_threshold;   /* points with rho < threshold give no XC contribution */
+  size_t workspace_bytes;  /* device workspace for streamed batch chunks; 0 = auto */
+  double metric_svd_thr;   /* 0: FP64 Cholesky of (A|B); > 0: the reference's preconditioned
+                              half inverse keeping singular values > thr (nukexc_utils.hpp:198-270) */
+} nkx_plan_options;
+
+typedef struct nkx_plan nkx_plan;
+
+typedef struct {
+  long npoints;            /* grid points after compaction */
+  long nbatches;
+  int nbf, naux, nblocks;  /* nblocks = ceil(nbf / 128) function blocks */
+  long npairs;             /* significant (batch, function block) pairs */
+  int nchunks;             /* batch chunks streamed per pass */
+  double metric_min_diag;  /* smallest diagonal of the Cholesky factor of (A|B) */
+} nkx_plan_info;
+
+/* Timing of the last nkx_fock_build, per stage, in milliseconds (CUDA events). */
+typedef struct {
+  float colloc_ms, density_ms, functional_ms, coulomb_ms, zbuild_ms, vgemm_ms, total_ms;
+  int launches;            /* kernels launched by the build */
+} nkx_build_timing;
+
+/* ---------------------------------------------------------------- grid -- */
+
+/* make_flat_grid (nukexc/grid.hpp:172-348): per-atom radial x Lebedev
+ * grids, Becke partition on the device (partition_becke_team,
+ * nukexc/partitioning.hpp:126-213), compaction of w <= threshold keeping the
+ * original order.  Two-call pattern: pass xyz == NULL to get *npoints, then
+ * host buffers xyz[3*npoints], w[npoints], owner[npoints]. */
+NKX_API nkx_status nkx_make_flat_grid(const nkx_molecule *mol, const nkx_grid_spec *spec, long *npoints,
+                                      double *xyz, double *w, int *owner);
+
+/* partition_becke_team / partition_becke (nukexc/partitioning.hpp:63-213)
+ * on device buffers: weights[g] *= P_owner(g) / sum_i P_i.  clamp > 0 is the
+ * Laqua-clamped team variant (R_ij = min(|A_i - A_j|, clamp)), clamp <= 0 the
+ * original Becke.  centers[3*natoms], points[3*npts] (AoS, like
+ * Kokkos::View<Point*>). */
+NKX_API nkx_status nkx_becke_partition(const double *d_centers, int natoms, const double *d_points,
+                                       const int *d_owner, long npts, double *d_weights, double clamp,
+                                       void *stream);
+
+/* ----------------------------------------------------- dense reference API */
+
+/* fill_collocation / fill_grad_collocation (nukexc/stobasis.hpp:494-584):
+ * Phi (nbf x npts column-major) and optionally its gradient (d_gx == NULL
+ * skips it) at device points[3*npts]. */
+NKX_API nkx_status nkx_fill_collocation(const nkx_basis *basis, const double *d_points, long npts,
+                                        double *d_phi, double *d_gx, double *d_gy, double *d_gz,
+                                        void *stream);
+
+/* compute_density_and_sigma (nukexc/density.hpp:188-255) and
+ * compute_density (:150-186) on dense collocation matrices.  C is
+ * nbf x nocc column-major, occ[nocc].  rho[npts]; d_grad (3*npts, x|y|z
+ * planes) and d_sigma may be NULL (then the gradient inputs may be NULL). */
+NKX_API nkx_status nkx_density_dense(int nbf, long npts, const double *d_phi, const double *d_gx,
+                                     const double *d_gy, const double *d_gz, int nocc, const double *d_C,
+                                     const double *d_occ, double *d_rho, double *d_grad, double *d_sigma,
+                                     void *stream);
+
+/* compute_lda / compute_gga (nspin 1) and compute_lsda / compute_gga_lsda
+ * (nspin 2) (nukexc/xc_integrals.hpp:73-726) on dense collocation: C and occ
+ * hold nspin blocks (nbf x nocc, nocc).  The functional ids of `opts` are
+ * summed.  E_xc is written to *E (host).  d_V receives nspin symmetric
+ * nbf x nbf matrices. */
+NKX_API nkx_status nkx_xc_dense(int nbf, long npts, const double *d_phi, const double *d_gx,
+                                const double *d_gy, const double *d_gz, const double *d_w, int nspin,
+                                int nocc, const double *d_C, const double *d_occ, const nkx_plan_options *opts,
+                                double *E, double *d_V, void *stream);
+
+/* Functional evaluation with libxc's array layouts (xc_lda_exc_vxc /
+ * xc_gga_exc_vxc, the host calls of nukexc/xc_integrals.hpp:113-617), on the
+ * device: nspin 1: rho[n], sigma[n]; nspin 2: rho[2n], sigma[3n]
+ * interleaved.  exc per particle.  sigma/vsigma may be NULL for LDA. */
+NKX_API nkx_status nkx_xc_eval(int func_id, int nspin, long n, const double *d_rho, const double *d_sigma,
+                               double dens_threshold, double *d_exc, double *d_vrho, double *d_vsigma,
+                               void *stream);
+
+/* sto_potential_collocation_scaled (nukexc/stopotential.hpp:101-124):
+ * Vw(alpha, g) = V_alpha(r_g) w_g, naux x npts column-major. */
+NKX_API nkx_status nkx_potential_collocation(const nkx_basis *aux, const double *d_points, const double *d_w,
+                                             long npts, double *d_Vw, void *stream);
+
+/* compute_half_inverse (nukexc/nukexc_utils.hpp:198-270): X = U s^-1/2 / D
+ * of the preconditioned metric, keeping s > thr (symmetric
+ * eigendecomposition on the device).  d_X must hold N*N; *K receives the
+ * kept column count. */
+NKX_API nkx_status nkx_half_inverse(int N, const double *d_S, double thr, double *d_X, int *K, void *stream);
+
+/* ---------------------------------------------------------------- plan -- */
+
+/* Once per geometry: Morton-ordered 256-point batches of the given grid
+ * (create_bounding_boxes, nukexc/octree.hpp:70-141), screening of basis
+ * function blocks per batch (build_neighbor_list, :317-390), the aux metric
+ * (A|B) on the grid and its FP64 Cholesky factor (replaces the SVD half
+ * inverse of nukexc/nukexc_utils.hpp:198-270; aux may be NULL for XC only).
+ * The caller's grid arrays (host) are copied, never permuted. */
+NKX_API nkx_status nkx_plan_create(const nkx_molecule *mol, const nkx_basis *prim, const nkx_basis *aux,
+                                   long npoints, const double *xyz, const double *w, const int *owner,
+                                   const nkx_plan_options *opts, nkx_plan **plan);
+
+NKX_API nkx_status nkx_plan_get_info(const nkx_plan *plan, nkx_plan_info *info);
+
+/* One Fock build (the per-SCF-iteration work of tests/standalone.cxx:572-846):
+ * E_xc and V_xc (compute_gga / compute_gga_lsda ...) and, when the plan
+ * has an aux basis and J != NULL, the grid-integrated RI-J
+ * (compute_coulomb, nukexc/coulomb.hpp:56-115).
+ *   nspin 1: C = nbf x nocc, occ[nocc]; V = nbf x nbf.
+ *   nspin 2: C = 2 blocks (alpha, beta), occ = 2 blocks; V = 2 matrices;
+ *            J is built from the total density.
+ * mem selects whether C/occ/V/J are host or device buffers (host buffers
+ * are copied inside the call).  With fuse_j != 0 (and nspin 1), J is folded
+ * into the XC contraction and V receives V_xc + J (J may then be NULL).
+ * E_xc is written to host *E.  The call is synchronous on return. */
+NKX_API nkx_status nkx_fock_build(nkx_plan *plan, int precision, int nspin, int nocc, const double *C,
+                                  const double *occ, int mem, int fuse_j, double *E, double *V, double *J,
+                                  void *stream);
+
+NKX_API nkx_status nkx_get_last_timing(const nkx_plan *plan, nkx_build_timing *t);
+
+/* Per-point density of the last build (rho[npoints*nspin], plan point order
+ * = Morton order) and the plan's permutation perm[npoints] (plan point p is
+ * caller point perm[p]); host buffers. */
+NKX_API nkx_status nkx_plan_last_density(const nkx_plan *plan, double *rho, long *perm);
+
+/* Number of significant 128-function blocks of every batch (counts[nbatches]). */
+NKX_API nkx_status nkx_plan_batch_blocks(const nkx_plan *plan, int *counts);
+
+NKX_API nkx_status nkx_plan_destroy(nkx_plan *plan);
+
+/* Message of the last failed call on this thread (static storage). */
+NKX_API const char *nkx_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NKX_H */

@@ -1,0 +1,373 @@
+"""Python mirror of the NuKEXC hot-path interface over the C ABI.
+
+Names and argument meanings follow the reference headers (grid.hpp,
+partitioning.hpp, stobasis.hpp, density.hpp, xc_integrals.hpp,
+coulomb.hpp, stopotential.hpp, nukexc_utils.hpp).  Device buffers are torch
+CUDA tensors (torch is used only as a device allocator); every computation
+runs in libnkx.so.  Matrices are returned in the reference's LayoutLeft
+convention as torch tensors M with M[i, j] = element (i, j).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from ._lib import check
+
+_FUNC_NAMES = {"LDA_X": 1, "LDA_C_VWN": 7, "GGA_X_PBE": 101, "GGA_C_PBE": 130}
+
+
+def _dev(x, dtype=torch.float64):
+    if isinstance(x, torch.Tensor):
+        return x.to(device="cuda", dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype, device="cuda")
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _np(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+# ----------------------------------------------------------------- basis --
+@dataclass
+class STOBasisSet:
+    """STOBasisSet (nukexc/stobasis.hpp:54-64): SoA host arrays."""
+    n: np.ndarray
+    l: np.ndarray
+    m: np.ndarray
+    zeta: np.ndarray
+    center: np.ndarray  # (nbf, 3)
+    cutoff_tol: float = 1e-10
+
+    def nbf(self):
+        return len(self.n)
+
+    def as_c(self):
+        self._keep = [_np(self.n, np.int32), _np(self.l, np.int32), _np(self.m, np.int32),
+                      _np(self.zeta, np.float64), _np(self.center, np.float64).reshape(-1)]
+        k = self._keep
+        return L.Basis(len(self.n), *(a.ctypes.data_as(C.c_void_p) for a in k), self.cutoff_tol)
+
+
+def make_manual_basis(funcs, cutoff_tol=1e-10):
+    """make_manual_basis (nukexc/stobasis.hpp:175-225); funcs = (n,l,m,zeta,ox,oy,oz)."""
+    f = list(funcs)
+    return STOBasisSet(np.array([x[0] for x in f], np.int32), np.array([x[1] for x in f], np.int32),
+                       np.array([x[2] for x in f], np.int32), np.array([x[3] for x in f], np.float64),
+                       np.array([[x[4], x[5], x[6]] for x in f], np.float64).reshape(-1, 3), cutoff_tol)
+
+
+# ------------------------------------------------------------------ grid --
+@dataclass
+class FlatGrid:
+    """FlatGrid (nukexc/grid.hpp:150-160), host numpy arrays in bohr."""
+    quad_points: np.ndarray  # (npts, 3)
+    weights: np.ndarray
+    atom_centers: np.ndarray
+    Z: np.ndarray
+    point_owner: np.ndarray
+
+
+def _mol(centers, Z):
+    c = _np(centers, np.float64).reshape(-1)
+    z = _np(Z, np.int32)
+    return L.Molecule(len(z), c.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p)), (c, z)
+
+
+def make_flat_grid(centers, Z, nrad=50, nang_order=30, weight_threshold=1e-30, ta_alpha=0.6,
+                   radial="ta", sizing="uniform", becke_clamp=5.0):
+    """make_flat_grid (nukexc/grid.hpp:172-348)."""
+    mol, keep = _mol(centers, Z)
+    spec = L.GridSpec({"becke": L.RADIAL_BECKE, "ta": L.RADIAL_TA}[radial], nrad, nang_order,
+                      weight_threshold, ta_alpha, {"uniform": 0, "pyscf": 1}[sizing], becke_clamp)
+    n = C.c_long(0)
+    check(L.lib().nkx_make_flat_grid(C.byref(mol), C.byref(spec), C.byref(n), None, None, None))
+    xyz = np.zeros((n.value, 3))
+    w = np.zeros(n.value)
+    own = np.zeros(n.value, np.int32)
+    check(L.lib().nkx_make_flat_grid(C.byref(mol), C.byref(spec), C.byref(n), xyz.ctypes.data_as(C.c_void_p),
+                                     w.ctypes.data_as(C.c_void_p), own.ctypes.data_as(C.c_void_p)))
+    return FlatGrid(xyz, w, np.asarray(centers, float).reshape(-1, 3), np.asarray(Z), own)
+
+
+def partition_becke_team(atom_centers, quadrature_points, point_owner, weights, clamp=5.0):
+    """partition_becke_team (nukexc/partitioning.hpp:126-213); returns new weights
+    (a CUDA tensor).  clamp <= 0 gives partition_becke (:63-120)."""
+    c = _dev(atom_centers).reshape(-1)
+    p = _dev(quadrature_points).reshape(-1)
+    o = _dev(point_owner, torch.int32)
+    w = _dev(weights).clone()
+    check(L.lib().nkx_becke_partition(_p(c), c.numel() // 3, _p(p), _p(o), w.numel(), _p(w), clamp, None))
+    return w
+
+
+def partition_becke(atom_centers, quadrature_points, point_owner, weights):
+    return partition_becke_team(atom_centers, quadrature_points, point_owner, weights, clamp=0.0)
+
+
+# ------------------------------------------------------------ collocation --
+def _lmat(flat, rows, cols):
+    """column-major flat buffer -> tensor M[i, j]"""
+    return flat.view(cols, rows).t()
+
+
+def fill_collocation(basis, points):
+    """fill_collocation (nukexc/stobasis.hpp:494-532): Phi[nbf, npts]."""
+    pts = _dev(points).reshape(-1)
+    npts = pts.numel() // 3
+    phi = torch.empty(basis.nbf() * npts, dtype=torch.float64, device="cuda")
+    b = basis.as_c()
+    check(L.lib().nkx_fill_collocation(C.byref(b), _p(pts), npts, _p(phi), None, None, None, None))
+    return _lmat(phi, basis.nbf(), npts)
+
+
+def fill_grad_collocation(basis, points):
+    """fill_collocation + fill_grad_collocation (stobasis.hpp:494-584)."""
+    pts = _dev(points).reshape(-1)
+    npts = pts.numel() // 3
+    bufs = [torch.empty(basis.nbf() * npts, dtype=torch.float64, device="cuda") for _ in range(4)]
+    b = basis.as_c()
+    check(L.lib().nkx_fill_collocation(C.byref(b), _p(pts), npts, *[_p(x) for x in bufs], None))
+    return tuple(_lmat(x, basis.nbf(), npts) for x in bufs)
+
+
+def _flat_lmat(M):
+    """tensor M[i, j] -> column-major contiguous flat buffer"""
+    return _dev(M).t().contiguous().reshape(-1)
+
+
+# ---------------------------------------------------------------- density --
+def compute_density_and_sigma(phi, gx, gy, gz, mo_orbitals, mo_coeff):
+    """compute_density_and_sigma (nukexc/density.hpp:188-255): returns
+    (rho, grad[3, npts], sigma) as CUDA tensors."""
+    nbf, npts = phi.shape
+    C_ = _flat_lmat(mo_orbitals)
+    occ = _dev(mo_coeff)
+    rho = torch.empty(npts, dtype=torch.float64, device="cuda")
+    grad = torch.empty(3 * npts, dtype=torch.float64, device="cuda")
+    sig = torch.empty(npts, dtype=torch.float64, device="cuda")
+    fl = [_flat_lmat(x) for x in (phi, gx, gy, gz)]
+    check(L.lib().nkx_density_dense(nbf, npts, *[_p(x) for x in fl], occ.numel(), _p(C_), _p(occ),
+                                    _p(rho), _p(grad), _p(sig), None))
+    return rho, grad.view(3, npts), sig
+
+
+def compute_density(phi, mo_orbitals, mo_coeff):
+    """compute_density (nukexc/density.hpp:150-186)."""
+    nbf, npts = phi.shape
+    C_ = _flat_lmat(mo_orbitals)
+    occ = _dev(mo_coeff)
+    rho = torch.empty(npts, dtype=torch.float64, device="cuda")
+    f = _flat_lmat(phi)
+    check(L.lib().nkx_density_dense(nbf, npts, _p(f), None, None, None, occ.numel(), _p(C_), _p(occ),
+                                    _p(rho), None, None, None))
+    return rho
+
+
+# --------------------------------------------------------------------- XC --
+def _opts(func_ids, dens_threshold=1e-15, metric_svd_thr=0.0, workspace_bytes=0):
+    ids = [(_FUNC_NAMES[f] if isinstance(f, str) else int(f)) for f in func_ids]
+    arr = (C.c_int * 4)(*(ids + [0] * (4 - len(ids))))
+    return L.PlanOptions(256, 1e-10, len(ids), arr, dens_threshold, workspace_bytes, metric_svd_thr)
+
+
+def _xc_dense(phi, grads, weights, C_list, occ_list, func_ids, dens_threshold):
+    nbf, npts = phi.shape
+    nspin = len(C_list)
+    nocc = C_list[0].shape[1]
+    Cc = torch.cat([_flat_lmat(c) for c in C_list])
+    oc = torch.cat([_dev(o) for o in occ_list])
+    fl = [_flat_lmat(phi)] + ([_flat_lmat(g) for g in grads] if grads else [None] * 3)
+    w = _dev(weights)
+    V = torch.empty(nspin * nbf * nbf, dtype=torch.float64, device="cuda")
+    E = C.c_double(0)
+    o = _opts(func_ids, dens_threshold)
+    check(L.lib().nkx_xc_dense(nbf, npts, *[_p(x) for x in fl], _p(w), nspin, nocc, _p(Cc), _p(oc),
+                               C.byref(o), C.byref(E), _p(V), None))
+    Vs = [V[s * nbf * nbf:(s + 1) * nbf * nbf].view(nbf, nbf).t() for s in range(nspin)]
+    return E.value, Vs
+
+
+def compute_lda(phi, weights, mo_orbitals, mo_coeff, func_ids=("LDA_X",), dens_threshold=1e-15):
+    """compute_lda (nukexc/xc_integrals.hpp:73-166): (E_xc, V)."""
+    E, V = _xc_dense(phi, None, weights, [mo_orbitals], [mo_coeff], func_ids, dens_threshold)
+    return E, V[0]
+
+
+def compute_gga(phi, gx, gy, gz, weights, mo_orbitals, mo_coeff, func_ids=("GGA_X_PBE",),
+                dens_threshold=1e-15):
+    """compute_gga (nukexc/xc_integrals.hpp:424-541): (E_xc, V)."""
+    E, V = _xc_dense(phi, (gx, gy, gz), weights, [mo_orbitals], [mo_coeff], func_ids, dens_threshold)
+    return E, V[0]
+
+
+def compute_lsda(phi, weights, mo_alpha, occ_alpha, mo_beta, occ_beta, func_ids=("LDA_X",),
+                 dens_threshold=1e-15):
+    """compute_lsda (nukexc/xc_integrals.hpp:168-261): (E_xc, V_alpha, V_beta)."""
+    E, V = _xc_dense(phi, None, weights, [mo_alpha, mo_beta], [occ_alpha, occ_beta], func_ids, dens_threshold)
+    return E, V[0], V[1]
+
+
+def compute_gga_lsda(phi, gx, gy, gz, weights, mo_alpha, occ_alpha, mo_beta, occ_beta,
+                     func_ids=("GGA_X_PBE",), dens_threshold=1e-15):
+    """compute_gga_lsda (nukexc/xc_integrals.hpp:543-726)."""
+    E, V = _xc_dense(phi, (gx, gy, gz), weights, [mo_alpha, mo_beta], [occ_alpha, occ_beta], func_ids,
+                     dens_threshold)
+    return E, V[0], V[1]
+
+
+def xc_eval(func_id, nspin, rho, sigma=None, dens_threshold=1e-15):
+    """libxc-layout functional evaluation on the device: (exc, vrho, vsigma)."""
+    fid = _FUNC_NAMES[func_id] if isinstance(func_id, str) else int(func_id)
+    r = _dev(rho)
+    n = r.numel() // nspin
+    s = _dev(sigma) if sigma is not None else None
+    exc = torch.empty(n, dtype=torch.float64, device="cuda")
+    vr = torch.empty(n * nspin, dtype=torch.float64, device="cuda")
+    vs = torch.empty(n * (1 if nspin == 1 else 3), dtype=torch.float64, device="cuda") if s is not None else None
+    check(L.lib().nkx_xc_eval(fid, nspin, n, _p(r), _p(s), dens_threshold, _p(exc), _p(vr), _p(vs), None))
+    return exc, vr, vs
+
+
+# ---------------------------------------------------------------- Coulomb --
+def sto_potential_collocation_scaled(basis_aux, points, weights):
+    """sto_potential_collocation_scaled (nukexc/stopotential.hpp:101-124)."""
+    pts = _dev(points).reshape(-1)
+    npts = pts.numel() // 3
+    w = _dev(weights)
+    out = torch.empty(basis_aux.nbf() * npts, dtype=torch.float64, device="cuda")
+    b = basis_aux.as_c()
+    check(L.lib().nkx_potential_collocation(C.byref(b), _p(pts), _p(w), npts, _p(out), None))
+    return _lmat(out, basis_aux.nbf(), npts)
+
+
+def compute_half_inverse(S, lin_dep_threshold=1e-5):
+    """compute_half_inverse (nukexc/nukexc_utils.hpp:198-270): X (N x K)."""
+    N = S.shape[0]
+    Sf = _flat_lmat(S)
+    X = torch.empty(N * N, dtype=torch.float64, device="cuda")
+    K = C.c_int(0)
+    check(L.lib().nkx_half_inverse(N, _p(Sf), lin_dep_threshold, _p(X), C.byref(K), None))
+    return _lmat(X, N, N)[:, :K.value]
+
+
+def compute_coulomb(mo_orbitals, mo_coeff, basis_collocation, basis_aux_collocation,
+                    potential_collocation_scaled, half_inverse_X):
+    """compute_coulomb (nukexc/coulomb.hpp:56-115), dense: J (nbf x nbf).
+    The contractions are device GEMVs/GEMMs of torch (plain library calls)
+    around the nkx density kernel, as the reference does with KokkosBlas."""
+    rho = compute_density(basis_collocation, mo_orbitals, mo_coeff)
+    y = potential_collocation_scaled @ rho
+    c = half_inverse_X @ (half_inverse_X.t() @ y)
+    v = potential_collocation_scaled.t() @ c
+    return basis_collocation @ (basis_collocation * v[None, :]).t()
+
+
+# ------------------------------------------------------------------ plan --
+class FockBuilder:
+    """The batched grid-integration Fock build behind nkx_plan_* (the hot
+    path): once per geometry the grid is batched and screened and the aux
+    metric factorised; each build() is one SCF iteration's XC (+ J) work.
+
+    grid: FlatGrid or (points, weights); basis/aux: STOBasisSet.
+    """
+
+    def __init__(self, centers, Z, basis, grid, aux=None, func_ids=("GGA_X_PBE", "GGA_C_PBE"),
+                 dens_threshold=1e-15, metric_svd_thr=0.0, workspace_bytes=0):
+        if isinstance(grid, FlatGrid):
+            pts, w = grid.quad_points, grid.weights
+        else:
+            pts, w = grid
+        self._pts = _np(pts, np.float64).reshape(-1)
+        self._w = _np(w, np.float64)
+        mol, self._mk = _mol(centers, Z)
+        self.basis = basis
+        self._b = basis.as_c()
+        self._a = aux.as_c() if aux is not None else None
+        self._o = _opts(func_ids, dens_threshold, metric_svd_thr, workspace_bytes)
+        self.nbf = basis.nbf()
+        self.naux = aux.nbf() if aux is not None else 0
+        h = C.c_void_p()
+        check(L.lib().nkx_plan_create(C.byref(mol), C.byref(self._b), C.byref(self._a) if self._a else None,
+                                      len(self._w), self._pts.ctypes.data_as(C.c_void_p),
+                                      self._w.ctypes.data_as(C.c_void_p), None, C.byref(self._o), C.byref(h)))
+        self._h = h
+
+    def info(self):
+        i = L.PlanInfo()
+        check(L.lib().nkx_plan_get_info(self._h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in L.PlanInfo._fields_}
+
+    def timing(self):
+        t = L.BuildTiming()
+        check(L.lib().nkx_get_last_timing(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in L.BuildTiming._fields_}
+
+    def build(self, C_list, occ_list, precision="fp64", want_J=False, fuse_j=False, stream=None):
+        """One Fock build.  C_list/occ_list: one (nbf x nocc, nocc) per spin,
+        numpy (host: copied inside the call) or CUDA tensors (device).
+        Returns (E_xc, [V per spin], J or None); with fuse_j, V includes J."""
+        nspin = len(C_list)
+        host = not isinstance(C_list[0], torch.Tensor)
+        nocc = C_list[0].shape[1]
+        prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
+        nn = self.nbf * self.nbf
+        if host:
+            Cc = np.concatenate([np.ascontiguousarray(np.asarray(c, np.float64).T).reshape(-1) for c in C_list])
+            oc = np.concatenate([_np(o, np.float64) for o in occ_list])
+            V = np.zeros(nspin * nn)
+            J = np.zeros(nn) if want_J and not fuse_j else None
+            pC, po, pV = (a.ctypes.data_as(C.c_void_p) for a in (Cc, oc, V))
+            pJ = J.ctypes.data_as(C.c_void_p) if J is not None else None
+        else:
+            Cc = torch.cat([c.t().contiguous().reshape(-1) for c in C_list])
+            oc = torch.cat([o.reshape(-1) for o in occ_list]).to(torch.float64)
+            V = torch.empty(nspin * nn, dtype=torch.float64, device="cuda")
+            J = torch.empty(nn, dtype=torch.float64, device="cuda") if want_J and not fuse_j else None
+            pC, po, pV, pJ = _p(Cc), _p(oc), _p(V), _p(J)
+        E = C.c_double(0)
+        s = C.c_void_p(stream) if stream else None
+        check(L.lib().nkx_fock_build(self._h, prec, nspin, nocc, pC, po, L.MEM_HOST if host else L.MEM_DEVICE,
+                                     1 if fuse_j else 0, C.byref(E), pV, pJ, s))
+        if host:
+            Vs = [V[k * nn:(k + 1) * nn].reshape(self.nbf, self.nbf).T.copy() for k in range(nspin)]
+            Jm = J.reshape(self.nbf, self.nbf).T.copy() if J is not None else None
+        else:
+            Vs = [V[k * nn:(k + 1) * nn].view(self.nbf, self.nbf).t() for k in range(nspin)]
+            Jm = J.view(self.nbf, self.nbf).t() if J is not None else None
+        return E.value, Vs, Jm
+
+    def batch_blocks(self):
+        """Significant 128-function blocks per batch."""
+        n = self.info()["nbatches"]
+        out = np.zeros(n, np.int32)
+        check(L.lib().nkx_plan_batch_blocks(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def last_density(self, nspin=1):
+        npts = self.info()["npoints"]
+        rho = np.zeros(npts * nspin)
+        perm = np.zeros(npts, np.int64)
+        check(L.lib().nkx_plan_last_density(self._h, rho.ctypes.data_as(C.c_void_p),
+                                            perm.ctypes.data_as(C.c_void_p)))
+        out = np.zeros((npts, nspin))
+        out[perm] = rho.reshape(npts, nspin)
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().nkx_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

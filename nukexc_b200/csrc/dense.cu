@@ -1,0 +1,389 @@
+// Dense-matrix entry points with the shapes of the reference's dense
+// algorithm (fill_collocation, compute_density_and_sigma, compute_gga ...,
+// sto_potential_collocation_scaled, compute_half_inverse).  They operate on
+// caller-owned device buffers.  The batched, screened Fock build of plan.cu
+// is the hot path; these exist so the reference's dense call sequence can be
+// replaced one function at a time.
+#include <cusolverDn.h>
+
+#include <functional>
+#include <vector>
+
+#include "functionals.cuh"
+#include "host_setup.hpp"
+
+namespace nkx {
+
+nkx_status run_guarded(const char *where, const std::function<void()> &fn);
+
+template <class T>
+struct DevBuf {
+  T *p = nullptr;
+  explicit DevBuf(size_t n) {
+    if (n) NKX_CUDA(cudaMalloc(&p, n * sizeof(T)));
+  }
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+};
+
+__global__ void colloc_dense_kernel(const StoFunc *__restrict__ f, int nbf, const double *__restrict__ pts,
+                                    long npts, double *phi, double *gx, double *gy, double *gz) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)nbf * npts) return;
+  const int mu = (int)(idx % nbf);
+  const long g = idx / nbf;
+  const double px = pts[3 * g], py = pts[3 * g + 1], pz = pts[3 * g + 2];
+  if (gx) {
+    double v, a, b, c;
+    sto_value_grad(f[mu], px, py, pz, v, a, b, c);
+    phi[idx] = v;
+    gx[idx] = a;
+    gy[idx] = b;
+    gz[idx] = c;
+  } else {
+    phi[idx] = sto_value(f[mu], px, py, pz);
+  }
+}
+
+// One warp per point: T_i = sum_mu C(mu,i) phi(mu,g); rho = sum occ_i T_i^2,
+// grad rho = 2 sum occ_i T_i grad T_i (density.hpp:188-255).
+__global__ void density_dense_kernel(int nbf, long npts, const double *__restrict__ phi,
+                                     const double *__restrict__ gx, const double *__restrict__ gy,
+                                     const double *__restrict__ gz, int nocc, const double *__restrict__ C,
+                                     const double *__restrict__ occ, double *rho, double *grad, double *sigma) {
+  const long g = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= npts) return;
+  const double *ph = phi + g * (long)nbf;
+  double r = 0, sx = 0, sy = 0, sz = 0;
+  for (int i = 0; i < nocc; ++i) {
+    const double *ci = C + (long)i * nbf;
+    double t = 0, tx = 0, ty = 0, tz = 0;
+    for (int mu = lane; mu < nbf; mu += 32) {
+      t += ci[mu] * ph[mu];
+      if (gx) {
+        tx += ci[mu] * gx[g * (long)nbf + mu];
+        ty += ci[mu] * gy[g * (long)nbf + mu];
+        tz += ci[mu] * gz[g * (long)nbf + mu];
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      t += __shfl_xor_sync(0xffffffffu, t, o);
+      tx += __shfl_xor_sync(0xffffffffu, tx, o);
+      ty += __shfl_xor_sync(0xffffffffu, ty, o);
+      tz += __shfl_xor_sync(0xffffffffu, tz, o);
+    }
+    r += occ[i] * t * t;
+    sx += occ[i] * tx * t;
+    sy += occ[i] * ty * t;
+    sz += occ[i] * tz * t;
+  }
+  if (lane == 0) {
+    rho[g] = r;
+    if (grad) {
+      grad[g] = 2 * sx;
+      grad[npts + g] = 2 * sy;
+      grad[2 * npts + g] = 2 * sz;
+    }
+    if (sigma) sigma[g] = 4.0 * (sx * sx + sy * sy + sz * sz);
+  }
+}
+
+// libxc-layout functional evaluation (thread per point)
+__global__ void xc_eval_kernel(XcSpec s, int nspin, long n, const double *rho, const double *sigma, double *exc,
+                               double *vrho, double *vsigma) {
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  if (nspin == 1) {
+    double f, vr, vs;
+    const double r = rho[g];
+    xc_unpol(s, r, sigma ? sigma[g] : 0.0, f, vr, vs);
+    exc[g] = (r > 0 && f != 0.0) ? f / r : 0.0;
+    vrho[g] = vr;
+    if (vsigma) vsigma[g] = vs;
+  } else {
+    double f, d[5];
+    const double ra = rho[2 * g], rb = rho[2 * g + 1];
+    xc_pol(s, ra, rb, sigma ? sigma[3 * g] : 0.0, sigma ? sigma[3 * g + 1] : 0.0, sigma ? sigma[3 * g + 2] : 0.0,
+           f, d);
+    exc[g] = (ra + rb > 0 && f != 0.0) ? f / (ra + rb) : 0.0;
+    vrho[2 * g] = d[0];
+    vrho[2 * g + 1] = d[1];
+    if (vsigma) {
+      vsigma[3 * g] = d[2];
+      vsigma[3 * g + 1] = d[3];
+      vsigma[3 * g + 2] = d[4];
+    }
+  }
+}
+
+// Per point: functional of the (spin) densities, energy, and the Z matrix
+// Z(mu, g) = w (1/2 phi vrho + vec . grad phi) (xc_integrals.hpp:486-515,
+// :655-697).  Z holds nspin blocks of nbf x npts.
+__global__ void xc_z_dense_kernel(XcSpec s, bool gga, int nbf, long npts, int nspin, const double *phi,
+                                  const double *gx, const double *gy, const double *gz, const double *w,
+                                  const double *rho, const double *grad, double *Z, double *Eacc) {
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (g < npts) {
+    double vr[2] = {0, 0}, vec[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    double gr[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    for (int sp = 0; sp < nspin; ++sp)
+      if (gga)
+        for (int k = 0; k < 3; ++k) gr[sp][k] = grad[(size_t)sp * 3 * npts + k * npts + g];
+    if (nspin == 1) {
+      const double r = rho[g];
+      const double sg = gr[0][0] * gr[0][0] + gr[0][1] * gr[0][1] + gr[0][2] * gr[0][2];
+      double f, vrho, vs;
+      xc_unpol(s, r, sg, f, vrho, vs);
+      e = w[g] * f;
+      vr[0] = vrho;
+      for (int k = 0; k < 3; ++k) vec[0][k] = 2.0 * vs * gr[0][k];
+    } else {
+      const double ra = rho[g], rb = rho[npts + g];
+      const double saa = gr[0][0] * gr[0][0] + gr[0][1] * gr[0][1] + gr[0][2] * gr[0][2];
+      const double sab = gr[0][0] * gr[1][0] + gr[0][1] * gr[1][1] + gr[0][2] * gr[1][2];
+      const double sbb = gr[1][0] * gr[1][0] + gr[1][1] * gr[1][1] + gr[1][2] * gr[1][2];
+      double f, d[5];
+      xc_pol(s, ra, rb, saa, sab, sbb, f, d);
+      e = w[g] * f;
+      vr[0] = d[0];
+      vr[1] = d[1];
+      for (int k = 0; k < 3; ++k) {
+        vec[0][k] = 2.0 * d[2] * gr[0][k] + d[3] * gr[1][k];
+        vec[1][k] = 2.0 * d[4] * gr[1][k] + d[3] * gr[0][k];
+      }
+    }
+    for (int sp = 0; sp < nspin; ++sp) {
+      double *Zs = Z + (size_t)sp * nbf * npts;
+      for (int mu = 0; mu < nbf; ++mu) {
+        const size_t i = (size_t)mu + (size_t)g * nbf;
+        double z = 0.5 * phi[i] * vr[sp];
+        if (gga) z += vec[sp][0] * gx[i] + vec[sp][1] * gy[i] + vec[sp][2] * gz[i];
+        Zs[i] = w[g] * z;
+      }
+    }
+  }
+  for (int o = 16; o; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(Eacc, e);
+}
+
+// Vbar(i,j) = sum_g A(i,g) B(j,g); A, B column-major n x npts.  16x16 tiles.
+__global__ void nt_gemm_dense_kernel(int n, long npts, const double *A, const double *B, double *V) {
+  __shared__ double As[16][17], Bs[16][17];
+  const int i = blockIdx.y * 16 + threadIdx.y, j = blockIdx.x * 16 + threadIdx.x;
+  double acc = 0.0;
+  for (long g0 = 0; g0 < npts; g0 += 16) {
+    const long ga = g0 + threadIdx.x;
+    const int ia = blockIdx.y * 16 + threadIdx.y, jb = blockIdx.x * 16 + threadIdx.y;
+    As[threadIdx.y][threadIdx.x] = (ia < n && ga < npts) ? A[(size_t)ia + (size_t)ga * n] : 0.0;
+    Bs[threadIdx.y][threadIdx.x] = (jb < n && ga < npts) ? B[(size_t)jb + (size_t)ga * n] : 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 16; ++k) acc += As[threadIdx.y][k] * Bs[threadIdx.x][k];
+    __syncthreads();
+  }
+  if (i < n && j < n) V[(size_t)i + (size_t)j * n] = acc;
+}
+
+// V = Vbar + Vbar^T in place (xc_integrals.hpp:148-153)
+__global__ void symmetrize_kernel(int n, double *V) {
+  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && j < n && i <= j) {
+    const double v = V[(size_t)i + (size_t)j * n] + V[(size_t)j + (size_t)i * n];
+    V[(size_t)i + (size_t)j * n] = v;
+    V[(size_t)j + (size_t)i * n] = v;
+  }
+}
+
+__global__ void potential_dense_kernel(const AuxFunc *__restrict__ f, int naux, const double *__restrict__ pts,
+                                       const double *__restrict__ w, long npts, double *Vw) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)naux * npts) return;
+  const int a = (int)(idx % naux);
+  const long g = idx / naux;
+  Vw[idx] = aux_potential(f[a], pts[3 * g], pts[3 * g + 1], pts[3 * g + 2]) * w[g];
+}
+
+__global__ void precondition_kernel(int N, const double *S, double *A, double *D) {
+  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N && j < N) A[(size_t)i + (size_t)j * N] = S[(size_t)i + (size_t)j * N] /
+                                                      sqrt(S[(size_t)i + (size_t)i * N] * S[(size_t)j + (size_t)j * N]);
+  if (j == 0 && i < N) D[i] = sqrt(S[(size_t)i + (size_t)i * N]);
+}
+
+XcSpec make_spec(const nkx_plan_options *o) {
+  XcSpec s;
+  NKX_REQUIRE(o && o->nfunc >= 1 && o->nfunc <= 4, NKX_ERR_ARG, "opts.nfunc must be 1..4");
+  s.nfunc = o->nfunc;
+  for (int i = 0; i < 4; ++i) s.ids[i] = i < o->nfunc ? o->func_ids[i] : 0;
+  for (int i = 0; i < o->nfunc; ++i)
+    NKX_REQUIRE(func_supported(o->func_ids[i]), NKX_ERR_UNSUPPORTED, "unsupported functional id");
+  s.thr = o->dens_threshold > 0 ? o->dens_threshold : 1e-15;
+  return s;
+}
+
+bool spec_is_gga(const XcSpec &s) {
+  for (int i = 0; i < s.nfunc; ++i)
+    if (func_is_gga(s.ids[i])) return true;
+  return false;
+}
+
+}  // namespace nkx
+
+using namespace nkx;
+
+static unsigned nblk(long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+extern "C" nkx_status nkx_fill_collocation(const nkx_basis *basis, const double *d_points, long npts, double *d_phi,
+                                           double *d_gx, double *d_gy, double *d_gz, void *stream) {
+  return run_guarded("nkx_fill_collocation", [&] {
+    NKX_REQUIRE(basis && basis->nbf > 0 && npts >= 0 && d_points && d_phi, NKX_ERR_ARG, "invalid arguments");
+    NKX_REQUIRE(!d_gx || (d_gy && d_gz), NKX_ERR_ARG, "gradient buffers must be given together");
+    for (int i = 0; i < basis->nbf; ++i)
+      NKX_REQUIRE(basis->l[i] >= 0 && basis->l[i] <= 7 && basis->n[i] > basis->l[i] &&
+                      abs(basis->m[i]) <= basis->l[i] && basis->zeta[i] > 0,
+                  NKX_ERR_UNSUPPORTED, "basis function outside n > l, |m| <= l <= 7, zeta > 0");
+    auto tab = make_sto_table(*basis);
+    DevBuf<StoFunc> df(tab.size());
+    cudaStream_t s = (cudaStream_t)stream;
+    NKX_CUDA(cudaMemcpyAsync(df.p, tab.data(), tab.size() * sizeof(StoFunc), cudaMemcpyHostToDevice, s));
+    const long tot = (long)basis->nbf * npts;
+    if (tot > 0) colloc_dense_kernel<<<nblk(tot, 128), 128, 0, s>>>(df.p, basis->nbf, d_points, npts, d_phi, d_gx, d_gy, d_gz);
+    NKX_LAUNCH_CHECK();
+    NKX_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+extern "C" nkx_status nkx_density_dense(int nbf, long npts, const double *d_phi, const double *d_gx,
+                                        const double *d_gy, const double *d_gz, int nocc, const double *d_C,
+                                        const double *d_occ, double *d_rho, double *d_grad, double *d_sigma,
+                                        void *stream) {
+  return run_guarded("nkx_density_dense", [&] {
+    NKX_REQUIRE(nbf > 0 && npts >= 0 && nocc > 0 && d_phi && d_C && d_occ && d_rho, NKX_ERR_ARG,
+                "invalid arguments");
+    NKX_REQUIRE(!(d_grad || d_sigma) || (d_gx && d_gy && d_gz), NKX_ERR_ARG, "gradient output needs grad inputs");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (npts > 0)
+      density_dense_kernel<<<nblk(npts * 32, 256), 256, 0, s>>>(nbf, npts, d_phi, (d_grad || d_sigma) ? d_gx : nullptr,
+                                                                d_gy, d_gz, nocc, d_C, d_occ, d_rho, d_grad, d_sigma);
+    NKX_LAUNCH_CHECK();
+    NKX_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+extern "C" nkx_status nkx_xc_eval(int func_id, int nspin, long n, const double *d_rho, const double *d_sigma,
+                                  double dens_threshold, double *d_exc, double *d_vrho, double *d_vsigma,
+                                  void *stream) {
+  return run_guarded("nkx_xc_eval", [&] {
+    NKX_REQUIRE((nspin == 1 || nspin == 2) && n >= 0 && d_rho && d_exc && d_vrho, NKX_ERR_ARG, "invalid arguments");
+    NKX_REQUIRE(func_supported(func_id), NKX_ERR_UNSUPPORTED, "unsupported functional id");
+    NKX_REQUIRE(!func_is_gga(func_id) || (d_sigma && d_vsigma), NKX_ERR_ARG, "GGA needs sigma and vsigma");
+    XcSpec sp;
+    sp.nfunc = 1;
+    sp.ids[0] = func_id;
+    sp.ids[1] = sp.ids[2] = sp.ids[3] = 0;
+    sp.thr = dens_threshold > 0 ? dens_threshold : 1e-15;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n > 0) xc_eval_kernel<<<nblk(n, 128), 128, 0, s>>>(sp, nspin, n, d_rho, d_sigma, d_exc, d_vrho, d_vsigma);
+    NKX_LAUNCH_CHECK();
+    NKX_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+extern "C" nkx_status nkx_xc_dense(int nbf, long npts, const double *d_phi, const double *d_gx, const double *d_gy,
+                                   const double *d_gz, const double *d_w, int nspin, int nocc, const double *d_C,
+                                   const double *d_occ, const nkx_plan_options *opts, double *E, double *d_V,
+                                   void *stream) {
+  return run_guarded("nkx_xc_dense", [&] {
+    NKX_REQUIRE(nbf > 0 && npts > 0 && (nspin == 1 || nspin == 2) && nocc > 0 && d_phi && d_w && d_C && d_occ &&
+                    E && d_V,
+                NKX_ERR_ARG, "invalid arguments");
+    const XcSpec sp = make_spec(opts);
+    const bool gga = spec_is_gga(sp);
+    NKX_REQUIRE(!gga || (d_gx && d_gy && d_gz), NKX_ERR_ARG, "GGA needs collocation gradients");
+    cudaStream_t s = (cudaStream_t)stream;
+    DevBuf<double> rho((size_t)nspin * npts), grad((size_t)nspin * 3 * npts), Z((size_t)nspin * nbf * npts), Ed(1);
+    for (int sp_i = 0; sp_i < nspin; ++sp_i)
+      density_dense_kernel<<<nblk(npts * 32, 256), 256, 0, s>>>(
+          nbf, npts, d_phi, gga ? d_gx : nullptr, d_gy, d_gz, nocc, d_C + (size_t)sp_i * nbf * nocc,
+          d_occ + (size_t)sp_i * nocc, rho.p + (size_t)sp_i * npts, gga ? grad.p + (size_t)sp_i * 3 * npts : nullptr,
+          nullptr);
+    NKX_LAUNCH_CHECK();
+    NKX_CUDA(cudaMemsetAsync(Ed.p, 0, sizeof(double), s));
+    xc_z_dense_kernel<<<nblk(npts, 128), 128, 0, s>>>(sp, gga, nbf, npts, nspin, d_phi, d_gx, d_gy, d_gz, d_w,
+                                                     rho.p, grad.p, Z.p, Ed.p);
+    NKX_LAUNCH_CHECK();
+    dim3 tb(16, 16), gb(nblk(nbf, 16), nblk(nbf, 16));
+    for (int sp_i = 0; sp_i < nspin; ++sp_i) {
+      double *Vs = d_V + (size_t)sp_i * nbf * nbf;
+      nt_gemm_dense_kernel<<<gb, tb, 0, s>>>(nbf, npts, d_phi, Z.p + (size_t)sp_i * nbf * npts, Vs);
+      symmetrize_kernel<<<gb, tb, 0, s>>>(nbf, Vs);
+    }
+    NKX_LAUNCH_CHECK();
+    NKX_CUDA(cudaMemcpyAsync(E, Ed.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    NKX_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+extern "C" nkx_status nkx_potential_collocation(const nkx_basis *aux, const double *d_points, const double *d_w,
+                                                long npts, double *d_Vw, void *stream) {
+  return run_guarded("nkx_potential_collocation", [&] {
+    NKX_REQUIRE(aux && aux->nbf > 0 && npts >= 0 && d_points && d_w && d_Vw, NKX_ERR_ARG, "invalid arguments");
+    auto tab = make_aux_table(*aux);
+    DevBuf<AuxFunc> df(tab.size());
+    cudaStream_t s = (cudaStream_t)stream;
+    NKX_CUDA(cudaMemcpyAsync(df.p, tab.data(), tab.size() * sizeof(AuxFunc), cudaMemcpyHostToDevice, s));
+    const long tot = (long)aux->nbf * npts;
+    if (tot > 0) potential_dense_kernel<<<nblk(tot, 128), 128, 0, s>>>(df.p, aux->nbf, d_points, d_w, npts, d_Vw);
+    NKX_LAUNCH_CHECK();
+    NKX_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+extern "C" nkx_status nkx_half_inverse(int N, const double *d_S, double thr, double *d_X, int *K, void *stream) {
+  return run_guarded("nkx_half_inverse", [&] {
+    NKX_REQUIRE(N > 0 && d_S && d_X && K, NKX_ERR_ARG, "invalid arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    DevBuf<double> A((size_t)N * N), D(N), lam(N);
+    DevBuf<int> info(1);
+    dim3 tb(16, 16), gb(nblk(N, 16), nblk(N, 16));
+    precondition_kernel<<<gb, tb, 0, s>>>(N, d_S, A.p, D.p);
+    NKX_LAUNCH_CHECK();
+    cusolverDnHandle_t h;
+    NKX_REQUIRE(cusolverDnCreate(&h) == CUSOLVER_STATUS_SUCCESS, NKX_ERR_CUDA, "cusolverDnCreate failed");
+    cusolverDnSetStream(h, s);
+    int lwork = 0;
+    cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, N, A.p, N, lam.p, &lwork);
+    DevBuf<double> work(lwork > 0 ? lwork : 1);
+    const cusolverStatus_t st =
+        cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, N, A.p, N, lam.p, work.p, lwork, info.p);
+    cusolverDnDestroy(h);
+    NKX_REQUIRE(st == CUSOLVER_STATUS_SUCCESS, NKX_ERR_CUDA, "cusolverDnDsyevd failed");
+    std::vector<double> hl(N), hU((size_t)N * N), hD(N);
+    NKX_CUDA(cudaMemcpyAsync(hl.data(), lam.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+    NKX_CUDA(cudaMemcpyAsync(hU.data(), A.p, sizeof(double) * N * N, cudaMemcpyDeviceToHost, s));
+    NKX_CUDA(cudaMemcpyAsync(hD.data(), D.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+    NKX_CUDA(cudaStreamSynchronize(s));
+    // singular values of a symmetric matrix are |eigenvalues|; keep s > thr,
+    // largest first (the reference's SVD ordering)
+    std::vector<int> order(N);
+    for (int i = 0; i < N; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return fabs(hl[a]) > fabs(hl[b]); });
+    std::vector<double> hX((size_t)N * N, 0.0);
+    int k = 0;
+    for (int oi = 0; oi < N; ++oi) {
+      const int e = order[oi];
+      const double sv = fabs(hl[e]);
+      if (!(sv > thr)) continue;
+      for (int i = 0; i < N; ++i) hX[(size_t)i + (size_t)k * N] = hU[(size_t)i + (size_t)e * N] / sqrt(sv) / hD[i];
+      ++k;
+    }
+    NKX_CUDA(cudaMemcpyAsync(d_X, hX.data(), sizeof(double) * N * N, cudaMemcpyHostToDevice, s));
+    NKX_CUDA(cudaStreamSynchronize(s));
+    *K = k;
+  });
+}

@@ -1,0 +1,1018 @@
+// The batched, screened grid-integration Fock build (the hot path).
+//
+// Once per geometry (nkx_plan_create): the grid is sorted into Morton order
+// and cut into 256-point batches (create_bounding_boxes,
+// nukexc/octree.hpp:70-141); basis functions are grouped into blocks of 128
+// in basis order and a block is significant for a batch when the cutoff
+// sphere of any of its functions meets the batch's bounding box
+// (build_neighbor_list, nukexc/octree.hpp:317-390); the aux Coulomb metric is
+// integrated on the grid and Cholesky-factorised in FP64.
+//
+// Per SCF iteration (nkx_fock_build), streamed over chunks of batches that
+// fit the workspace:
+//   pass A  collocation  PhiT[pair][g][f] (value + gradient)       colloc_*
+//           density      T = PhiT C, rho = sum occ T^2, grad rho    density_*
+//   J       y = (Vw rho), c = (A|B)^-1 y, v_g = sum c_a V_a(g) w_g  aux_*
+//   XC      functional on every point, E_xc, Z coefficients         functional_kernel
+//   pass B  Z^T[pair][g][f] = a_g phi + b_g . grad phi              zbuild_*
+//           Vbar(I,J) += sum_b PhiT_bI^T Z_bJ  per function-block tile
+//   end     V = Vbar + Vbar^T, unpadded to nbf x nbf
+// (compute_gga / compute_gga_lsda, nukexc/xc_integrals.hpp:424-726, and
+// compute_coulomb, nukexc/coulomb.hpp:56-115, reorganised into batches).
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "functionals.cuh"
+#include "host_setup.hpp"
+#include "plan.cuh"
+
+namespace nkx {
+
+// ------------------------------------------------------------- errors ----
+static thread_local std::string g_last_error;
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+nkx_status run_guarded(const char *where, const std::function<void()> &fn) {
+  try {
+    fn();
+    return NKX_OK;
+  } catch (const Error &e) {
+    set_error(std::string(where) + ": " + e.msg);
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    set_error(std::string(where) + ": host allocation failed");
+    return NKX_ERR_ALLOC;
+  } catch (const std::exception &e) {
+    set_error(std::string(where) + ": " + e.what());
+    return NKX_ERR_ARG;
+  }
+}
+
+XcSpec make_spec(const nkx_plan_options *o);
+bool spec_is_gga(const XcSpec &s);
+
+template <class T>
+static T *dalloc(size_t n) {
+  T *p = nullptr;
+  if (n == 0) return nullptr;
+  const cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error{NKX_ERR_ALLOC, "cudaMalloc of " + std::to_string(n * sizeof(T)) + " bytes failed"};
+  }
+  return p;
+}
+
+static unsigned nblk(long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// ========================================================== kernels ======
+
+// Collocation of one (batch, function block) pair per CTA.  Lane l of a warp
+// owns functions f = l + 32c (c < 4) of the block; warp w owns points
+// g = w + 8j.  Each store of 32 consecutive f is coalesced.  Output
+// PhiT[pair][comp][g][f], comp 0 = value, 1..3 = gradient (GRAD only).
+template <bool GRAD>
+__global__ void __launch_bounds__(256) colloc_fp64_kernel(const StoFunc *__restrict__ sto, const double *__restrict__ px,
+                                                          const double *__restrict__ py, const double *__restrict__ pz,
+                                                          const int *__restrict__ pair_batch,
+                                                          const int *__restrict__ pair_blk, long p0,
+                                                          double *__restrict__ out) {
+  const long p = p0 + blockIdx.x;
+  const int b = pair_batch[p], I = pair_blk[p];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ double sx[kBatch], sy[kBatch], sz[kBatch];
+  for (int g = threadIdx.x; g < kBatch; g += blockDim.x) {
+    sx[g] = px[(long)b * kBatch + g];
+    sy[g] = py[(long)b * kBatch + g];
+    sz[g] = pz[(long)b * kBatch + g];
+  }
+  __syncthreads();
+  StoFunc f[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) f[c] = sto[I * kBlockF + lane + 32 * c];
+  const size_t tile = (size_t)kBatch * kBlockF;
+  double *o = out + (size_t)blockIdx.x * (GRAD ? 4 : 1) * tile;
+  for (int g = warp; g < kBatch; g += 8) {
+    const double x = sx[g], y = sy[g], z = sz[g];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const size_t idx = (size_t)g * kBlockF + lane + 32 * c;
+      if (GRAD) {
+        double v, gx, gy, gz;
+        sto_value_grad(f[c], x, y, z, v, gx, gy, gz);
+        o[idx] = v;
+        o[tile + idx] = gx;
+        o[2 * tile + idx] = gy;
+        o[3 * tile + idx] = gz;
+      } else {
+        o[idx] = sto_value(f[c], x, y, z);
+      }
+    }
+  }
+}
+
+// Density of one 64-point tile of one batch for one spin, FP64.
+// T(g,i) = sum_f PhiT(g,f) Ct(i,f) over the batch's significant blocks (and
+// the three gradient components), then rho = sum_i occ_i T^2 and
+// grad rho = 2 sum_i occ_i T grad T (density.hpp:188-255).  Thread (ty, tx)
+// owns points g = ty + 16a (a < 4) and orbitals i = tx + 16c (c < 4) of the
+// current 64-orbital tile.
+template <bool GRAD>
+__global__ void __launch_bounds__(256) density_fp64_kernel(const double *__restrict__ phiT, const double *__restrict__ Ct,
+                                                           const double *__restrict__ occ, int nocc, int nbf_pad,
+                                                           const int *__restrict__ pair_off,
+                                                           const int *__restrict__ pair_blk, long b0, long p0,
+                                                           double *__restrict__ rho, double *__restrict__ grad,
+                                                           long npad) {
+  constexpr int NC = GRAD ? 4 : 1;
+  constexpr int KS = 16;
+  __shared__ double Ps[NC][KS][64 + 1];
+  __shared__ double Cs[KS][64 + 1];
+  const int spin = blockIdx.y;
+  const long b = b0 + blockIdx.x / 4;
+  const int g0 = (blockIdx.x % 4) * 64;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const double *C = Ct + (size_t)spin * nocc * nbf_pad;
+  const double *oc = occ + (size_t)spin * nocc;
+  const int q0 = pair_off[b], q1 = pair_off[b + 1];
+  const size_t tile = (size_t)kBatch * kBlockF;
+  double racc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) racc[a][k] = 0.0;
+
+  for (int i0 = 0; i0 < nocc; i0 += 64) {
+    double acc[NC][4][4];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[c][a][j] = 0.0;
+    for (int q = q0; q < q1; ++q) {
+      const int I = pair_blk[q];
+      const double *P = phiT + (size_t)(q - p0) * NC * tile;
+      for (int f0 = 0; f0 < kBlockF; f0 += KS) {
+        // stage PhiT(g0..g0+63, f0..f0+15) of each comp and Ct(i0..i0+63, f0..)
+        for (int e = threadIdx.x; e < NC * 64 * KS; e += 256) {
+          const int c = e / (64 * KS), r = (e / KS) % 64, k = e % KS;
+          Ps[c][k][r] = P[c * tile + (size_t)(g0 + r) * kBlockF + f0 + k];
+        }
+        for (int e = threadIdx.x; e < 64 * KS; e += 256) {
+          const int r = e / KS, k = e % KS;
+          const int i = i0 + r;
+          Cs[k][r] = i < nocc ? C[(size_t)i * nbf_pad + I * kBlockF + f0 + k] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < KS; ++k) {
+          double bv[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) bv[j] = Cs[k][tx + 16 * j];
+#pragma unroll
+          for (int c = 0; c < NC; ++c)
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+              const double av = Ps[c][k][ty + 16 * a];
+#pragma unroll
+              for (int j = 0; j < 4; ++j) acc[c][a][j] += av * bv[j];
+            }
+        }
+        __syncthreads();
+      }
+    }
+    // contract over this orbital tile
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      double s[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int i = i0 + tx + 16 * j;
+        const double o = i < nocc ? oc[i] : 0.0;
+        const double t = acc[0][a][j];
+        s[0] += o * t * t;
+        if (GRAD) {
+          s[1] += o * t * acc[NC > 1 ? 1 : 0][a][j];
+          s[2] += o * t * acc[NC > 2 ? 2 : 0][a][j];
+          s[3] += o * t * acc[NC > 3 ? 3 : 0][a][j];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+#pragma unroll
+        for (int off = 8; off; off >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], off);
+        racc[a][k] += s[k];
+      }
+    }
+  }
+  if (tx == 0) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const long g = b * kBatch + g0 + ty + 16 * a;
+      rho[(size_t)spin * npad + g] = racc[a][0];
+      if (GRAD) {
+        grad[((size_t)spin * 3 + 0) * npad + g] = 2.0 * racc[a][1];
+        grad[((size_t)spin * 3 + 1) * npad + g] = 2.0 * racc[a][2];
+        grad[((size_t)spin * 3 + 2) * npad + g] = 2.0 * racc[a][3];
+      }
+    }
+  }
+}
+
+// Functional on every point: E_xc, and the Z coefficients
+// coef[spin][0][g] = w (1/2 vrho + 1/2 vJ), coef[spin][1..3][g] = w vec
+// (xc_integrals.hpp:506-514 closed shell, :655-664 open shell).  vj (may be
+// null) is the weighted fitted Coulomb potential folded into both spins.
+__global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, const double *__restrict__ w,
+                                  const double *__restrict__ rho, const double *__restrict__ grad,
+                                  const double *__restrict__ vj, double *__restrict__ coef, double *Eacc) {
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (g < npad) {
+    const double wg = w[g];
+    double vr[2] = {0, 0}, vec[2][3] = {{0, 0, 0}, {0, 0, 0}}, gr[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    if (gga)
+      for (int sp = 0; sp < nspin; ++sp)
+        for (int k = 0; k < 3; ++k) gr[sp][k] = grad[((size_t)sp * 3 + k) * npad + g];
+    if (wg != 0.0) {
+      if (nspin == 1) {
+        const double sg = gr[0][0] * gr[0][0] + gr[0][1] * gr[0][1] + gr[0][2] * gr[0][2];
+        double f, vrho, vs;
+        xc_unpol(s, rho[g], sg, f, vrho, vs);
+        e = wg * f;
+        vr[0] = vrho;
+        for (int k = 0; k < 3; ++k) vec[0][k] = 2.0 * vs * gr[0][k];
+      } else {
+        const double saa = gr[0][0] * gr[0][0] + gr[0][1] * gr[0][1] + gr[0][2] * gr[0][2];
+        const double sab = gr[0][0] * gr[1][0] + gr[0][1] * gr[1][1] + gr[0][2] * gr[1][2];
+        const double sbb = gr[1][0] * gr[1][0] + gr[1][1] * gr[1][1] + gr[1][2] * gr[1][2];
+        double f, d[5];
+        xc_pol(s, rho[g], rho[npad + g], saa, sab, sbb, f, d);
+        e = wg * f;
+        vr[0] = d[0];
+        vr[1] = d[1];
+        for (int k = 0; k < 3; ++k) {
+          vec[0][k] = 2.0 * d[2] * gr[0][k] + d[3] * gr[1][k];
+          vec[1][k] = 2.0 * d[4] * gr[1][k] + d[3] * gr[0][k];
+        }
+      }
+    }
+    const double vjg = vj ? vj[g] : 0.0;
+    for (int sp = 0; sp < nspin; ++sp) {
+      coef[((size_t)sp * 4 + 0) * npad + g] = wg * 0.5 * vr[sp] + 0.5 * vjg;
+      coef[((size_t)sp * 4 + 1) * npad + g] = wg * vec[sp][0];
+      coef[((size_t)sp * 4 + 2) * npad + g] = wg * vec[sp][1];
+      coef[((size_t)sp * 4 + 3) * npad + g] = wg * vec[sp][2];
+    }
+  }
+  __shared__ double red[32];
+  for (int o = 16; o; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    e = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if (threadIdx.x == 0) atomicAdd(Eacc, e);
+  }
+}
+
+// Z^T[pair][spin][g][f] = coef0 phi + coef1 dphi/dx + coef2 dphi/dy + coef3 dphi/dz.
+// Spin index nspin (when jonly) builds Z_J = 1/2 vJ phi for a separate J.
+template <bool GRAD>
+__global__ void zbuild_fp64_kernel(const double *__restrict__ phiT, const double *__restrict__ coef,
+                                   const double *__restrict__ vj, const int *__restrict__ pair_batch, long p0,
+                                   int nz, int nspin, long npad, double *__restrict__ zT) {
+  constexpr int NC = GRAD ? 4 : 1;
+  const long q = blockIdx.x;
+  const int b = pair_batch[p0 + q];
+  const size_t tile = (size_t)kBatch * kBlockF;
+  const double *P = phiT + q * NC * tile;
+  for (int e = threadIdx.x; e < kBatch * kBlockF; e += blockDim.x) {
+    const int g = e / kBlockF;
+    const long gg = (long)b * kBatch + g;
+    const double v = P[e];
+    double dx = 0, dy = 0, dz = 0;
+    if (GRAD) {
+      dx = P[tile + e];
+      dy = P[2 * tile + e];
+      dz = P[3 * tile + e];
+    }
+    for (int s = 0; s < nz; ++s) {
+      double z;
+      if (s < nspin) {
+        const double *c = coef + (size_t)s * 4 * npad;
+        z = c[gg] * v;
+        if (GRAD) z += c[npad + gg] * dx + c[2 * npad + gg] * dy + c[3 * npad + gg] * dz;
+      } else {
+        z = 0.5 * vj[gg] * v;
+      }
+      zT[(q * nz + s) * tile + e] = z;
+    }
+  }
+}
+
+__device__ __forceinline__ int block_pos(const uint32_t *m, int I) {
+  int pos = 0;
+  for (int w = 0; w < (I >> 5); ++w) pos += __popc(m[w]);
+  return pos + __popc(m[I >> 5] & ((1u << (I & 31)) - 1u));
+}
+__device__ __forceinline__ bool block_has(const uint32_t *m, int I) { return (m[I >> 5] >> (I & 31)) & 1u; }
+
+// Vbar(I,J) tile += sum over the chunk's batches b with I, J significant of
+// PhiT_bI^T ZT_bJ, FP64.  One CTA per (I, J, z) tile of 128 x 128; thread
+// (ty, tx) owns rows ty + 16i, cols tx + 16j; K slabs of 16 points staged in
+// shared memory straight from the [g][f] layout.
+__global__ void __launch_bounds__(256) vgemm_fp64_kernel(const double *__restrict__ phiT, const double *__restrict__ zT,
+                                                         int phi_stride_tiles, int nz, const int *__restrict__ pair_off,
+                                                         const uint32_t *__restrict__ mask, int mask_words, long b0,
+                                                         long b1, long p0, int nbf_pad, double *__restrict__ V) {
+  constexpr int KS = 16;
+  __shared__ double As[KS][128];
+  __shared__ double Bs[KS][128];
+  const int J = blockIdx.x, I = blockIdx.y, zi = blockIdx.z;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const size_t tile = (size_t)kBatch * kBlockF;
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  bool any = false;
+  for (long b = b0; b < b1; ++b) {
+    const uint32_t *m = mask + b * mask_words;
+    if (!block_has(m, I) || !block_has(m, J)) continue;
+    any = true;
+    const long qb = pair_off[b] - p0;
+    const double *A = phiT + (size_t)(qb + block_pos(m, I)) * phi_stride_tiles * tile;
+    const double *B = zT + ((size_t)(qb + block_pos(m, J)) * nz + zi) * tile;
+    for (int g0 = 0; g0 < kBatch; g0 += KS) {
+#pragma unroll
+      for (int r = 0; r < (KS * 128) / 256; ++r) {
+        const int e = threadIdx.x + 256 * r;
+        const int k = e >> 7, f = e & 127;
+        As[k][f] = A[(size_t)(g0 + k) * kBlockF + f];
+        Bs[k][f] = B[(size_t)(g0 + k) * kBlockF + f];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < KS; ++k) {
+        double a[8], bb[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a[i] = As[k][ty + 16 * i];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) bb[j] = Bs[k][tx + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * bb[j];
+      }
+      __syncthreads();
+    }
+  }
+  if (!any) return;
+  double *Vz = V + (size_t)zi * nbf_pad * nbf_pad;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const size_t r = (size_t)I * 128 + ty + 16 * i, c = (size_t)J * 128 + tx + 16 * j;
+      Vz[r + c * nbf_pad] += acc[i][j];
+    }
+}
+
+// out(i,j) = Vp(i,j) + Vp(j,i) for i, j < n (symmetrise and unpad)
+__global__ void symmetrize_unpad_kernel(int n, int npad, const double *__restrict__ Vp, double *__restrict__ out) {
+  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && j < n) out[(size_t)i + (size_t)j * n] = Vp[(size_t)i + (size_t)j * npad] + Vp[(size_t)j + (size_t)i * npad];
+}
+
+// C (nbf x nocc column-major, per spin) -> Ct[spin][i][f], f padded to nbf_pad
+__global__ void pack_orbitals_kernel(const double *__restrict__ C, int nbf, int nocc, int nspin, int nbf_pad,
+                                     double *__restrict__ Ct) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long tot = (long)nspin * nocc * nbf_pad;
+  if (e >= tot) return;
+  const int f = (int)(e % nbf_pad);
+  const long si = e / nbf_pad;
+  Ct[e] = f < nbf ? C[si * nbf + f] : 0.0;
+}
+
+// y_a += sum over a slice of points of w_g V_a(g) rho_g   (coulomb.hpp:84-85)
+__global__ void aux_y_kernel(const AuxFunc *__restrict__ aux, const double *__restrict__ px,
+                             const double *__restrict__ py, const double *__restrict__ pz,
+                             const double *__restrict__ w, const double *__restrict__ rho, int nspin, long npad,
+                             long slice, double *__restrict__ y) {
+  const int a = blockIdx.x;
+  const AuxFunc f = aux[a];
+  const long g0 = blockIdx.y * slice, g1 = min(npad, g0 + slice);
+  double s = 0.0;
+  for (long g = g0 + threadIdx.x; g < g1; g += blockDim.x) {
+    double r = rho[g];
+    if (nspin == 2) r += rho[npad + g];
+    const double wr = w[g] * r;
+    if (wr != 0.0) s += wr * aux_potential(f, px[g], py[g], pz[g]);
+  }
+  __shared__ double red[32];
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) atomicAdd(y + a, s);
+  }
+}
+
+// v_g = w_g sum_a c_a V_a(g)   (coulomb.hpp:93-95)
+__global__ void aux_v_kernel(const AuxFunc *__restrict__ aux, int naux, const double *__restrict__ c,
+                             const double *__restrict__ px, const double *__restrict__ py,
+                             const double *__restrict__ pz, const double *__restrict__ w, long npad,
+                             double *__restrict__ v) {
+  __shared__ AuxFunc sf[64];
+  __shared__ double sc[64];
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const bool on = g < npad;
+  const double x = on ? px[g] : 0.0, y = on ? py[g] : 0.0, z = on ? pz[g] : 0.0;
+  double s = 0.0;
+  for (int a0 = 0; a0 < naux; a0 += 64) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < 64; e += blockDim.x)
+      if (a0 + e < naux) {
+        sf[e] = aux[a0 + e];
+        sc[e] = c[a0 + e];
+      }
+    __syncthreads();
+    const int na = min(64, naux - a0);
+    if (on)
+      for (int k = 0; k < na; ++k) s += sc[k] * aux_potential(sf[k], x, y, z);
+  }
+  if (on) v[g] = s * w[g];
+}
+
+// Aux collocation phi_A(g) and weighted potential Vw_B(g) of a slice of
+// points, column-major naux x np (metric (A|B) set-up, standalone.cxx:443-461)
+__global__ void aux_tables_kernel(const StoFunc *__restrict__ sto, const AuxFunc *__restrict__ aux, int naux,
+                                  const double *__restrict__ px, const double *__restrict__ py,
+                                  const double *__restrict__ pz, const double *__restrict__ w, long g0, long np,
+                                  double *__restrict__ phi, double *__restrict__ vw) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= (long)naux * np) return;
+  const int a = (int)(e % naux);
+  const long g = g0 + e / naux;
+  phi[e] = sto_value(sto[a], px[g], py[g], pz[g]);
+  vw[e] = aux_potential(aux[a], px[g], py[g], pz[g]) * w[g];
+}
+
+__global__ void sym_half_kernel(int n, double *S) {
+  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && j < n && i < j) {
+    const double v = 0.5 * (S[(size_t)i + (size_t)j * n] + S[(size_t)j + (size_t)i * n]);
+    S[(size_t)i + (size_t)j * n] = v;
+    S[(size_t)j + (size_t)i * n] = v;
+  }
+}
+
+// ========================================================= plan set-up ==
+
+static uint64_t spread3(uint64_t v) {
+  v &= 0x1fffff;
+  v = (v | v << 32) & 0x1f00000000ffffULL;
+  v = (v | v << 16) & 0x1f0000ff0000ffULL;
+  v = (v | v << 8) & 0x100f00f00f00f00fULL;
+  v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+  v = (v | v << 2) & 0x1249249249249249ULL;
+  return v;
+}
+
+Plan::~Plan() {
+  for (void *p : allocs) cudaFree(p);
+  if (cublas) cublasDestroy((cublasHandle_t)cublas);
+  if (cusolver) cusolverDnDestroy((cusolverDnHandle_t)cusolver);
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+template <class T>
+T *Plan::alloc(size_t n) {
+  T *p = dalloc<T>(n);
+  if (p) allocs.push_back(p);
+  return p;
+}
+
+static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, const nkx_basis *aux, long npoints,
+                       const double *xyz, const double *w, const nkx_plan_options *opts) {
+  NKX_REQUIRE(prim && prim->nbf > 0 && npoints > 0 && xyz && w && opts, NKX_ERR_ARG, "invalid arguments");
+  NKX_REQUIRE(opts->batch_points == 0 || opts->batch_points == kBatch, NKX_ERR_UNSUPPORTED,
+              "batch_points must be 256");
+  for (int i = 0; i < prim->nbf; ++i)
+    NKX_REQUIRE(prim->l[i] >= 0 && prim->l[i] <= 7 && prim->n[i] > prim->l[i] && abs(prim->m[i]) <= prim->l[i] &&
+                    prim->zeta[i] > 0,
+                NKX_ERR_UNSUPPORTED, "basis function outside n > l, |m| <= l <= 7, zeta > 0");
+  P.xc = make_spec(opts);
+  P.gga = spec_is_gga(P.xc);
+  NKX_CUDA(cudaGetDevice(&P.device));
+  NKX_CUDA(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
+  for (auto &e : P.ev) NKX_CUDA(cudaEventCreate(&e));
+  P.nbf = prim->nbf;
+  P.nblk = (P.nbf + kBlockF - 1) / kBlockF;
+  P.nbf_pad = P.nblk * kBlockF;
+  P.mask_words = (P.nblk + 31) / 32;
+  P.npts = npoints;
+  P.nbatch = (npoints + kBatch - 1) / kBatch;
+  P.npad = P.nbatch * kBatch;
+
+  // --- Morton order of the points (create_bounding_boxes, octree.hpp:70-110)
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (long g = 0; g < npoints; ++g)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], xyz[3 * g + d]);
+      hi[d] = std::max(hi[d], xyz[3 * g + d]);
+    }
+  std::vector<uint64_t> code(npoints);
+  for (long g = 0; g < npoints; ++g) {
+    uint64_t c = 0;
+    for (int d = 0; d < 3; ++d) {
+      const double span = hi[d] > lo[d] ? hi[d] - lo[d] : 1.0;
+      const double u = (xyz[3 * g + d] - lo[d]) / span;
+      c |= spread3((uint64_t)std::min(2097151.0, std::max(0.0, u * 2097151.0))) << d;
+    }
+    code[g] = c;
+  }
+  P.perm.resize(npoints);
+  std::iota(P.perm.begin(), P.perm.end(), 0L);
+  std::stable_sort(P.perm.begin(), P.perm.end(), [&](long a, long b) { return code[a] < code[b]; });
+  std::vector<double> hx(P.npad), hy(P.npad), hz(P.npad), hw(P.npad, 0.0);
+  for (long p = 0; p < P.npad; ++p) {
+    const long g = P.perm[std::min(p, npoints - 1)];
+    hx[p] = xyz[3 * g];
+    hy[p] = xyz[3 * g + 1];
+    hz[p] = xyz[3 * g + 2];
+    if (p < npoints) hw[p] = w[g];
+  }
+
+  // --- basis table (padded functions have norm 0)
+  auto tab = make_sto_table(*prim);
+  tab.resize(P.nbf_pad);
+  for (int i = P.nbf; i < P.nbf_pad; ++i) {
+    tab[i] = tab[0];
+    tab[i].norm = 0.0;
+  }
+  const double tol = opts->screen_tol > 0 ? opts->screen_tol : 1e-10;
+  auto cut = make_cutoffs(*prim, tol);
+
+  // --- screening: block I is significant for batch b if any function's
+  // cutoff sphere meets the batch bounding box (octree.hpp:331-366)
+  P.h_mask.assign((size_t)P.nbatch * P.mask_words, 0u);
+  P.h_pair_off.assign(P.nbatch + 1, 0);
+  std::vector<int> pblk, pbatch;
+  for (long b = 0; b < P.nbatch; ++b) {
+    double bl[3] = {1e300, 1e300, 1e300}, bh[3] = {-1e300, -1e300, -1e300};
+    for (int g = 0; g < kBatch; ++g) {
+      const long p = b * kBatch + g;
+      const double v[3] = {hx[p], hy[p], hz[p]};
+      for (int d = 0; d < 3; ++d) {
+        bl[d] = std::min(bl[d], v[d]);
+        bh[d] = std::max(bh[d], v[d]);
+      }
+    }
+    for (int I = 0; I < P.nblk; ++I) {
+      bool sig = false;
+      for (int f = I * kBlockF; f < std::min(P.nbf, (I + 1) * kBlockF) && !sig; ++f) {
+        double d2 = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          const double c = prim->center[3 * f + d];
+          const double e = c < bl[d] ? bl[d] - c : (c > bh[d] ? c - bh[d] : 0.0);
+          d2 += e * e;
+        }
+        sig = d2 <= cut[f] * cut[f];
+      }
+      if (sig) {
+        P.h_mask[b * P.mask_words + I / 32] |= 1u << (I % 32);
+        pblk.push_back(I);
+        pbatch.push_back((int)b);
+      }
+    }
+    P.h_pair_off[b + 1] = (int)pblk.size();
+  }
+  P.npairs = (long)pblk.size();
+
+  // --- device copies
+  P.d_px = P.alloc<double>(P.npad);
+  P.d_py = P.alloc<double>(P.npad);
+  P.d_pz = P.alloc<double>(P.npad);
+  P.d_w = P.alloc<double>(P.npad);
+  NKX_CUDA(cudaMemcpy(P.d_px, hx.data(), sizeof(double) * P.npad, cudaMemcpyHostToDevice));
+  NKX_CUDA(cudaMemcpy(P.d_py, hy.data(), sizeof(double) * P.npad, cudaMemcpyHostToDevice));
+  NKX_CUDA(cudaMemcpy(P.d_pz, hz.data(), sizeof(double) * P.npad, cudaMemcpyHostToDevice));
+  NKX_CUDA(cudaMemcpy(P.d_w, hw.data(), sizeof(double) * P.npad, cudaMemcpyHostToDevice));
+  P.d_sto = P.alloc<StoFunc>(P.nbf_pad);
+  NKX_CUDA(cudaMemcpy(P.d_sto, tab.data(), sizeof(StoFunc) * P.nbf_pad, cudaMemcpyHostToDevice));
+  P.d_mask = P.alloc<uint32_t>(P.h_mask.size());
+  NKX_CUDA(cudaMemcpy(P.d_mask, P.h_mask.data(), sizeof(uint32_t) * P.h_mask.size(), cudaMemcpyHostToDevice));
+  P.d_pair_off = P.alloc<int>(P.nbatch + 1);
+  NKX_CUDA(cudaMemcpy(P.d_pair_off, P.h_pair_off.data(), sizeof(int) * (P.nbatch + 1), cudaMemcpyHostToDevice));
+  P.d_pair_blk = P.alloc<int>(std::max<long>(1, P.npairs));
+  P.d_pair_batch = P.alloc<int>(std::max<long>(1, P.npairs));
+  if (P.npairs) {
+    NKX_CUDA(cudaMemcpy(P.d_pair_blk, pblk.data(), sizeof(int) * P.npairs, cudaMemcpyHostToDevice));
+    NKX_CUDA(cudaMemcpy(P.d_pair_batch, pbatch.data(), sizeof(int) * P.npairs, cudaMemcpyHostToDevice));
+  }
+
+  // --- chunks of batches sized by the workspace
+  const size_t tile = (size_t)kBatch * kBlockF;
+  const size_t per_pair = tile * sizeof(double) * (4 + 3);  // PhiT (4) + Z (up to 3: a, b, J)
+  size_t ws = opts->workspace_bytes;
+  if (ws == 0) {
+    size_t fr = 0, tot = 0;
+    NKX_CUDA(cudaMemGetInfo(&fr, &tot));
+    ws = std::min<size_t>((size_t)12 << 30, fr / 3);
+  }
+  long maxp = std::max<long>(1, (long)(ws / per_pair));
+  long b = 0;
+  while (b < P.nbatch) {
+    Chunk c;
+    c.b0 = b;
+    c.p0 = P.h_pair_off[b];
+    while (b < P.nbatch && (P.h_pair_off[b + 1] - c.p0 <= maxp || b == c.b0)) ++b;
+    c.b1 = b;
+    c.p1 = P.h_pair_off[b];
+    P.max_chunk_pairs = std::max(P.max_chunk_pairs, c.p1 - c.p0);
+    P.chunks.push_back(c);
+  }
+  P.ws_phi = P.alloc<double>(std::max<long>(1, P.max_chunk_pairs) * 4 * tile);
+  P.ws_z = P.alloc<double>(std::max<long>(1, P.max_chunk_pairs) * 3 * tile);
+
+  // per-point arrays (two spins)
+  P.d_rho = P.alloc<double>(2 * P.npad);
+  P.d_grad = P.alloc<double>(6 * P.npad);
+  P.d_coef = P.alloc<double>(8 * P.npad);
+  P.d_vj = P.alloc<double>(P.npad);
+  P.d_V = P.alloc<double>(3 * (size_t)P.nbf_pad * P.nbf_pad);
+  P.d_E = P.alloc<double>(1);
+  NKX_CUDA(cudaMemset(P.d_rho, 0, sizeof(double) * 2 * P.npad));
+  NKX_CUDA(cudaMemset(P.d_grad, 0, sizeof(double) * 6 * P.npad));
+
+  // --- aux metric and its factor
+  if (aux && aux->nbf > 0) {
+    P.naux = aux->nbf;
+    auto atab = make_aux_table(*aux);
+    auto astab = make_sto_table(*aux);
+    P.d_aux = P.alloc<AuxFunc>(P.naux);
+    NKX_CUDA(cudaMemcpy(P.d_aux, atab.data(), sizeof(AuxFunc) * P.naux, cudaMemcpyHostToDevice));
+    StoFunc *d_asto = dalloc<StoFunc>(P.naux);
+    NKX_CUDA(cudaMemcpy(d_asto, astab.data(), sizeof(StoFunc) * P.naux, cudaMemcpyHostToDevice));
+    const size_t NA = P.naux;
+    P.d_L = P.alloc<double>(NA * NA);
+    P.d_y = P.alloc<double>(NA);
+    P.d_c = P.alloc<double>(NA);
+    P.d_info = P.alloc<int>(1);
+    cublasHandle_t hb;
+    NKX_REQUIRE(cublasCreate(&hb) == CUBLAS_STATUS_SUCCESS, NKX_ERR_CUDA, "cublasCreate failed");
+    P.cublas = hb;
+    cublasSetStream(hb, P.stream);
+    // (A|B) = sum_g phi_A(g) Vw_B(g), FP64, in point slices
+    const long slice = std::max<long>(kBatch, std::min<long>(P.npad, (long)((size_t)1 << 28) / (16 * NA)));
+    double *sphi = dalloc<double>(NA * slice), *svw = dalloc<double>(NA * slice);
+    NKX_CUDA(cudaMemsetAsync(P.d_L, 0, sizeof(double) * NA * NA, P.stream));
+    for (long g0 = 0; g0 < P.npad; g0 += slice) {
+      const long np = std::min(slice, P.npad - g0);
+      aux_tables_kernel<<<nblk(NA * np, 128), 128, 0, P.stream>>>(d_asto, P.d_aux, P.naux, P.d_px, P.d_py, P.d_pz,
+                                                                  P.d_w, g0, np, sphi, svw);
+      NKX_LAUNCH_CHECK();
+      const double one = 1.0;
+      NKX_REQUIRE(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, P.naux, P.naux, (int)np, &one, sphi, P.naux, svw, P.naux,
+                              &one, P.d_L, P.naux) == CUBLAS_STATUS_SUCCESS,
+                  NKX_ERR_CUDA, "cublasDgemm failed");
+    }
+    dim3 tb(16, 16), gb(nblk(P.naux, 16), nblk(P.naux, 16));
+    sym_half_kernel<<<gb, tb, 0, P.stream>>>(P.naux, P.d_L);
+    NKX_LAUNCH_CHECK();
+    NKX_CUDA(cudaStreamSynchronize(P.stream));
+    cudaFree(sphi);
+    cudaFree(svw);
+    cudaFree(d_asto);
+    P.h_metric.resize(NA * NA);
+    NKX_CUDA(cudaMemcpy(P.h_metric.data(), P.d_L, sizeof(double) * NA * NA, cudaMemcpyDeviceToHost));
+    cusolverDnHandle_t hs;
+    NKX_REQUIRE(cusolverDnCreate(&hs) == CUSOLVER_STATUS_SUCCESS, NKX_ERR_CUDA, "cusolverDnCreate failed");
+    P.cusolver = hs;
+    cusolverDnSetStream(hs, P.stream);
+    if (opts->metric_svd_thr > 0) {
+      // the reference's preconditioned half inverse: c = X X^T y
+      P.svd_mode = true;
+      P.d_X = P.alloc<double>(NA * NA);
+      P.d_t = P.alloc<double>(NA);
+      int K = 0;
+      NKX_REQUIRE(nkx_half_inverse(P.naux, P.d_L, opts->metric_svd_thr, P.d_X, &K, P.stream) == NKX_OK,
+                  NKX_ERR_NUMERIC, "half inverse of the metric failed");
+      P.K = K;
+      P.metric_min_diag = 0.0;
+    } else {
+      int lwork = 0;
+      cusolverDnDpotrf_bufferSize(hs, CUBLAS_FILL_MODE_LOWER, P.naux, P.d_L, P.naux, &lwork);
+      P.d_work = P.alloc<double>(std::max(1, lwork));
+      P.lwork = lwork;
+      NKX_REQUIRE(cusolverDnDpotrf(hs, CUBLAS_FILL_MODE_LOWER, P.naux, P.d_L, P.naux, P.d_work, lwork, P.d_info) ==
+                      CUSOLVER_STATUS_SUCCESS,
+                  NKX_ERR_CUDA, "cusolverDnDpotrf failed");
+      int info = 0;
+      NKX_CUDA(cudaMemcpyAsync(&info, P.d_info, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
+      NKX_CUDA(cudaStreamSynchronize(P.stream));
+      NKX_REQUIRE(info == 0, NKX_ERR_NUMERIC, "aux metric (A|B) is not positive definite");
+      std::vector<double> hL(NA * NA);
+      NKX_CUDA(cudaMemcpy(hL.data(), P.d_L, sizeof(double) * NA * NA, cudaMemcpyDeviceToHost));
+      double mn = 1e300;
+      for (size_t i = 0; i < NA; ++i) mn = std::min(mn, hL[i + i * NA]);
+      P.metric_min_diag = mn;
+    }
+  }
+  NKX_CUDA(cudaStreamSynchronize(P.stream));
+}
+
+// ========================================================= Fock build ===
+
+void launch_colloc(Plan &P, const Chunk &c, cudaStream_t s) {
+  const long np = c.p1 - c.p0;
+  if (np <= 0) return;
+  if (P.gga)
+    colloc_fp64_kernel<true><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
+                                                          P.d_pair_blk, c.p0, P.ws_phi);
+  else
+    colloc_fp64_kernel<false><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
+                                                           P.d_pair_blk, c.p0, P.ws_phi);
+  NKX_LAUNCH_CHECK();
+  ++P.launches;
+}
+
+void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
+                     StageTimer &T) {
+  const bool multi = P.chunks.size() > 1;
+  const int nzs = nspin + (separateJ ? 1 : 0);
+  // ---- pass A: collocation + density
+  for (const Chunk &c : P.chunks) {
+    const long nb = c.b1 - c.b0;
+    if (c.p1 - c.p0 > 0) {
+      T.begin(ST_COLLOC, s);
+      launch_colloc(P, c, s);
+      T.end(s);
+    }
+    T.begin(ST_DENSITY, s);
+    dim3 grid((unsigned)(nb * 4), nspin);
+    if (P.gga)
+      density_fp64_kernel<true><<<grid, 256, 0, s>>>(P.ws_phi, P.d_Ct, P.d_occ, nocc, P.nbf_pad, P.d_pair_off,
+                                                     P.d_pair_blk, c.b0, c.p0, P.d_rho, P.d_grad, P.npad);
+    else
+      density_fp64_kernel<false><<<grid, 256, 0, s>>>(P.ws_phi, P.d_Ct, P.d_occ, nocc, P.nbf_pad, P.d_pair_off,
+                                                      P.d_pair_blk, c.b0, c.p0, P.d_rho, P.d_grad, P.npad);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+    T.end(s);
+  }
+  // ---- J: fit coefficients and fitted potential
+  if (needJ) {
+    T.begin(ST_COULOMB, s);
+    NKX_CUDA(cudaMemsetAsync(P.d_y, 0, sizeof(double) * P.naux, s));
+    const long nsl = std::max<long>(1, std::min<long>(64, (P.npad + 4095) / 4096));
+    const long slice = (P.npad + nsl - 1) / nsl;
+    aux_y_kernel<<<dim3(P.naux, (unsigned)nsl), 256, 0, s>>>(P.d_aux, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin,
+                                                            P.npad, slice, P.d_y);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+    if (P.svd_mode) {
+      const double one = 1.0, zero = 0.0;
+      cublasHandle_t hb = (cublasHandle_t)P.cublas;
+      cublasSetStream(hb, s);
+      NKX_REQUIRE(cublasDgemv(hb, CUBLAS_OP_T, P.naux, P.K, &one, P.d_X, P.naux, P.d_y, 1, &zero, P.d_t, 1) ==
+                          CUBLAS_STATUS_SUCCESS &&
+                      cublasDgemv(hb, CUBLAS_OP_N, P.naux, P.K, &one, P.d_X, P.naux, P.d_t, 1, &zero, P.d_c, 1) ==
+                          CUBLAS_STATUS_SUCCESS,
+                  NKX_ERR_CUDA, "cublasDgemv failed");
+    } else {
+      NKX_CUDA(cudaMemcpyAsync(P.d_c, P.d_y, sizeof(double) * P.naux, cudaMemcpyDeviceToDevice, s));
+      cusolverDnHandle_t hs = (cusolverDnHandle_t)P.cusolver;
+      cusolverDnSetStream(hs, s);
+      NKX_REQUIRE(cusolverDnDpotrs(hs, CUBLAS_FILL_MODE_LOWER, P.naux, 1, P.d_L, P.naux, P.d_c, P.naux, P.d_info) ==
+                      CUSOLVER_STATUS_SUCCESS,
+                  NKX_ERR_CUDA, "cusolverDnDpotrs failed");
+    }
+    aux_v_kernel<<<nblk(P.npad, 128), 128, 0, s>>>(P.d_aux, P.naux, P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad,
+                                                   P.d_vj);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+    T.end(s);
+  }
+  // ---- functional
+  T.begin(ST_FUNC, s);
+  NKX_CUDA(cudaMemsetAsync(P.d_E, 0, sizeof(double), s));
+  functional_kernel<<<nblk(P.npad, 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.d_w, P.d_rho, P.d_grad,
+                                                      (needJ && fuse) ? P.d_vj : nullptr, P.d_coef, P.d_E);
+  NKX_LAUNCH_CHECK();
+  ++P.launches;
+  T.end(s);
+  // ---- pass B: Z and the V contraction
+  const size_t tile = (size_t)kBatch * kBlockF;
+  NKX_CUDA(cudaMemsetAsync(P.d_V, 0, sizeof(double) * nzs * P.nbf_pad * P.nbf_pad, s));
+  for (const Chunk &c : P.chunks) {
+    const long np = c.p1 - c.p0;
+    if (np <= 0) continue;
+    if (multi) {
+      T.begin(ST_COLLOC, s);
+      launch_colloc(P, c, s);
+      T.end(s);
+    }
+    T.begin(ST_ZBUILD, s);
+    if (P.gga)
+      zbuild_fp64_kernel<true><<<(unsigned)np, 256, 0, s>>>(P.ws_phi, P.d_coef, P.d_vj, P.d_pair_batch, c.p0, nzs,
+                                                            nspin, P.npad, P.ws_z);
+    else
+      zbuild_fp64_kernel<false><<<(unsigned)np, 256, 0, s>>>(P.ws_phi, P.d_coef, P.d_vj, P.d_pair_batch, c.p0, nzs,
+                                                             nspin, P.npad, P.ws_z);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+    T.end(s);
+    T.begin(ST_VGEMM, s);
+    vgemm_fp64_kernel<<<dim3(P.nblk, P.nblk, nzs), 256, 0, s>>>(P.ws_phi, P.ws_z, P.gga ? 4 : 1, nzs, P.d_pair_off,
+                                                                P.d_mask, P.mask_words, c.b0, c.b1, c.p0, P.nbf_pad,
+                                                                P.d_V);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+    T.end(s);
+  }
+  (void)tile;
+}
+
+void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, const double *occ, int mem, int fuse_j,
+                double *E, double *V, double *J, cudaStream_t user) {
+  NKX_REQUIRE(nspin == 1 || nspin == 2, NKX_ERR_ARG, "nspin must be 1 or 2");
+  NKX_REQUIRE(nocc > 0 && C && occ && E && (V || (fuse_j && J)), NKX_ERR_ARG, "invalid arguments");
+  NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
+  NKX_REQUIRE(precision == NKX_PREC_FP64 || precision == NKX_PREC_MIXED, NKX_ERR_ARG, "unknown precision");
+  const bool needJ = P.naux > 0 && (J != nullptr || fuse_j);
+  NKX_REQUIRE(!(fuse_j && P.naux == 0), NKX_ERR_ARG, "fuse_j needs a plan with an aux basis");
+  NKX_REQUIRE(V != nullptr, NKX_ERR_ARG, "V must be given");
+  const bool separateJ = needJ && !fuse_j && J;
+  cudaStream_t s = user ? user : P.stream;
+  P.launches = 0;
+  StageTimer T;
+  cudaEvent_t t0, t1;
+  NKX_CUDA(cudaEventCreate(&t0));
+  NKX_CUDA(cudaEventCreate(&t1));
+  NKX_CUDA(cudaEventRecord(t0, s));
+
+  // orbitals -> Ct[spin][i][f_pad]
+  if (nocc > P.nocc_cap) {
+    P.nocc_cap = nocc;
+    P.d_Ct = P.alloc<double>((size_t)2 * nocc * P.nbf_pad);
+    P.d_occ = P.alloc<double>((size_t)2 * nocc);
+    P.d_Cin = P.alloc<double>((size_t)2 * nocc * P.nbf);
+  }
+  const double *Cd = C;
+  if (mem == NKX_MEM_HOST) {
+    NKX_CUDA(cudaMemcpyAsync(P.d_Cin, C, sizeof(double) * nspin * nocc * P.nbf, cudaMemcpyHostToDevice, s));
+    NKX_CUDA(cudaMemcpyAsync(P.d_occ, occ, sizeof(double) * nspin * nocc, cudaMemcpyHostToDevice, s));
+    Cd = P.d_Cin;
+  } else {
+    NKX_CUDA(cudaMemcpyAsync(P.d_occ, occ, sizeof(double) * nspin * nocc, cudaMemcpyDeviceToDevice, s));
+  }
+  pack_orbitals_kernel<<<nblk((long)nspin * nocc * P.nbf_pad, 256), 256, 0, s>>>(Cd, P.nbf, nocc, nspin, P.nbf_pad,
+                                                                                  P.d_Ct);
+  NKX_LAUNCH_CHECK();
+  ++P.launches;
+
+  if (precision == NKX_PREC_MIXED && mixed_available(P))
+    fock_build_mixed(P, nspin, nocc, needJ, fuse_j != 0, separateJ, s, T);
+  else {
+    NKX_REQUIRE(precision == NKX_PREC_FP64, NKX_ERR_UNSUPPORTED, "mixed precision path unavailable");
+    fock_build_fp64(P, nspin, nocc, needJ, fuse_j != 0, separateJ, s, T);
+  }
+
+  // symmetrise + unpad into the output (device) or a staging buffer (host)
+  const size_t nn = (size_t)P.nbf * P.nbf;
+  const int nout = nspin + (separateJ ? 1 : 0);
+  double *dst = nullptr;
+  if (mem == NKX_MEM_DEVICE) {
+    dst = V;
+  } else {
+    if (!P.d_out) P.d_out = P.alloc<double>(3 * nn);
+    dst = P.d_out;
+  }
+  dim3 tb(16, 16), gb(nblk(P.nbf, 16), nblk(P.nbf, 16));
+  for (int z = 0; z < nout; ++z) {
+    double *o = (z < nspin) ? dst + z * nn : (mem == NKX_MEM_DEVICE ? J : dst + nspin * nn);
+    symmetrize_unpad_kernel<<<gb, tb, 0, s>>>(P.nbf, P.nbf_pad, P.d_V + (size_t)z * P.nbf_pad * P.nbf_pad, o);
+    ++P.launches;
+  }
+  NKX_LAUNCH_CHECK();
+  if (mem == NKX_MEM_HOST) {
+    NKX_CUDA(cudaMemcpyAsync(V, dst, sizeof(double) * nspin * nn, cudaMemcpyDeviceToHost, s));
+    if (separateJ) NKX_CUDA(cudaMemcpyAsync(J, dst + nspin * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
+  }
+  NKX_CUDA(cudaMemcpyAsync(E, P.d_E, sizeof(double), cudaMemcpyDeviceToHost, s));
+  NKX_CUDA(cudaEventRecord(t1, s));
+  NKX_CUDA(cudaStreamSynchronize(s));
+  float st[6];
+  T.collect(st);
+  P.last.colloc_ms = st[ST_COLLOC];
+  P.last.density_ms = st[ST_DENSITY];
+  P.last.functional_ms = st[ST_FUNC];
+  P.last.coulomb_ms = st[ST_COULOMB];
+  P.last.zbuild_ms = st[ST_ZBUILD];
+  P.last.vgemm_ms = st[ST_VGEMM];
+  cudaEventElapsedTime(&P.last.total_ms, t0, t1);
+  P.last.launches = P.launches;
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  P.last_nspin = nspin;
+}
+
+}  // namespace nkx
+
+using namespace nkx;
+
+extern "C" {
+
+NKX_API const char *nkx_last_error(void) { return g_last_error.c_str(); }
+
+NKX_API nkx_status nkx_plan_create(const nkx_molecule *mol, const nkx_basis *prim, const nkx_basis *aux, long npoints,
+                                   const double *xyz, const double *w, const int *owner, const nkx_plan_options *opts,
+                                   nkx_plan **plan) {
+  (void)owner;
+  return run_guarded("nkx_plan_create", [&] {
+    NKX_REQUIRE(plan, NKX_ERR_ARG, "plan pointer is NULL");
+    *plan = nullptr;
+    auto P = std::make_unique<Plan>();
+    build_plan(*P, mol, prim, aux, npoints, xyz, w, opts);
+    *plan = reinterpret_cast<nkx_plan *>(P.release());
+  });
+}
+
+NKX_API nkx_status nkx_plan_get_info(const nkx_plan *plan, nkx_plan_info *info) {
+  return run_guarded("nkx_plan_get_info", [&] {
+    NKX_REQUIRE(plan && info, NKX_ERR_ARG, "invalid arguments");
+    const Plan &P = *reinterpret_cast<const Plan *>(plan);
+    info->npoints = P.npts;
+    info->nbatches = P.nbatch;
+    info->nbf = P.nbf;
+    info->naux = P.naux;
+    info->nblocks = P.nblk;
+    info->npairs = P.npairs;
+    info->nchunks = (int)P.chunks.size();
+    info->metric_min_diag = P.metric_min_diag;
+  });
+}
+
+NKX_API nkx_status nkx_fock_build(nkx_plan *plan, int precision, int nspin, int nocc, const double *C,
+                                  const double *occ, int mem, int fuse_j, double *E, double *V, double *J,
+                                  void *stream) {
+  return run_guarded("nkx_fock_build", [&] {
+    NKX_REQUIRE(plan, NKX_ERR_ARG, "plan is NULL");
+    Plan &P = *reinterpret_cast<Plan *>(plan);
+    fock_build(P, precision, nspin, nocc, C, occ, mem, fuse_j, E, V, J, (cudaStream_t)stream);
+  });
+}
+
+NKX_API nkx_status nkx_get_last_timing(const nkx_plan *plan, nkx_build_timing *t) {
+  return run_guarded("nkx_get_last_timing", [&] {
+    NKX_REQUIRE(plan && t, NKX_ERR_ARG, "invalid arguments");
+    *t = reinterpret_cast<const Plan *>(plan)->last;
+  });
+}
+
+NKX_API nkx_status nkx_plan_last_density(const nkx_plan *plan, double *rho, long *perm) {
+  return run_guarded("nkx_plan_last_density", [&] {
+    NKX_REQUIRE(plan, NKX_ERR_ARG, "plan is NULL");
+    const Plan &P = *reinterpret_cast<const Plan *>(plan);
+    if (rho) {
+      std::vector<double> h(2 * P.npad);
+      NKX_CUDA(cudaMemcpy(h.data(), P.d_rho, sizeof(double) * 2 * P.npad, cudaMemcpyDeviceToHost));
+      const int ns = std::max(1, P.last_nspin);
+      for (long p = 0; p < P.npts; ++p)
+        for (int s = 0; s < ns; ++s) rho[p * ns + s] = h[(size_t)s * P.npad + p];
+    }
+    if (perm)
+      for (long p = 0; p < P.npts; ++p) perm[p] = P.perm[p];
+  });
+}
+
+NKX_API nkx_status nkx_plan_batch_blocks(const nkx_plan *plan, int *counts) {
+  return run_guarded("nkx_plan_batch_blocks", [&] {
+    NKX_REQUIRE(plan && counts, NKX_ERR_ARG, "invalid arguments");
+    const Plan &P = *reinterpret_cast<const Plan *>(plan);
+    for (long b = 0; b < P.nbatch; ++b) counts[b] = P.h_pair_off[b + 1] - P.h_pair_off[b];
+  });
+}
+
+NKX_API nkx_status nkx_plan_destroy(nkx_plan *plan) {
+  return run_guarded("nkx_plan_destroy", [&] { delete reinterpret_cast<Plan *>(plan); });
+}
+
+}  // extern "C"

@@ -1,0 +1,116 @@
+// The plan object behind nkx_plan (internal).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "functionals.cuh"
+#include "potential.cuh"
+
+namespace nkx {
+
+struct Chunk {
+  long b0 = 0, b1 = 0;  // batch range
+  long p0 = 0, p1 = 0;  // (batch, block) pair range
+};
+
+struct Plan {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  std::vector<void *> allocs;
+  void *cublas = nullptr, *cusolver = nullptr;
+
+  XcSpec xc{};
+  bool gga = false;
+
+  int nbf = 0, nbf_pad = 0, nblk = 0, mask_words = 0, naux = 0;
+  long npts = 0, nbatch = 0, npad = 0, npairs = 0;
+  std::vector<long> perm;  // plan point p <- caller point perm[p]
+
+  // grid (Morton order, padded to nbatch * 256; padded points have w = 0)
+  double *d_px = nullptr, *d_py = nullptr, *d_pz = nullptr, *d_w = nullptr;
+  StoFunc *d_sto = nullptr;
+  AuxFunc *d_aux = nullptr;
+
+  // screening: pairs of (batch, significant function block), CSR by batch
+  std::vector<int> h_pair_off;
+  std::vector<uint32_t> h_mask;
+  int *d_pair_off = nullptr, *d_pair_blk = nullptr, *d_pair_batch = nullptr;
+  uint32_t *d_mask = nullptr;
+
+  std::vector<Chunk> chunks;
+  long max_chunk_pairs = 0;
+  double *ws_phi = nullptr;  // PhiT tiles of a chunk: [pair][comp][g][f]
+  double *ws_z = nullptr;    // Z^T tiles of a chunk:  [pair][z][g][f]
+
+  // per point (two spins)
+  double *d_rho = nullptr, *d_grad = nullptr, *d_coef = nullptr, *d_vj = nullptr;
+  // orbitals
+  int nocc_cap = 0;
+  double *d_Ct = nullptr, *d_occ = nullptr, *d_Cin = nullptr;
+  // accumulators / outputs
+  double *d_V = nullptr, *d_E = nullptr, *d_out = nullptr;
+
+  // Coulomb metric
+  bool svd_mode = false;
+  int K = 0, lwork = 0;
+  double *d_L = nullptr, *d_X = nullptr, *d_t = nullptr, *d_y = nullptr, *d_c = nullptr, *d_work = nullptr;
+  int *d_info = nullptr;
+  double metric_min_diag = 0.0;
+  std::vector<double> h_metric;
+
+  // mixed-precision workspaces (tensor-core path)
+  float *mx_phi = nullptr, *mx_a = nullptr, *mx_b = nullptr, *mx_c = nullptr;
+  void *mx_state = nullptr;
+
+  nkx_build_timing last{};
+  int launches = 0;
+  int last_nspin = 1;
+
+  ~Plan();
+  template <class T>
+  T *alloc(size_t n);
+};
+
+// Accumulates CUDA-event time per build stage.
+struct StageTimer {
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  cudaEvent_t begin_ev = nullptr;
+  int cur = -1;
+  ~StageTimer() {
+    for (auto &m : marks) {
+      cudaEventDestroy(m.second.first);
+      cudaEventDestroy(m.second.second);
+    }
+  }
+  void begin(int stage, cudaStream_t s) {
+    cudaEvent_t e;
+    NKX_CUDA(cudaEventCreate(&e));
+    NKX_CUDA(cudaEventRecord(e, s));
+    begin_ev = e;
+    cur = stage;
+  }
+  void end(cudaStream_t s) {
+    cudaEvent_t e;
+    NKX_CUDA(cudaEventCreate(&e));
+    NKX_CUDA(cudaEventRecord(e, s));
+    marks.push_back({cur, {begin_ev, e}});
+  }
+  void collect(float out[6]) {
+    for (int i = 0; i < 6; ++i) out[i] = 0.f;
+    for (auto &m : marks) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, m.second.first, m.second.second);
+      out[m.first] += ms;
+    }
+  }
+};
+
+enum { ST_COLLOC = 0, ST_DENSITY = 1, ST_FUNC = 2, ST_COULOMB = 3, ST_ZBUILD = 4, ST_VGEMM = 5 };
+
+bool mixed_available(const Plan &P);
+void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
+                      StageTimer &T);
+
+}  // namespace nkx

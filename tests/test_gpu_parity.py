@@ -1,0 +1,216 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle and with
+the reference's golden values.  FP64 tolerances are written per test."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+from nukexc_b200 import api as A  # noqa: E402
+from nukexc_b200 import molecules as M  # noqa: E402
+
+
+def basis_pair(funcs):
+    return A.make_manual_basis(funcs), O.make_manual_basis(funcs)
+
+
+def h1s():
+    return basis_pair([(1, 0, 0, 1.0, 0, 0, 0)])
+
+
+# ------------------------------------------------------------- golden ----
+def test_golden_lda_x_h1s_plan():
+    # tests/test_hydrogen.cxx:815-857 through the batched plan (FP64)
+    g = A.make_flat_grid([[0, 0, 0]], [1], 100, 20, radial="becke")
+    b, _ = h1s()
+    fb = A.FockBuilder([[0, 0, 0]], [1], b, g, func_ids=("LDA_X",))
+    E, V, _ = fb.build([np.ones((1, 1))], [np.ones(1)])
+    assert E == pytest.approx(-0.2127415030860106, rel=1e-10)
+
+
+def test_golden_pbe_x_h1s_dense_and_plan():
+    # tests/test_hydrogen.cxx:859-912
+    g = A.make_flat_grid([[0, 0, 0]], [1], 100, 20, radial="becke")
+    b, _ = h1s()
+    phi, gx, gy, gz = A.fill_grad_collocation(b, g.quad_points)
+    E, V = A.compute_gga(phi, gx, gy, gz, g.weights, np.ones((1, 1)), np.ones(1), ("GGA_X_PBE",))
+    assert E == pytest.approx(-0.253995708307881, rel=1e-10)
+    assert V[0, 0].item() == pytest.approx(-0.320733669386709, rel=1e-10)
+    fb = A.FockBuilder([[0, 0, 0]], [1], b, g, func_ids=("GGA_X_PBE",))
+    E2, V2, _ = fb.build([np.ones((1, 1))], [np.ones(1)])
+    assert E2 == pytest.approx(-0.253995708307881, rel=1e-10)
+    assert V2[0][0, 0] == pytest.approx(-0.320733669386709, rel=1e-10)
+
+
+def test_golden_pbe_x_he1s():
+    # tests/test_helium.cxx:67-119 (Becke 2000 radial; spherical integrand)
+    g = A.make_flat_grid([[0, 0, 0]], [2], 2000, 41, radial="becke")
+    b = A.make_manual_basis([(1, 0, 0, 1.6875, 0, 0, 0)])
+    fb = A.FockBuilder([[0, 0, 0]], [2], b, g, func_ids=("GGA_X_PBE",))
+    E, V, _ = fb.build([np.ones((1, 1))], [2 * np.ones(1)])
+    assert E == pytest.approx(-1.032549417787429, rel=1e-10)
+    assert V[0][0, 0] == pytest.approx(-0.657943275538615, rel=1e-10)
+
+
+@pytest.mark.parametrize("svd", [0.0, 1e-4])
+def test_golden_coulomb_h1s(svd):
+    # tests/test_hydrogen.cxx:562-631: J_00 = 5/8 (Cholesky, and the
+    # reference's half-inverse with threshold 1e-4)
+    g = A.make_flat_grid([[0, 0, 0]], [1], 100, 20, radial="becke")
+    b, _ = h1s()
+    aux = A.make_manual_basis([(1, 0, 0, z, 0, 0, 0) for z in (0.5, 1.0, 2.0, 3.0, 4.0)])
+    fb = A.FockBuilder([[0, 0, 0]], [1], b, g, aux=aux, func_ids=("LDA_X",), metric_svd_thr=svd)
+    E, V, J = fb.build([np.ones((1, 1))], [np.ones(1)], want_J=True)
+    assert J[0, 0] == pytest.approx(5 / 8, rel=1e-10)
+
+
+def test_golden_density_sigma():
+    # tests/test_density.cxx:252-307
+    g = A.make_flat_grid([[0, 0, 0]], [1], 200, 20, radial="becke")
+    b, _ = h1s()
+    phi, gx, gy, gz = A.fill_grad_collocation(b, g.quad_points)
+    rho, grad, sig = A.compute_density_and_sigma(phi, gx, gy, gz, np.ones((1, 1)), np.ones(1))
+    w = torch.as_tensor(g.weights, device="cuda")
+    assert (rho * w).sum().item() == pytest.approx(1.0, rel=1e-10)
+    assert (sig * w).sum().item() == pytest.approx(1 / (2 * math.pi), rel=1e-10)
+
+
+# ------------------------------------------------------- kernel parity ----
+def test_becke_grid_matches_oracle():
+    c, Z = M.water()
+    g = A.make_flat_grid(c, Z, 40, 17, weight_threshold=1e-15, radial="ta")
+    pts, w, own = O.make_flat_grid(c, Z, 40, 17, 1e-15, scheme="ta")
+    assert g.quad_points.shape == pts.shape
+    assert np.array_equal(g.point_owner, own)
+    np.testing.assert_allclose(g.quad_points, pts, rtol=0, atol=1e-13)
+    # tiny weights come from 1/2 (1 - p) near p = 1, where rounding of the
+    # fused multiply-adds differs between CPU and GPU: absolute tolerance
+    np.testing.assert_allclose(g.weights, w, rtol=1e-12, atol=1e-13)
+
+
+def test_becke_unclamped_one_half():
+    # tests/test_partition.cxx:140-195 on the device
+    centers = np.array([[-1.0, 0, 0], [1.0, 0, 0]])
+    pts = np.array([[0, j / 10, k / 10] for i in range(2) for j in range(10) for k in range(10)], float)
+    owner = np.repeat([0, 1], 100)
+    w = A.partition_becke(centers, pts, owner, np.ones(200)).cpu().numpy()
+    assert np.abs(w - 0.5).max() < 1e-15
+
+
+def test_becke_screening_exact_on_cluster():
+    # clamped Becke with the exact r_min + 2 Rc screening vs the full loop
+    c, Z = M.water_cluster(8, seed=3)
+    rng = np.random.default_rng(0)
+    owner = rng.integers(0, len(Z), 4000)
+    pts = c[owner] + rng.normal(scale=2.0, size=(4000, 3))
+    w0 = np.ones(4000)
+    wd = A.partition_becke_team(c, pts, owner, w0).cpu().numpy()
+    wo = O.becke(c, pts, owner, w0)
+    np.testing.assert_allclose(wd, wo, rtol=1e-12, atol=1e-14)
+
+
+def test_collocation_matches_oracle():
+    funcs = [(l + 1 + k, l, m, 0.7 + 0.9 * k, 0.1 * l, -0.2, 0.3 * k)
+             for l in range(0, 5) for m in range(-l, l + 1) for k in range(2)]
+    b, ob = basis_pair(funcs)
+    pts = np.random.default_rng(1).normal(scale=1.5, size=(500, 3))
+    d = [x.cpu().numpy() for x in A.fill_grad_collocation(b, pts)]
+    o = O.collocation(ob, pts, grad=True)
+    for x, y in zip(d, o):
+        np.testing.assert_allclose(x, y, rtol=1e-12, atol=1e-14 * np.abs(y).max())
+
+
+@pytest.mark.parametrize("fid", [1, 7, 101, 130])
+@pytest.mark.parametrize("nspin", [1, 2])
+def test_functionals_match_oracle(fid, nspin):
+    rng = np.random.default_rng(fid + nspin)
+    n = 2000
+    rho = 10 ** rng.uniform(-12, 2, size=n * nspin)
+    sig = 10 ** rng.uniform(-14, 3, size=n * (1 if nspin == 1 else 3))
+    if nspin == 2:
+        s = sig.reshape(n, 3)
+        s[:, 1] = rng.uniform(-1, 1, size=n) * np.sqrt(s[:, 0] * s[:, 2])
+    de, dv, ds = A.xc_eval(fid, nspin, rho, sig)
+    oe, ov, os_ = O.xc_eval(fid, nspin, rho, sig)
+    np.testing.assert_allclose(de.cpu().numpy(), oe, rtol=1e-11, atol=1e-300)
+    np.testing.assert_allclose(dv.cpu().numpy(), ov, rtol=1e-9, atol=1e-14)
+    np.testing.assert_allclose(ds.cpu().numpy(), os_, rtol=1e-9, atol=1e-14 * np.abs(os_).max())
+
+
+# --------------------------------------------------------- plan parity ----
+def water_case(n=1, seed=0, nrad=40, order=17):
+    c, Z = (M.water() if n == 1 else M.water_cluster(n, seed))
+    funcs = M.sto_basis(c, Z)
+    g = A.make_flat_grid(c, Z, nrad, order, weight_threshold=1e-15, radial="ta")
+    return c, Z, funcs, g
+
+
+@pytest.mark.parametrize("funcs_xc", [("LDA_X", "LDA_C_VWN"), ("GGA_X_PBE", "GGA_C_PBE")])
+def test_plan_xc_fp64_matches_oracle_water(funcs_xc):
+    c, Z, funcs, g = water_case()
+    b, ob = basis_pair(funcs)
+    nbf = len(funcs)
+    Cm = M.random_orbitals(nbf, 5, seed=4)
+    occ = np.ones(5)
+    fb = A.FockBuilder(c, Z, b, g, func_ids=funcs_xc)
+    E, V, _ = fb.build([Cm], [occ])
+    ids = [A._FUNC_NAMES[f] for f in funcs_xc]
+    Eo, Vo = O.xc_build(ob, g.quad_points, g.weights, ids, [Cm], [occ])
+    assert abs(E - Eo) < 1e-10 * abs(Eo)
+    assert np.abs(V[0] - Vo[0]).max() < 1e-10 * max(1.0, np.abs(Vo).max())
+
+
+def test_plan_xc_fp64_polarized_and_device_buffers():
+    c, Z, funcs, g = water_case(2, seed=1, nrad=30, order=11)
+    b, ob = basis_pair(funcs)
+    nbf = len(funcs)
+    Ca = M.random_orbitals(nbf, 6, seed=5)
+    Cb = M.random_orbitals(nbf, 4, seed=6)
+    occ = [np.ones(6), np.ones(6)]
+    Cb6 = np.concatenate([Cb, np.zeros((nbf, 2))], 1)
+    fb = A.FockBuilder(c, Z, b, g, func_ids=("GGA_X_PBE", "GGA_C_PBE"))
+    E, V, _ = fb.build([torch.as_tensor(Ca, device="cuda"), torch.as_tensor(Cb6, device="cuda")],
+                       [torch.as_tensor(o, device="cuda") for o in occ])
+    Eo, Vo = O.xc_build(ob, g.quad_points, g.weights, [101, 130], [Ca, Cb6], occ)
+    assert abs(E - Eo) < 1e-10 * abs(Eo)
+    for s in range(2):
+        assert np.abs(V[s].cpu().numpy() - Vo[s]).max() < 1e-10 * max(1.0, np.abs(Vo).max())
+
+
+def test_plan_chunked_equals_single_chunk():
+    # a tiny workspace forces many chunks (two-pass collocation)
+    c, Z, funcs, g = water_case(2, seed=2, nrad=30, order=11)
+    b, _ = basis_pair(funcs)
+    Cm = M.random_orbitals(len(funcs), 10, seed=7)
+    f1 = A.FockBuilder(c, Z, b, g)
+    f2 = A.FockBuilder(c, Z, b, g, workspace_bytes=3 << 20)
+    assert f2.info()["nchunks"] > 3
+    E1, V1, _ = f1.build([Cm], [np.ones(10)])
+    E2, V2, _ = f2.build([Cm], [np.ones(10)])
+    assert abs(E1 - E2) < 1e-12 * abs(E1)
+    assert np.abs(V1[0] - V2[0]).max() < 1e-12
+
+
+def test_plan_coulomb_matches_oracle():
+    c, Z, funcs, g = water_case(1, nrad=30, order=11)
+    b, ob = basis_pair(funcs)
+    afuncs = M.aux_basis(c, Z)
+    aux, oaux = basis_pair(afuncs)
+    Cm = M.random_orbitals(len(funcs), 5, seed=8)
+    occ = np.ones(5)
+    fb = A.FockBuilder(c, Z, b, g, aux=aux, func_ids=("LDA_X",))
+    E, V, J = fb.build([Cm], [occ], want_J=True)
+    S = O.aux_metric(oaux, g.quad_points, g.weights)
+    Jo, _ = O.coulomb(ob, oaux, g.quad_points, g.weights, Cm, occ, S=S)
+    assert np.abs(J - Jo).max() < 1e-8 * np.abs(Jo).max()
+    # fused J folds into the XC contraction: V_fused = V_xc + J
+    Ef, Vf, _ = fb.build([Cm], [occ], fuse_j=True)
+    assert abs(Ef - E) < 1e-12 * abs(E)
+    assert np.abs(Vf[0] - (V[0] + J)).max() < 1e-10 * np.abs(Jo).max()
