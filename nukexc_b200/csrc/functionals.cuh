@@ -131,6 +131,10 @@ NKX_HD inline Dual<N> dexp(const Dual<N> &a) {
   return chain(a, v, v);
 }
 template <int N>
+NKX_HD inline Dual<N> dexpm1(const Dual<N> &a) {
+  return chain(a, expm1(a.v), exp(a.v));
+}
+template <int N>
 NKX_HD inline Dual<N> dlog(const Dual<N> &a) {
   return chain(a, log(a.v), 1.0 / a.v);
 }
@@ -228,7 +232,7 @@ NKX_HD inline T f_pbe_c(const T &ra, const T &rb, const T &sigma) {
   const T ks2 = 4.0 * kF / kPi;
   const T t2 = sigma / (4.0 * phi * phi * ks2 * rho * rho);
   const T phi3 = phi * phi * phi;
-  const T A = (beta / gamma) / (dexp(-ec / (gamma * phi3)) - 1.0);
+  const T A = (beta / gamma) / dexpm1(-ec / (gamma * phi3));
   const T At2 = A * t2;
   const T H = gamma * phi3 * dlog(1.0 + (beta / gamma) * t2 * (1.0 + At2) / (1.0 + At2 + At2 * At2));
   return rho * (ec + H);

@@ -146,6 +146,12 @@ using cplx = std::complex<double>;
 
 cplx cbrt_c(cplx x) { return std::pow(x, 1.0 / 3.0); }
 
+// exp(z) - 1 without cancellation for the complex-step argument a + i b
+cplx expm1_c(cplx z) {
+  const double a = z.real(), b = z.imag();
+  return cplx(std::expm1(a) * std::cos(b) - 2.0 * std::sin(0.5 * b) * std::sin(0.5 * b), std::exp(a) * std::sin(b));
+}
+
 // spin-polarised Slater exchange per volume
 cplx f_lda_x(cplx ra, cplx rb) {
   const double c = -0.75 * std::cbrt(6.0 / kPi);
@@ -223,7 +229,7 @@ cplx f_pbe_c(cplx ra, cplx rb, cplx sigma) {
   const cplx ks = std::sqrt(4.0 * kF / kPi);
   const cplx t2 = sigma / (4.0 * phi * phi * ks * ks * rho * rho);
   const cplx phi3 = phi * phi * phi;
-  const cplx A = beta / gamma / (std::exp(-ec / (gamma * phi3)) - 1.0);
+  const cplx A = beta / gamma / expm1_c(-ec / (gamma * phi3));
   const cplx At2 = A * t2;
   const cplx H = gamma * phi3 * std::log(1.0 + beta / gamma * t2 * (1.0 + At2) / (1.0 + At2 + At2 * At2));
   return rho * (ec + H);
