@@ -166,6 +166,24 @@ NKX_API nkx_status nkx_xc_dense(int nbf, long npts, const double *d_phi, const d
                                 int nocc, const double *d_C, const double *d_occ, const nkx_plan_options *opts,
                                 double *E, double *d_V, void *stream);
 
+/* The dense XC build of nkx_xc_dense for callers that cannot allocate device
+ * memory (for example while a CUDA graph is being captured, or under a fixed
+ * memory budget handed over at start-up).  No counterpart in the reference.
+ * Same arguments and results as nkx_xc_dense; it calls no cudaMalloc/cudaFree
+ * and no allocating library routine.  Its scratch is one fixed array of
+ * NKX_NOALLOC_SCRATCH_DOUBLES doubles (32 MiB) in the library's device
+ * memory, held by every GPU that loads the library until exit; problems with
+ * 32 + pad(nspin*npts) + pad(3*nspin*npts) + pad(nspin*nbf*npts) > that
+ * (pad = round up to 32) are rejected with NKX_ERR_ARG.  The first call on a
+ * device looks up the array's address (cudaGetSymbolAddress) and should come
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller. */
+#define NKX_NOALLOC_SCRATCH_DOUBLES (4u << 20)
+NKX_API nkx_status nkx_xc_dense_noalloc(int nbf, long npts, const double *d_phi, const double *d_gx,
+                                        const double *d_gy, const double *d_gz, const double *d_w, int nspin,
+                                        int nocc, const double *d_C, const double *d_occ,
+                                        const nkx_plan_options *opts, double *E, double *d_V, void *stream);
+
 /* Functional evaluation with libxc's array layouts (xc_lda_exc_vxc /
  * xc_gga_exc_vxc, the host calls of nukexc/xc_integrals.hpp:113-617), on the
  * device: nspin 1: rho[n], sigma[n]; nspin 2: rho[2n], sigma[3n]

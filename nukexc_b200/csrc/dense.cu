@@ -387,3 +387,85 @@ extern "C" nkx_status nkx_half_inverse(int N, const double *d_S, double thr, dou
     *K = k;
   });
 }
+
+// ---------------------------------------------------------------------------
+// nkx_xc_dense_noalloc: the dense XC build for callers that cannot allocate
+// device memory -- code running while a CUDA graph is being captured, a host
+// that hands the library a fixed memory budget up front, or a process whose
+// allocator must not see cudaMalloc/cudaFree after start-up.  The scratch
+// (per-point density and gradient, the Z matrix, the energy accumulator)
+// lives in one file-scope __device__ array of kNoAllocScratchDoubles doubles
+// (32 MiB) that every GPU loading the library keeps until process exit.
+// Its device address is looked up once per device with
+// cudaGetSymbolAddress on the first call made with that device current; that
+// first call should therefore happen before any stream capture.  All calls
+// share the array: calls whose work overlaps on the GPU (different streams,
+// or host threads) race on it and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace nkx {
+
+constexpr size_t kNoAllocScratchDoubles = (size_t)4 << 20;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+static double *noalloc_scratch_address() {
+  static std::mutex mu;
+  static double *addr[128] = {nullptr};
+  int dev = 0;
+  NKX_CUDA(cudaGetDevice(&dev));
+  NKX_REQUIRE(dev >= 0 && dev < 128, NKX_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void *p = nullptr;
+    NKX_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    addr[dev] = static_cast<double *>(p);
+  }
+  return addr[dev];
+}
+
+}  // namespace nkx
+
+extern "C" nkx_status nkx_xc_dense_noalloc(int nbf, long npts, const double *d_phi, const double *d_gx,
+                                           const double *d_gy, const double *d_gz, const double *d_w, int nspin,
+                                           int nocc, const double *d_C, const double *d_occ,
+                                           const nkx_plan_options *opts, double *E, double *d_V, void *stream) {
+  return run_guarded("nkx_xc_dense_noalloc", [&] {
+    NKX_REQUIRE(nbf > 0 && npts > 0 && (nspin == 1 || nspin == 2) && nocc > 0 && d_phi && d_w && d_C && d_occ &&
+                    E && d_V,
+                NKX_ERR_ARG, "invalid arguments");
+    const XcSpec sp = make_spec(opts);
+    const bool gga = spec_is_gga(sp);
+    NKX_REQUIRE(!gga || (d_gx && d_gy && d_gz), NKX_ERR_ARG, "GGA needs collocation gradients");
+    // layout in doubles, each piece 256-byte aligned: E | rho | grad | Z
+    auto up = [](size_t n) { return (n + 31) & ~(size_t)31; };
+    const size_t nE = 32, nrho = up((size_t)nspin * npts), ngrad = up((size_t)nspin * 3 * npts);
+    const size_t nZ = up((size_t)nspin * nbf * npts);
+    const size_t need = nE + nrho + ngrad + nZ;
+    NKX_REQUIRE(need <= kNoAllocScratchDoubles, NKX_ERR_ARG,
+                "problem too large for the fixed 32 MiB scratch: needs nspin*npts*(nbf+4) doubles <= 4194304 (" +
+                    std::to_string(need) + " requested)");
+    double *base = noalloc_scratch_address();
+    double *Ed = base, *rho = base + nE, *grad = rho + nrho, *Z = grad + ngrad;
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int sp_i = 0; sp_i < nspin; ++sp_i)
+      density_dense_kernel<<<nblk(npts * 32, 256), 256, 0, s>>>(
+          nbf, npts, d_phi, gga ? d_gx : nullptr, d_gy, d_gz, nocc, d_C + (size_t)sp_i * nbf * nocc,
+          d_occ + (size_t)sp_i * nocc, rho + (size_t)sp_i * npts, gga ? grad + (size_t)sp_i * 3 * npts : nullptr,
+          nullptr);
+    NKX_LAUNCH_CHECK();
+    NKX_CUDA(cudaMemsetAsync(Ed, 0, sizeof(double), s));  // the array keeps the previous call's sum
+    xc_z_dense_kernel<<<nblk(npts, 128), 128, 0, s>>>(sp, gga, nbf, npts, nspin, d_phi, d_gx, d_gy, d_gz, d_w,
+                                                     rho, grad, Z, Ed);
+    NKX_LAUNCH_CHECK();
+    dim3 tb(16, 16), gb(nblk(nbf, 16), nblk(nbf, 16));
+    for (int sp_i = 0; sp_i < nspin; ++sp_i) {
+      double *Vs = d_V + (size_t)sp_i * nbf * nbf;
+      nt_gemm_dense_kernel<<<gb, tb, 0, s>>>(nbf, npts, d_phi, Z + (size_t)sp_i * nbf * npts, Vs);
+      symmetrize_kernel<<<gb, tb, 0, s>>>(nbf, Vs);
+    }
+    NKX_LAUNCH_CHECK();
+    NKX_CUDA(cudaMemcpyAsync(E, Ed, sizeof(double), cudaMemcpyDeviceToHost, s));
+    NKX_CUDA(cudaStreamSynchronize(s));
+  });
+}
