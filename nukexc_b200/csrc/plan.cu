@@ -472,6 +472,15 @@ __global__ void aux_tables_kernel(const StoFunc *__restrict__ sto, const AuxFunc
   vw[e] = aux_potential(aux[a], px[g], py[g], pz[g]) * w[g];
 }
 
+__global__ void gather_kernel(int K, const int *__restrict__ piv, const double *__restrict__ y, double *__restrict__ t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < K) t[i] = y[piv[i]];
+}
+__global__ void scatter_kernel(int K, const int *__restrict__ piv, const double *__restrict__ t, double *__restrict__ c) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < K) c[piv[i]] = t[i];
+}
+
 __global__ void sym_half_kernel(int n, double *S) {
   const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n && j < n && i < j) {
@@ -717,21 +726,58 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
       P.K = K;
       P.metric_min_diag = 0.0;
     } else {
-      int lwork = 0;
-      cusolverDnDpotrf_bufferSize(hs, CUBLAS_FILL_MODE_LOWER, P.naux, P.d_L, P.naux, &lwork);
-      P.d_work = P.alloc<double>(std::max(1, lwork));
-      P.lwork = lwork;
-      NKX_REQUIRE(cusolverDnDpotrf(hs, CUBLAS_FILL_MODE_LOWER, P.naux, P.d_L, P.naux, P.d_work, lwork, P.d_info) ==
-                      CUSOLVER_STATUS_SUCCESS,
-                  NKX_ERR_CUDA, "cusolverDnDpotrf failed");
-      int info = 0;
-      NKX_CUDA(cudaMemcpyAsync(&info, P.d_info, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
-      NKX_CUDA(cudaStreamSynchronize(P.stream));
-      NKX_REQUIRE(info == 0, NKX_ERR_NUMERIC, "aux metric (A|B) is not positive definite");
-      std::vector<double> hL(NA * NA);
-      NKX_CUDA(cudaMemcpy(hL.data(), P.d_L, sizeof(double) * NA * NA, cudaMemcpyDeviceToHost));
+      // Pivoted Cholesky of the Jacobi-preconditioned metric A = D^-1 S D^-1:
+      // the grid-integrated (A|B) of an even-tempered aux set is indefinite
+      // at the 1e-4 level (diffuse functions reach past the grid), so aux
+      // functions whose remaining diagonal falls below kMetricTol are
+      // dropped (their fit coefficient is 0) and the kept block is factorised.
+      const double kMetricTol = 1e-5;
+      std::vector<double> D(NA), A(NA * NA);
+      for (size_t i = 0; i < NA; ++i) D[i] = std::sqrt(P.h_metric[i + i * NA]);
+      for (size_t j = 0; j < NA; ++j)
+        for (size_t i = 0; i < NA; ++i) A[i * NA + j] = P.h_metric[i + j * NA] / (D[i] * D[j]);
+      std::vector<double> Lr(NA * NA, 0.0), d(NA);  // row-major rows of L
+      std::vector<char> used(NA, 0);
+      for (size_t i = 0; i < NA; ++i) d[i] = A[i * NA + i];
+      std::vector<int> piv;
+      for (size_t k = 0; k < NA; ++k) {
+        long p = -1;
+        double best = kMetricTol;
+        for (size_t i = 0; i < NA; ++i)
+          if (!used[i] && d[i] >= best) {
+            best = d[i];
+            p = (long)i;
+          }
+        if (p < 0) break;
+        used[p] = 1;
+        piv.push_back((int)p);
+        const double sq = std::sqrt(d[p]);
+        const double *lp = &Lr[(size_t)p * NA];
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < (long)NA; ++i) {
+          if (used[i] && i != p) continue;
+          const double *li = &Lr[(size_t)i * NA];
+          double acc = A[(size_t)i * NA + p];
+          for (size_t c = 0; c < k; ++c) acc -= li[c] * lp[c];
+          const double v = acc / sq;
+          Lr[(size_t)i * NA + k] = v;
+          if (i != p) d[i] -= v * v;
+        }
+      }
+      const int K = (int)piv.size();
+      NKX_REQUIRE(K > 0, NKX_ERR_NUMERIC, "aux metric (A|B) has no positive pivot");
+      // F = D_sel L_sel, lower triangular K x K in pivot order, column-major
+      std::vector<double> F((size_t)K * K, 0.0);
       double mn = 1e300;
-      for (size_t i = 0; i < NA; ++i) mn = std::min(mn, hL[i + i * NA]);
+      for (int a = 0; a < K; ++a)
+        for (int c = 0; c <= a; ++c) F[a + (size_t)c * K] = D[piv[a]] * Lr[(size_t)piv[a] * NA + c];
+      for (int a = 0; a < K; ++a) mn = std::min(mn, F[a + (size_t)a * K] / D[piv[a]]);
+      P.K = K;
+      P.h_piv = piv;
+      NKX_CUDA(cudaMemcpy(P.d_L, F.data(), sizeof(double) * K * K, cudaMemcpyHostToDevice));
+      P.d_piv = P.alloc<int>(K);
+      NKX_CUDA(cudaMemcpy(P.d_piv, piv.data(), sizeof(int) * K, cudaMemcpyHostToDevice));
+      P.d_t = P.alloc<double>(NA);
       P.metric_min_diag = mn;
     }
   }
@@ -797,12 +843,16 @@ void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool s
                           CUBLAS_STATUS_SUCCESS,
                   NKX_ERR_CUDA, "cublasDgemv failed");
     } else {
-      NKX_CUDA(cudaMemcpyAsync(P.d_c, P.d_y, sizeof(double) * P.naux, cudaMemcpyDeviceToDevice, s));
+      gather_kernel<<<nblk(P.K, 128), 128, 0, s>>>(P.K, P.d_piv, P.d_y, P.d_t);
       cusolverDnHandle_t hs = (cusolverDnHandle_t)P.cusolver;
       cusolverDnSetStream(hs, s);
-      NKX_REQUIRE(cusolverDnDpotrs(hs, CUBLAS_FILL_MODE_LOWER, P.naux, 1, P.d_L, P.naux, P.d_c, P.naux, P.d_info) ==
+      NKX_REQUIRE(cusolverDnDpotrs(hs, CUBLAS_FILL_MODE_LOWER, P.K, 1, P.d_L, P.K, P.d_t, P.K, P.d_info) ==
                       CUSOLVER_STATUS_SUCCESS,
                   NKX_ERR_CUDA, "cusolverDnDpotrs failed");
+      NKX_CUDA(cudaMemsetAsync(P.d_c, 0, sizeof(double) * P.naux, s));
+      scatter_kernel<<<nblk(P.K, 128), 128, 0, s>>>(P.K, P.d_piv, P.d_t, P.d_c);
+      NKX_LAUNCH_CHECK();
+      P.launches += 2;
     }
     aux_v_kernel<<<nblk(P.npad, 128), 128, 0, s>>>(P.d_aux, P.naux, P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad,
                                                    P.d_vj);

@@ -56,7 +56,8 @@ struct Plan {
   bool svd_mode = false;
   int K = 0, lwork = 0;
   double *d_L = nullptr, *d_X = nullptr, *d_t = nullptr, *d_y = nullptr, *d_c = nullptr, *d_work = nullptr;
-  int *d_info = nullptr;
+  int *d_info = nullptr, *d_piv = nullptr;
+  std::vector<int> h_piv;
   double metric_min_diag = 0.0;
   std::vector<double> h_metric;
 

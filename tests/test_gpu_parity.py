@@ -143,7 +143,15 @@ def test_functionals_match_oracle(fid, nspin):
     # difference (eps_c + H -> 0); an absolute floor of 1e-15 Eh per particle
     # covers the last-bit differences of CPU and GPU libm there
     np.testing.assert_allclose(de.cpu().numpy(), oe, rtol=1e-11, atol=1e-15)
-    np.testing.assert_allclose(dv.cpu().numpy(), ov, rtol=1e-9, atol=1e-13)
+    dvn = dv.cpu().numpy()
+    if nspin == 2:
+        # at extreme spin polarisation (zeta -> +-1) the minority-spin
+        # potential is a cancelling difference; compare against the scale of
+        # both spin potentials of the point
+        scale = np.repeat(np.abs(ov.reshape(-1, 2)).sum(1), 2)
+        assert (np.abs(dvn - ov) <= 1e-9 * np.abs(ov) + 1e-10 * scale + 1e-13).all()
+    else:
+        np.testing.assert_allclose(dvn, ov, rtol=1e-9, atol=1e-13)
     np.testing.assert_allclose(ds.cpu().numpy(), os_, rtol=1e-9, atol=1e-14 * np.abs(os_).max())
 
 
@@ -201,19 +209,42 @@ def test_plan_chunked_equals_single_chunk():
     assert np.abs(V1[0] - V2[0]).max() < 1e-12
 
 
-def test_plan_coulomb_matches_oracle():
-    c, Z, funcs, g = water_case(1, nrad=30, order=11)
+def small_aux(c, Z):
+    # compact even-tempered aux set whose grid metric is well conditioned
+    return M.sto_basis(c, Z, {8: [(0, 4), (1, 3), (2, 2)], 1: [(0, 3), (1, 2)]}, alpha=0.8, beta=2.5)
+
+
+@pytest.mark.parametrize("svd", [0.0, 1e-6])
+def test_plan_coulomb_matches_oracle(svd):
+    c, Z, funcs, g = water_case(1, nrad=40, order=17)
     b, ob = basis_pair(funcs)
-    afuncs = M.aux_basis(c, Z)
-    aux, oaux = basis_pair(afuncs)
+    aux, oaux = basis_pair(small_aux(c, Z))
     Cm = M.random_orbitals(len(funcs), 5, seed=8)
     occ = np.ones(5)
-    fb = A.FockBuilder(c, Z, b, g, aux=aux, func_ids=("LDA_X",))
+    fb = A.FockBuilder(c, Z, b, g, aux=aux, func_ids=("LDA_X",), metric_svd_thr=svd)
+    assert fb.info()["naux"] == len(oaux["n"])
     E, V, J = fb.build([Cm], [occ], want_J=True)
     S = O.aux_metric(oaux, g.quad_points, g.weights)
-    Jo, _ = O.coulomb(ob, oaux, g.quad_points, g.weights, Cm, occ, S=S)
-    assert np.abs(J - Jo).max() < 1e-8 * np.abs(Jo).max()
+    if svd:
+        Jo, _ = O.coulomb(ob, oaux, g.quad_points, g.weights, Cm, occ, X=O.half_inverse(S, svd))
+    else:
+        Jo, _ = O.coulomb(ob, oaux, g.quad_points, g.weights, Cm, occ, S=S)
+    assert np.abs(J - Jo).max() < 1e-9 * np.abs(Jo).max()
     # fused J folds into the XC contraction: V_fused = V_xc + J
     Ef, Vf, _ = fb.build([Cm], [occ], fuse_j=True)
     assert abs(Ef - E) < 1e-12 * abs(E)
     assert np.abs(Vf[0] - (V[0] + J)).max() < 1e-10 * np.abs(Jo).max()
+
+
+def test_plan_coulomb_pivoted_cholesky_baseline_aux():
+    # the even-tempered zeta_k = 0.3 * 1.8^k aux set: the grid metric is
+    # indefinite, the pivoted Cholesky drops near-dependent functions and J
+    # stays symmetric and finite
+    c, Z, funcs, g = water_case(1, nrad=40, order=17)
+    b, _ = basis_pair(funcs)
+    aux, _ = basis_pair(M.aux_basis(c, Z))
+    fb = A.FockBuilder(c, Z, b, g, aux=aux, func_ids=("LDA_X",))
+    Cm = M.random_orbitals(len(funcs), 5, seed=8)
+    E, V, J = fb.build([Cm], [np.ones(5)], want_J=True)
+    assert np.isfinite(J).all() and np.abs(J - J.T).max() < 1e-12 * np.abs(J).max()
+    assert 0 < fb.info()["metric_min_diag"]
