@@ -502,7 +502,10 @@ static uint64_t spread3(uint64_t v) {
   return v;
 }
 
+void destroy_mixed_state(void *p);
+
 Plan::~Plan() {
+  if (mx_state) destroy_mixed_state(mx_state);
   for (void *p : allocs) cudaFree(p);
   if (cublas) cublasDestroy((cublasHandle_t)cublas);
   if (cusolver) cusolverDnDestroy((cusolverDnHandle_t)cusolver);
@@ -799,33 +802,9 @@ void launch_colloc(Plan &P, const Chunk &c, cudaStream_t s) {
   ++P.launches;
 }
 
-void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
-                     StageTimer &T) {
-  const bool multi = P.chunks.size() > 1;
-  const int nzs = nspin + (separateJ ? 1 : 0);
-  // ---- pass A: collocation + density
-  for (const Chunk &c : P.chunks) {
-    const long nb = c.b1 - c.b0;
-    if (c.p1 - c.p0 > 0) {
-      T.begin(ST_COLLOC, s);
-      launch_colloc(P, c, s);
-      T.end(s);
-    }
-    T.begin(ST_DENSITY, s);
-    dim3 grid((unsigned)(nb * 4), nspin);
-    if (P.gga)
-      density_fp64_kernel<true><<<grid, 256, 0, s>>>(P.ws_phi, P.d_Ct, P.d_occ, nocc, P.nbf_pad, P.d_pair_off,
-                                                     P.d_pair_blk, c.b0, c.p0, P.d_rho, P.d_grad, P.npad);
-    else
-      density_fp64_kernel<false><<<grid, 256, 0, s>>>(P.ws_phi, P.d_Ct, P.d_occ, nocc, P.nbf_pad, P.d_pair_off,
-                                                      P.d_pair_blk, c.b0, c.p0, P.d_rho, P.d_grad, P.npad);
-    NKX_LAUNCH_CHECK();
-    ++P.launches;
-    T.end(s);
-  }
-  // ---- J: fit coefficients and fitted potential
-  if (needJ) {
-    T.begin(ST_COULOMB, s);
+// y = (Vw rho_total), c = (A|B)^-1 y (pivoted Cholesky or half inverse),
+// v_g = w_g sum_a c_a V_a(g)  (coulomb.hpp:84-95)
+void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
     NKX_CUDA(cudaMemsetAsync(P.d_y, 0, sizeof(double) * P.naux, s));
     const long nsl = std::max<long>(1, std::min<long>(64, (P.npad + 4095) / 4096));
     const long slice = (P.npad + nsl - 1) / nsl;
@@ -858,6 +837,36 @@ void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool s
                                                    P.d_vj);
     NKX_LAUNCH_CHECK();
     ++P.launches;
+}
+
+void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
+                     StageTimer &T) {
+  const bool multi = P.chunks.size() > 1;
+  const int nzs = nspin + (separateJ ? 1 : 0);
+  // ---- pass A: collocation + density
+  for (const Chunk &c : P.chunks) {
+    const long nb = c.b1 - c.b0;
+    if (c.p1 - c.p0 > 0) {
+      T.begin(ST_COLLOC, s);
+      launch_colloc(P, c, s);
+      T.end(s);
+    }
+    T.begin(ST_DENSITY, s);
+    dim3 grid((unsigned)(nb * 4), nspin);
+    if (P.gga)
+      density_fp64_kernel<true><<<grid, 256, 0, s>>>(P.ws_phi, P.d_Ct, P.d_occ, nocc, P.nbf_pad, P.d_pair_off,
+                                                     P.d_pair_blk, c.b0, c.p0, P.d_rho, P.d_grad, P.npad);
+    else
+      density_fp64_kernel<false><<<grid, 256, 0, s>>>(P.ws_phi, P.d_Ct, P.d_occ, nocc, P.nbf_pad, P.d_pair_off,
+                                                      P.d_pair_blk, c.b0, c.p0, P.d_rho, P.d_grad, P.npad);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+    T.end(s);
+  }
+  // ---- J: fit coefficients and fitted potential
+  if (needJ) {
+    T.begin(ST_COULOMB, s);
+    coulomb_fit(P, nspin, s);
     T.end(s);
   }
   // ---- functional

@@ -1,0 +1,88 @@
+"""The tensor-core (tcgen05 TF32x3) Fock build against the FP64 CUDA path and
+the CPU oracle.  Accuracy gates: |dE_xc| <= 1e-6 Eh and max|dV_xc| <= 1e-7
+(the mixed-precision target), tighter where the systems are small."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+from nukexc_b200 import api as A  # noqa: E402
+from nukexc_b200 import molecules as M  # noqa: E402
+
+E_TOL = 1e-6
+V_TOL = 1e-7
+
+
+def case(n, seed=0, nrad=40, order=17):
+    c, Z = (M.water() if n == 1 else M.water_cluster(n, seed))
+    funcs = M.sto_basis(c, Z)
+    g = A.make_flat_grid(c, Z, nrad, order, weight_threshold=1e-15, radial="ta")
+    return c, Z, funcs, g
+
+
+@pytest.mark.parametrize("xc", [("LDA_X", "LDA_C_VWN"), ("GGA_X_PBE", "GGA_C_PBE")])
+def test_mixed_water_vs_oracle(xc):
+    c, Z, funcs, g = case(1)
+    b = A.make_manual_basis(funcs)
+    Cm = M.random_orbitals(len(funcs), 5, seed=1)
+    occ = np.ones(5)
+    fb = A.FockBuilder(c, Z, b, g, func_ids=xc)
+    E, V, _ = fb.build([Cm], [occ], precision="mixed")
+    ids = [A._FUNC_NAMES[f] for f in xc]
+    Eo, Vo = O.xc_build(O.make_manual_basis(funcs), g.quad_points, g.weights, ids, [Cm], [occ])
+    assert abs(E - Eo) < E_TOL
+    assert np.abs(V[0] - Vo[0]).max() < V_TOL
+
+
+def test_mixed_cluster_polarized_vs_fp64():
+    c, Z, funcs, g = case(4, seed=2, nrad=30, order=11)
+    b = A.make_manual_basis(funcs)
+    nbf = len(funcs)
+    Ca = M.random_orbitals(nbf, 20, seed=3)
+    Cb = M.random_orbitals(nbf, 20, seed=4)
+    occ = [np.ones(20), np.r_[np.ones(18), np.zeros(2)]]
+    fb = A.FockBuilder(c, Z, b, g)
+    E64, V64, _ = fb.build([Ca, Cb], occ, precision="fp64")
+    Em, Vm, _ = fb.build([Ca, Cb], occ, precision="mixed")
+    assert abs(Em - E64) < E_TOL
+    for s in range(2):
+        assert np.abs(Vm[s] - V64[s]).max() < V_TOL
+
+
+def test_mixed_chunked_and_nocc_over_128():
+    # nocc 150 spans two orbital tiles; a small workspace forces chunks
+    c, Z, funcs, g = case(4, seed=5, nrad=30, order=11)
+    b = A.make_manual_basis(funcs)
+    Cm = M.random_orbitals(len(funcs), 150, seed=6)
+    occ = np.ones(150)
+    f1 = A.FockBuilder(c, Z, b, g)
+    f2 = A.FockBuilder(c, Z, b, g, workspace_bytes=24 << 20)
+    assert f2.info()["nchunks"] > 2
+    E64, V64, _ = f1.build([Cm], [occ], precision="fp64")
+    for fb in (f1, f2):
+        Em, Vm, _ = fb.build([Cm], [occ], precision="mixed")
+        assert abs(Em - E64) < E_TOL
+        assert np.abs(Vm[0] - V64[0]).max() < V_TOL
+
+
+def test_mixed_fused_coulomb_vs_fp64():
+    c, Z, funcs, g = case(2, seed=7, nrad=30, order=11)
+    b = A.make_manual_basis(funcs)
+    aux = A.make_manual_basis(M.sto_basis(c, Z, {8: [(0, 4), (1, 3), (2, 2)], 1: [(0, 3), (1, 2)]},
+                                          alpha=0.8, beta=2.5))
+    Cm = M.random_orbitals(len(funcs), 10, seed=8)
+    occ = np.ones(10)
+    fb = A.FockBuilder(c, Z, b, g, aux=aux)
+    E64, V64, J64 = fb.build([Cm], [occ], precision="fp64", want_J=True)
+    Em, Vm, Jm = fb.build([Cm], [occ], precision="mixed", want_J=True)
+    assert abs(Em - E64) < E_TOL
+    assert np.abs(Vm[0] - V64[0]).max() < V_TOL
+    assert np.abs(Jm - J64).max() < 1e-6 * np.abs(J64).max()
+    Ef, Vf, _ = fb.build([Cm], [occ], precision="mixed", fuse_j=True)
+    assert np.abs(Vf[0] - (V64[0] + J64)).max() < 1e-6 * np.abs(J64).max()
