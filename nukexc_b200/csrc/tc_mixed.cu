@@ -1,22 +1,29 @@
-// Mixed-precision Fock build on the 5th-generation tensor cores (sm_100a).
+// Mixed-precision Fock build on the 5th-generation tensor cores (sm_100a):
+// error-free int8 digit contractions with exact int32 accumulation.
 //
-// Both dense contractions of the Fock build run as one warp-specialised
-// tcgen05 kernel (tc_gemm_kernel):
+// Both dense contractions of the Fock build,
 //   density  T_c(g, i) = sum_f PhiT_c(g, f) Ct(i, f)      c = value, d/dx, d/dy, d/dz
 //   V        Vbar(mu, nu) += sum_g Phi(mu, g) Z(nu, g)    per (batch, block) pair
-// Operands are stored pre-split as TF32 pairs x = hi + lo and each product is
-// hi*hi + hi*lo + lo*hi (three kind::tf32 MMAs into one FP32 TMEM
-// accumulator).  The V contraction flushes the FP32 accumulator after every
-// 256-point batch into FP64 registers; the density accumulates the whole
-// function range of a batch in FP32 and is contracted to rho and grad rho in
-// FP64 (density.hpp:188-255, xc_integrals.hpp:424-726).
+// (density.hpp:188-255, xc_integrals.hpp:424-726), run on one
+// warp-specialised tcgen05 kernel of kind::i8.  Every operand row r of a
+// tile is scaled by a power of two s_r >= max|row| and rounded to a 27-bit
+// integer written as four balanced base-128 digits (digits4, tc_ptx.cuh).
+// A contraction over K is then
+//   sum_k a_k b_k = s_a s_b 2^-54 sum_{L=0..3} 2^(7(6-L)) Acc_L,
+//   Acc_L = sum_k sum_{i+j=L} d_i(a_k) d_j(b_k)            (int32, exact)
+// i.e. ten int8 MMAs per K step into four int32 TMEM accumulators, combined
+// in FP64 after every accumulation group (one 256-point batch for V, one
+// 128-function block for the density).  Products with i + j >= 4 (below
+// 2^-28 of s_a s_b) are dropped; everything kept is exact, so unlike FP32
+// tensor-core accumulation the result carries no rounding bias.
 //
-// Roles (320 threads): warp 0 lane 0 issues TMA tile loads into a 3-stage
-// ring of 64 KB stages (A_hi, A_lo, B_hi, B_lo tiles of 128 x 32 FP32,
-// 128-byte swizzle); warp 1 lane 0 issues the MMAs (M = N = 128, K = 8) and
-// owns the TMEM allocation (2 x 128 columns, double-buffered accumulator);
-// warps 2..9 are the epilogue (warp w reads TMEM lanes 32 (w % 4) .. + 31,
-// columns 64 ((w - 2) / 4) .. + 63).  All waits are bounded (tc_ptx.cuh).
+// Roles (320 threads): warp 0 lane 0 issues 3-D TMA loads of the four digit
+// planes of A (128 rows) and B (64 rows), 64 K-bytes per stage, into a
+// 4-stage ring of 48 KB (64-byte swizzle); warp 1 lane 0 issues the MMAs
+// (M = 128, N = 64, K = 32) and owns TMEM (2 buffers x 4 levels x 64
+// columns); warps 2..9 are the epilogue (warp w reads TMEM lanes
+// 32 (w % 4) .. + 31, columns 32 ((w - 2) / 4) .. + 31 of each level) with
+// FP64 accumulators in registers.  All waits are bounded (tc_ptx.cuh).
 #include <cuda.h>
 
 #include <algorithm>
@@ -29,11 +36,13 @@ namespace nkx {
 
 using namespace tc;
 
-constexpr int kStages = 3;
-constexpr int kTileBytes = 128 * 128;  // 128 rows x 128 B
-constexpr int kStageBytes = 4 * kTileBytes;
+constexpr int kStages = 4;
+constexpr int kABytes = 4 * 128 * 64;  // four digit planes, 128 rows x 64 B
+constexpr int kBBytes = 4 * 64 * 64;   // four digit planes, 64 rows x 64 B
+constexpr int kStageBytes = kABytes + kBBytes;
 constexpr int kGemmThreads = 320;
-constexpr uint32_t kIdesc = idesc_tf32(128, 128);
+constexpr uint32_t kIdesc = idesc_i8(128, 64);
+constexpr double kTwoM54 = 5.551115123125783e-17;  // 2^-54
 
 enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1 };
 
@@ -42,32 +51,28 @@ struct TcArgs {
   long b0, b1, p0;
   const int *pair_off, *pair_blk;
   const uint32_t *mask;
-  int mask_words;
+  int mask_words, nblk;
   // V mode
-  int nblk, nz, nbf_pad;
+  int nz, nbf_pad;
+  const double *sA, *sB;  // row scales: V: sph[q][128], sz[q*nz+z][128]
   double *V;
-  // density mode
+  // density mode: sA = sphT[q][nc][256], sB = sct[s][i][blk]
   int nspin, ncomp, ntile_i, nocc_pad;
-  float *T;
+  double *T;
   long nunits;
   int *err;
 };
 
-// Iterates the accumulation groups and K steps of one work unit; the three
-// roles run the same iteration so their barrier phases stay in step.
 struct UnitIter {
-  const TcArgs &a;
-  long u;
-  // decoded unit
-  int I = 0, J = 0, zi = 0;               // V
-  long bl = 0;                            // density: batch within chunk
-  int h = 0, c = 0, s = 0, t = 0;         // density: point half, comp, spin, orbital tile
-  __device__ UnitIter(const TcArgs &args, long unit) : a(args), u(unit) {
+  int I = 0, J = 0, zi = 0;        // V: row block, 64-column block, Z plane
+  long bl = 0;                     // density: batch within chunk
+  int h = 0, c = 0, s = 0, t = 0;  // density: point half, comp, spin, 64-orbital tile
+  __device__ UnitIter(const TcArgs &a, long u) {
     if (a.mode == TC_MODE_V) {
-      const long n2 = (long)a.nblk * a.nblk;
+      const long n2 = (long)a.nblk * 2 * a.nblk;
       zi = (int)(u / n2);
-      I = (int)((u % n2) / a.nblk);
-      J = (int)(u % a.nblk);
+      I = (int)((u % n2) / (2 * a.nblk));
+      J = (int)(u % (2 * a.nblk));
     } else {
       long r = u;
       t = (int)(r % a.ntile_i);
@@ -82,6 +87,12 @@ struct UnitIter {
   }
 };
 
+struct Group {
+  int nsteps;   // K steps of 64 bytes
+  long qa, qb;  // V: chunk-relative pairs of the row / column blocks
+  int blk;      // density: function block (-1: empty batch)
+};
+
 __device__ __forceinline__ int blk_pos(const uint32_t *m, int I) {
   int pos = 0;
   for (int w = 0; w < (I >> 5); ++w) pos += __popc(m[w]);
@@ -89,48 +100,64 @@ __device__ __forceinline__ int blk_pos(const uint32_t *m, int I) {
 }
 __device__ __forceinline__ bool blk_has(const uint32_t *m, int I) { return (m[I >> 5] >> (I & 31)) & 1u; }
 
-// Calls fn(group_index_within_unit, nsteps, coords_fn) for each group.
-// For the V mode a group is one batch with both blocks significant (8 K
-// steps of 32 points); for the density mode the single group runs over all
-// significant blocks of the batch (4 K steps of 32 functions per block).
-template <class GroupFn>
-__device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &it, GroupFn &&fn) {
+// Calls fn(group, coords) for each accumulation group of a unit; the three
+// roles run the same iteration so their barrier phases stay in step.
+// coords(k, xa, ya, za, xb, yb, zb) gives the 3-D TMA box origins of step k.
+template <class Fn>
+__device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &it, Fn &&fn) {
   if (a.mode == TC_MODE_V) {
+    const int Jb = it.J >> 1, jh = it.J & 1;
     for (long b = a.b0; b < a.b1; ++b) {
       const uint32_t *m = a.mask + b * a.mask_words;
-      if (!blk_has(m, it.I) || !blk_has(m, it.J)) continue;
-      const long qb = a.pair_off[b] - a.p0;
-      const int ya = (int)((qb + blk_pos(m, it.I)) * 128);
-      const int yb = (int)(((qb + blk_pos(m, it.J)) * a.nz + it.zi) * 128);
-      fn(8, [=](int k, int &xa, int &yA, int &xb, int &yB) {
-        xa = 32 * k;
-        yA = ya;
-        xb = 32 * k;
+      if (!blk_has(m, it.I) || !blk_has(m, Jb)) continue;
+      const long qb0 = a.pair_off[b] - a.p0;
+      Group g;
+      g.nsteps = 4;
+      g.qa = qb0 + blk_pos(m, it.I);
+      g.qb = qb0 + blk_pos(m, Jb);
+      g.blk = 0;
+      const int za = (int)(g.qa * 4), zb = (int)((g.qb * a.nz + it.zi) * 4), yb = 64 * jh;
+      fn(g, [=](int k, int &xa, int &ya, int &zA, int &xb, int &yB, int &zB) {
+        xa = 64 * k;
+        ya = 0;
+        zA = za;
+        xb = 64 * k;
         yB = yb;
+        zB = zb;
       });
     }
   } else {
     const long b = a.b0 + it.bl;
     const int q0 = a.pair_off[b], q1 = a.pair_off[b + 1];
-    const int ncomp = a.ncomp;
-    const long p0 = a.p0;
-    const int *pb = a.pair_blk;
-    const int rowB = it.s * a.nocc_pad + it.t * 128;
-    const int c = it.c, h = it.h;
-    fn(4 * (q1 - q0), [=](int k, int &xa, int &yA, int &xb, int &yB) {
-      const int q = q0 + k / 4, sub = k % 4;
-      xa = 32 * sub;
-      yA = (int)((((long)(q - p0) * ncomp + c) * 256) + 128 * h);
-      xb = pb[q] * 128 + 32 * sub;
-      yB = rowB;
-    });
+    for (int q = q0; q < q1; ++q) {
+      Group g;
+      g.nsteps = 2;
+      g.qa = q - a.p0;
+      g.qb = 0;
+      g.blk = a.pair_blk[q];
+      const int za = (int)((g.qa * a.ncomp + it.c) * 4), ya = 128 * it.h;
+      const int xb0 = g.blk * 128, yb = 64 * it.t, zb = it.s * 4;
+      fn(g, [=](int k, int &xa, int &yA, int &zA, int &xb, int &yB, int &zB) {
+        xa = 64 * k;
+        yA = ya;
+        zA = za;
+        xb = xb0 + 64 * k;
+        yB = yb;
+        zB = zb;
+      });
+    }
+    if (q1 == q0) {  // batch without significant functions: one empty group
+      Group g;
+      g.nsteps = 0;
+      g.qa = g.qb = 0;
+      g.blk = -1;
+      fn(g, [=](int, int &, int &, int &, int &, int &, int &) {});
+    }
   }
 }
 
 __global__ void __launch_bounds__(kGemmThreads, 1)
-    tc_gemm_kernel(const __grid_constant__ CUtensorMap mapA_hi, const __grid_constant__ CUtensorMap mapA_lo,
-                   const __grid_constant__ CUtensorMap mapB_hi, const __grid_constant__ CUtensorMap mapB_lo,
-                   TcArgs a) {
+    tc_i8_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs a) {
   extern __shared__ __align__(1024) uint8_t dsmem[];
   __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar[2], tempty_bar[2], drain_bar;
   __shared__ uint32_t tmem_base_sh;
@@ -150,13 +177,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     }
     mbar_init(&drain_bar, 1);
     fence_mbar_init();
-    prefetch_tmap(&mapA_hi);
-    prefetch_tmap(&mapA_lo);
-    prefetch_tmap(&mapB_hi);
-    prefetch_tmap(&mapB_lo);
+    prefetch_tmap(&mapA);
+    prefetch_tmap(&mapB);
   }
   if (warp == 1) {
-    tmem_alloc(&tmem_base_sh, 256);
+    tmem_alloc(&tmem_base_sh, 512);
     tmem_relinquish();
   }
   tc_fence_before();
@@ -170,23 +195,19 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       uint32_t step = 0;
       for (long u = blockIdx.x; u < a.nunits && !abort_flag; u += gridDim.x) {
         UnitIter it(a, u);
-        for_each_group(a, it, [&](int nsteps, auto coords) {
-          for (int k = 0; k < nsteps && !abort_flag; ++k, ++step) {
+        for_each_group(a, it, [&](const Group &g, auto coords) {
+          for (int k = 0; k < g.nsteps && !abort_flag; ++k, ++step) {
             const int st = step % kStages;
             if (!mbar_wait(&empty_bar[st], ((step / kStages) & 1) ^ 1, a.err, 1, &abort_flag)) return;
-            int xa, ya, xb, yb;
-            coords(k, xa, ya, xb, yb);
+            int xa, ya, za, xb, yb, zb;
+            coords(k, xa, ya, za, xb, yb, zb);
             uint8_t *base = smem + st * kStageBytes;
             mbar_arrive_expect_tx(&full_bar[st], kStageBytes);
-            tma_load_2d(base, &mapA_hi, xa, ya, &full_bar[st]);
-            tma_load_2d(base + kTileBytes, &mapA_lo, xa, ya, &full_bar[st]);
-            tma_load_2d(base + 2 * kTileBytes, &mapB_hi, xb, yb, &full_bar[st]);
-            tma_load_2d(base + 3 * kTileBytes, &mapB_lo, xb, yb, &full_bar[st]);
+            tma_load_3d(base, &mapA, xa, ya, za, &full_bar[st]);
+            tma_load_3d(base + kABytes, &mapB, xb, yb, zb, &full_bar[st]);
           }
         });
       }
-      // drain: every issued stage has been consumed (or, after an abort,
-      // its copy has landed) before the CTA may exit
       volatile int keep_waiting = 0;
       for (uint32_t k = (step > kStages ? step - kStages : 0); k < step; ++k)
         mbar_wait(&full_bar[k % kStages], (k / kStages) & 1, a.err, 2, &keep_waiting);
@@ -197,85 +218,98 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       uint32_t step = 0, grp = 0;
       for (long u = blockIdx.x; u < a.nunits && !abort_flag; u += gridDim.x) {
         UnitIter it(a, u);
-        for_each_group(a, it, [&](int nsteps, auto) {
+        for_each_group(a, it, [&](const Group &g, auto) {
           if (abort_flag) return;
           const uint32_t buf = grp & 1, use = grp >> 1;
           if (!mbar_wait(&tempty_bar[buf], (use & 1) ^ 1, a.err, 3, &abort_flag)) return;
           tc_fence_after();
-          const uint32_t d = tmem + buf * 128;
-          for (int k = 0; k < nsteps; ++k, ++step) {
+          const uint32_t d = tmem + buf * 256;
+          for (int k = 0; k < g.nsteps; ++k, ++step) {
             const int st = step % kStages;
             if (!mbar_wait(&full_bar[st], (step / kStages) & 1, a.err, 4, &abort_flag)) return;
             tc_fence_after();
             const uint32_t base = smem_u32(smem + st * kStageBytes);
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
-              const uint64_t ah = smem_desc_k128(base + kk * 32);
-              const uint64_t al = smem_desc_k128(base + kTileBytes + kk * 32);
-              const uint64_t bh = smem_desc_k128(base + 2 * kTileBytes + kk * 32);
-              const uint64_t bo = smem_desc_k128(base + 3 * kTileBytes + kk * 32);
-              mma_tf32(d, ah, bh, kIdesc, (k > 0 || kk > 0) ? 1u : 0u);
-              mma_tf32(d, ah, bo, kIdesc, 1u);
-              mma_tf32(d, al, bh, kIdesc, 1u);
-            }
+            for (int kk = 0; kk < 2; ++kk)
+#pragma unroll
+              for (int L = 0; L < 4; ++L)
+#pragma unroll
+                for (int i = 0; i <= L; ++i) {
+                  const int j = L - i;
+                  const uint64_t ad = smem_desc_k64(base + i * (128 * 64) + kk * 32);
+                  const uint64_t bd = smem_desc_k64(base + kABytes + j * (64 * 64) + kk * 32);
+                  mma_i8(d + L * 64, ad, bd, kIdesc, (k == 0 && kk == 0 && i == 0) ? 0u : 1u);
+                }
             mma_commit(&empty_bar[st]);
           }
           mma_commit(&tfull_bar[buf]);
           ++grp;
         });
       }
-      // all MMAs done before TMEM is released
       volatile int keep_waiting = 0;
       mma_commit(&drain_bar);
       mbar_wait(&drain_bar, 0, a.err, 5, &keep_waiting);
     }
   } else {
     // ------------------------------------------------------ epilogue
-    const int q = warp & 3, half = (warp - 2) >> 2;
+    const int q = warp & 3, hc = (warp - 2) >> 2;
     const int row = 32 * q + lane;
     const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
     uint32_t grp = 0;
     for (long u = blockIdx.x; u < a.nunits && !abort_flag; u += gridDim.x) {
       UnitIter it(a, u);
-      double acc[64];
+      double acc[32];
 #pragma unroll
-      for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+      for (int j = 0; j < 32; ++j) acc[j] = 0.0;
       bool any = false;
-      for_each_group(a, it, [&](int nsteps, auto) {
+      for_each_group(a, it, [&](const Group &g, auto) {
         if (abort_flag) return;
         const uint32_t buf = grp & 1, use = grp >> 1;
         if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag)) return;
         tc_fence_after();
-        any = true;
         __syncwarp();
-#pragma unroll
-        for (int part = 0; part < 2; ++part) {
-          float v[32];
-          tmem_ld32(tmem + lane_addr + buf * 128 + 64 * half + 32 * part, v);
+        const bool live = g.nsteps > 0;
+        double sa = 0.0;
+        const double *sb = nullptr;
+        size_t sbs = 1;
+        if (live) {
           if (a.mode == TC_MODE_V) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j) acc[32 * part + j] += (double)v[j];
+            sa = a.sA[g.qa * 128 + row] * kTwoM54;
+            sb = a.sB + (g.qb * a.nz + it.zi) * 128 + 64 * (it.J & 1) + 32 * hc;
           } else {
-            // T[bl][s][c][i][g]: lanes write consecutive g
-            const long plane = ((it.bl * a.nspin + it.s) * a.ncomp + it.c);
-            float *Tp = a.T + plane * (long)a.nocc_pad * 256 + 128 * it.h + row;
-            const int i0 = it.t * 128 + 64 * half + 32 * part;
+            sa = a.sA[(g.qa * a.ncomp + it.c) * 256 + 128 * it.h + row] * kTwoM54;
+            sb = a.sB + ((size_t)it.s * a.nocc_pad + 64 * it.t + 32 * hc) * a.nblk + g.blk;
+            sbs = a.nblk;
+          }
+        }
+        // level L carries weight 2^(7 (3 - L)) relative to the 2^-54 s_a s_b unit
 #pragma unroll
-            for (int j = 0; j < 32; ++j) Tp[(long)(i0 + j) * 256] = nsteps > 0 ? v[j] : 0.0f;
+        for (int L = 0; L < 4; ++L) {
+          uint32_t v[32];
+          tmem_ld32u(tmem + lane_addr + buf * 256 + L * 64 + 32 * hc, v);
+          if (live) {
+            const double wl = sa * (double)(1 << (7 * (3 - L)));
+#pragma unroll
+            for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], wl * sb[j * sbs], acc[j]);
           }
         }
         tc_fence_before();
         mbar_arrive(&tempty_bar[buf]);
         ++grp;
+        any = any || live;
       });
-      if (a.mode == TC_MODE_V && any) {
-        double *Vz = a.V + (size_t)it.zi * a.nbf_pad * a.nbf_pad;
-        const size_t r = (size_t)it.I * 128 + row;
+      if (a.mode == TC_MODE_V) {
+        if (any) {
+          double *Vz = a.V + (size_t)it.zi * a.nbf_pad * a.nbf_pad;
+          const size_t r = (size_t)it.I * 128 + row;
 #pragma unroll
-        for (int j = 0; j < 64; ++j) {
-          const size_t col = (size_t)it.J * 128 + 64 * half + j;
-          Vz[r + col * a.nbf_pad] += acc[j];
+          for (int j = 0; j < 32; ++j) Vz[r + ((size_t)it.J * 64 + 32 * hc + j) * a.nbf_pad] += acc[j];
         }
+      } else {
+        const long plane = (it.bl * a.nspin + it.s) * a.ncomp + it.c;
+        double *Tp = a.T + plane * (long)a.nocc_pad * 256 + 128 * it.h + row;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) Tp[(size_t)(64 * it.t + 32 * hc + j) * 256] = acc[j];
       }
     }
   }
@@ -284,95 +318,191 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   if (warp == 1) {
     __syncwarp();
     tc_fence_after();
-    tmem_dealloc(tmem, 256);
+    tmem_dealloc(tmem, 512);
   }
 }
 
+// ----------------------------------------------------- quantisation ----
 
-// ------------------------------------------------------ data kernels ----
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ uint32_t pack4(int8_t a, int8_t b, int8_t c, int8_t d) {
+  return (uint32_t)(uint8_t)a | ((uint32_t)(uint8_t)b << 8) | ((uint32_t)(uint8_t)c << 16) |
+         ((uint32_t)(uint8_t)d << 24);
+}
+// four consecutive values -> four digit planes (one packed word per plane)
+__device__ __forceinline__ void quant4(const double v[4], double inv, uint32_t w[4]) {
+  int8_t d[4][4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) digits4(v[k], inv, d[0][k], d[1][k], d[2][k], d[3][k]);
+#pragma unroll
+  for (int p = 0; p < 4; ++p) w[p] = pack4(d[p][0], d[p][1], d[p][2], d[p][3]);
+}
 
-// Collocation of one (batch, block) pair per CTA as TF32 pairs:
-// out_hi/out_lo[pair][comp][g][f] (layout of colloc_fp64_kernel).
+// Density operand A: rows (pair, comp, g) of PhiT over the 128 functions of
+// the block, one warp per row.  qphT[pair][comp][digit][g][f], sphT[pair][comp][g].
+__global__ void quant_phiT_kernel(const double *__restrict__ phiT, int nc, long nrows, uint8_t *__restrict__ q,
+                                  double *__restrict__ sc) {
+  const long r = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= nrows) return;
+  const long pc = r / 256;  // pair * nc + comp
+  const int g = (int)(r % 256);
+  const double *src = phiT + r * 128 + 4 * lane;
+  double v[4] = {src[0], src[1], src[2], src[3]};
+  const double m = warp_max(fmax(fmax(fabs(v[0]), fabs(v[1])), fmax(fabs(v[2]), fabs(v[3]))));
+  double s;
+  const double inv = inv_pow2_scale(m, s);
+  uint32_t w[4];
+  quant4(v, inv, w);
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+    reinterpret_cast<uint32_t *>(q + ((pc * 4 + p) * 256 + g) * 128)[lane] = w[p];
+  if (lane == 0) sc[r] = s;
+  (void)nc;
+}
+
+// Density operand B: orbital rows (spin, i) over each 128-function block.
+// qct[spin][digit][i][f], sct[spin][i][blk]; rows i >= nocc are zero.
+__global__ void quant_ct_kernel(const double *__restrict__ Ct, int nocc, int nocc_pad, int nspin, int nbf_pad,
+                                int nblk, uint8_t *__restrict__ q, double *__restrict__ sc) {
+  const long r = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= (long)nspin * nocc_pad * nblk) return;
+  const int blk = (int)(r % nblk);
+  const long si = r / nblk;
+  const int s = (int)(si / nocc_pad), i = (int)(si % nocc_pad);
+  const int f0 = blk * 128 + 4 * lane;
+  double v[4] = {0, 0, 0, 0};
+  if (i < nocc)
+    for (int k = 0; k < 4; ++k) v[k] = Ct[((size_t)s * nocc + i) * nbf_pad + f0 + k];
+  const double m = warp_max(fmax(fmax(fabs(v[0]), fabs(v[1])), fmax(fabs(v[2]), fabs(v[3]))));
+  double scl;
+  const double inv = inv_pow2_scale(m, scl);
+  uint32_t w[4];
+  quant4(v, inv, w);
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+    *reinterpret_cast<uint32_t *>(q + (((size_t)s * 4 + p) * nocc_pad + i) * nbf_pad + f0) = w[p];
+  if (lane == 0) sc[((size_t)s * nocc_pad + i) * nblk + blk] = scl;
+}
+
+// V operands of one (batch, block) pair: Phi (value) and Z_z (z < nz: the
+// XC coefficients c0 phi + c . grad phi, z == nspin for a separate J:
+// 1/2 vJ phi), each row f scaled over the 256 points and written transposed
+// as qph[pair][digit][f][g], qz[pair][z][digit][f][g] with scales sph, sz.
 template <bool GRAD>
-__global__ void __launch_bounds__(256) colloc_split_kernel(const StoFunc *__restrict__ sto, const double *__restrict__ px,
-                                                           const double *__restrict__ py, const double *__restrict__ pz,
-                                                           const int *__restrict__ pair_batch,
-                                                           const int *__restrict__ pair_blk, long p0,
-                                                           float *__restrict__ out_hi, float *__restrict__ out_lo) {
-  const long p = p0 + blockIdx.x;
-  const int b = pair_batch[p], I = pair_blk[p];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  __shared__ double sx[kBatch], sy[kBatch], sz[kBatch];
-  for (int g = threadIdx.x; g < kBatch; g += blockDim.x) {
-    sx[g] = px[(long)b * kBatch + g];
-    sy[g] = py[(long)b * kBatch + g];
-    sz[g] = pz[(long)b * kBatch + g];
-  }
-  __syncthreads();
-  StoFunc f[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) f[c] = sto[I * kBlockF + lane + 32 * c];
-  const size_t tile = (size_t)kBatch * kBlockF;
-  const size_t off = (size_t)blockIdx.x * (GRAD ? 4 : 1) * tile;
-  float *oh = out_hi + off, *ol = out_lo + off;
-  for (int g = warp; g < kBatch; g += 8) {
-    const double x = sx[g], y = sy[g], z = sz[g];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const size_t idx = (size_t)g * kBlockF + lane + 32 * c;
-      double v[4];
-      if (GRAD)
-        sto_value_grad(f[c], x, y, z, v[0], v[1], v[2], v[3]);
-      else
-        v[0] = sto_value(f[c], x, y, z);
-#pragma unroll
-      for (int k = 0; k < (GRAD ? 4 : 1); ++k) {
-        float hi, lo;
-        split_tf32(v[k], hi, lo);
-        oh[k * tile + idx] = hi;
-        ol[k * tile + idx] = lo;
+__global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ phiT, const double *__restrict__ coef,
+                                                     const double *__restrict__ vj, const int *__restrict__ pair_batch,
+                                                     long p0, int nz, int nspin, long npad, uint8_t *__restrict__ qph,
+                                                     double *__restrict__ sph, uint8_t *__restrict__ qz,
+                                                     double *__restrict__ sz) {
+  constexpr int NC = GRAD ? 4 : 1;
+  extern __shared__ __align__(16) uint8_t tile[];  // [(1 + nz)][4][128][64]
+  __shared__ double mx[2][4][128];
+  const long q = blockIdx.x;
+  const int b = pair_batch[p0 + q];
+  const size_t T = (size_t)kBatch * kBlockF;
+  const double *P = phiT + q * NC * T;
+  const int f = threadIdx.x & 127, gs = threadIdx.x >> 7;
+  const int nop = 1 + nz;
+  auto values = [&](int g, double out[4]) {
+    const size_t e = (size_t)g * kBlockF + f;
+    const double v = P[e];
+    double dx = 0, dy = 0, dz = 0;
+    if (GRAD) {
+      dx = P[T + e];
+      dy = P[2 * T + e];
+      dz = P[3 * T + e];
+    }
+    const long gg = (long)b * kBatch + g;
+    out[0] = v;
+    for (int z = 0; z < 3; ++z) {
+      double r = 0.0;
+      if (z < nspin) {
+        const double *c = coef + (size_t)z * 4 * npad;
+        r = c[gg] * v;
+        if (GRAD) r += c[npad + gg] * dx + c[2 * npad + gg] * dy + c[3 * npad + gg] * dz;
+      } else if (z < nz) {
+        r = 0.5 * vj[gg] * v;
       }
+      out[1 + z] = r;
+    }
+  };
+  // pass 1: row maxima over the 256 points
+  double m[4] = {0, 0, 0, 0};
+  for (int g = gs; g < kBatch; g += 2) {
+    double v[4];
+    values(g, v);
+    for (int o = 0; o < 4; ++o) m[o] = fmax(m[o], fabs(v[o]));
+  }
+  for (int o = 0; o < 4; ++o) mx[gs][o][f] = m[o];
+  __syncthreads();
+  double inv[4];
+  for (int o = 0; o < 4; ++o) {
+    double s;
+    inv[o] = inv_pow2_scale(fmax(mx[0][o][f], mx[1][o][f]), s);
+    if (gs == 0 && o < nop) {
+      if (o == 0)
+        sph[q * 128 + f] = s;
+      else
+        sz[(q * nz + (o - 1)) * 128 + f] = s;
     }
   }
+  // pass 2: digits, transposed through shared memory in slabs of 64 points
+  for (int g0 = 0; g0 < kBatch; g0 += 64) {
+    for (int k = 0; k < 32; ++k) {
+      const int gl = gs + 2 * k;
+      double v[4];
+      values(g0 + gl, v);
+      for (int o = 0; o < nop; ++o) {
+        int8_t d0, d1, d2, d3;
+        digits4(v[o], inv[o], d0, d1, d2, d3);
+        uint8_t *t = tile + ((size_t)o * 4 * 128 + f) * 64 + gl;
+        t[0] = (uint8_t)d0;
+        t[128 * 64] = (uint8_t)d1;
+        t[2 * 128 * 64] = (uint8_t)d2;
+        t[3 * 128 * 64] = (uint8_t)d3;
+      }
+    }
+    __syncthreads();
+    // rows (operand, digit, f) of 64 bytes -> 4 x 16-byte stores each
+    const int nrow = nop * 4 * 128;
+    for (int e = threadIdx.x; e < nrow * 4; e += 256) {
+      const int rw = e >> 2, part = e & 3;
+      const int o = rw / 512, d = (rw / 128) & 3, ff = rw & 127;
+      const uint4 val = *reinterpret_cast<const uint4 *>(tile + (size_t)rw * 64 + 16 * part);
+      uint8_t *dst = (o == 0) ? qph + ((q * 4 + d) * 128 + ff) * 256
+                              : qz + (((q * nz + (o - 1)) * 4 + d) * 128 + ff) * 256;
+      *reinterpret_cast<uint4 *>(dst + g0 + 16 * part) = val;
+    }
+    __syncthreads();
+  }
 }
 
-// Orbitals Ct[spin][i][f] (FP64, f padded) -> TF32 pairs with orbital rows
-// padded to nocc_pad (zeros).
-__global__ void split_orbitals_kernel(const double *__restrict__ Ct, int nocc, int nocc_pad, int nspin, int nbf_pad,
-                                      float *__restrict__ hi, float *__restrict__ lo) {
-  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const long tot = (long)nspin * nocc_pad * nbf_pad;
-  if (e >= tot) return;
-  const int f = (int)(e % nbf_pad);
-  const long si = e / nbf_pad;
-  const int s = (int)(si / nocc_pad), i = (int)(si % nocc_pad);
-  const double v = i < nocc ? Ct[((size_t)s * nocc + i) * nbf_pad + f] : 0.0;
-  float h, l;
-  split_tf32(v, h, l);
-  hi[e] = h;
-  lo[e] = l;
-}
-
-// rho(g) = sum_i occ_i T0(g,i)^2, grad rho = 2 sum_i occ_i T0 Tc in FP64 from
-// the FP32 tensor-core products T[bl][s][c][i][g] (density.hpp:188-255).
+// rho(g) = sum_i occ_i T0(g,i)^2, grad rho = 2 sum_i occ_i T0 Tc from the
+// FP64 products T[bl][s][c][i][g] (density.hpp:188-255).
 template <bool GRAD>
-__global__ void density_contract_kernel(const float *__restrict__ T, const double *__restrict__ occ, int nocc,
+__global__ void density_contract_kernel(const double *__restrict__ T, const double *__restrict__ occ, int nocc,
                                         int nocc_pad, int nspin, long b0, double *__restrict__ rho,
                                         double *__restrict__ grad, long npad) {
   constexpr int NC = GRAD ? 4 : 1;
   const long bl = blockIdx.x;
   const int s = blockIdx.y, g = threadIdx.x;
-  const float *Tp = T + ((bl * nspin + s) * NC) * (size_t)nocc_pad * 256 + g;
   const size_t plane = (size_t)nocc_pad * 256;
+  const double *Tp = T + ((bl * nspin + s) * NC) * plane + g;
   double r = 0, gx = 0, gy = 0, gz = 0;
   for (int i = 0; i < nocc; ++i) {
     const double o = occ[(size_t)s * nocc + i];
     const double t = Tp[(size_t)i * 256];
     r += o * t * t;
     if (GRAD) {
-      gx += o * t * (double)Tp[plane + (size_t)i * 256];
-      gy += o * t * (double)Tp[2 * plane + (size_t)i * 256];
-      gz += o * t * (double)Tp[3 * plane + (size_t)i * 256];
+      gx += o * t * Tp[plane + (size_t)i * 256];
+      gy += o * t * Tp[2 * plane + (size_t)i * 256];
+      gz += o * t * Tp[3 * plane + (size_t)i * 256];
     }
   }
   const long gg = (b0 + bl) * kBatch + g;
@@ -381,75 +511,6 @@ __global__ void density_contract_kernel(const float *__restrict__ T, const doubl
     grad[((size_t)s * 3 + 0) * npad + gg] = 2 * gx;
     grad[((size_t)s * 3 + 1) * npad + gg] = 2 * gy;
     grad[((size_t)s * 3 + 2) * npad + gg] = 2 * gz;
-  }
-}
-
-// Z build for the tensor-core V contraction: from PhiT (TF32 pairs,
-// [pair][comp][g][f]) and the per-point coefficients, write Phi[pair][f][g]
-// and Z[pair][z][f][g] as TF32 pairs (transposed through shared memory in
-// slabs of 32 points).  z < nspin: Z_s = c0 phi + c . grad phi; z == nspin
-// (separate J): Z_J = 1/2 vJ phi.
-template <bool GRAD>
-__global__ void __launch_bounds__(256) zbuild_split_kernel(const float *__restrict__ ph_hi, const float *__restrict__ ph_lo,
-                                                           const double *__restrict__ coef, const double *__restrict__ vj,
-                                                           const int *__restrict__ pair_batch, long p0, int nz, int nspin,
-                                                           long npad, float *__restrict__ phi_hi, float *__restrict__ phi_lo,
-                                                           float *__restrict__ z_hi, float *__restrict__ z_lo) {
-  constexpr int NC = GRAD ? 4 : 1;
-  __shared__ float tile[128][33];
-  const long q = blockIdx.x;
-  const int b = pair_batch[p0 + q];
-  const size_t T = (size_t)kBatch * kBlockF;
-  const float *H = ph_hi + q * NC * T, *L = ph_lo + q * NC * T;
-  const int f = threadIdx.x & 127, gsub = threadIdx.x >> 7;  // 2 point rows per pass
-  for (int g0 = 0; g0 < kBatch; g0 += 32) {
-    double val[16], zv[3][16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      const int g = g0 + gsub + 2 * k;
-      const size_t e = (size_t)g * kBlockF + f;
-      const double v = (double)H[e] + (double)L[e];
-      double dx = 0, dy = 0, dz = 0;
-      if (GRAD) {
-        dx = (double)H[T + e] + (double)L[T + e];
-        dy = (double)H[2 * T + e] + (double)L[2 * T + e];
-        dz = (double)H[3 * T + e] + (double)L[3 * T + e];
-      }
-      val[k] = v;
-      const long gg = (long)b * kBatch + g;
-      for (int z = 0; z < 3; ++z) {
-        double r = 0.0;
-        if (z < nspin) {
-          const double *c = coef + (size_t)z * 4 * npad;
-          r = c[gg] * v;
-          if (GRAD) r += c[npad + gg] * dx + c[2 * npad + gg] * dy + c[3 * npad + gg] * dz;
-        } else if (z < nz) {
-          r = 0.5 * vj[gg] * v;
-        }
-        zv[z][k] = r;
-      }
-    }
-    // planes: phi hi, phi lo, then (z hi, z lo) for z < nz
-    for (int pl = 0; pl < 2 + 2 * nz; ++pl) {
-#pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        const double x = pl < 2 ? val[k] : zv[(pl - 2) / 2][k];
-        float hi, lo;
-        split_tf32(x, hi, lo);
-        tile[f][gsub + 2 * k] = (pl & 1) ? lo : hi;
-      }
-      __syncthreads();
-      float *dst;
-      if (pl < 2)
-        dst = (pl == 0 ? phi_hi : phi_lo) + q * T;
-      else
-        dst = ((pl & 1) ? z_lo : z_hi) + (q * nz + (pl - 2) / 2) * T;
-      // 128 rows (f) x 32 points; each thread writes 16 consecutive points
-      const int rf = threadIdx.x >> 1, part = threadIdx.x & 1;
-#pragma unroll
-      for (int k = 0; k < 16; ++k) dst[(size_t)rf * kBatch + g0 + 16 * part + k] = tile[rf][16 * part + k];
-      __syncthreads();
-    }
   }
 }
 
@@ -463,51 +524,48 @@ static EncodeTiledFn encode_fn() {
   static EncodeTiledFn fn = nullptr;
   if (!fn) {
     void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    NKX_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
-    NKX_REQUIRE(p && q == cudaDriverEntryPointSuccess, NKX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    cudaDriverEntryPointQueryResult qr;
+    NKX_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &qr));
+    NKX_REQUIRE(p && qr == cudaDriverEntryPointSuccess, NKX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     fn = reinterpret_cast<EncodeTiledFn>(p);
   }
   return fn;
 }
 
-// 2-D FP32 tensor map over a row-major [rows][cols] array, box 32 x 128,
-// 128-byte swizzle.  cols * 4 must be a multiple of 16 and >= 32 elements.
-static CUtensorMap make_map(const float *base, long rows, long cols) {
-  NKX_REQUIRE(cols % 32 == 0 && rows >= 128 && ((uintptr_t)base % 16) == 0, NKX_ERR_ARG, "bad tensor map shape");
+// 3-D byte tensor [planes][rows][cols] (cols contiguous), box
+// {64 bytes, box_rows, 4 planes}, 64-byte swizzle.
+static CUtensorMap make_map3(const uint8_t *base, long cols, long rows, long planes, int box_rows) {
+  NKX_REQUIRE(cols % 64 == 0 && rows % box_rows == 0 && planes % 4 == 0 && ((uintptr_t)base % 16) == 0,
+              NKX_ERR_ARG, "bad tensor map shape");
   CUtensorMap m;
-  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)cols * sizeof(float)};
-  const cuuint32_t box[2] = {32, 128};
-  const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides, box,
-                                 estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+  const cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)rows, (cuuint64_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)cols, (cuuint64_t)cols * rows};
+  const cuuint32_t box[3] = {64, (cuuint32_t)box_rows, 4};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t *>(base), dims, strides,
+                                 box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   NKX_REQUIRE(r == CUDA_SUCCESS, NKX_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
   return m;
 }
 
 struct MixedState {
-  long cap_pairs = 0;
-  int nocc_pad = 0, nspin = 0, nbatch_chunk = 0;
-  float *phT_hi = nullptr, *phT_lo = nullptr;  // [pair][4][256][128]
-  float *ph_hi = nullptr, *ph_lo = nullptr;    // [pair][128][256]
-  float *z_hi = nullptr, *z_lo = nullptr;      // [pair][3][128][256]
-  float *ct_hi = nullptr, *ct_lo = nullptr;    // [2][nocc_pad][nbf_pad]
-  float *T = nullptr;                          // [batch][spin][4][nocc_pad][256]
+  long cap = 0;  // pairs per chunk
+  int nocc_pad = 0, nbatch_chunk = 0, nsm = 148;
+  uint8_t *qphT = nullptr, *qph = nullptr, *qz = nullptr, *qct = nullptr;
+  double *sphT = nullptr, *sph = nullptr, *sz = nullptr, *sct = nullptr, *T = nullptr;
   int *err = nullptr;
-  CUtensorMap m_phT_hi, m_phT_lo, m_ph_hi, m_ph_lo, m_z_hi, m_z_lo, m_ct_hi, m_ct_lo;
+  CUtensorMap m_phT, m_ph, m_z, m_ct;
   std::vector<void *> bufs;
-  int nsm = 148;
   ~MixedState() {
     for (void *p : bufs) cudaFree(p);
   }
-  template <class T>
-  T *alloc(size_t n) {
-    T *p = nullptr;
-    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
+  template <class X>
+  X *alloc(size_t n) {
+    X *p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(1, n) * sizeof(X)) != cudaSuccess) {
       cudaGetLastError();
-      throw Error{NKX_ERR_ALLOC, "mixed workspace allocation of " + std::to_string(n * sizeof(T)) + " bytes failed"};
+      throw Error{NKX_ERR_ALLOC, "mixed workspace allocation of " + std::to_string(n * sizeof(X)) + " bytes failed"};
     }
     bufs.push_back(p);
     return p;
@@ -522,53 +580,49 @@ bool mixed_available(const Plan &) {
   return major == 10 && minor == 0;
 }
 
-static MixedState &mixed_state(Plan &P, int nspin, int nocc) {
-  if (!P.mx_state) P.mx_state = new MixedState();
-  MixedState &M = *static_cast<MixedState *>(P.mx_state);
-  const size_t T = (size_t)kBatch * kBlockF;
-  if (!M.phT_hi) {
-    M.cap_pairs = std::max<long>(1, P.max_chunk_pairs);
+static MixedState &mixed_state(Plan &P, int nocc) {
+  if (!P.mx_state) {
+    MixedState *M = new MixedState();
+    P.mx_state = M;
+    M->cap = std::max<long>(1, P.max_chunk_pairs);
     long nb = 1;
     for (const Chunk &c : P.chunks) nb = std::max(nb, c.b1 - c.b0);
-    M.nbatch_chunk = (int)nb;
-    M.phT_hi = M.alloc<float>(M.cap_pairs * 4 * T);
-    M.phT_lo = M.alloc<float>(M.cap_pairs * 4 * T);
-    M.ph_hi = M.alloc<float>(M.cap_pairs * T);
-    M.ph_lo = M.alloc<float>(M.cap_pairs * T);
-    M.z_hi = M.alloc<float>(M.cap_pairs * 3 * T);
-    M.z_lo = M.alloc<float>(M.cap_pairs * 3 * T);
-    M.err = M.alloc<int>(1);
-    NKX_CUDA(cudaMemset(M.err, 0, sizeof(int)));
-    M.m_phT_hi = make_map(M.phT_hi, M.cap_pairs * 4 * 256, 128);
-    M.m_phT_lo = make_map(M.phT_lo, M.cap_pairs * 4 * 256, 128);
-    M.m_ph_hi = make_map(M.ph_hi, M.cap_pairs * 128, 256);
-    M.m_ph_lo = make_map(M.ph_lo, M.cap_pairs * 128, 256);
-    M.m_z_hi = make_map(M.z_hi, M.cap_pairs * 3 * 128, 256);
-    M.m_z_lo = make_map(M.z_lo, M.cap_pairs * 3 * 128, 256);
+    M->nbatch_chunk = (int)nb;
+    const size_t tile = (size_t)kBatch * kBlockF;
+    M->qphT = M->alloc<uint8_t>(M->cap * 4 * 4 * tile);
+    M->sphT = M->alloc<double>(M->cap * 4 * 256);
+    M->qph = M->alloc<uint8_t>(M->cap * 4 * tile);
+    M->sph = M->alloc<double>(M->cap * 128);
+    M->qz = M->alloc<uint8_t>(M->cap * 3 * 4 * tile);
+    M->sz = M->alloc<double>(M->cap * 3 * 128);
+    M->err = M->alloc<int>(1);
+    M->m_phT = make_map3(M->qphT, 128, 256, M->cap * 4 * 4, 128);
+    M->m_ph = make_map3(M->qph, 256, 128, M->cap * 4, 128);
+    M->m_z = make_map3(M->qz, 256, 128, M->cap * 3 * 4, 64);
     int dev = 0;
     NKX_CUDA(cudaGetDevice(&dev));
-    NKX_CUDA(cudaDeviceGetAttribute(&M.nsm, cudaDevAttrMultiProcessorCount, dev));
-    NKX_CUDA(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    NKX_CUDA(cudaDeviceGetAttribute(&M->nsm, cudaDevAttrMultiProcessorCount, dev));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kStages * kStageBytes + 1024));
+    NKX_CUDA(cudaFuncSetAttribute(zquant_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 64));
+    NKX_CUDA(cudaFuncSetAttribute(zquant_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 64));
   }
-  const int nocc_pad = ((nocc + 127) / 128) * 128;
-  if (nocc_pad > M.nocc_pad || nspin > M.nspin) {
-    M.nocc_pad = std::max(nocc_pad, M.nocc_pad);
-    M.nspin = std::max(nspin, M.nspin);
-    M.ct_hi = M.alloc<float>((size_t)2 * M.nocc_pad * P.nbf_pad);
-    M.ct_lo = M.alloc<float>((size_t)2 * M.nocc_pad * P.nbf_pad);
-    M.m_ct_hi = make_map(M.ct_hi, (long)2 * M.nocc_pad, P.nbf_pad);
-    M.m_ct_lo = make_map(M.ct_lo, (long)2 * M.nocc_pad, P.nbf_pad);
-    M.T = M.alloc<float>((size_t)M.nbatch_chunk * 2 * 4 * M.nocc_pad * 256);
+  MixedState &M = *static_cast<MixedState *>(P.mx_state);
+  const int nocc_pad = ((nocc + 63) / 64) * 64;
+  if (nocc_pad > M.nocc_pad) {
+    M.nocc_pad = nocc_pad;
+    M.qct = M.alloc<uint8_t>((size_t)2 * 4 * nocc_pad * P.nbf_pad);
+    M.sct = M.alloc<double>((size_t)2 * nocc_pad * P.nblk);
+    M.T = M.alloc<double>((size_t)M.nbatch_chunk * 2 * 4 * nocc_pad * 256);
+    M.m_ct = make_map3(M.qct, P.nbf_pad, nocc_pad, 8, 64);
   }
   return M;
 }
 
-static void launch_gemm(MixedState &M, const CUtensorMap &ah, const CUtensorMap &al, const CUtensorMap &bh,
-                        const CUtensorMap &bl, const TcArgs &a, cudaStream_t s) {
+static void launch_i8(MixedState &M, const CUtensorMap &mA, const CUtensorMap &mB, const TcArgs &a, cudaStream_t s) {
   if (a.nunits <= 0) return;
   const unsigned grid = (unsigned)std::min<long>(a.nunits, M.nsm);
-  tc_gemm_kernel<<<grid, kGemmThreads, kStages * kStageBytes + 1024, s>>>(ah, al, bh, bl, a);
+  tc_i8_kernel<<<grid, kGemmThreads, kStages * kStageBytes + 1024, s>>>(mA, mB, a);
   NKX_LAUNCH_CHECK();
 }
 
@@ -576,41 +630,39 @@ __global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, cons
                                   const double *__restrict__ rho, const double *__restrict__ grad,
                                   const double *__restrict__ vj, double *__restrict__ coef, double *Eacc);
 void coulomb_fit(Plan &P, int nspin, cudaStream_t s);
+void launch_colloc(Plan &P, const Chunk &c, cudaStream_t s);
 
 void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
                       StageTimer &Tm) {
-  MixedState &M = mixed_state(P, nspin, nocc);
-  const int ncomp = P.gga ? 4 : 1;
+  MixedState &M = mixed_state(P, nocc);
+  const int nc = P.gga ? 4 : 1;
   const int nzs = nspin + (separateJ ? 1 : 0);
   NKX_REQUIRE(nzs <= 3, NKX_ERR_ARG, "too many Z planes");
   const bool multi = P.chunks.size() > 1;
+  const size_t tile = (size_t)kBatch * kBlockF;
   NKX_CUDA(cudaMemsetAsync(M.err, 0, sizeof(int), s));
   {
-    const long tot = (long)nspin * M.nocc_pad * P.nbf_pad;
-    split_orbitals_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(P.d_Ct, nocc, M.nocc_pad, nspin, P.nbf_pad,
-                                                                          M.ct_hi, M.ct_lo);
+    const long rows = (long)nspin * M.nocc_pad * P.nblk;
+    quant_ct_kernel<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(P.d_Ct, nocc, M.nocc_pad, nspin, P.nbf_pad,
+                                                                         P.nblk, M.qct, M.sct);
     NKX_LAUNCH_CHECK();
     ++P.launches;
   }
-  auto colloc = [&](const Chunk &c) {
-    const long np = c.p1 - c.p0;
-    if (np <= 0) return;
-    Tm.begin(ST_COLLOC, s);
-    if (P.gga)
-      colloc_split_kernel<true><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
-                                                             P.d_pair_blk, c.p0, M.phT_hi, M.phT_lo);
-    else
-      colloc_split_kernel<false><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
-                                                              P.d_pair_blk, c.p0, M.phT_hi, M.phT_lo);
-    NKX_LAUNCH_CHECK();
-    ++P.launches;
-    Tm.end(s);
-  };
-  // ---- pass A: collocation, density GEMM, contraction
+  // ---- pass A: collocation, int8 density contraction, FP64 rho / grad rho
   for (const Chunk &c : P.chunks) {
-    colloc(c);
-    const long nb = c.b1 - c.b0;
+    const long np = c.p1 - c.p0, nb = c.b1 - c.b0;
+    if (np > 0) {
+      Tm.begin(ST_COLLOC, s);
+      launch_colloc(P, c, s);
+      Tm.end(s);
+    }
     Tm.begin(ST_DENSITY, s);
+    if (np > 0) {
+      const long rows = np * nc * 256;
+      quant_phiT_kernel<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(P.ws_phi, nc, rows, M.qphT, M.sphT);
+      NKX_LAUNCH_CHECK();
+      ++P.launches;
+    }
     TcArgs a{};
     a.mode = TC_MODE_DENSITY;
     a.b0 = c.b0;
@@ -620,14 +672,17 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.pair_blk = P.d_pair_blk;
     a.mask = P.d_mask;
     a.mask_words = P.mask_words;
+    a.nblk = P.nblk;
+    a.sA = M.sphT;
+    a.sB = M.sct;
     a.nspin = nspin;
-    a.ncomp = ncomp;
-    a.ntile_i = M.nocc_pad / 128;
+    a.ncomp = nc;
+    a.ntile_i = M.nocc_pad / 64;
     a.nocc_pad = M.nocc_pad;
     a.T = M.T;
     a.err = M.err;
-    a.nunits = nb * nspin * 2 * ncomp * a.ntile_i;
-    launch_gemm(M, M.m_phT_hi, M.m_phT_lo, M.m_ct_hi, M.m_ct_lo, a, s);
+    a.nunits = nb * nspin * 2 * nc * a.ntile_i;
+    launch_i8(M, M.m_phT, M.m_ct, a, s);
     ++P.launches;
     if (P.gga)
       density_contract_kernel<true><<<dim3((unsigned)nb, nspin), 256, 0, s>>>(M.T, P.d_occ, nocc, M.nocc_pad, nspin,
@@ -653,21 +708,24 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
   NKX_LAUNCH_CHECK();
   ++P.launches;
   Tm.end(s);
-  // ---- pass B: Z and the V contraction
+  // ---- pass B: quantised Phi and Z, int8 V contraction
   NKX_CUDA(cudaMemsetAsync(P.d_V, 0, sizeof(double) * nzs * P.nbf_pad * P.nbf_pad, s));
   for (const Chunk &c : P.chunks) {
     const long np = c.p1 - c.p0;
     if (np <= 0) continue;
-    if (multi) colloc(c);
+    if (multi) {
+      Tm.begin(ST_COLLOC, s);
+      launch_colloc(P, c, s);
+      Tm.end(s);
+    }
     Tm.begin(ST_ZBUILD, s);
+    const size_t zsm = (size_t)(1 + nzs) * 4 * 128 * 64;
     if (P.gga)
-      zbuild_split_kernel<true><<<(unsigned)np, 256, 0, s>>>(M.phT_hi, M.phT_lo, P.d_coef, P.d_vj, P.d_pair_batch,
-                                                             c.p0, nzs, nspin, P.npad, M.ph_hi, M.ph_lo, M.z_hi,
-                                                             M.z_lo);
+      zquant_kernel<true><<<(unsigned)np, 256, zsm, s>>>(P.ws_phi, P.d_coef, P.d_vj, P.d_pair_batch, c.p0, nzs,
+                                                        nspin, P.npad, M.qph, M.sph, M.qz, M.sz);
     else
-      zbuild_split_kernel<false><<<(unsigned)np, 256, 0, s>>>(M.phT_hi, M.phT_lo, P.d_coef, P.d_vj, P.d_pair_batch,
-                                                              c.p0, nzs, nspin, P.npad, M.ph_hi, M.ph_lo, M.z_hi,
-                                                              M.z_lo);
+      zquant_kernel<false><<<(unsigned)np, 256, zsm, s>>>(P.ws_phi, P.d_coef, P.d_vj, P.d_pair_batch, c.p0, nzs,
+                                                         nspin, P.npad, M.qph, M.sph, M.qz, M.sz);
     NKX_LAUNCH_CHECK();
     ++P.launches;
     Tm.end(s);
@@ -684,13 +742,16 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.nblk = P.nblk;
     a.nz = nzs;
     a.nbf_pad = P.nbf_pad;
+    a.sA = M.sph;
+    a.sB = M.sz;
     a.V = P.d_V;
     a.err = M.err;
-    a.nunits = (long)P.nblk * P.nblk * nzs;
-    launch_gemm(M, M.m_ph_hi, M.m_ph_lo, M.m_z_hi, M.m_z_lo, a, s);
+    a.nunits = (long)nzs * P.nblk * 2 * P.nblk;
+    launch_i8(M, M.m_ph, M.m_z, a, s);
     ++P.launches;
     Tm.end(s);
   }
+  (void)tile;
   int herr = 0;
   NKX_CUDA(cudaMemcpyAsync(&herr, M.err, sizeof(int), cudaMemcpyDeviceToHost, s));
   NKX_CUDA(cudaStreamSynchronize(s));

@@ -70,6 +70,14 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
 }
+// 3-D TMA box load (x innermost), completing on `bar`.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
 __device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
@@ -97,6 +105,30 @@ __device__ __forceinline__ uint64_t smem_desc_k128(uint32_t saddr) {
   return lo | (hi << 32);
 }
 
+// K-major tile with 64-byte swizzle (rows of 64 B, 8-row atoms of 512 B):
+// LBO field 1, SBO 512 B, version 1, layout type SWIZZLE_64B (4).
+__device__ __forceinline__ uint64_t smem_desc_k64(uint32_t saddr) {
+  const uint64_t lo = (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16);
+  const uint64_t hi = (uint64_t)(512u >> 4) | ((uint64_t)1u << 14) | ((uint64_t)4u << 29);
+  return lo | (hi << 32);
+}
+
+// Instruction descriptor of kind::i8: signed int8 A and B, S32 accumulator,
+// both operands K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 // Instruction descriptor of kind::tf32, FP32 accumulator, both operands
 // K-major, M x N.
 __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
@@ -116,6 +148,19 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint6
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
+}
+
+// 32 lanes x 32 columns of 32-bit words from TMEM (lane base in bits 31:16)
+__device__ __forceinline__ void tmem_ld32u(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
 // 32 lanes x 32 columns of FP32 from TMEM (lane base in bits 31:16 of taddr)
@@ -146,6 +191,35 @@ __device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
   const float xf = (float)x;
   hi = to_tf32(xf);
   lo = to_tf32((float)(x - (double)hi));
+}
+
+// Exact integer decomposition used by the int8 tensor-core contractions:
+// x / 2^E with 2^E >= max|row| is rounded to a 27-bit integer X and written
+// as X = d0 2^21 + d1 2^14 + d2 2^7 + d3 with balanced digits d in [-65, 64].
+__device__ __forceinline__ void digits4(double x, double inv_scale, int8_t &d0, int8_t &d1, int8_t &d2, int8_t &d3) {
+  long long X = __double2ll_rn(x * inv_scale * 134217728.0);
+  long long r;
+  r = ((X + 64) & 127) - 64;
+  d3 = (int8_t)r;
+  X = (X - r) >> 7;
+  r = ((X + 64) & 127) - 64;
+  d2 = (int8_t)r;
+  X = (X - r) >> 7;
+  r = ((X + 64) & 127) - 64;
+  d1 = (int8_t)r;
+  X = (X - r) >> 7;
+  d0 = (int8_t)X;
+}
+// power-of-two scale 2^E >= m (E from frexp; 1 for m == 0), as its inverse
+__device__ __forceinline__ double inv_pow2_scale(double m, double &scale) {
+  if (!(m > 0.0)) {
+    scale = 1.0;
+    return 1.0;
+  }
+  int e;
+  frexp(m, &e);
+  scale = ldexp(1.0, e);
+  return ldexp(1.0, -e);
 }
 
 }  // namespace tc
