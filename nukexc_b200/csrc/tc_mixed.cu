@@ -6,15 +6,15 @@
 //   V        Vbar(mu, nu) += sum_g Phi(mu, g) Z(nu, g)    per (batch, block) pair
 // (density.hpp:188-255, xc_integrals.hpp:424-726), run on one
 // warp-specialised tcgen05 kernel of kind::i8.  Every operand row r of a
-// tile is scaled by a power of two s_r >= max|row| and rounded to a 27-bit
-// integer written as four balanced base-128 digits (digits4, tc_ptx.cuh).
+// tile is scaled by a power of two s_r >= max|row| and rounded to a 31-bit
+// integer written as four balanced base-256 digits (digits4, tc_ptx.cuh).
 // A contraction over K is then
-//   sum_k a_k b_k = s_a s_b 2^-54 sum_{L=0..3} 2^(7(6-L)) Acc_L,
+//   sum_k a_k b_k = s_a s_b 2^-60 sum_{L=0..3} 2^(8(6-L)) Acc_L,
 //   Acc_L = sum_k sum_{i+j=L} d_i(a_k) d_j(b_k)            (int32, exact)
 // i.e. ten int8 MMAs per K step into four int32 TMEM accumulators, combined
 // in FP64 after every accumulation group (one 256-point batch for V, one
-// 128-function block for the density).  Products with i + j >= 4 (below
-// 2^-28 of s_a s_b) are dropped; everything kept is exact, so unlike FP32
+// 128-function block for the density).  Products with i + j >= 4 (at most
+// 2^-30 s_a s_b each) are dropped; everything kept is exact, so unlike FP32
 // tensor-core accumulation the result carries no rounding bias.
 //
 // Roles (320 threads): warp 0 lane 0 issues 3-D TMA loads of the four digit
@@ -42,7 +42,7 @@ constexpr int kBBytes = 4 * 64 * 64;   // four digit planes, 64 rows x 64 B
 constexpr int kStageBytes = kABytes + kBBytes;
 constexpr int kGemmThreads = 320;
 constexpr uint32_t kIdesc = idesc_i8(128, 64);
-constexpr double kTwoM54 = 5.551115123125783e-17;  // 2^-54
+constexpr double kTwoM60 = 8.673617379884035e-19;  // 2^-60
 
 enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1 };
 
@@ -274,21 +274,21 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         size_t sbs = 1;
         if (live) {
           if (a.mode == TC_MODE_V) {
-            sa = a.sA[g.qa * 128 + row] * kTwoM54;
+            sa = a.sA[g.qa * 128 + row] * kTwoM60;
             sb = a.sB + (g.qb * a.nz + it.zi) * 128 + 64 * (it.J & 1) + 32 * hc;
           } else {
-            sa = a.sA[(g.qa * a.ncomp + it.c) * 256 + 128 * it.h + row] * kTwoM54;
+            sa = a.sA[(g.qa * a.ncomp + it.c) * 256 + 128 * it.h + row] * kTwoM60;
             sb = a.sB + ((size_t)it.s * a.nocc_pad + 64 * it.t + 32 * hc) * a.nblk + g.blk;
             sbs = a.nblk;
           }
         }
-        // level L carries weight 2^(7 (3 - L)) relative to the 2^-54 s_a s_b unit
+        // level L carries weight 2^(8 (6 - L)) relative to the 2^-60 s_a s_b unit
 #pragma unroll
         for (int L = 0; L < 4; ++L) {
           uint32_t v[32];
           tmem_ld32u(tmem + lane_addr + buf * 256 + L * 64 + 32 * hc, v);
           if (live) {
-            const double wl = sa * (double)(1 << (7 * (3 - L)));
+            const double wl = sa * ldexp(1.0, 8 * (6 - L));
 #pragma unroll
             for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], wl * sb[j * sbs], acc[j]);
           }

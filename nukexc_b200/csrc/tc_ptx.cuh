@@ -194,20 +194,21 @@ __device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
 }
 
 // Exact integer decomposition used by the int8 tensor-core contractions:
-// x / 2^E with 2^E >= max|row| is rounded to a 27-bit integer X and written
-// as X = d0 2^21 + d1 2^14 + d2 2^7 + d3 with balanced digits d in [-65, 64].
+// x / 2^E with 2^E >= max|row| is rounded to a 31-bit integer
+// X = RN(x 2^(30-E)) and written as X = d0 2^24 + d1 2^16 + d2 2^8 + d3 with
+// balanced digits d1..d3 in [-128, 127] and d0 in [-65, 65].
 __device__ __forceinline__ void digits4(double x, double inv_scale, int8_t &d0, int8_t &d1, int8_t &d2, int8_t &d3) {
-  long long X = __double2ll_rn(x * inv_scale * 134217728.0);
+  long long X = __double2ll_rn(x * inv_scale * 1073741824.0);
   long long r;
-  r = ((X + 64) & 127) - 64;
+  r = ((X + 128) & 255) - 128;
   d3 = (int8_t)r;
-  X = (X - r) >> 7;
-  r = ((X + 64) & 127) - 64;
+  X = (X - r) >> 8;
+  r = ((X + 128) & 255) - 128;
   d2 = (int8_t)r;
-  X = (X - r) >> 7;
-  r = ((X + 64) & 127) - 64;
+  X = (X - r) >> 8;
+  r = ((X + 128) & 255) - 128;
   d1 = (int8_t)r;
-  X = (X - r) >> 7;
+  X = (X - r) >> 8;
   d0 = (int8_t)X;
 }
 // power-of-two scale 2^E >= m (E from frexp; 1 for m == 0), as its inverse
