@@ -149,9 +149,11 @@ NKX_HD inline Dual<N> datan(const Dual<N> &a) {
 }
 
 // ------------------------------------------------------------ formulas ----
+// f(zeta) of the spin interpolation, from 1 + zeta = 2 ra / rho and
+// 1 - zeta = 2 rb / rho (no cancellation at zeta -> +-1)
 template <class T>
-NKX_HD inline T fzeta(const T &zeta) {
-  return (dpow(1.0 + zeta, 4.0 / 3.0) + dpow(1.0 - zeta, 4.0 / 3.0) - 2.0) / (pow(2.0, 4.0 / 3.0) - 2.0);
+NKX_HD inline T fzeta(const T &opz, const T &omz) {
+  return (dpow(opz, 4.0 / 3.0) + dpow(omz, 4.0 / 3.0) - 2.0) / (pow(2.0, 4.0 / 3.0) - 2.0);
 }
 
 template <class T>
@@ -176,11 +178,12 @@ NKX_HD inline T f_vwn5(const T &ra, const T &rb) {
   const T rs = dpow(3.0 / (4.0 * kPi * rho), 1.0 / 3.0);
   const T x = dsqrt(rs);
   const T zeta = (ra - rb) / rho;
+  const T opz = 2.0 * ra / rho, omz = 2.0 * rb / rho;
   const T eP = vwn_g(x, 0.0310907, 3.72744, 12.9352, -0.10498);
   const T eF = vwn_g(x, 0.01554535, 7.06042, 18.0578, -0.32500);
   const T eA = vwn_g(x, -1.0 / (6.0 * kPi * kPi), 1.13107, 13.0045, -0.0047584);
   const double fpp0 = 4.0 / (9.0 * (cbrt(2.0) - 1.0));
-  const T fz = fzeta(zeta);
+  const T fz = fzeta(opz, omz);
   const T z2 = zeta * zeta;
   const T z4 = z2 * z2;
   return rho * (eP + eA * fz * (1.0 / fpp0) * (1.0 - z4) + (eF - eP) * fz * z4);
@@ -194,12 +197,12 @@ NKX_HD inline T pw92_g(const T &rs, double A, double a1, double b1, double b2, d
 }
 
 template <class T>
-NKX_HD inline T eps_pw92(const T &rs, const T &zeta) {
+NKX_HD inline T eps_pw92(const T &rs, const T &zeta, const T &opz, const T &omz) {
   const T gP = pw92_g(rs, 0.0310907, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294);
   const T gF = pw92_g(rs, 0.01554535, 0.20548, 14.1189, 6.1977, 3.3662, 0.62517);
   const T gA = pw92_g(rs, 0.0168869, 0.11125, 10.357, 3.6231, 0.88026, 0.49671);
   const double fz20 = 1.709920934161365617563962776245;
-  const T fz = fzeta(zeta);
+  const T fz = fzeta(opz, omz);
   const T z2 = zeta * zeta;
   const T z4 = z2 * z2;
   return gP - gA * fz * (1.0 / fz20) * (1.0 - z4) + (gF - gP) * fz * z4;
@@ -225,9 +228,10 @@ NKX_HD inline T f_pbe_c(const T &ra, const T &rb, const T &sigma) {
   const double gamma = (1.0 - log(2.0)) / (kPi * kPi);
   const T rho = ra + rb;
   const T zeta = (ra - rb) / rho;
+  const T opz = 2.0 * ra / rho, omz = 2.0 * rb / rho;
   const T rs = dpow(3.0 / (4.0 * kPi * rho), 1.0 / 3.0);
-  const T ec = eps_pw92(rs, zeta);
-  const T phi = 0.5 * (dpow(1.0 + zeta, 2.0 / 3.0) + dpow(1.0 - zeta, 2.0 / 3.0));
+  const T ec = eps_pw92(rs, zeta, opz, omz);
+  const T phi = 0.5 * (dpow(opz, 2.0 / 3.0) + dpow(omz, 2.0 / 3.0));
   const T kF = dpow(3.0 * kPi * kPi * rho, 1.0 / 3.0);
   const T ks2 = 4.0 * kF / kPi;
   const T t2 = sigma / (4.0 * phi * phi * ks2 * rho * rho);

@@ -169,20 +169,21 @@ cplx vwn_g(cplx x, double A, double b, double c, double x0) {
   return A * (std::log(x * x / X) + 2.0 * b / Q * at -
               b * x0 / X0 * (std::log((x - x0) * (x - x0) / X) + 2.0 * (b + 2.0 * x0) / Q * at));
 }
-cplx fzeta(cplx zeta) {
-  return (std::pow(1.0 + zeta, 4.0 / 3.0) + std::pow(1.0 - zeta, 4.0 / 3.0) - 2.0) /
-         (std::pow(2.0, 4.0 / 3.0) - 2.0);
+// f(zeta) from 1 + zeta = 2 ra / rho, 1 - zeta = 2 rb / rho (exact at zeta -> +-1)
+cplx fzeta(cplx opz, cplx omz) {
+  return (std::pow(opz, 4.0 / 3.0) + std::pow(omz, 4.0 / 3.0) - 2.0) / (std::pow(2.0, 4.0 / 3.0) - 2.0);
 }
 cplx f_vwn5(cplx ra, cplx rb) {
   const cplx rho = ra + rb;
   const cplx rs = cbrt_c(3.0 / (4.0 * kPi * rho));
   const cplx x = std::sqrt(rs);
   const cplx zeta = (ra - rb) / rho;
+  const cplx opz = 2.0 * ra / rho, omz = 2.0 * rb / rho;
   const cplx eP = vwn_g(x, 0.0310907, 3.72744, 12.9352, -0.10498);
   const cplx eF = vwn_g(x, 0.01554535, 7.06042, 18.0578, -0.32500);
   const cplx eA = vwn_g(x, -1.0 / (6.0 * kPi * kPi), 1.13107, 13.0045, -0.0047584);
   const double fpp0 = 4.0 / (9.0 * (std::cbrt(2.0) - 1.0));
-  const cplx fz = fzeta(zeta);
+  const cplx fz = fzeta(opz, omz);
   const cplx z4 = zeta * zeta * zeta * zeta;
   return rho * (eP + eA * fz / fpp0 * (1.0 - z4) + (eF - eP) * fz * z4);
 }
@@ -193,12 +194,12 @@ cplx pw92_g(cplx rs, double A, double a1, double b1, double b2, double b3, doubl
   const cplx den = 2.0 * A * (b1 * srs + b2 * rs + b3 * rs * srs + b4 * rs * rs);
   return -2.0 * A * (1.0 + a1 * rs) * std::log(1.0 + 1.0 / den);
 }
-cplx eps_pw92(cplx rs, cplx zeta) {
+cplx eps_pw92(cplx rs, cplx zeta, cplx opz, cplx omz) {
   const cplx gP = pw92_g(rs, 0.0310907, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294);
   const cplx gF = pw92_g(rs, 0.01554535, 0.20548, 14.1189, 6.1977, 3.3662, 0.62517);
   const cplx gA = pw92_g(rs, 0.0168869, 0.11125, 10.357, 3.6231, 0.88026, 0.49671);
   const double fz20 = 1.709920934161365617563962776245;
-  const cplx fz = fzeta(zeta);
+  const cplx fz = fzeta(opz, omz);
   const cplx z4 = zeta * zeta * zeta * zeta;
   return gP - gA * fz / fz20 * (1.0 - z4) + (gF - gP) * fz * z4;
 }
@@ -222,9 +223,10 @@ cplx f_pbe_c(cplx ra, cplx rb, cplx sigma) {
   const double gamma = (1.0 - std::log(2.0)) / (kPi * kPi);
   const cplx rho = ra + rb;
   const cplx zeta = (ra - rb) / rho;
+  const cplx opz = 2.0 * ra / rho, omz = 2.0 * rb / rho;
   const cplx rs = cbrt_c(3.0 / (4.0 * kPi * rho));
-  const cplx ec = eps_pw92(rs, zeta);
-  const cplx phi = 0.5 * (std::pow(1.0 + zeta, 2.0 / 3.0) + std::pow(1.0 - zeta, 2.0 / 3.0));
+  const cplx ec = eps_pw92(rs, zeta, opz, omz);
+  const cplx phi = 0.5 * (std::pow(opz, 2.0 / 3.0) + std::pow(omz, 2.0 / 3.0));
   const cplx kF = cbrt_c(3.0 * kPi * kPi * rho);
   const cplx ks = std::sqrt(4.0 * kF / kPi);
   const cplx t2 = sigma / (4.0 * phi * phi * ks * ks * rho * rho);
