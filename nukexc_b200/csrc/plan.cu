@@ -76,9 +76,10 @@ static unsigned nblk(long n, int t) { return (unsigned)((n + t - 1) / t); }
 // ========================================================== kernels ======
 
 // Collocation of one (batch, function block) pair per CTA.  Lane l of a warp
-// owns functions f = l + 32c (c < 4) of the block; warp w owns points
-// g = w + 8j.  Each store of 32 consecutive f is coalesced.  Output
-// PhiT[pair][comp][g][f], comp 0 = value, 1..3 = gradient (GRAD only).
+// owns the four consecutive functions f = 4l .. 4l+3 of the block (so the
+// functions of a shell share one radial factor, RadialCache); warp w owns
+// points g = w + 8j.  Output PhiT[pair][comp][g][f], comp 0 = value,
+// 1..3 = gradient (GRAD only); each warp store covers 32 x 4 consecutive f.
 template <bool GRAD>
 __global__ void __launch_bounds__(256) colloc_fp64_kernel(const StoFunc *__restrict__ sto, const double *__restrict__ px,
                                                           const double *__restrict__ py, const double *__restrict__ pz,
@@ -97,24 +98,26 @@ __global__ void __launch_bounds__(256) colloc_fp64_kernel(const StoFunc *__restr
   __syncthreads();
   StoFunc f[4];
 #pragma unroll
-  for (int c = 0; c < 4; ++c) f[c] = sto[I * kBlockF + lane + 32 * c];
+  for (int c = 0; c < 4; ++c) f[c] = sto[I * kBlockF + 4 * lane + c];
   const size_t tile = (size_t)kBatch * kBlockF;
   double *o = out + (size_t)blockIdx.x * (GRAD ? 4 : 1) * tile;
   for (int g = warp; g < kBatch; g += 8) {
     const double x = sx[g], y = sy[g], z = sz[g];
+    RadialCache rc;
+    double v[4][4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const size_t idx = (size_t)g * kBlockF + lane + 32 * c;
-      if (GRAD) {
-        double v, gx, gy, gz;
-        sto_value_grad(f[c], x, y, z, v, gx, gy, gz);
-        o[idx] = v;
-        o[tile + idx] = gx;
-        o[2 * tile + idx] = gy;
-        o[3 * tile + idx] = gz;
-      } else {
-        o[idx] = sto_value(f[c], x, y, z);
-      }
+      if (GRAD)
+        sto_value_grad_cached(f[c], x, y, z, rc, v[0][c], v[1][c], v[2][c], v[3][c]);
+      else
+        v[0][c] = sto_value_cached(f[c], x, y, z, rc);
+    }
+    const size_t idx = (size_t)g * kBlockF + 4 * lane;
+#pragma unroll
+    for (int k = 0; k < (GRAD ? 4 : 1); ++k) {
+      double2 *dst = reinterpret_cast<double2 *>(o + k * tile + idx);
+      dst[0] = make_double2(v[k][0], v[k][1]);
+      dst[1] = make_double2(v[k][2], v[k][3]);
     }
   }
 }

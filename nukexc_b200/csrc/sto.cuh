@@ -48,4 +48,124 @@ NKX_HD inline void sto_value_grad(const StoFunc &f, double px, double py, double
   gz = R * sz + s * dz * cR;
 }
 
+// Radial factor cache for consecutive functions of one lane: functions of a
+// shell (same centre, zeta and n - l - 1) share r, R(r) and dR/dr / r.
+struct RadialCache {
+  double cx = 1e300, cy = 0, cz = 0, zeta = -1;
+  int k = -1;
+  double r, R, cR;
+};
+
+// value + gradient reusing the radial factor of the previous call when the
+// function shares centre, zeta and k with it (same results as sto_value_grad)
+NKX_HD inline void sto_value_grad_cached(const StoFunc &f, double px, double py, double pz, RadialCache &rc,
+                                         double &v, double &gx, double &gy, double &gz) {
+  const double dx = px - f.cx, dy = py - f.cy, dz = pz - f.cz;
+  if (!(f.cx == rc.cx && f.cy == rc.cy && f.cz == rc.cz && f.zeta == rc.zeta && f.k == rc.k)) {
+    rc.cx = f.cx;
+    rc.cy = f.cy;
+    rc.cz = f.cz;
+    rc.zeta = f.zeta;
+    rc.k = f.k;
+    rc.r = sqrt(dx * dx + dy * dy + dz * dz);
+    rc.R = ipow(rc.r, f.k) * exp(-f.zeta * rc.r);
+    rc.cR = rc.r > 0.0 ? (f.k / rc.r - f.zeta) / rc.r : 0.0;
+  }
+  const double R = f.norm * rc.R;
+  double s, sx, sy, sz;
+  solid_harmonic_grad(f.l, f.m, dx, dy, dz, s, sx, sy, sz);
+  v = R * s;
+  const double cR = rc.cR * R;
+  gx = R * sx + s * dx * cR;
+  gy = R * sy + s * dy * cR;
+  gz = R * sz + s * dz * cR;
+}
+
+NKX_HD inline double sto_value_cached(const StoFunc &f, double px, double py, double pz, RadialCache &rc) {
+  const double dx = px - f.cx, dy = py - f.cy, dz = pz - f.cz;
+  if (!(f.cx == rc.cx && f.cy == rc.cy && f.cz == rc.cz && f.zeta == rc.zeta && f.k == rc.k)) {
+    rc.cx = f.cx;
+    rc.cy = f.cy;
+    rc.cz = f.cz;
+    rc.zeta = f.zeta;
+    rc.k = f.k;
+    rc.r = sqrt(dx * dx + dy * dy + dz * dz);
+    rc.R = ipow(rc.r, f.k) * exp(-f.zeta * rc.r);
+    rc.cR = 0.0;
+  }
+  return f.norm * rc.R * solid_harmonic(f.l, f.m, dx, dy, dz);
+}
+
+#ifdef __CUDACC__
+// One 128-function block in shared memory, laid out for kernels in which lane
+// l of a warp evaluates functions 4l .. 4l+3: field[c][l] holds function
+// 4l + c, so the 32 reads of one field by a warp are consecutive.  same[c][l]
+// is 1 when function 4l + c shares centre, zeta and n - l - 1 with function
+// 4l + c - 1 (the radial factor is then reused).  Keeping the table here
+// instead of in registers leaves room for the per-point operands.
+struct BlockFuncs {
+  double cx[4][32], cy[4][32], cz[4][32], zeta[4][32], norm[4][32];
+  int k[4][32], l[4][32], m[4][32], same[4][32];
+};
+
+// fill B from functions [I*128, I*128 + 128) of sto; the caller synchronises
+__device__ inline void load_block_funcs(BlockFuncs &B, const StoFunc *__restrict__ sto, int I, int tid, int nthr) {
+  for (int t = tid; t < 128; t += nthr) {
+    const int lane = t >> 2, c = t & 3;
+    const StoFunc f = sto[I * 128 + t];
+    B.cx[c][lane] = f.cx;
+    B.cy[c][lane] = f.cy;
+    B.cz[c][lane] = f.cz;
+    B.zeta[c][lane] = f.zeta;
+    B.norm[c][lane] = f.norm;
+    B.k[c][lane] = f.k;
+    B.l[c][lane] = f.l;
+    B.m[c][lane] = f.m;
+    int same = 0;
+    if (c > 0) {
+      const StoFunc &g = sto[I * 128 + t - 1];
+      same = (f.cx == g.cx && f.cy == g.cy && f.cz == g.cz && f.zeta == g.zeta && f.k == g.k) ? 1 : 0;
+    }
+    B.same[c][lane] = same;
+  }
+}
+
+// bit c set when function 4 lane + c reuses the radial factor of 4 lane + c - 1
+__device__ inline unsigned block_funcs_same_mask(const BlockFuncs &B, int lane) {
+  return (unsigned)B.same[1][lane] << 1 | (unsigned)B.same[2][lane] << 2 | (unsigned)B.same[3][lane] << 3;
+}
+
+// the four functions of one lane at one point: values v[c] and, with GRAD,
+// gradients gx/gy/gz[c]; same arithmetic as sto_value(_grad)_cached
+template <bool GRAD>
+__device__ __forceinline__ void block_funcs_eval4(const BlockFuncs &B, int lane, unsigned same, double x, double y,
+                                                  double z, double v[4], double gx[4], double gy[4], double gz[4]) {
+  double dx = 0, dy = 0, dz = 0, Rr = 0, cRr = 0;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    if (c == 0 || !((same >> c) & 1)) {
+      dx = x - B.cx[c][lane];
+      dy = y - B.cy[c][lane];
+      dz = z - B.cz[c][lane];
+      const double r = sqrt(dx * dx + dy * dy + dz * dz);
+      const int k = B.k[c][lane];
+      Rr = ipow(r, k) * exp(-B.zeta[c][lane] * r);
+      if (GRAD) cRr = r > 0.0 ? (k / r - B.zeta[c][lane]) / r : 0.0;
+    }
+    const double R = B.norm[c][lane] * Rr;
+    if (GRAD) {
+      double s, sx, sy, sz;
+      solid_harmonic_grad(B.l[c][lane], B.m[c][lane], dx, dy, dz, s, sx, sy, sz);
+      v[c] = R * s;
+      const double cR = cRr * R;
+      gx[c] = R * sx + s * dx * cR;
+      gy[c] = R * sy + s * dy * cR;
+      gz[c] = R * sz + s * dz * cR;
+    } else {
+      v[c] = R * solid_harmonic(B.l[c][lane], B.m[c][lane], dx, dy, dz);
+    }
+  }
+}
+#endif
+
 }  // namespace nkx

@@ -342,29 +342,6 @@ __device__ __forceinline__ void quant4(const double v[4], double inv, uint32_t w
   for (int p = 0; p < 4; ++p) w[p] = pack4(d[p][0], d[p][1], d[p][2], d[p][3]);
 }
 
-// Density operand A: rows (pair, comp, g) of PhiT over the 128 functions of
-// the block, one warp per row.  qphT[pair][comp][digit][g][f], sphT[pair][comp][g].
-__global__ void quant_phiT_kernel(const double *__restrict__ phiT, int nc, long nrows, uint8_t *__restrict__ q,
-                                  double *__restrict__ sc) {
-  const long r = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (r >= nrows) return;
-  const long pc = r / 256;  // pair * nc + comp
-  const int g = (int)(r % 256);
-  const double *src = phiT + r * 128 + 4 * lane;
-  double v[4] = {src[0], src[1], src[2], src[3]};
-  const double m = warp_max(fmax(fmax(fabs(v[0]), fabs(v[1])), fmax(fabs(v[2]), fabs(v[3]))));
-  double s;
-  const double inv = inv_pow2_scale(m, s);
-  uint32_t w[4];
-  quant4(v, inv, w);
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-    reinterpret_cast<uint32_t *>(q + ((pc * 4 + p) * 256 + g) * 128)[lane] = w[p];
-  if (lane == 0) sc[r] = s;
-  (void)nc;
-}
-
 // Density operand B: orbital rows (spin, i) over each 128-function block.
 // qct[spin][digit][i][f], sct[spin][i][blk]; rows i >= nocc are zero.
 __global__ void quant_ct_kernel(const double *__restrict__ Ct, int nocc, int nocc_pad, int nspin, int nbf_pad,
@@ -390,94 +367,182 @@ __global__ void quant_ct_kernel(const double *__restrict__ Ct, int nocc, int noc
   if (lane == 0) sc[((size_t)s * nocc_pad + i) * nblk + blk] = scl;
 }
 
-// V operands of one (batch, block) pair: Phi (value) and Z_z (z < nz: the
-// XC coefficients c0 phi + c . grad phi, z == nspin for a separate J:
-// 1/2 vJ phi), each row f scaled over the 256 points and written transposed
-// as qph[pair][digit][f][g], qz[pair][z][digit][f][g] with scales sph, sz.
+// Pass A, fused: collocation of one (batch, block) pair straight into the
+// density operand digits.  Lane l owns functions f = 4l .. 4l+3, warp w the
+// points g = w + 8j; the row scale of (comp, g) over the 128 functions of
+// the block is a warp maximum.  qphT[pair][comp][digit][g][f],
+// sphT[pair][comp][g].
 template <bool GRAD>
-__global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ phiT, const double *__restrict__ coef,
-                                                     const double *__restrict__ vj, const int *__restrict__ pair_batch,
-                                                     long p0, int nz, int nspin, long npad, uint8_t *__restrict__ qph,
-                                                     double *__restrict__ sph, uint8_t *__restrict__ qz,
-                                                     double *__restrict__ sz) {
+__global__ void __launch_bounds__(256) colloc_quantT_kernel(const StoFunc *__restrict__ sto, const double *__restrict__ px,
+                                                            const double *__restrict__ py, const double *__restrict__ pz,
+                                                            const int *__restrict__ pair_batch,
+                                                            const int *__restrict__ pair_blk, long p0,
+                                                            uint8_t *__restrict__ q, double *__restrict__ sc) {
   constexpr int NC = GRAD ? 4 : 1;
-  extern __shared__ __align__(16) uint8_t tile[];  // [(1 + nz)][4][128][64]
-  __shared__ double mx[2][4][128];
-  const long q = blockIdx.x;
-  const int b = pair_batch[p0 + q];
+  const long p = p0 + blockIdx.x;
+  const int b = pair_batch[p], I = pair_blk[p];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ double sx[kBatch], sy[kBatch], sz[kBatch];
+  __shared__ BlockFuncs B;
+  for (int g = threadIdx.x; g < kBatch; g += blockDim.x) {
+    sx[g] = px[(long)b * kBatch + g];
+    sy[g] = py[(long)b * kBatch + g];
+    sz[g] = pz[(long)b * kBatch + g];
+  }
+  load_block_funcs(B, sto, I, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const long qrel = blockIdx.x;
+  const unsigned same = block_funcs_same_mask(B, lane);
+  for (int g = warp; g < kBatch; g += 8) {
+    double v[4][4];
+    block_funcs_eval4<GRAD>(B, lane, same, sx[g], sy[g], sz[g], v[0], v[1], v[2], v[3]);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) {
+      const double m = warp_max(fmax(fmax(fabs(v[k][0]), fabs(v[k][1])), fmax(fabs(v[k][2]), fabs(v[k][3]))));
+      double s;
+      const double inv = inv_pow2_scale(m, s);
+      uint32_t w[4];
+      quant4(v[k], inv, w);
+      const long pc = qrel * NC + k;
+#pragma unroll
+      for (int d = 0; d < 4; ++d) reinterpret_cast<uint32_t *>(q + ((pc * 4 + d) * 256 + g) * 128)[lane] = w[d];
+      if (lane == 0) sc[pc * 256 + g] = s;
+    }
+  }
+}
+
+// Pass B, part 1: collocation of one (batch, block) pair and the operand
+// values of the V contraction, o = 0: phi, o = 1 + z: Z_z (z < nspin:
+// c0 phi + c . grad phi with the functional's per-point coefficients;
+// z == nspin for a separate J: 1/2 vJ phi), written as FP64 ws[pair][o][g][f]
+// (lane l owns f = 4l .. 4l+3, warp w the points g = w + 8j), together with
+// the row scale of every (o, f) over the 256 points: sph[pair][f],
+// sz[pair][z][f].
+template <bool GRAD, int NZ>
+__global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restrict__ sto, const double *__restrict__ px,
+                                                       const double *__restrict__ py, const double *__restrict__ pz,
+                                                       const int *__restrict__ pair_batch,
+                                                       const int *__restrict__ pair_blk, long p0,
+                                                       const double *__restrict__ coef, const double *__restrict__ vj,
+                                                       int nspin, long npad, double *__restrict__ ws,
+                                                       double *__restrict__ sph, double *__restrict__ szs) {
+  __shared__ double red[8][4][128];
+  const long p = p0 + blockIdx.x, qrel = blockIdx.x;
+  const int b = pair_batch[p], I = pair_blk[p];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int nz = NZ, nop = 1 + NZ;
   const size_t T = (size_t)kBatch * kBlockF;
-  const double *P = phiT + q * NC * T;
+  __shared__ BlockFuncs B;
+  load_block_funcs(B, sto, I, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const unsigned same = block_funcs_same_mask(B, lane);
+  double m[nop][4];
+#pragma unroll
+  for (int o = 0; o < nop; ++o)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) m[o][c] = 0.0;
+  double *out = ws + qrel * 4 * T;
+  for (int g = warp; g < kBatch; g += 8) {
+    const long gg = (long)b * kBatch + g;
+    const double x = px[gg], y = py[gg], z = pz[gg];
+    double cf[NZ][4];
+#pragma unroll
+    for (int s = 0; s < NZ; ++s) {
+      cf[s][0] = cf[s][1] = cf[s][2] = cf[s][3] = 0.0;
+      if (s < nspin) {
+        const double *cs = coef + (size_t)s * 4 * npad;
+        cf[s][0] = cs[gg];
+        if (GRAD) {
+          cf[s][1] = cs[npad + gg];
+          cf[s][2] = cs[2 * npad + gg];
+          cf[s][3] = cs[3 * npad + gg];
+        }
+      } else {
+        cf[s][0] = 0.5 * vj[gg];
+      }
+    }
+    double v[nop][4], gx[4], gy[4], gz[4];
+    block_funcs_eval4<GRAD>(B, lane, same, x, y, z, v[0], gx, gy, gz);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double val = v[0][c];
+#pragma unroll
+      for (int s = 0; s < NZ; ++s) {
+        v[1 + s][c] = cf[s][0] * val;
+        if (GRAD) v[1 + s][c] += cf[s][1] * gx[c] + cf[s][2] * gy[c] + cf[s][3] * gz[c];
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < nop; ++o) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) m[o][c] = fmax(m[o][c], fabs(v[o][c]));
+      double2 *dst = reinterpret_cast<double2 *>(out + o * T + (size_t)g * kBlockF + 4 * lane);
+      dst[0] = make_double2(v[o][0], v[o][1]);
+      dst[1] = make_double2(v[o][2], v[o][3]);
+    }
+  }
+#pragma unroll
+  for (int o = 0; o < nop; ++o)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) red[warp][o][4 * lane + c] = m[o][c];
+  __syncthreads();
+  for (int e = threadIdx.x; e < nop * 128; e += 256) {
+    const int o = e / 128, ff = e % 128;
+    double mm = 0.0;
+    for (int w = 0; w < 8; ++w) mm = fmax(mm, red[w][o][ff]);
+    double s;
+    inv_pow2_scale(mm, s);
+    if (o == 0)
+      sph[qrel * 128 + ff] = s;
+    else
+      szs[(qrel * nz + (o - 1)) * 128 + ff] = s;
+  }
+}
+
+// Pass B, part 2: digits of the V operands, transposed to
+// qph[pair][digit][f][g] and qz[pair][z][digit][f][g] through a shared
+// tile in slabs of 64 points (rows padded to 68 bytes: conflict-free).
+__global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ ws, const double *__restrict__ sph,
+                                                     const double *__restrict__ szs, int nz, uint8_t *__restrict__ qph,
+                                                     uint8_t *__restrict__ qz) {
+  extern __shared__ __align__(16) uint8_t tile[];  // [(1 + nz)][4][128][68]
+  const long q = blockIdx.x;
+  const size_t T = (size_t)kBatch * kBlockF;
   const int f = threadIdx.x & 127, gs = threadIdx.x >> 7;
   const int nop = 1 + nz;
-  auto values = [&](int g, double out[4]) {
-    const size_t e = (size_t)g * kBlockF + f;
-    const double v = P[e];
-    double dx = 0, dy = 0, dz = 0;
-    if (GRAD) {
-      dx = P[T + e];
-      dy = P[2 * T + e];
-      dz = P[3 * T + e];
-    }
-    const long gg = (long)b * kBatch + g;
-    out[0] = v;
-    for (int z = 0; z < 3; ++z) {
-      double r = 0.0;
-      if (z < nspin) {
-        const double *c = coef + (size_t)z * 4 * npad;
-        r = c[gg] * v;
-        if (GRAD) r += c[npad + gg] * dx + c[2 * npad + gg] * dy + c[3 * npad + gg] * dz;
-      } else if (z < nz) {
-        r = 0.5 * vj[gg] * v;
-      }
-      out[1 + z] = r;
-    }
-  };
-  // pass 1: row maxima over the 256 points
-  double m[4] = {0, 0, 0, 0};
-  for (int g = gs; g < kBatch; g += 2) {
-    double v[4];
-    values(g, v);
-    for (int o = 0; o < 4; ++o) m[o] = fmax(m[o], fabs(v[o]));
-  }
-  for (int o = 0; o < 4; ++o) mx[gs][o][f] = m[o];
-  __syncthreads();
-  double inv[4];
+  double inv[4] = {1.0, 1.0, 1.0, 1.0};
+#pragma unroll
   for (int o = 0; o < 4; ++o) {
-    double s;
-    inv[o] = inv_pow2_scale(fmax(mx[0][o][f], mx[1][o][f]), s);
-    if (gs == 0 && o < nop) {
-      if (o == 0)
-        sph[q * 128 + f] = s;
-      else
-        sz[(q * nz + (o - 1)) * 128 + f] = s;
-    }
+    if (o >= nop) break;
+    const double s = (o == 0) ? sph[q * 128 + f] : szs[(q * nz + (o - 1)) * 128 + f];
+    inv[o] = 1.0 / s;  // exact: s is a power of two
   }
-  // pass 2: digits, transposed through shared memory in slabs of 64 points
+  const double *src = ws + q * 4 * T;
   for (int g0 = 0; g0 < kBatch; g0 += 64) {
     for (int k = 0; k < 32; ++k) {
       const int gl = gs + 2 * k;
-      double v[4];
-      values(g0 + gl, v);
-      for (int o = 0; o < nop; ++o) {
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        if (o >= nop) break;
+        const double v = src[o * T + (size_t)(g0 + gl) * kBlockF + f];
         int8_t d0, d1, d2, d3;
-        digits4(v[o], inv[o], d0, d1, d2, d3);
-        uint8_t *t = tile + ((size_t)o * 4 * 128 + f) * 64 + gl;
+        digits4(v, inv[o], d0, d1, d2, d3);
+        uint8_t *t = tile + ((size_t)o * 4 * 128 + f) * 68 + gl;
         t[0] = (uint8_t)d0;
-        t[128 * 64] = (uint8_t)d1;
-        t[2 * 128 * 64] = (uint8_t)d2;
-        t[3 * 128 * 64] = (uint8_t)d3;
+        t[128 * 68] = (uint8_t)d1;
+        t[2 * 128 * 68] = (uint8_t)d2;
+        t[3 * 128 * 68] = (uint8_t)d3;
       }
     }
     __syncthreads();
-    // rows (operand, digit, f) of 64 bytes -> 4 x 16-byte stores each
     const int nrow = nop * 4 * 128;
-    for (int e = threadIdx.x; e < nrow * 4; e += 256) {
-      const int rw = e >> 2, part = e & 3;
+    for (int e = threadIdx.x; e < nrow * 16; e += 256) {
+      const int rw = e >> 4, part = e & 15;
       const int o = rw / 512, d = (rw / 128) & 3, ff = rw & 127;
-      const uint4 val = *reinterpret_cast<const uint4 *>(tile + (size_t)rw * 64 + 16 * part);
+      const uint32_t val = *reinterpret_cast<const uint32_t *>(tile + (size_t)rw * 68 + 4 * part);
       uint8_t *dst = (o == 0) ? qph + ((q * 4 + d) * 128 + ff) * 256
                               : qz + (((q * nz + (o - 1)) * 4 + d) * 128 + ff) * 256;
-      *reinterpret_cast<uint4 *>(dst + g0 + 16 * part) = val;
+      *reinterpret_cast<uint32_t *>(dst + g0 + 4 * part) = val;
     }
     __syncthreads();
   }
@@ -604,8 +669,7 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     NKX_CUDA(cudaDeviceGetAttribute(&M->nsm, cudaDevAttrMultiProcessorCount, dev));
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kStages * kStageBytes + 1024));
-    NKX_CUDA(cudaFuncSetAttribute(zquant_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 64));
-    NKX_CUDA(cudaFuncSetAttribute(zquant_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 64));
+    NKX_CUDA(cudaFuncSetAttribute(zquant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 68));
   }
   MixedState &M = *static_cast<MixedState *>(P.mx_state);
   const int nocc_pad = ((nocc + 63) / 64) * 64;
@@ -630,7 +694,28 @@ __global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, cons
                                   const double *__restrict__ rho, const double *__restrict__ grad,
                                   const double *__restrict__ vj, double *__restrict__ coef, double *Eacc);
 void coulomb_fit(Plan &P, int nspin, cudaStream_t s);
-void launch_colloc(Plan &P, const Chunk &c, cudaStream_t s);
+
+template <bool GRAD>
+static void launch_colloc_z_g(Plan &P, MixedState &M, const Chunk &c, int nzs, int nspin, cudaStream_t s) {
+  const unsigned np = (unsigned)(c.p1 - c.p0);
+#define NKX_CZ(NZ)                                                                                                   \
+  colloc_z_kernel<GRAD, NZ><<<np, 256, 0, s>>>(P.d_sto, P.d_px, P.d_py, P.d_pz, P.d_pair_batch, P.d_pair_blk, c.p0, \
+                                               P.d_coef, P.d_vj, nspin, P.npad, P.ws_phi, M.sph, M.sz)
+  if (nzs == 1)
+    NKX_CZ(1);
+  else if (nzs == 2)
+    NKX_CZ(2);
+  else
+    NKX_CZ(3);
+#undef NKX_CZ
+}
+
+static void launch_colloc_z(Plan &P, MixedState &M, const Chunk &c, int nzs, int nspin, cudaStream_t s) {
+  if (P.gga)
+    launch_colloc_z_g<true>(P, M, c, nzs, nspin, s);
+  else
+    launch_colloc_z_g<false>(P, M, c, nzs, nspin, s);
+}
 
 void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
                       StageTimer &Tm) {
@@ -638,8 +723,6 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
   const int nc = P.gga ? 4 : 1;
   const int nzs = nspin + (separateJ ? 1 : 0);
   NKX_REQUIRE(nzs <= 3, NKX_ERR_ARG, "too many Z planes");
-  const bool multi = P.chunks.size() > 1;
-  const size_t tile = (size_t)kBatch * kBlockF;
   NKX_CUDA(cudaMemsetAsync(M.err, 0, sizeof(int), s));
   {
     const long rows = (long)nspin * M.nocc_pad * P.nblk;
@@ -653,16 +736,17 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     const long np = c.p1 - c.p0, nb = c.b1 - c.b0;
     if (np > 0) {
       Tm.begin(ST_COLLOC, s);
-      launch_colloc(P, c, s);
+      if (P.gga)
+        colloc_quantT_kernel<true><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
+                                                                P.d_pair_blk, c.p0, M.qphT, M.sphT);
+      else
+        colloc_quantT_kernel<false><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
+                                                                 P.d_pair_blk, c.p0, M.qphT, M.sphT);
+      NKX_LAUNCH_CHECK();
+      ++P.launches;
       Tm.end(s);
     }
     Tm.begin(ST_DENSITY, s);
-    if (np > 0) {
-      const long rows = np * nc * 256;
-      quant_phiT_kernel<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(P.ws_phi, nc, rows, M.qphT, M.sphT);
-      NKX_LAUNCH_CHECK();
-      ++P.launches;
-    }
     TcArgs a{};
     a.mode = TC_MODE_DENSITY;
     a.b0 = c.b0;
@@ -713,19 +797,13 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
   for (const Chunk &c : P.chunks) {
     const long np = c.p1 - c.p0;
     if (np <= 0) continue;
-    if (multi) {
-      Tm.begin(ST_COLLOC, s);
-      launch_colloc(P, c, s);
-      Tm.end(s);
-    }
+    Tm.begin(ST_COLLOC, s);
+    launch_colloc_z(P, M, c, nzs, nspin, s);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+    Tm.end(s);
     Tm.begin(ST_ZBUILD, s);
-    const size_t zsm = (size_t)(1 + nzs) * 4 * 128 * 64;
-    if (P.gga)
-      zquant_kernel<true><<<(unsigned)np, 256, zsm, s>>>(P.ws_phi, P.d_coef, P.d_vj, P.d_pair_batch, c.p0, nzs,
-                                                        nspin, P.npad, M.qph, M.sph, M.qz, M.sz);
-    else
-      zquant_kernel<false><<<(unsigned)np, 256, zsm, s>>>(P.ws_phi, P.d_coef, P.d_vj, P.d_pair_batch, c.p0, nzs,
-                                                         nspin, P.npad, M.qph, M.sph, M.qz, M.sz);
+    zquant_kernel<<<(unsigned)np, 256, (size_t)(1 + nzs) * 4 * 128 * 68, s>>>(P.ws_phi, M.sph, M.sz, nzs, M.qph, M.qz);
     NKX_LAUNCH_CHECK();
     ++P.launches;
     Tm.end(s);
@@ -751,7 +829,6 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     ++P.launches;
     Tm.end(s);
   }
-  (void)tile;
   int herr = 0;
   NKX_CUDA(cudaMemcpyAsync(&herr, M.err, sizeof(int), cudaMemcpyDeviceToHost, s));
   NKX_CUDA(cudaStreamSynchronize(s));
