@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--cpu-sample", type=int, default=8192, help="points in the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workspace-mb", type=int, default=0,
+                    help="cap on the per-chunk collocation workspace in MiB (0: automatic); more chunks, same work")
     return ap.parse_args()
 
 
@@ -236,7 +238,7 @@ def run_nkx(args):
     pts, w = g.quad_points[sel], g.weights[sel]
     b = A.make_manual_basis(funcs)
     t0 = time.perf_counter()
-    fb = A.FockBuilder(c, Z, b, (pts, w), func_ids=FUNCS)
+    fb = A.FockBuilder(c, Z, b, (pts, w), func_ids=FUNCS, workspace_bytes=args.workspace_mb << 20)
     setup_s = time.perf_counter() - t0
     info = fb.info()
     nbf = len(funcs)

@@ -42,7 +42,7 @@ constexpr int kBBytes = 4 * 64 * 64;   // four digit planes, 64 rows x 64 B
 constexpr int kStageBytes = kABytes + kBBytes;
 constexpr int kGemmThreads = 320;
 constexpr uint32_t kIdesc = idesc_i8(128, 64);
-constexpr double kTwoM60 = 8.673617379884035e-19;  // 2^-60
+constexpr double kTwoM36 = 0x1p-36;
 
 enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1 };
 
@@ -274,23 +274,36 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         size_t sbs = 1;
         if (live) {
           if (a.mode == TC_MODE_V) {
-            sa = a.sA[g.qa * 128 + row] * kTwoM60;
+            sa = a.sA[g.qa * 128 + row] * kTwoM36;
             sb = a.sB + (g.qb * a.nz + it.zi) * 128 + 64 * (it.J & 1) + 32 * hc;
           } else {
-            sa = a.sA[(g.qa * a.ncomp + it.c) * 256 + 128 * it.h + row] * kTwoM60;
+            sa = a.sA[(g.qa * a.ncomp + it.c) * 256 + 128 * it.h + row] * kTwoM36;
             sb = a.sB + ((size_t)it.s * a.nocc_pad + 64 * it.t + 32 * hc) * a.nblk + g.blk;
             sbs = a.nblk;
           }
         }
-        // level L carries weight 2^(8 (6 - L)) relative to the 2^-60 s_a s_b unit
+        // exact integer combine of the four levels, S = sum_L 2^(8 (3 - L)) Acc_L:
+        // |Acc_L| < 2^24 for K <= 256, so |S| < 2^49 converts to FP64 exactly;
+        // the product is s_a s_b 2^-36 S (one rounding per group and element)
 #pragma unroll
-        for (int L = 0; L < 4; ++L) {
-          uint32_t v[32];
-          tmem_ld32u(tmem + lane_addr + buf * 256 + L * 64 + 32 * hc, v);
+        for (int hh = 0; hh < 2; ++hh) {
+          uint32_t v0[16], v1[16], v2[16], v3[16];
+          const uint32_t ta = tmem + lane_addr + buf * 256 + 32 * hc + 16 * hh;
+          tmem_ld16u_async(ta, v0);
+          tmem_ld16u_async(ta + 64, v1);
+          tmem_ld16u_async(ta + 128, v2);
+          tmem_ld16u_async(ta + 192, v3);
+          tmem_wait16(v0);
+          tmem_wait16(v1);
+          tmem_wait16(v2);
+          tmem_wait16(v3);
           if (live) {
-            const double wl = sa * ldexp(1.0, 8 * (6 - L));
 #pragma unroll
-            for (int j = 0; j < 32; ++j) acc[j] = fma((double)(int)v[j], wl * sb[j * sbs], acc[j]);
+            for (int j = 0; j < 16; ++j) {
+              const long long S = (long long)(int)v0[j] * (1LL << 24) + (long long)(int)v1[j] * (1LL << 16) +
+                                  (long long)(int)v2[j] * (1LL << 8) + (long long)(int)v3[j];
+              acc[16 * hh + j] = fma((double)S, sa * sb[(16 * hh + j) * sbs], acc[16 * hh + j]);
+            }
           }
         }
         tc_fence_before();
