@@ -392,21 +392,27 @@ __global__ void __launch_bounds__(256) vgemm_fp64_kernel(const double *__restric
     }
 }
 
-// out(i,j) = Vp(i,j) + Vp(j,i) for i, j < n (symmetrise and unpad)
-__global__ void symmetrize_unpad_kernel(int n, int npad, const double *__restrict__ Vp, double *__restrict__ out) {
-  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && j < n) out[(size_t)i + (size_t)j * n] = Vp[(size_t)i + (size_t)j * npad] + Vp[(size_t)j + (size_t)i * npad];
+// out(i, j) = Vp(pi, pj) + Vp(pj, pi), p = finv[.] the plan position of
+// caller function i (symmetrise, unpad and undo the plan order)
+__global__ void symmetrize_unpad_kernel(int n, int npad, const int *__restrict__ finv, const double *__restrict__ Vp,
+                                        double *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i < n && j < n) {
+    const size_t pi = finv[i], pj = finv[j];
+    out[(size_t)i + (size_t)j * n] = Vp[pi + pj * npad] + Vp[pj + pi * npad];
+  }
 }
 
-// C (nbf x nocc column-major, per spin) -> Ct[spin][i][f], f padded to nbf_pad
-__global__ void pack_orbitals_kernel(const double *__restrict__ C, int nbf, int nocc, int nspin, int nbf_pad,
-                                     double *__restrict__ Ct) {
+// C (nbf x nocc column-major, per spin) -> Ct[spin][i][p] = C(fperm[p], i)
+// in plan order, zero at padding positions (fperm < 0)
+__global__ void pack_orbitals_kernel(const double *__restrict__ C, const int *__restrict__ fperm, int nbf, int nocc,
+                                     int nspin, int nbf_pad, double *__restrict__ Ct) {
   const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long tot = (long)nspin * nocc * nbf_pad;
   if (e >= tot) return;
-  const int f = (int)(e % nbf_pad);
+  const int f = fperm[e % nbf_pad];
   const long si = e / nbf_pad;
-  Ct[e] = f < nbf ? C[si * nbf + f] : 0.0;
+  Ct[e] = f >= 0 ? C[si * nbf + f] : 0.0;
 }
 
 // y_a += sum over a slice of points of w_g V_a(g) rho_g   (coulomb.hpp:84-85)
@@ -574,13 +580,40 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
     if (p < npoints) hw[p] = w[g];
   }
 
-  // --- basis table (padded functions have norm 0)
-  auto tab = make_sto_table(*prim);
-  tab.resize(P.nbf_pad);
-  for (int i = P.nbf; i < P.nbf_pad; ++i) {
-    tab[i] = tab[0];
-    tab[i].norm = 0.0;
+  // --- basis table in plan order (padded positions have norm 0).  Within
+  // each 128-function block, position p = 4 lane + c holds the block's
+  // function of rank 32 c + lane, ranks sorted by (l, m): the collocation
+  // kernels give lane l of a warp positions 4l .. 4l+3, so the 32 lanes
+  // evaluating slot c take the same solid-harmonic branch.  Blocks keep
+  // their function sets, so screening is unchanged.
+  auto tab0 = make_sto_table(*prim);
+  std::vector<StoFunc> tab(P.nbf_pad);
+  P.h_fperm.assign(P.nbf_pad, -1);
+  std::vector<int> finv(std::max(1, P.nbf), 0);
+  for (int I = 0; I < P.nblk; ++I) {
+    std::vector<int> fs;
+    for (int f = I * kBlockF; f < std::min(P.nbf, (I + 1) * kBlockF); ++f) fs.push_back(f);
+    std::stable_sort(fs.begin(), fs.end(), [&](int x, int y) {
+      return tab0[x].l != tab0[y].l ? tab0[x].l < tab0[y].l : tab0[x].m < tab0[y].m;
+    });
+    for (int k = 0; k < (int)fs.size(); ++k) {
+      const int pos = I * kBlockF + 4 * (k % 32) + k / 32;
+      P.h_fperm[pos] = fs[k];
+      finv[fs[k]] = pos;
+    }
   }
+  for (int p = 0; p < P.nbf_pad; ++p) {
+    if (P.h_fperm[p] >= 0) {
+      tab[p] = tab0[P.h_fperm[p]];
+    } else {
+      tab[p] = tab0[0];
+      tab[p].norm = 0.0;
+    }
+  }
+  P.d_fperm = P.alloc<int>(P.nbf_pad);
+  NKX_CUDA(cudaMemcpy(P.d_fperm, P.h_fperm.data(), sizeof(int) * P.nbf_pad, cudaMemcpyHostToDevice));
+  P.d_finv = P.alloc<int>(finv.size());
+  NKX_CUDA(cudaMemcpy(P.d_finv, finv.data(), sizeof(int) * finv.size(), cudaMemcpyHostToDevice));
   const double tol = opts->screen_tol > 0 ? opts->screen_tol : 1e-10;
   auto cut = make_cutoffs(*prim, tol);
 
@@ -945,8 +978,8 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
   } else {
     NKX_CUDA(cudaMemcpyAsync(P.d_occ, occ, sizeof(double) * nspin * nocc, cudaMemcpyDeviceToDevice, s));
   }
-  pack_orbitals_kernel<<<nblk((long)nspin * nocc * P.nbf_pad, 256), 256, 0, s>>>(Cd, P.nbf, nocc, nspin, P.nbf_pad,
-                                                                                  P.d_Ct);
+  pack_orbitals_kernel<<<nblk((long)nspin * nocc * P.nbf_pad, 256), 256, 0, s>>>(Cd, P.d_fperm, P.nbf, nocc, nspin,
+                                                                                  P.nbf_pad, P.d_Ct);
   NKX_LAUNCH_CHECK();
   ++P.launches;
 
@@ -970,7 +1003,8 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
   dim3 tb(16, 16), gb(nblk(P.nbf, 16), nblk(P.nbf, 16));
   for (int z = 0; z < nout; ++z) {
     double *o = (z < nspin) ? dst + z * nn : (mem == NKX_MEM_DEVICE ? J : dst + nspin * nn);
-    symmetrize_unpad_kernel<<<gb, tb, 0, s>>>(P.nbf, P.nbf_pad, P.d_V + (size_t)z * P.nbf_pad * P.nbf_pad, o);
+    symmetrize_unpad_kernel<<<gb, tb, 0, s>>>(P.nbf, P.nbf_pad, P.d_finv, P.d_V + (size_t)z * P.nbf_pad * P.nbf_pad,
+                                              o);
     ++P.launches;
   }
   NKX_LAUNCH_CHECK();

@@ -30,7 +30,9 @@ struct Plan {
 
   // grid (Morton order, padded to nbatch * 256; padded points have w = 0)
   double *d_px = nullptr, *d_py = nullptr, *d_pz = nullptr, *d_w = nullptr;
-  StoFunc *d_sto = nullptr;
+  StoFunc *d_sto = nullptr;  // basis in plan order (see build_plan)
+  std::vector<int> h_fperm;  // plan position -> caller function (-1: padding)
+  int *d_fperm = nullptr, *d_finv = nullptr;
   AuxFunc *d_aux = nullptr;
 
   // screening: pairs of (batch, significant function block), CSR by batch
