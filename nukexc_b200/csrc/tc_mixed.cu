@@ -532,19 +532,27 @@ __global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ 
   }
   const double *src = ws + q * 4 * T;
   for (int g0 = 0; g0 < kBatch; g0 += 64) {
-    for (int k = 0; k < 32; ++k) {
-      const int gl = gs + 2 * k;
+    // thread (f, gs) quantises points 4 gq .. 4 gq + 3 of the slab, gq = gs + 2 kq:
+    // all loads of a step are issued before use, and the four digit bytes of
+    // four consecutive points go to shared memory as one word
+    for (int kq = 0; kq < 8; ++kq) {
+      const int gq = gs + 2 * kq;
+      double v[4][4];
 #pragma unroll
       for (int o = 0; o < 4; ++o) {
         if (o >= nop) break;
-        const double v = src[o * T + (size_t)(g0 + gl) * kBlockF + f];
-        int8_t d0, d1, d2, d3;
-        digits4(v, inv[o], d0, d1, d2, d3);
-        uint8_t *t = tile + ((size_t)o * 4 * 128 + f) * 68 + gl;
-        t[0] = (uint8_t)d0;
-        t[128 * 68] = (uint8_t)d1;
-        t[2 * 128 * 68] = (uint8_t)d2;
-        t[3 * 128 * 68] = (uint8_t)d3;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) v[o][r] = src[o * T + (size_t)(g0 + 4 * gq + r) * kBlockF + f];
+      }
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        if (o >= nop) break;
+        int8_t d[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) digits4(v[o][r], inv[o], d[0][r], d[1][r], d[2][r], d[3][r]);
+        uint32_t *t = reinterpret_cast<uint32_t *>(tile + ((size_t)o * 4 * 128 + f) * 68) + gq;
+#pragma unroll
+        for (int dd = 0; dd < 4; ++dd) t[dd * 128 * 17] = pack4(d[dd][0], d[dd][1], d[dd][2], d[dd][3]);
       }
     }
     __syncthreads();
