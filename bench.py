@@ -177,6 +177,16 @@ def fp64_gemm_peak(torch):
     return 2 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def measured_traffic(workload):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu capture
+    of this workload (profiles/roofline_traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d["dram_bytes_per_launch"] if d.get("workload") == workload else None
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -367,7 +377,10 @@ def run_nkx(args):
                                     "parallelism": f"grid split by atoms over {world} GPU(s)"}),
             "stage_ms_per_step": {k: v / args.steps for k, v in stage.items() if k.endswith("_ms")},
             "roofline": {"bound": "tensor", "kernel": "vgemm (V = Phi Z^T)", "achieved": ach, "peak": peak,
-                         "unit": unit, "frac": ach / peak, "traffic": None, "peak_source": peak_note,
+                         "unit": unit, "frac": ach / peak,
+                         "traffic": measured_traffic(config(args)["workload"]) if prec == "mixed" else None,
+                         "traffic_unit": "DRAM bytes per V launch (ncu, profiles/roofline_traffic.json)",
+                         "peak_source": peak_note,
                          "algorithmic_flops_per_step": flops,
                          "fp64_equivalent_tflops": flops / (vg_ms * 1e-3) / 1e12},
             "fp64_same_gpu": fp64,
