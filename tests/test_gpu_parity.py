@@ -1,11 +1,15 @@
 """Parity of the CUDA path (through the C ABI) with the CPU oracle and with
 the reference's golden values.  FP64 tolerances are written per test."""
+import json
 import math
+import os
 
 import numpy as np
 import pytest
 
 from oracle import oracle as O
+
+KAT = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_kats.json")))
 
 pytestmark = pytest.mark.gpu
 
@@ -32,7 +36,7 @@ def test_golden_lda_x_h1s_plan():
     b, _ = h1s()
     fb = A.FockBuilder([[0, 0, 0]], [1], b, g, func_ids=("LDA_X",))
     E, V, _ = fb.build([np.ones((1, 1))], [np.ones(1)])
-    assert E == pytest.approx(-0.2127415030860106, rel=1e-10)
+    assert E == pytest.approx(KAT["h1s_lda_x"]["E"], rel=1e-10)
 
 
 def test_golden_pbe_x_h1s_dense_and_plan():
@@ -41,12 +45,12 @@ def test_golden_pbe_x_h1s_dense_and_plan():
     b, _ = h1s()
     phi, gx, gy, gz = A.fill_grad_collocation(b, g.quad_points)
     E, V = A.compute_gga(phi, gx, gy, gz, g.weights, np.ones((1, 1)), np.ones(1), ("GGA_X_PBE",))
-    assert E == pytest.approx(-0.253995708307881, rel=1e-10)
-    assert V[0, 0].item() == pytest.approx(-0.320733669386709, rel=1e-10)
+    assert E == pytest.approx(KAT["h1s_pbe_x"]["E"], rel=1e-10)
+    assert V[0, 0].item() == pytest.approx(KAT["h1s_pbe_x"]["V00"], rel=1e-10)
     fb = A.FockBuilder([[0, 0, 0]], [1], b, g, func_ids=("GGA_X_PBE",))
     E2, V2, _ = fb.build([np.ones((1, 1))], [np.ones(1)])
-    assert E2 == pytest.approx(-0.253995708307881, rel=1e-10)
-    assert V2[0][0, 0] == pytest.approx(-0.320733669386709, rel=1e-10)
+    assert E2 == pytest.approx(KAT["h1s_pbe_x"]["E"], rel=1e-10)
+    assert V2[0][0, 0] == pytest.approx(KAT["h1s_pbe_x"]["V00"], rel=1e-10)
 
 
 def test_golden_pbe_x_he1s():
@@ -55,8 +59,8 @@ def test_golden_pbe_x_he1s():
     b = A.make_manual_basis([(1, 0, 0, 1.6875, 0, 0, 0)])
     fb = A.FockBuilder([[0, 0, 0]], [2], b, g, func_ids=("GGA_X_PBE",))
     E, V, _ = fb.build([np.ones((1, 1))], [2 * np.ones(1)])
-    assert E == pytest.approx(-1.032549417787429, rel=1e-10)
-    assert V[0][0, 0] == pytest.approx(-0.657943275538615, rel=1e-10)
+    assert E == pytest.approx(KAT["he1s_pbe_x"]["E"], rel=1e-10)
+    assert V[0][0, 0] == pytest.approx(KAT["he1s_pbe_x"]["V00"], rel=1e-10)
 
 
 @pytest.mark.parametrize("svd", [0.0, 1e-4])
@@ -68,7 +72,7 @@ def test_golden_coulomb_h1s(svd):
     aux = A.make_manual_basis([(1, 0, 0, z, 0, 0, 0) for z in (0.5, 1.0, 2.0, 3.0, 4.0)])
     fb = A.FockBuilder([[0, 0, 0]], [1], b, g, aux=aux, func_ids=("LDA_X",), metric_svd_thr=svd)
     E, V, J = fb.build([np.ones((1, 1))], [np.ones(1)], want_J=True)
-    assert J[0, 0] == pytest.approx(5 / 8, rel=1e-10)
+    assert J[0, 0] == pytest.approx(KAT["h1s_coulomb"]["J00"], rel=1e-10)
 
 
 def test_golden_density_sigma():

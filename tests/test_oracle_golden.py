@@ -6,12 +6,16 @@ single-atom test only has to integrate a spherically symmetric integrand,
 which every Lebedev rule does exactly, so where the reference asks for a
 Lebedev order above 41 (the He test's order 100) the order-41 rule is used.
 """
+import json
 import math
+import os
 
 import numpy as np
 import pytest
 
 from oracle import oracle as O
+
+KAT = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_kats.json")))
 
 
 def one(n=1):
@@ -81,7 +85,7 @@ def test_h1s_lda_x():
     pts, w, _ = O.make_flat_grid([[0, 0, 0]], [1], 100, 20, scheme="becke")
     b = O.make_manual_basis([(1, 0, 0, 1.0, 0, 0, 0)])
     E, V = O.xc_build(b, pts, w, [1], *one())
-    assert E == pytest.approx(-0.2127415030860106, rel=1e-10)
+    assert E == pytest.approx(KAT["h1s_lda_x"]["E"], rel=KAT["h1s_lda_x"]["rel"])
 
 
 def test_h1s_pbe_x():
@@ -89,8 +93,9 @@ def test_h1s_pbe_x():
     pts, w, _ = O.make_flat_grid([[0, 0, 0]], [1], 100, 20, scheme="becke")
     b = O.make_manual_basis([(1, 0, 0, 1.0, 0, 0, 0)])
     E, V = O.xc_build(b, pts, w, [101], *one())
-    assert E == pytest.approx(-0.253995708307881, rel=1e-10)
-    assert V[0, 0, 0] == pytest.approx(-0.320733669386709, rel=1e-10)
+    k = KAT["h1s_pbe_x"]
+    assert E == pytest.approx(k["E"], rel=k["rel"])
+    assert V[0, 0, 0] == pytest.approx(k["V00"], rel=k["rel"])
 
 
 def test_he1s_pbe_x():
@@ -98,8 +103,9 @@ def test_he1s_pbe_x():
     pts, w, _ = O.make_flat_grid([[0, 0, 0]], [2], 2000, 41, scheme="becke")
     b = O.make_manual_basis([(1, 0, 0, 1.6875, 0, 0, 0)])
     E, V = O.xc_build(b, pts, w, [101], *one(2.0))
-    assert E == pytest.approx(-1.032549417787429, rel=1e-10)
-    assert V[0, 0, 0] == pytest.approx(-0.657943275538615, rel=1e-10)
+    k = KAT["he1s_pbe_x"]
+    assert E == pytest.approx(k["E"], rel=k["rel"])
+    assert V[0, 0, 0] == pytest.approx(k["V00"], rel=k["rel"])
 
 
 @pytest.mark.parametrize("use_cholesky", [False, True])
@@ -113,7 +119,7 @@ def test_h1s_coulomb_self_repulsion(use_cholesky):
         J, _ = O.coulomb(b, aux, pts, w, np.ones((1, 1)), np.ones(1), S=S)
     else:
         J, _ = O.coulomb(b, aux, pts, w, np.ones((1, 1)), np.ones(1), X=O.half_inverse(S, 1e-4))
-    assert J[0, 0] == pytest.approx(5 / 8, rel=1e-10)
+    assert J[0, 0] == pytest.approx(KAT["h1s_coulomb"]["J00"], rel=KAT["h1s_coulomb"]["rel"])
 
 
 def test_becke_one_half_original():
