@@ -197,6 +197,14 @@ NKX_API nkx_status nkx_xc_eval(int func_id, int nspin, long n, const double *d_r
 NKX_API nkx_status nkx_potential_collocation(const nkx_basis *aux, const double *d_points, const double *d_w,
                                              long npts, double *d_Vw, void *stream);
 
+/* compute_coulomb (nukexc/coulomb.hpp:56-115) on dense matrices: rho from
+ * Phi (nbf x npts) and C (nbf x nocc), y = Vw rho (Vw naux x npts), c = X X^T y
+ * (X naux x K), v = Vw^T c, J = Phi diag(v) Phi^T (nbf x nbf column-major).
+ * All pointers are device buffers. */
+NKX_API nkx_status nkx_coulomb_dense(int nbf, int naux, long npts, const double *d_phi, const double *d_Vw,
+                                     const double *d_X, int K, int nocc, const double *d_C, const double *d_occ,
+                                     double *d_J, void *stream);
+
 /* compute_half_inverse (nukexc/nukexc_utils.hpp:198-270): X = U s^-1/2 / D
  * of the preconditioned metric, keeping s > thr (symmetric
  * eigendecomposition on the device).  d_X must hold N*N; *K receives the

@@ -260,14 +260,21 @@ def compute_half_inverse(S, lin_dep_threshold=1e-5):
 
 def compute_coulomb(mo_orbitals, mo_coeff, basis_collocation, basis_aux_collocation,
                     potential_collocation_scaled, half_inverse_X):
-    """compute_coulomb (nukexc/coulomb.hpp:56-115), dense: J (nbf x nbf).
-    The contractions are device GEMVs/GEMMs of torch (plain library calls)
-    around the nkx density kernel, as the reference does with KokkosBlas."""
-    rho = compute_density(basis_collocation, mo_orbitals, mo_coeff)
-    y = potential_collocation_scaled @ rho
-    c = half_inverse_X @ (half_inverse_X.t() @ y)
-    v = potential_collocation_scaled.t() @ c
-    return basis_collocation @ (basis_collocation * v[None, :]).t()
+    """compute_coulomb (nukexc/coulomb.hpp:56-115), dense, through
+    nkx_coulomb_dense: J (nbf x nbf) from rho, y = Vw rho, c = X X^T y,
+    v = Vw^T c and J = Phi diag(v) Phi^T."""
+    nbf, npts = basis_collocation.shape
+    naux, K = half_inverse_X.shape
+    f = _flat_lmat(basis_collocation)
+    Vw = _flat_lmat(potential_collocation_scaled)
+    X = _flat_lmat(half_inverse_X)
+    C_ = _flat_lmat(mo_orbitals)
+    occ = _dev(mo_coeff)
+    J = torch.empty(nbf * nbf, dtype=torch.float64, device="cuda")
+    check(L.lib().nkx_coulomb_dense(nbf, naux, npts, _p(f), _p(Vw), _p(X), K, occ.numel(), _p(C_), _p(occ),
+                                    _p(J), None))
+    J = J.view(nbf, nbf).t()
+    return J
 
 
 # ------------------------------------------------------------------ plan --

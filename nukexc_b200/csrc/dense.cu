@@ -4,6 +4,7 @@
 // caller-owned device buffers.  The batched, screened Fock build of plan.cu
 // is the hot path; these exist so the reference's dense call sequence can be
 // replaced one function at a time.
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <functional>
@@ -341,6 +342,47 @@ extern "C" nkx_status nkx_potential_collocation(const nkx_basis *aux, const doub
     if (tot > 0) potential_dense_kernel<<<nblk(tot, 128), 128, 0, s>>>(df.p, aux->nbf, d_points, d_w, npts, d_Vw);
     NKX_LAUNCH_CHECK();
     NKX_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+// S(f, g) = Phi(f, g) v(g)
+__global__ void scale_columns_kernel(int nbf, long npts, const double *__restrict__ phi, const double *__restrict__ v,
+                                     double *__restrict__ S) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e < (long)nbf * npts) S[e] = phi[e] * v[e / nbf];
+}
+
+extern "C" nkx_status nkx_coulomb_dense(int nbf, int naux, long npts, const double *d_phi, const double *d_Vw,
+                                        const double *d_X, int K, int nocc, const double *d_C, const double *d_occ,
+                                        double *d_J, void *stream) {
+  return run_guarded("nkx_coulomb_dense", [&] {
+    NKX_REQUIRE(nbf > 0 && naux > 0 && npts > 0 && K > 0 && K <= naux && nocc > 0 && d_phi && d_Vw && d_X && d_C &&
+                    d_occ && d_J,
+                NKX_ERR_ARG, "invalid arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    DevBuf<double> rho(npts), y(naux), t(K), c(naux), v(npts), S((size_t)nbf * npts);
+    density_dense_kernel<<<nblk(npts * 32, 256), 256, 0, s>>>(nbf, npts, d_phi, nullptr, nullptr, nullptr, nocc, d_C,
+                                                              d_occ, rho.p, nullptr, nullptr);
+    NKX_LAUNCH_CHECK();
+    cublasHandle_t h;
+    NKX_REQUIRE(cublasCreate(&h) == CUBLAS_STATUS_SUCCESS, NKX_ERR_CUDA, "cublasCreate failed");
+    cublasSetStream(h, s);
+    const double one = 1.0, zero = 0.0;
+    bool ok = cublasDgemv(h, CUBLAS_OP_N, naux, (int)npts, &one, d_Vw, naux, rho.p, 1, &zero, y.p, 1) ==
+              CUBLAS_STATUS_SUCCESS;
+    ok = ok && cublasDgemv(h, CUBLAS_OP_T, naux, K, &one, d_X, naux, y.p, 1, &zero, t.p, 1) == CUBLAS_STATUS_SUCCESS;
+    ok = ok && cublasDgemv(h, CUBLAS_OP_N, naux, K, &one, d_X, naux, t.p, 1, &zero, c.p, 1) == CUBLAS_STATUS_SUCCESS;
+    ok = ok && cublasDgemv(h, CUBLAS_OP_T, naux, (int)npts, &one, d_Vw, naux, c.p, 1, &zero, v.p, 1) ==
+                   CUBLAS_STATUS_SUCCESS;
+    if (ok) {
+      scale_columns_kernel<<<nblk((long)nbf * npts, 256), 256, 0, s>>>(nbf, npts, d_phi, v.p, S.p);
+      ok = cudaGetLastError() == cudaSuccess;
+    }
+    ok = ok && cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, (int)npts, &one, d_phi, nbf, S.p, nbf, &zero, d_J,
+                           nbf) == CUBLAS_STATUS_SUCCESS;
+    NKX_CUDA(cudaStreamSynchronize(s));
+    cublasDestroy(h);
+    NKX_REQUIRE(ok, NKX_ERR_CUDA, "cuBLAS call in nkx_coulomb_dense failed");
   });
 }
 

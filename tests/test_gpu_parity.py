@@ -252,3 +252,18 @@ def test_plan_coulomb_pivoted_cholesky_baseline_aux():
     E, V, J = fb.build([Cm], [np.ones(5)], want_J=True)
     assert np.isfinite(J).all() and np.abs(J - J.T).max() < 1e-12 * np.abs(J).max()
     assert 0 < fb.info()["metric_min_diag"]
+
+
+def test_golden_coulomb_h1s_dense():
+    # tests/test_hydrogen.cxx:562-631 through the dense compute_coulomb
+    # (nkx_coulomb_dense) with the reference's half inverse (thr 1e-4)
+    g = A.make_flat_grid([[0, 0, 0]], [1], 100, 20, radial="becke")
+    b, _ = h1s()
+    aux = A.make_manual_basis([(1, 0, 0, z, 0, 0, 0) for z in (0.5, 1.0, 2.0, 3.0, 4.0)])
+    phi = A.fill_collocation(b, g.quad_points)
+    phi_aux = A.fill_collocation(aux, g.quad_points)
+    Vw = A.sto_potential_collocation_scaled(aux, g.quad_points, g.weights)
+    S = 0.5 * (phi_aux @ Vw.t() + Vw @ phi_aux.t())
+    X = A.compute_half_inverse(S, 1e-4)
+    J = A.compute_coulomb(np.ones((1, 1)), np.ones(1), phi, phi_aux, Vw, X)
+    assert J[0, 0].item() == pytest.approx(KAT["h1s_coulomb"]["J00"], rel=1e-10)
