@@ -240,6 +240,17 @@ NKX_API nkx_status nkx_fock_build(nkx_plan *plan, int precision, int nspin, int 
                                   const double *occ, int mem, int fuse_j, double *E, double *V, double *J,
                                   void *stream);
 
+/* XC nuclear gradient at fixed orbitals, FP64 (no counterpart in the
+ * reference): grad[3*natoms] (host, Eh/bohr) = dE_xc/dR of
+ * E_xc = sum_g w_g f(rho(r_g)) with every grid point moving with its owner
+ * atom and the Becke weights differentiated (becke_clamp as in
+ * nkx_becke_partition; the plan's weights must be radial x angular weights
+ * times that Becke partition).  The plan must have been created with the
+ * molecule and the point owners, with every basis function centred on an
+ * atom.  C / occ as in nkx_fock_build (mem selects host or device). */
+NKX_API nkx_status nkx_xc_gradient(nkx_plan *plan, int nspin, int nocc, const double *C, const double *occ,
+                                   int mem, double becke_clamp, double *grad, void *stream);
+
 NKX_API nkx_status nkx_get_last_timing(const nkx_plan *plan, nkx_build_timing *t);
 
 /* Per-point density of the last build (rho[npoints*nspin], plan point order

@@ -283,17 +283,23 @@ class FockBuilder:
     path): once per geometry the grid is batched and screened and the aux
     metric factorised; each build() is one SCF iteration's XC (+ J) work.
 
-    grid: FlatGrid or (points, weights); basis/aux: STOBasisSet.
+    grid: FlatGrid or (points, weights) or (points, weights, point_owner);
+    basis/aux: STOBasisSet.  The point owners (given by a FlatGrid or the
+    3-tuple) are needed only by xc_gradient.
     """
 
     def __init__(self, centers, Z, basis, grid, aux=None, func_ids=("GGA_X_PBE", "GGA_C_PBE"),
                  dens_threshold=1e-15, metric_svd_thr=0.0, workspace_bytes=0):
+        owner = None
         if isinstance(grid, FlatGrid):
-            pts, w = grid.quad_points, grid.weights
+            pts, w, owner = grid.quad_points, grid.weights, grid.point_owner
+        elif len(grid) == 3:
+            pts, w, owner = grid
         else:
             pts, w = grid
         self._pts = _np(pts, np.float64).reshape(-1)
         self._w = _np(w, np.float64)
+        self._owner = _np(owner, np.int32) if owner is not None else None
         mol, self._mk = _mol(centers, Z)
         self.basis = basis
         self._b = basis.as_c()
@@ -304,7 +310,9 @@ class FockBuilder:
         h = C.c_void_p()
         check(L.lib().nkx_plan_create(C.byref(mol), C.byref(self._b), C.byref(self._a) if self._a else None,
                                       len(self._w), self._pts.ctypes.data_as(C.c_void_p),
-                                      self._w.ctypes.data_as(C.c_void_p), None, C.byref(self._o), C.byref(h)))
+                                      self._w.ctypes.data_as(C.c_void_p),
+                                      self._owner.ctypes.data_as(C.c_void_p) if self._owner is not None else None,
+                                      C.byref(self._o), C.byref(h)))
         self._h = h
 
     def info(self):
@@ -350,6 +358,22 @@ class FockBuilder:
             Vs = [V[k * nn:(k + 1) * nn].view(self.nbf, self.nbf).t() for k in range(nspin)]
             Jm = J.view(self.nbf, self.nbf).t() if J is not None else None
         return E.value, Vs, Jm
+
+    def xc_gradient(self, C_list, occ_list, becke_clamp=5.0, stream=None):
+        """dE_xc/dR (natoms x 3, Eh/bohr) at fixed orbitals, FP64, with the grid
+        points moving with their owner atoms and the Becke weights
+        differentiated (nkx_xc_gradient)."""
+        nspin = len(C_list)
+        nocc = C_list[0].shape[1]
+        Cc = np.concatenate([np.ascontiguousarray(np.asarray(c, np.float64).T).reshape(-1) for c in C_list])
+        oc = np.concatenate([_np(o, np.float64) for o in occ_list])
+        natoms = len(self._mk[0]) // 3
+        g = np.zeros(3 * natoms)
+        s = C.c_void_p(stream) if stream else None
+        check(L.lib().nkx_xc_gradient(self._h, nspin, nocc, Cc.ctypes.data_as(C.c_void_p),
+                                      oc.ctypes.data_as(C.c_void_p), L.MEM_HOST, becke_clamp,
+                                      g.ctypes.data_as(C.c_void_p), s))
+        return g.reshape(natoms, 3)
 
     def batch_blocks(self):
         """Significant 128-function blocks per batch."""

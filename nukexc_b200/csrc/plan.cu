@@ -237,9 +237,10 @@ __global__ void __launch_bounds__(256) density_fp64_kernel(const double *__restr
 // null) is the weighted fitted Coulomb potential folded into both spins.
 __global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, const double *__restrict__ w,
                                   const double *__restrict__ rho, const double *__restrict__ grad,
-                                  const double *__restrict__ vj, double *__restrict__ coef, double *Eacc) {
+                                  const double *__restrict__ vj, double *__restrict__ coef, double *Eacc,
+                                  double *__restrict__ edens) {
   const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  double e = 0.0;
+  double e = 0.0, fdens = 0.0;
   if (g < npad) {
     const double wg = w[g];
     double vr[2] = {0, 0}, vec[2][3] = {{0, 0, 0}, {0, 0, 0}}, gr[2][3] = {{0, 0, 0}, {0, 0, 0}};
@@ -251,6 +252,7 @@ __global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, cons
         const double sg = gr[0][0] * gr[0][0] + gr[0][1] * gr[0][1] + gr[0][2] * gr[0][2];
         double f, vrho, vs;
         xc_unpol(s, rho[g], sg, f, vrho, vs);
+        fdens = f;
         e = wg * f;
         vr[0] = vrho;
         for (int k = 0; k < 3; ++k) vec[0][k] = 2.0 * vs * gr[0][k];
@@ -260,6 +262,7 @@ __global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, cons
         const double sbb = gr[1][0] * gr[1][0] + gr[1][1] * gr[1][1] + gr[1][2] * gr[1][2];
         double f, d[5];
         xc_pol(s, rho[g], rho[npad + g], saa, sab, sbb, f, d);
+        fdens = f;
         e = wg * f;
         vr[0] = d[0];
         vr[1] = d[1];
@@ -269,6 +272,7 @@ __global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, cons
         }
       }
     }
+    if (edens) edens[g] = fdens;
     const double vjg = vj ? vj[g] : 0.0;
     for (int sp = 0; sp < nspin; ++sp) {
       coef[((size_t)sp * 4 + 0) * npad + g] = wg * 0.5 * vr[sp] + 0.5 * vjg;
@@ -515,6 +519,7 @@ void destroy_mixed_state(void *p);
 
 Plan::~Plan() {
   if (mx_state) destroy_mixed_state(mx_state);
+  if (grad_state) destroy_grad_state(grad_state);
   for (void *p : allocs) cudaFree(p);
   if (cublas) cublasDestroy((cublasHandle_t)cublas);
   if (cusolver) cusolverDnDestroy((cusolverDnHandle_t)cusolver);
@@ -530,7 +535,7 @@ T *Plan::alloc(size_t n) {
 }
 
 static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, const nkx_basis *aux, long npoints,
-                       const double *xyz, const double *w, const nkx_plan_options *opts) {
+                       const double *xyz, const double *w, const int *owner, const nkx_plan_options *opts) {
   NKX_REQUIRE(prim && prim->nbf > 0 && npoints > 0 && xyz && w && opts, NKX_ERR_ARG, "invalid arguments");
   NKX_REQUIRE(opts->batch_points == 0 || opts->batch_points == kBatch, NKX_ERR_UNSUPPORTED,
               "batch_points must be 256");
@@ -608,6 +613,43 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
     } else {
       tab[p] = tab0[0];
       tab[p].norm = 0.0;
+    }
+  }
+  // --- atoms, point owners (plan order) and the atom of every function, for
+  // the nuclear gradient; functions whose centre is on no atom get -1
+  if (mol && mol->natoms > 0 && mol->xyz) {
+    P.natoms = mol->natoms;
+    P.h_centers.assign(mol->xyz, mol->xyz + 3 * (size_t)mol->natoms);
+    P.d_centers = P.alloc<double>(3 * (size_t)P.natoms);
+    NKX_CUDA(cudaMemcpy(P.d_centers, P.h_centers.data(), sizeof(double) * 3 * P.natoms, cudaMemcpyHostToDevice));
+    std::vector<int> fatom(P.nbf_pad, 0);
+    P.all_funcs_on_atoms = true;
+    for (int q = 0; q < P.nbf_pad; ++q) {
+      const int f = P.h_fperm[q];
+      if (f < 0) continue;
+      int best = -1;
+      for (int a = 0; a < P.natoms; ++a) {
+        double d2 = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          const double e = prim->center[3 * f + d] - mol->xyz[3 * a + d];
+          d2 += e * e;
+        }
+        if (d2 < 1e-20) best = a;
+      }
+      if (best < 0) P.all_funcs_on_atoms = false;
+      fatom[q] = std::max(best, 0);
+    }
+    P.d_fatom = P.alloc<int>(P.nbf_pad);
+    NKX_CUDA(cudaMemcpy(P.d_fatom, fatom.data(), sizeof(int) * P.nbf_pad, cudaMemcpyHostToDevice));
+    if (owner) {
+      std::vector<int> ho(P.npad, 0);
+      for (long p = 0; p < npoints; ++p) {
+        const int o = owner[P.perm[p]];
+        NKX_REQUIRE(o >= 0 && o < P.natoms, NKX_ERR_ARG, "point owner outside [0, natoms)");
+        ho[p] = o;
+      }
+      P.d_owner = P.alloc<int>(P.npad);
+      NKX_CUDA(cudaMemcpy(P.d_owner, ho.data(), sizeof(int) * P.npad, cudaMemcpyHostToDevice));
     }
   }
   P.d_fperm = P.alloc<int>(P.nbf_pad);
@@ -875,11 +917,8 @@ void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
     ++P.launches;
 }
 
-void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
-                     StageTimer &T) {
-  const bool multi = P.chunks.size() > 1;
-  const int nzs = nspin + (separateJ ? 1 : 0);
-  // ---- pass A: collocation + density
+// FP64 pass A: collocation + density of every chunk into d_rho / d_grad
+void fp64_density_pass(Plan &P, int nspin, int nocc, cudaStream_t s, StageTimer &T) {
   for (const Chunk &c : P.chunks) {
     const long nb = c.b1 - c.b0;
     if (c.p1 - c.p0 > 0) {
@@ -899,6 +938,14 @@ void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool s
     ++P.launches;
     T.end(s);
   }
+}
+
+void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
+                     StageTimer &T) {
+  const bool multi = P.chunks.size() > 1;
+  const int nzs = nspin + (separateJ ? 1 : 0);
+  // ---- pass A: collocation + density
+  fp64_density_pass(P, nspin, nocc, s, T);
   // ---- J: fit coefficients and fitted potential
   if (needJ) {
     T.begin(ST_COULOMB, s);
@@ -909,7 +956,8 @@ void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool s
   T.begin(ST_FUNC, s);
   NKX_CUDA(cudaMemsetAsync(P.d_E, 0, sizeof(double), s));
   functional_kernel<<<nblk(P.npad, 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.d_w, P.d_rho, P.d_grad,
-                                                      (needJ && fuse) ? P.d_vj : nullptr, P.d_coef, P.d_E);
+                                                      (needJ && fuse) ? P.d_vj : nullptr, P.d_coef, P.d_E,
+                                                      nullptr);
   NKX_LAUNCH_CHECK();
   ++P.launches;
   T.end(s);
@@ -945,25 +993,8 @@ void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool s
   (void)tile;
 }
 
-void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, const double *occ, int mem, int fuse_j,
-                double *E, double *V, double *J, cudaStream_t user) {
-  NKX_REQUIRE(nspin == 1 || nspin == 2, NKX_ERR_ARG, "nspin must be 1 or 2");
-  NKX_REQUIRE(nocc > 0 && C && occ && E && (V || (fuse_j && J)), NKX_ERR_ARG, "invalid arguments");
-  NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
-  NKX_REQUIRE(precision == NKX_PREC_FP64 || precision == NKX_PREC_MIXED, NKX_ERR_ARG, "unknown precision");
-  const bool needJ = P.naux > 0 && (J != nullptr || fuse_j);
-  NKX_REQUIRE(!(fuse_j && P.naux == 0), NKX_ERR_ARG, "fuse_j needs a plan with an aux basis");
-  NKX_REQUIRE(V != nullptr, NKX_ERR_ARG, "V must be given");
-  const bool separateJ = needJ && !fuse_j && J;
-  cudaStream_t s = user ? user : P.stream;
-  P.launches = 0;
-  StageTimer T;
-  cudaEvent_t t0, t1;
-  NKX_CUDA(cudaEventCreate(&t0));
-  NKX_CUDA(cudaEventCreate(&t1));
-  NKX_CUDA(cudaEventRecord(t0, s));
-
-  // orbitals -> Ct[spin][i][f_pad]
+// orbitals -> Ct[spin][i][p] in plan order (host or device C / occ)
+void upload_orbitals(Plan &P, int nspin, int nocc, const double *C, const double *occ, int mem, cudaStream_t s) {
   if (nocc > P.nocc_cap) {
     P.nocc_cap = nocc;
     P.d_Ct = P.alloc<double>((size_t)2 * nocc * P.nbf_pad);
@@ -982,6 +1013,27 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
                                                                                   P.nbf_pad, P.d_Ct);
   NKX_LAUNCH_CHECK();
   ++P.launches;
+}
+
+void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, const double *occ, int mem, int fuse_j,
+                double *E, double *V, double *J, cudaStream_t user) {
+  NKX_REQUIRE(nspin == 1 || nspin == 2, NKX_ERR_ARG, "nspin must be 1 or 2");
+  NKX_REQUIRE(nocc > 0 && C && occ && E && (V || (fuse_j && J)), NKX_ERR_ARG, "invalid arguments");
+  NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
+  NKX_REQUIRE(precision == NKX_PREC_FP64 || precision == NKX_PREC_MIXED, NKX_ERR_ARG, "unknown precision");
+  const bool needJ = P.naux > 0 && (J != nullptr || fuse_j);
+  NKX_REQUIRE(!(fuse_j && P.naux == 0), NKX_ERR_ARG, "fuse_j needs a plan with an aux basis");
+  NKX_REQUIRE(V != nullptr, NKX_ERR_ARG, "V must be given");
+  const bool separateJ = needJ && !fuse_j && J;
+  cudaStream_t s = user ? user : P.stream;
+  P.launches = 0;
+  StageTimer T;
+  cudaEvent_t t0, t1;
+  NKX_CUDA(cudaEventCreate(&t0));
+  NKX_CUDA(cudaEventCreate(&t1));
+  NKX_CUDA(cudaEventRecord(t0, s));
+
+  upload_orbitals(P, nspin, nocc, C, occ, mem, s);
 
   if (precision == NKX_PREC_MIXED && mixed_available(P))
     fock_build_mixed(P, nspin, nocc, needJ, fuse_j != 0, separateJ, s, T);
@@ -1041,12 +1093,11 @@ NKX_API const char *nkx_last_error(void) { return g_last_error.c_str(); }
 NKX_API nkx_status nkx_plan_create(const nkx_molecule *mol, const nkx_basis *prim, const nkx_basis *aux, long npoints,
                                    const double *xyz, const double *w, const int *owner, const nkx_plan_options *opts,
                                    nkx_plan **plan) {
-  (void)owner;
   return run_guarded("nkx_plan_create", [&] {
     NKX_REQUIRE(plan, NKX_ERR_ARG, "plan pointer is NULL");
     *plan = nullptr;
     auto P = std::make_unique<Plan>();
-    build_plan(*P, mol, prim, aux, npoints, xyz, w, opts);
+    build_plan(*P, mol, prim, aux, npoints, xyz, w, owner, opts);
     *plan = reinterpret_cast<nkx_plan *>(P.release());
   });
 }

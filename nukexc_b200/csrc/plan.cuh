@@ -33,6 +33,14 @@ struct Plan {
   StoFunc *d_sto = nullptr;  // basis in plan order (see build_plan)
   std::vector<int> h_fperm;  // plan position -> caller function (-1: padding)
   int *d_fperm = nullptr, *d_finv = nullptr;
+  // atoms (for the nuclear gradient)
+  int natoms = 0;
+  std::vector<double> h_centers;
+  double *d_centers = nullptr;
+  int *d_fatom = nullptr;  // atom of each function, plan order
+  int *d_owner = nullptr;  // owner atom of each point, plan order (null if not given)
+  bool all_funcs_on_atoms = false;
+  void *grad_state = nullptr;
   AuxFunc *d_aux = nullptr;
 
   // screening: pairs of (batch, significant function block), CSR by batch
@@ -113,6 +121,14 @@ struct StageTimer {
 enum { ST_COLLOC = 0, ST_DENSITY = 1, ST_FUNC = 2, ST_COULOMB = 3, ST_ZBUILD = 4, ST_VGEMM = 5 };
 
 bool mixed_available(const Plan &P);
+void upload_orbitals(Plan &P, int nspin, int nocc, const double *C, const double *occ, int mem, cudaStream_t s);
+void fp64_density_pass(Plan &P, int nspin, int nocc, cudaStream_t s, StageTimer &T);
+void launch_colloc(Plan &P, const Chunk &c, cudaStream_t s);
+void destroy_grad_state(void *p);
+__global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, const double *__restrict__ w,
+                                  const double *__restrict__ rho, const double *__restrict__ grad,
+                                  const double *__restrict__ vj, double *__restrict__ coef, double *Eacc,
+                                  double *__restrict__ edens);
 void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
                       StageTimer &T);
 

@@ -48,6 +48,39 @@ NKX_HD inline void sto_value_grad(const StoFunc &f, double px, double py, double
   gz = R * sz + s * dz * cR;
 }
 
+// value, gradient and Hessian (h = xx, xy, xz, yy, yz, zz):
+// with R(r) = N r^k e^(-zeta r), R' = (k/r - zeta) R, R'' = ((k/r - zeta)^2 - k/r^2) R,
+// d_j R = (R'/r) d_j and d_j d_k R = (R'/r) delta_jk + (R'' - R'/r) d_j d_k / r^2;
+// phi = R S gives d_j d_k phi = d_j d_k R S + d_j R d_k S + d_k R d_j S + R d_j d_k S.
+// The radial derivative terms are dropped at r = 0 (as in sto_value_grad).
+NKX_HD inline void sto_value_grad_hess(const StoFunc &f, double px, double py, double pz, double &v, double g[3],
+                                       double h[6]) {
+  const double d[3] = {px - f.cx, py - f.cy, pz - f.cz};
+  const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  const double R = f.norm * ipow(r, f.k) * exp(-f.zeta * r);
+  double s, sg[3], sh[6];
+  solid_harmonic_grad(f.l, f.m, d[0], d[1], d[2], s, sg[0], sg[1], sg[2]);
+  solid_harmonic_hess(f.l, f.m, d[0], d[1], d[2], sh[0], sh[1], sh[2], sh[3], sh[4], sh[5]);
+  double cR = 0.0, dd = 0.0;
+  if (r > 0.0) {
+    const double a = f.k / r - f.zeta;
+    cR = a * R / r;
+    dd = ((a * a - f.k / (r * r)) * R - cR) / (r * r);
+  }
+  v = R * s;
+  double dR[3];
+  for (int j = 0; j < 3; ++j) {
+    dR[j] = cR * d[j];
+    g[j] = dR[j] * s + R * sg[j];
+  }
+  const int ij[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  for (int e = 0; e < 6; ++e) {
+    const int j = ij[e][0], k = ij[e][1];
+    const double d2R = (j == k ? cR : 0.0) + dd * d[j] * d[k];
+    h[e] = d2R * s + dR[j] * sg[k] + dR[k] * sg[j] + R * sh[e];
+  }
+}
+
 // Radial factor cache for consecutive functions of one lane: functions of a
 // shell (same centre, zeta and n - l - 1) share r, R(r) and dR/dr / r.
 struct RadialCache {

@@ -711,9 +711,6 @@ static void launch_i8(MixedState &M, const CUtensorMap &mA, const CUtensorMap &m
   NKX_LAUNCH_CHECK();
 }
 
-__global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, const double *__restrict__ w,
-                                  const double *__restrict__ rho, const double *__restrict__ grad,
-                                  const double *__restrict__ vj, double *__restrict__ coef, double *Eacc);
 void coulomb_fit(Plan &P, int nspin, cudaStream_t s);
 
 template <bool GRAD>
@@ -809,7 +806,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
   NKX_CUDA(cudaMemsetAsync(P.d_E, 0, sizeof(double), s));
   functional_kernel<<<(unsigned)((P.npad + 255) / 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.d_w, P.d_rho,
                                                                       P.d_grad, (needJ && fuse) ? P.d_vj : nullptr,
-                                                                      P.d_coef, P.d_E);
+                                                                      P.d_coef, P.d_E, nullptr);
   NKX_LAUNCH_CHECK();
   ++P.launches;
   Tm.end(s);
