@@ -228,6 +228,7 @@ def run_nkx(args):
     import torch
     from nukexc_b200 import api as A
     from nukexc_b200 import molecules as M  # noqa: F401
+    from nukexc_b200 import shard as S
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -243,8 +244,7 @@ def run_nkx(args):
     c, Z, funcs, Cm = workload(args.waters)
     g = A.make_flat_grid(c, Z, 75, 29, weight_threshold=1e-15, radial="ta")
     # strong scaling: rank r integrates the points of its share of atoms
-    lo, hi = (len(Z) * rank) // world, (len(Z) * (rank + 1)) // world
-    sel = (g.point_owner >= lo) & (g.point_owner < hi)
+    sel = S.select_points(g.point_owner, len(Z), rank, world)
     pts, w = g.quad_points[sel], g.weights[sel]
     b = A.make_manual_basis(funcs)
     t0 = time.perf_counter()
@@ -272,9 +272,7 @@ def run_nkx(args):
             E, V, _ = fb.build([Cd], [od], precision=prec, stream=stream.cuda_stream)
             V = V[0]
         if dist is not None:
-            buf = torch.cat([V.reshape(-1), torch.tensor([E], dtype=torch.float64, device="cuda")])
-            dist.all_reduce(buf)
-            E = buf[-1].item()
+            E, _ = S.allreduce_fock(E, [V], dist)
         return E
 
     for _ in range(args.warmup):
