@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--cpu-sample", type=int, default=8192, help="points in the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--aux", action="store_true",
+                    help="add the grid density-fitted J (aux zeta_k = 0.3*1.8^k up to l = 3) fused into V")
     ap.add_argument("--workspace-mb", type=int, default=0,
                     help="cap on the per-chunk collocation workspace in MiB (0: automatic); more chunks, same work")
     return ap.parse_args()
@@ -62,7 +64,8 @@ def workload(n):
 
 
 def config(args, extra=None):
-    cfg = {"workload": f"(H2O)_{args.waters} PBE XC Fock build", "waters": args.waters,
+    name = f"(H2O)_{args.waters} PBE XC" + (" + DF-J" if getattr(args, "aux", False) else "") + " Fock build"
+    cfg = {"workload": name, "waters": args.waters,
            "basis": "even-tempered STO zeta_k=0.5*2.2^k, O 6s4p2d, H 4s2p",
            "grid": "Treutler-Ahlrichs M4 75 x Lebedev 302 per atom, Becke (Laqua clamp), w>1e-15",
            "batch_points": 256, "screen_tol": 1e-10, "nocc": 5 * args.waters, "occ": 1.0,
@@ -248,7 +251,11 @@ def run_nkx(args):
     pts, w = g.quad_points[sel], g.weights[sel]
     b = A.make_manual_basis(funcs)
     t0 = time.perf_counter()
-    fb = A.FockBuilder(c, Z, b, (pts, w), func_ids=FUNCS, workspace_bytes=args.workspace_mb << 20)
+    if args.aux and world > 1:
+        raise SystemExit("--aux: the fitted J needs the all-reduced y before the solve; run it on one GPU")
+    aux = A.make_manual_basis(M.aux_basis(c, Z)) if args.aux else None
+    fb = A.FockBuilder(c, Z, b, (pts, w), aux=aux, func_ids=FUNCS, workspace_bytes=args.workspace_mb << 20)
+    fuse = bool(args.aux)
     setup_s = time.perf_counter() - t0
     info = fb.info()
     nbf = len(funcs)
@@ -259,17 +266,17 @@ def run_nkx(args):
     prec = args.precision
     if prec == "auto":
         try:
-            fb.build([Cd], [od], precision="mixed", stream=stream.cuda_stream)
+            fb.build([Cd], [od], precision="mixed", fuse_j=fuse, stream=stream.cuda_stream)
             prec = "mixed"
         except Exception:
             prec = "fp64"
 
     def step(host=False):
         if host:
-            E, V, _ = fb.build([Cm], [occ], precision=prec, stream=stream.cuda_stream)
+            E, V, _ = fb.build([Cm], [occ], precision=prec, fuse_j=fuse, stream=stream.cuda_stream)
             V = torch.as_tensor(V[0], device="cuda")
         else:
-            E, V, _ = fb.build([Cd], [od], precision=prec, stream=stream.cuda_stream)
+            E, V, _ = fb.build([Cd], [od], precision=prec, fuse_j=fuse, stream=stream.cuda_stream)
             V = V[0]
         if dist is not None:
             E, _ = S.allreduce_fock(E, [V], dist)
@@ -306,15 +313,15 @@ def run_nkx(args):
     # the same-GPU FP64 kernels on the same build, and the accuracy gate
     fp64 = None
     if prec == "mixed":
-        E_m, V_m, _ = fb.build([Cd], [od], precision="mixed", stream=stream.cuda_stream)
+        E_m, V_m, _ = fb.build([Cd], [od], precision="mixed", fuse_j=fuse, stream=stream.cuda_stream)
         V_m = V_m[0].clone()
-        E_d, V_d, _ = fb.build([Cd], [od], precision="fp64", stream=stream.cuda_stream)
+        E_d, V_d, _ = fb.build([Cd], [od], precision="fp64", fuse_j=fuse, stream=stream.cuda_stream)
         torch.cuda.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         nf = max(1, min(args.steps, 2))
         f0.record(stream)
         for _ in range(nf):
-            fb.build([Cd], [od], precision="fp64", stream=stream.cuda_stream)
+            fb.build([Cd], [od], precision="fp64", fuse_j=fuse, stream=stream.cuda_stream)
         f1.record(stream)
         torch.cuda.synchronize()
         fms = f0.elapsed_time(f1) / nf

@@ -89,6 +89,23 @@ std::vector<AuxFunc> make_aux_table(const nkx_basis &b) {
   return t;
 }
 
+std::vector<AuxShell> make_aux_shells(const std::vector<AuxFunc> &t) {
+  std::vector<AuxShell> sh;
+  for (int i = 0; i < (int)t.size(); ++i) {
+    if (!sh.empty()) {
+      AuxShell &s = sh.back();
+      const AuxFunc &f = s.f, &g = t[i];
+      if (g.cx == f.cx && g.cy == f.cy && g.cz == f.cz && g.zeta == f.zeta && g.a == f.a && g.l == f.l &&
+          g.m == f.m + s.nm && g.m <= g.l && s.first + s.nm == i) {
+        ++s.nm;
+        continue;
+      }
+    }
+    sh.push_back(AuxShell{t[i], i, 1});
+  }
+  return sh;
+}
+
 bool lebedev_rule(int order, std::vector<double> &xyz, std::vector<double> &w) {
   int ri = -1;
   for (int i = 0; i < kLebedevNumRules; ++i)

@@ -46,6 +46,8 @@ double sto_cutoff(int n, double zeta, double tol);
 
 std::vector<StoFunc> make_sto_table(const nkx_basis &b);
 std::vector<AuxFunc> make_aux_table(const nkx_basis &b);
+// shells of consecutive functions sharing centre, zeta, n and l with m rising by 1
+std::vector<AuxShell> make_aux_shells(const std::vector<AuxFunc> &t);
 std::vector<double> make_cutoffs(const nkx_basis &b, double tol);
 
 // Lebedev rule of algebraic order >= order: unit vectors (xyz) and weights

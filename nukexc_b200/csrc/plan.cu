@@ -419,56 +419,79 @@ __global__ void pack_orbitals_kernel(const double *__restrict__ C, const int *__
   Ct[e] = f >= 0 ? C[si * nbf + f] : 0.0;
 }
 
-// y_a += sum over a slice of points of w_g V_a(g) rho_g   (coulomb.hpp:84-85)
-__global__ void aux_y_kernel(const AuxFunc *__restrict__ aux, const double *__restrict__ px,
-                             const double *__restrict__ py, const double *__restrict__ pz,
-                             const double *__restrict__ w, const double *__restrict__ rho, int nspin, long npad,
-                             long slice, double *__restrict__ y) {
-  const int a = blockIdx.x;
-  const AuxFunc f = aux[a];
+// y_a += sum over a slice of points of w_g rho_g V_a(g) for the functions of
+// one aux shell: the radial factor once per point, then C S_lm per m
+// (coulomb.hpp:84-85).  Every thread of a block works on the same shell, so
+// the solid-harmonic branch is uniform.
+__global__ void aux_y_shell_kernel(const AuxShell *__restrict__ shells, const double *__restrict__ px,
+                                   const double *__restrict__ py, const double *__restrict__ pz,
+                                   const double *__restrict__ w, const double *__restrict__ rho, int nspin, long npad,
+                                   long slice, double *__restrict__ y) {
+  const AuxShell sh = shells[blockIdx.x];
+  const AuxFunc &f = sh.f;
   const long g0 = blockIdx.y * slice, g1 = min(npad, g0 + slice);
-  double s = 0.0;
+  double acc[15];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) acc[k] = 0.0;
   for (long g = g0 + threadIdx.x; g < g1; g += blockDim.x) {
     double r = rho[g];
     if (nspin == 2) r += rho[npad + g];
     const double wr = w[g] * r;
-    if (wr != 0.0) s += wr * aux_potential(f, px[g], py[g], pz[g]);
+    if (wr == 0.0) continue;
+    const double dx = px[g] - f.cx, dy = py[g] - f.cy, dz = pz[g] - f.cz;
+    const double wI = wr * aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz));
+#pragma unroll
+    for (int k = 0; k < 15; ++k)
+      if (k < sh.nm) acc[k] += wI * (f.C * solid_harmonic(f.l, f.m + k, dx, dy, dz));
   }
   __shared__ double red[32];
-  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+  for (int k = 0; k < sh.nm; ++k) {
+    double s = acc[0];
+#pragma unroll
+    for (int q = 1; q < 15; ++q)
+      if (q == k) s = acc[q];
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) atomicAdd(y + a, s);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+      for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (threadIdx.x == 0) atomicAdd(y + sh.first + k, s);
+    }
   }
 }
 
-// v_g = w_g sum_a c_a V_a(g)   (coulomb.hpp:93-95)
-__global__ void aux_v_kernel(const AuxFunc *__restrict__ aux, int naux, const double *__restrict__ c,
-                             const double *__restrict__ px, const double *__restrict__ py,
-                             const double *__restrict__ pz, const double *__restrict__ w, long npad,
-                             double *__restrict__ v) {
-  __shared__ AuxFunc sf[64];
-  __shared__ double sc[64];
+// v_g = w_g sum_a c_a V_a(g), shell by shell (coulomb.hpp:90-95)
+__global__ void aux_v_shell_kernel(const AuxShell *__restrict__ shells, int nshell, const double *__restrict__ c,
+                                   const double *__restrict__ px, const double *__restrict__ py,
+                                   const double *__restrict__ pz, const double *__restrict__ w, long npad,
+                                   double *__restrict__ v) {
+  __shared__ AuxShell ss[32];
+  __shared__ double sc[32][15];
   const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const bool on = g < npad;
-  const double x = on ? px[g] : 0.0, y = on ? py[g] : 0.0, z = on ? pz[g] : 0.0;
+  const bool on = g < npad && w[g] != 0.0;
+  const double x = g < npad ? px[g] : 0.0, y = g < npad ? py[g] : 0.0, z = g < npad ? pz[g] : 0.0;
   double s = 0.0;
-  for (int a0 = 0; a0 < naux; a0 += 64) {
+  for (int s0 = 0; s0 < nshell; s0 += 32) {
     __syncthreads();
-    for (int e = threadIdx.x; e < 64; e += blockDim.x)
-      if (a0 + e < naux) {
-        sf[e] = aux[a0 + e];
-        sc[e] = c[a0 + e];
+    for (int e = threadIdx.x; e < 32; e += blockDim.x)
+      if (s0 + e < nshell) {
+        ss[e] = shells[s0 + e];
+        for (int k = 0; k < 15; ++k) sc[e][k] = k < ss[e].nm ? c[ss[e].first + k] : 0.0;
       }
     __syncthreads();
-    const int na = min(64, naux - a0);
+    const int ns = min(32, nshell - s0);
     if (on)
-      for (int k = 0; k < na; ++k) s += sc[k] * aux_potential(sf[k], x, y, z);
+      for (int q = 0; q < ns; ++q) {
+        const AuxFunc &f = ss[q].f;
+        const double dx = x - f.cx, dy = y - f.cy, dz = z - f.cz;
+        double a = 0.0;
+        for (int k = 0; k < ss[q].nm; ++k) a += sc[q][k] * (f.C * solid_harmonic(f.l, f.m + k, dx, dy, dz));
+        if (a != 0.0) s += a * aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz));
+      }
   }
-  if (on) v[g] = s * w[g];
+  if (g < npad) v[g] = on ? s * w[g] : 0.0;
 }
 
 // Aux collocation phi_A(g) and weighted potential Vw_B(g) of a slice of
@@ -753,11 +776,19 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
 
   // --- aux metric and its factor
   if (aux && aux->nbf > 0) {
+    for (int i = 0; i < aux->nbf; ++i)
+      NKX_REQUIRE(aux->l[i] >= 0 && aux->l[i] <= 7 && aux->n[i] > aux->l[i] && abs(aux->m[i]) <= aux->l[i] &&
+                      aux->zeta[i] > 0,
+                  NKX_ERR_UNSUPPORTED, "aux function outside n > l, |m| <= l <= 7, zeta > 0");
     P.naux = aux->nbf;
     auto atab = make_aux_table(*aux);
     auto astab = make_sto_table(*aux);
     P.d_aux = P.alloc<AuxFunc>(P.naux);
     NKX_CUDA(cudaMemcpy(P.d_aux, atab.data(), sizeof(AuxFunc) * P.naux, cudaMemcpyHostToDevice));
+    const auto ash = make_aux_shells(atab);
+    P.nashell = (int)ash.size();
+    P.d_ashell = P.alloc<AuxShell>(ash.size());
+    NKX_CUDA(cudaMemcpy(P.d_ashell, ash.data(), sizeof(AuxShell) * ash.size(), cudaMemcpyHostToDevice));
     StoFunc *d_asto = dalloc<StoFunc>(P.naux);
     NKX_CUDA(cudaMemcpy(d_asto, astab.data(), sizeof(StoFunc) * P.naux, cudaMemcpyHostToDevice));
     const size_t NA = P.naux;
@@ -886,8 +917,8 @@ void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
     NKX_CUDA(cudaMemsetAsync(P.d_y, 0, sizeof(double) * P.naux, s));
     const long nsl = std::max<long>(1, std::min<long>(64, (P.npad + 4095) / 4096));
     const long slice = (P.npad + nsl - 1) / nsl;
-    aux_y_kernel<<<dim3(P.naux, (unsigned)nsl), 256, 0, s>>>(P.d_aux, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin,
-                                                            P.npad, slice, P.d_y);
+    aux_y_shell_kernel<<<dim3(P.nashell, (unsigned)nsl), 256, 0, s>>>(P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w,
+                                                                     P.d_rho, nspin, P.npad, slice, P.d_y);
     NKX_LAUNCH_CHECK();
     ++P.launches;
     if (P.svd_mode) {
@@ -911,8 +942,8 @@ void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
       NKX_LAUNCH_CHECK();
       P.launches += 2;
     }
-    aux_v_kernel<<<nblk(P.npad, 128), 128, 0, s>>>(P.d_aux, P.naux, P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad,
-                                                   P.d_vj);
+    aux_v_shell_kernel<<<nblk(P.npad, 128), 128, 0, s>>>(P.d_ashell, P.nashell, P.d_c, P.d_px, P.d_py, P.d_pz,
+                                                         P.d_w, P.npad, P.d_vj);
     NKX_LAUNCH_CHECK();
     ++P.launches;
 }

@@ -42,6 +42,8 @@ struct Plan {
   bool all_funcs_on_atoms = false;
   void *grad_state = nullptr;
   AuxFunc *d_aux = nullptr;
+  AuxShell *d_ashell = nullptr;
+  int nashell = 0;
 
   // screening: pairs of (batch, significant function block), CSR by batch
   std::vector<int> h_pair_off;

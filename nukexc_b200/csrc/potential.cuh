@@ -54,23 +54,27 @@ NKX_HD inline double lower_gamma_int(int n, double x) {
   return fact_d(n - 1) - upper_gamma_int(n, x);
 }
 
+// radial factor I(r) of V_a = C S_lm I(r); shared by the 2l+1 functions of a shell
+NKX_HD inline double aux_radial(const AuxFunc &f, double r) {
+  if (r < 1e-12) return fact_d(f.b - 1) * f.zb;
+  const double zr = f.zeta * r;
+  const double r2l1 = ipow(r, 2 * f.l + 1);
+  if (zr > f.xfar) return f.ga_full / r2l1;
+  return lower_gamma_int(f.a, zr) * (f.ga_full / fact_d(f.a - 1)) / r2l1 + upper_gamma_int(f.b, zr) * f.zb;
+}
+
 NKX_HD inline double aux_potential(const AuxFunc &f, double px, double py, double pz) {
   const double dx = px - f.cx, dy = py - f.cy, dz = pz - f.cz;
   const double r = sqrt(dx * dx + dy * dy + dz * dz);
-  const double S = solid_harmonic(f.l, f.m, dx, dy, dz);
-  double I;
-  if (r < 1e-12) {
-    I = fact_d(f.b - 1) * f.zb;
-  } else {
-    const double zr = f.zeta * r;
-    const double r2l1 = ipow(r, 2 * f.l + 1);
-    if (zr > f.xfar) {
-      I = f.ga_full / r2l1;
-    } else {
-      I = lower_gamma_int(f.a, zr) * (f.ga_full / fact_d(f.a - 1)) / r2l1 + upper_gamma_int(f.b, zr) * f.zb;
-    }
-  }
-  return f.C * S * I;
+  return f.C * solid_harmonic(f.l, f.m, dx, dy, dz) * aux_radial(f, r);
 }
+
+// Consecutive aux functions with one centre, zeta, n and l and m running
+// m0, m0+1, ... : the radial factor is evaluated once for all of them.
+struct AuxShell {
+  AuxFunc f;  // the shell's first function (its m is m0)
+  int first;  // index of the first function
+  int nm;     // number of functions (<= 2l+1)
+};
 
 }  // namespace nkx
