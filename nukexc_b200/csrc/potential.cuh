@@ -23,17 +23,37 @@ struct AuxFunc {
   int a, b, l, m;
 };
 
+#ifdef __CUDACC__
+__constant__ const double kInvIntDev[65] = {
+    0.0,        1.0 / 1,  1.0 / 2,  1.0 / 3,  1.0 / 4,  1.0 / 5,  1.0 / 6,  1.0 / 7,  1.0 / 8,  1.0 / 9,  1.0 / 10,
+    1.0 / 11,   1.0 / 12, 1.0 / 13, 1.0 / 14, 1.0 / 15, 1.0 / 16, 1.0 / 17, 1.0 / 18, 1.0 / 19, 1.0 / 20, 1.0 / 21,
+    1.0 / 22,   1.0 / 23, 1.0 / 24, 1.0 / 25, 1.0 / 26, 1.0 / 27, 1.0 / 28, 1.0 / 29, 1.0 / 30, 1.0 / 31, 1.0 / 32,
+    1.0 / 33,   1.0 / 34, 1.0 / 35, 1.0 / 36, 1.0 / 37, 1.0 / 38, 1.0 / 39, 1.0 / 40, 1.0 / 41, 1.0 / 42, 1.0 / 43,
+    1.0 / 44,   1.0 / 45, 1.0 / 46, 1.0 / 47, 1.0 / 48, 1.0 / 49, 1.0 / 50, 1.0 / 51, 1.0 / 52, 1.0 / 53, 1.0 / 54,
+    1.0 / 55,   1.0 / 56, 1.0 / 57, 1.0 / 58, 1.0 / 59, 1.0 / 60, 1.0 / 61, 1.0 / 62, 1.0 / 63, 1.0 / 64};
+#endif
+
 NKX_HD inline double fact_d(int n) {
   double r = 1.0;
   for (int i = 2; i <= n; ++i) r *= i;
   return r;
 }
 
+// 1/k for k = 0..64 (entry 0 unused): the series below multiply by these
+// instead of dividing
+NKX_HD inline double inv_int(int k) {
+#ifdef __CUDA_ARCH__
+  return kInvIntDev[k];
+#else
+  return 1.0 / k;
+#endif
+}
+
 // Gamma(n, x) for integer n >= 1: (n-1)! e^-x sum_{k<n} x^k/k!
 NKX_HD inline double upper_gamma_int(int n, double x) {
   double sum = 1.0, term = 1.0;
   for (int k = 1; k < n; ++k) {
-    term *= x / k;
+    term *= x * (k <= 64 ? inv_int(k) : 1.0 / k);
     sum += term;
   }
   return fact_d(n - 1) * exp(-x) * sum;
@@ -43,9 +63,9 @@ NKX_HD inline double upper_gamma_int(int n, double x) {
 // (n-1)! - Gamma(n, x) (nukexc_utils.hpp:169-196)
 NKX_HD inline double lower_gamma_int(int n, double x) {
   if (x < n) {
-    double sum = 1.0 / n, term = 1.0 / n;
+    double sum = n <= 64 ? inv_int(n) : 1.0 / n, term = sum;
     for (int k = 1; k < 1000; ++k) {
-      term *= x / (n + k);
+      term *= x * (n + k <= 64 ? inv_int(n + k) : 1.0 / (n + k));
       sum += term;
       if (term < 1e-16 * sum) break;
     }
