@@ -106,6 +106,30 @@ std::vector<AuxShell> make_aux_shells(const std::vector<AuxFunc> &t) {
   return sh;
 }
 
+std::vector<AuxGroup> make_aux_groups(const std::vector<AuxShell> &sh, std::vector<int> &loose) {
+  std::vector<AuxGroup> g;
+  loose.clear();
+  for (int i = 0; i < (int)sh.size(); ++i) {
+    const AuxFunc &f = sh[i].f;
+    const bool complete = f.l <= 3 && sh[i].nm == 2 * f.l + 1 && f.m == -f.l;
+    if (!complete) {
+      loose.push_back(i);
+      continue;
+    }
+    if (!g.empty()) {
+      AuxGroup &G = g.back();
+      if (G.first + G.n == i && G.l == f.l && G.cx == f.cx && G.cy == f.cy && G.cz == f.cz &&
+          G.n < aux_group_max(f.l)) {
+        ++G.n;
+        continue;
+      }
+    }
+    g.push_back(AuxGroup{f.cx, f.cy, f.cz, f.l, i, 1});
+  }
+  std::stable_sort(g.begin(), g.end(), [](const AuxGroup &a, const AuxGroup &b) { return a.l < b.l; });
+  return g;
+}
+
 bool lebedev_rule(int order, std::vector<double> &xyz, std::vector<double> &w) {
   int ri = -1;
   for (int i = 0; i < kLebedevNumRules; ++i)

@@ -48,6 +48,9 @@ std::vector<StoFunc> make_sto_table(const nkx_basis &b);
 std::vector<AuxFunc> make_aux_table(const nkx_basis &b);
 // shells of consecutive functions sharing centre, zeta, n and l with m rising by 1
 std::vector<AuxShell> make_aux_shells(const std::vector<AuxFunc> &t);
+// groups of complete shells (l <= 3) sharing a centre and l, sorted by l
+// (stable); loose receives the indices of the remaining shells
+std::vector<AuxGroup> make_aux_groups(const std::vector<AuxShell> &sh, std::vector<int> &loose);
 std::vector<double> make_cutoffs(const nkx_basis &b, double tol);
 
 // Lebedev rule of algebraic order >= order: unit vectors (xyz) and weights

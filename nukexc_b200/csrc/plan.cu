@@ -423,11 +423,12 @@ __global__ void pack_orbitals_kernel(const double *__restrict__ C, const int *__
 // one aux shell: the radial factor once per point, then C S_lm per m
 // (coulomb.hpp:84-85).  Every thread of a block works on the same shell, so
 // the solid-harmonic branch is uniform.
-__global__ void aux_y_shell_kernel(const AuxShell *__restrict__ shells, const double *__restrict__ px,
-                                   const double *__restrict__ py, const double *__restrict__ pz,
-                                   const double *__restrict__ w, const double *__restrict__ rho, int nspin, long npad,
-                                   long slice, double *__restrict__ y) {
-  const AuxShell sh = shells[blockIdx.x];
+__global__ void aux_y_shell_kernel(const AuxShell *__restrict__ shells, const int *__restrict__ list,
+                                   const double *__restrict__ px, const double *__restrict__ py,
+                                   const double *__restrict__ pz, const double *__restrict__ w,
+                                   const double *__restrict__ rho, int nspin, long npad, long slice,
+                                   double *__restrict__ y) {
+  const AuxShell sh = shells[list[blockIdx.x]];
   const AuxFunc &f = sh.f;
   const long g0 = blockIdx.y * slice, g1 = min(npad, g0 + slice);
   double acc[15];
@@ -462,36 +463,113 @@ __global__ void aux_y_shell_kernel(const AuxShell *__restrict__ shells, const do
   }
 }
 
-// v_g = w_g sum_a c_a V_a(g), shell by shell (coulomb.hpp:90-95)
-__global__ void aux_v_shell_kernel(const AuxShell *__restrict__ shells, int nshell, const double *__restrict__ c,
+// y over the functions of one (centre, l) group of complete shells: per
+// point one distance, one set of 2L+1 solid harmonics, then the radial factor
+// of each shell (coulomb.hpp:84-85).
+template <int L>
+__global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const AuxShell *__restrict__ shells,
                                    const double *__restrict__ px, const double *__restrict__ py,
-                                   const double *__restrict__ pz, const double *__restrict__ w, long npad,
-                                   double *__restrict__ v) {
-  __shared__ AuxShell ss[32];
-  __shared__ double sc[32][15];
-  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const bool on = g < npad && w[g] != 0.0;
-  const double x = g < npad ? px[g] : 0.0, y = g < npad ? py[g] : 0.0, z = g < npad ? pz[g] : 0.0;
-  double s = 0.0;
-  for (int s0 = 0; s0 < nshell; s0 += 32) {
-    __syncthreads();
-    for (int e = threadIdx.x; e < 32; e += blockDim.x)
-      if (s0 + e < nshell) {
-        ss[e] = shells[s0 + e];
-        for (int k = 0; k < 15; ++k) sc[e][k] = k < ss[e].nm ? c[ss[e].first + k] : 0.0;
-      }
-    __syncthreads();
-    const int ns = min(32, nshell - s0);
-    if (on)
-      for (int q = 0; q < ns; ++q) {
-        const AuxFunc &f = ss[q].f;
-        const double dx = x - f.cx, dy = y - f.cy, dz = z - f.cz;
-        double a = 0.0;
-        for (int k = 0; k < ss[q].nm; ++k) a += sc[q][k] * (f.C * solid_harmonic(f.l, f.m + k, dx, dy, dz));
-        if (a != 0.0) s += a * aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz));
-      }
+                                   const double *__restrict__ pz, const double *__restrict__ w,
+                                   const double *__restrict__ rho, int nspin, long npad, long slice,
+                                   double *__restrict__ y) {
+  constexpr int NM = 2 * L + 1, QM = aux_group_max(L);
+  const AuxGroup G = groups[blockIdx.x];
+  const long g0 = blockIdx.y * slice, g1 = min(npad, g0 + slice);
+  double acc[QM][NM];
+#pragma unroll
+  for (int q = 0; q < QM; ++q)
+#pragma unroll
+    for (int m = 0; m < NM; ++m) acc[q][m] = 0.0;
+  for (long g = g0 + threadIdx.x; g < g1; g += blockDim.x) {
+    double r = rho[g];
+    if (nspin == 2) r += rho[npad + g];
+    const double wr = w[g] * r;
+    if (wr == 0.0) continue;
+    const double dx = px[g] - G.cx, dy = py[g] - G.cy, dz = pz[g] - G.cz;
+    const double rr = sqrt(dx * dx + dy * dy + dz * dz);
+    double S[NM];
+    solid_harmonics_all<L>(dx, dy, dz, S);
+#pragma unroll
+    for (int q = 0; q < QM; ++q) {
+      if (q >= G.n) break;
+      const AuxFunc &f = shells[G.first + q].f;
+      const double wI = wr * aux_radial(f, rr);
+#pragma unroll
+      for (int m = 0; m < NM; ++m) acc[q][m] += wI * (f.C * S[m]);
+    }
   }
-  if (g < npad) v[g] = on ? s * w[g] : 0.0;
+  __shared__ double red[32];
+#pragma unroll
+  for (int q = 0; q < QM; ++q) {
+    if (q >= G.n) break;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+      double s = acc[q][m];
+      for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      __syncthreads();
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) atomicAdd(y + shells[G.first + q].first + m, s);
+      }
+    }
+  }
+}
+
+template <int L>
+__device__ __forceinline__ double aux_group_v(const AuxGroup &G, const AuxShell *__restrict__ shells,
+                                              const double *__restrict__ c, double x, double y, double z) {
+  constexpr int NM = 2 * L + 1;
+  const double dx = x - G.cx, dy = y - G.cy, dz = z - G.cz;
+  const double rr = sqrt(dx * dx + dy * dy + dz * dz);
+  double S[NM];
+  solid_harmonics_all<L>(dx, dy, dz, S);
+  double s = 0.0;
+  for (int q = 0; q < G.n; ++q) {
+    const AuxShell &sh = shells[G.first + q];
+    double a = 0.0;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) a += c[sh.first + m] * (sh.f.C * S[m]);
+    if (a != 0.0) s += a * aux_radial(sh.f, rr);
+  }
+  return s;
+}
+
+// v_g = w_g sum_a c_a V_a(g) over the groups, then the loose shells
+// (coulomb.hpp:90-95)
+__global__ void aux_v_group_kernel(const AuxGroup *__restrict__ groups, int ngroup,
+                                   const AuxShell *__restrict__ shells, const int *__restrict__ loose, int nloose,
+                                   const double *__restrict__ c, const double *__restrict__ px,
+                                   const double *__restrict__ py, const double *__restrict__ pz,
+                                   const double *__restrict__ w, long npad, double *__restrict__ v) {
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (g >= npad) return;
+  if (w[g] == 0.0) {
+    v[g] = 0.0;
+    return;
+  }
+  const double x = px[g], y = py[g], z = pz[g];
+  double s = 0.0;
+  for (int k = 0; k < ngroup; ++k) {
+    const AuxGroup G = groups[k];
+    switch (G.l) {
+      case 0: s += aux_group_v<0>(G, shells, c, x, y, z); break;
+      case 1: s += aux_group_v<1>(G, shells, c, x, y, z); break;
+      case 2: s += aux_group_v<2>(G, shells, c, x, y, z); break;
+      default: s += aux_group_v<3>(G, shells, c, x, y, z); break;
+    }
+  }
+  for (int k = 0; k < nloose; ++k) {
+    const AuxShell &sh = shells[loose[k]];
+    const AuxFunc &f = sh.f;
+    const double dx = x - f.cx, dy = y - f.cy, dz = z - f.cz;
+    double a = 0.0;
+    for (int m = 0; m < sh.nm; ++m) a += c[sh.first + m] * (f.C * solid_harmonic(f.l, f.m + m, dx, dy, dz));
+    if (a != 0.0) s += a * aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz));
+  }
+  v[g] = s * w[g];
 }
 
 // Aux collocation phi_A(g) and weighted potential Vw_B(g) of a slice of
@@ -789,6 +867,19 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
     P.nashell = (int)ash.size();
     P.d_ashell = P.alloc<AuxShell>(ash.size());
     NKX_CUDA(cudaMemcpy(P.d_ashell, ash.data(), sizeof(AuxShell) * ash.size(), cudaMemcpyHostToDevice));
+    std::vector<int> loose;
+    const auto grp = make_aux_groups(ash, loose);
+    P.nagroup = (int)grp.size();
+    P.nloose = (int)loose.size();
+    P.h_group_off.assign(5, 0);
+    for (const AuxGroup &G : grp) ++P.h_group_off[G.l + 1];
+    for (int L = 0; L < 4; ++L) P.h_group_off[L + 1] += P.h_group_off[L];
+    P.d_agroup = P.alloc<AuxGroup>(std::max<size_t>(1, grp.size()));
+    if (!grp.empty())
+      NKX_CUDA(cudaMemcpy(P.d_agroup, grp.data(), sizeof(AuxGroup) * grp.size(), cudaMemcpyHostToDevice));
+    P.d_loose = P.alloc<int>(std::max<size_t>(1, loose.size()));
+    if (!loose.empty())
+      NKX_CUDA(cudaMemcpy(P.d_loose, loose.data(), sizeof(int) * loose.size(), cudaMemcpyHostToDevice));
     StoFunc *d_asto = dalloc<StoFunc>(P.naux);
     NKX_CUDA(cudaMemcpy(d_asto, astab.data(), sizeof(StoFunc) * P.naux, cudaMemcpyHostToDevice));
     const size_t NA = P.naux;
@@ -917,10 +1008,26 @@ void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
     NKX_CUDA(cudaMemsetAsync(P.d_y, 0, sizeof(double) * P.naux, s));
     const long nsl = std::max<long>(1, std::min<long>(64, (P.npad + 4095) / 4096));
     const long slice = (P.npad + nsl - 1) / nsl;
-    aux_y_shell_kernel<<<dim3(P.nashell, (unsigned)nsl), 256, 0, s>>>(P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w,
-                                                                     P.d_rho, nspin, P.npad, slice, P.d_y);
-    NKX_LAUNCH_CHECK();
-    ++P.launches;
+    for (int L = 0; L <= 3; ++L) {
+      const int n = P.h_group_off[L + 1] - P.h_group_off[L];
+      if (n == 0) continue;
+      const AuxGroup *gp = P.d_agroup + P.h_group_off[L];
+      const dim3 gy((unsigned)n, (unsigned)nsl);
+      switch (L) {
+        case 0: aux_y_group_kernel<0><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, P.d_y); break;
+        case 1: aux_y_group_kernel<1><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, P.d_y); break;
+        case 2: aux_y_group_kernel<2><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, P.d_y); break;
+        default: aux_y_group_kernel<3><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, P.d_y); break;
+      }
+      NKX_LAUNCH_CHECK();
+      ++P.launches;
+    }
+    if (P.nloose > 0) {
+      aux_y_shell_kernel<<<dim3(P.nloose, (unsigned)nsl), 256, 0, s>>>(P.d_ashell, P.d_loose, P.d_px, P.d_py, P.d_pz,
+                                                                      P.d_w, P.d_rho, nspin, P.npad, slice, P.d_y);
+      NKX_LAUNCH_CHECK();
+      ++P.launches;
+    }
     if (P.svd_mode) {
       const double one = 1.0, zero = 0.0;
       cublasHandle_t hb = (cublasHandle_t)P.cublas;
@@ -942,8 +1049,8 @@ void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
       NKX_LAUNCH_CHECK();
       P.launches += 2;
     }
-    aux_v_shell_kernel<<<nblk(P.npad, 128), 128, 0, s>>>(P.d_ashell, P.nashell, P.d_c, P.d_px, P.d_py, P.d_pz,
-                                                         P.d_w, P.npad, P.d_vj);
+    aux_v_group_kernel<<<nblk(P.npad, 128), 128, 0, s>>>(P.d_agroup, P.nagroup, P.d_ashell, P.d_loose, P.nloose,
+                                                         P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, P.d_vj);
     NKX_LAUNCH_CHECK();
     ++P.launches;
 }

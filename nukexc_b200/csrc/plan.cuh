@@ -44,6 +44,10 @@ struct Plan {
   AuxFunc *d_aux = nullptr;
   AuxShell *d_ashell = nullptr;
   int nashell = 0;
+  AuxGroup *d_agroup = nullptr;  // (centre, l) groups, sorted by l
+  int nagroup = 0, nloose = 0;
+  std::vector<int> h_group_off;  // groups of l = L at [off[L], off[L+1])
+  int *d_loose = nullptr;        // shells outside the groups
 
   // screening: pairs of (batch, significant function block), CSR by batch
   std::vector<int> h_pair_off;

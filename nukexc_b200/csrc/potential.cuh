@@ -74,13 +74,43 @@ NKX_HD inline double lower_gamma_int(int n, double x) {
   return fact_d(n - 1) - upper_gamma_int(n, x);
 }
 
-// radial factor I(r) of V_a = C S_lm I(r); shared by the 2l+1 functions of a shell
+// radial factor I(r) of V_a = C S_lm I(r); shared by the 2l+1 functions of a
+// shell.  One exp(-x) serves both incomplete gammas: Gamma(b, x) =
+// (b-1)! e^-x sum_(k<b) x^k/k!, and gamma(a, x) by its ascending series
+// x^a e^-x sum_k x^k / (a (a+1) ... (a+k)) for x < a/2 (ratio below 1/2, so
+// a few tens of terms) or as (a-1)! - Gamma(a, x) above, where
+// P(a, x) >= P(a, a/2) keeps the subtraction's relative error near 1e-15.
 NKX_HD inline double aux_radial(const AuxFunc &f, double r) {
   if (r < 1e-12) return fact_d(f.b - 1) * f.zb;
-  const double zr = f.zeta * r;
+  const double x = f.zeta * r;
   const double r2l1 = ipow(r, 2 * f.l + 1);
-  if (zr > f.xfar) return f.ga_full / r2l1;
-  return lower_gamma_int(f.a, zr) * (f.ga_full / fact_d(f.a - 1)) / r2l1 + upper_gamma_int(f.b, zr) * f.zb;
+  if (x > f.xfar) return f.ga_full / r2l1;
+  const double ex = exp(-x);
+  double su = 1.0, t = 1.0;
+  for (int k = 1; k < f.b; ++k) {
+    t *= x * inv_int(k);
+    su += t;
+  }
+  const double upper = fact_d(f.b - 1) * ex * su;
+  double lower;
+  const int a = f.a;
+  if (2.0 * x < a) {
+    double sum = a <= 64 ? inv_int(a) : 1.0 / a, term = sum;
+    for (int k = 1; k < 200; ++k) {
+      term *= x * (a + k <= 64 ? inv_int(a + k) : 1.0 / (a + k));
+      sum += term;
+      if (term < 1e-17 * sum) break;
+    }
+    lower = ipow(x, a) * ex * sum;
+  } else {
+    double sl = 1.0, tl = 1.0;
+    for (int k = 1; k < a; ++k) {
+      tl *= x * (k <= 64 ? inv_int(k) : 1.0 / k);
+      sl += tl;
+    }
+    lower = fact_d(a - 1) * (1.0 - ex * sl);
+  }
+  return lower * (f.ga_full / fact_d(a - 1)) / r2l1 + upper * f.zb;
 }
 
 NKX_HD inline double aux_potential(const AuxFunc &f, double px, double py, double pz) {
@@ -96,5 +126,23 @@ struct AuxShell {
   int first;  // index of the first function
   int nm;     // number of functions (<= 2l+1)
 };
+
+// Complete shells (m = -l..l) of one centre and one l <= 3, consecutive in
+// the shell list: the solid harmonics of a point are evaluated once for the
+// group.  Groups hold at most kAuxGroupMax(l) shells.
+struct AuxGroup {
+  double cx, cy, cz;
+  int l;
+  int first;  // first shell
+  int n;      // shells in the group
+};
+NKX_HD constexpr int aux_group_max(int l) { return (32 / (2 * l + 1)) < 16 ? (32 / (2 * l + 1)) : 16; }
+
+// the 2L+1 real solid harmonics of degree L at (x, y, z), m = -L..L
+template <int L>
+NKX_HD inline void solid_harmonics_all(double x, double y, double z, double S[2 * L + 1]) {
+#pragma unroll
+  for (int m = -L; m <= L; ++m) S[m + L] = solid_harmonic(L, m, x, y, z);
+}
 
 }  // namespace nkx

@@ -240,6 +240,25 @@ def test_plan_coulomb_matches_oracle(svd):
     assert np.abs(Vf[0] - (V[0] + J)).max() < 1e-10 * np.abs(Jo).max()
 
 
+def test_plan_coulomb_loose_aux_shells():
+    # aux shells outside the (centre, l <= 3) groups -- a g shell (l = 4) and
+    # a lone m = 0 d function -- go through the per-shell kernels
+    c, Z, funcs, g = water_case(1, nrad=40, order=17)
+    b, ob = basis_pair(funcs)
+    af = list(small_aux(c, Z))
+    o = c[0]
+    af += [(5, 4, m, 2.0, o[0], o[1], o[2]) for m in range(-4, 5)]
+    af += [(3, 2, 0, 1.3, o[0], o[1], o[2])]
+    aux, oaux = basis_pair(af)
+    Cm = M.random_orbitals(len(funcs), 5, seed=9)
+    occ = np.ones(5)
+    fb = A.FockBuilder(c, Z, b, g, aux=aux, func_ids=("LDA_X",), metric_svd_thr=1e-6)
+    _, _, J = fb.build([Cm], [occ], want_J=True)
+    S = O.aux_metric(oaux, g.quad_points, g.weights)
+    Jo, _ = O.coulomb(ob, oaux, g.quad_points, g.weights, Cm, occ, X=O.half_inverse(S, 1e-6))
+    assert np.abs(J - Jo).max() < 1e-9 * np.abs(Jo).max()
+
+
 def test_plan_coulomb_pivoted_cholesky_baseline_aux():
     # the even-tempered zeta_k = 0.3 * 1.8^k aux set: the grid metric is
     # indefinite, the pivoted Cholesky drops near-dependent functions and J
