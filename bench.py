@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--aux", action="store_true",
                     help="add the grid density-fitted J (aux zeta_k = 0.3*1.8^k up to l = 3) fused into V")
+    ap.add_argument("--j-waters", type=int, default=32,
+                    help="size of the XC + DF-J comparison reported beside the headline (0: skip)")
     ap.add_argument("--workspace-mb", type=int, default=0,
                     help="cap on the per-chunk collocation workspace in MiB (0: automatic); more chunks, same work")
     return ap.parse_args()
@@ -218,6 +220,43 @@ def run_reference(args):
             "config": config(args, {"precision": "fp64 (CPU oracle port of the reference dense algorithm)"}),
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def xc_plus_j(n, steps, warmup, stream):
+    """Mixed vs FP64 XC + fused DF-J Fock build on (H2O)_n with the aux basis
+    zeta_k = 0.3*1.8^k up to l = 3 (CUDA events, device-resident C)."""
+    import torch
+    from nukexc_b200 import api as A
+    from nukexc_b200 import molecules as M
+    c, Z, funcs, Cm = workload(n)
+    g = A.make_flat_grid(c, Z, 75, 29, weight_threshold=1e-15, radial="ta")
+    t0 = time.perf_counter()
+    fb = A.FockBuilder(c, Z, A.make_manual_basis(funcs), (g.quad_points, g.weights),
+                       aux=A.make_manual_basis(M.aux_basis(c, Z)), func_ids=FUNCS)
+    setup = time.perf_counter() - t0
+    Cd = torch.as_tensor(Cm, device="cuda")
+    od = torch.ones(Cm.shape[1], dtype=torch.float64, device="cuda")
+    out = {"workload": f"(H2O)_{n} PBE XC + DF-J Fock build", "npoints": int(len(g.weights)),
+           "nbf": len(funcs), "naux": fb.naux, "plan_setup_s": setup}
+    for prec in ("mixed", "fp64"):
+        for _ in range(warmup):
+            fb.build([Cd], [od], precision=prec, fuse_j=True, stream=stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            fb.build([Cd], [od], precision=prec, fuse_j=True, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[prec + "_ms_per_step"] = e0.elapsed_time(e1) / steps
+        out[prec + "_coulomb_ms"] = fb.timing()["coulomb_ms"]
+    out["mixed_speedup"] = out["fp64_ms_per_step"] / out["mixed_ms_per_step"]
+    Em, Vm, Jm = fb.build([Cd], [od], precision="mixed", want_J=True, stream=stream.cuda_stream)
+    Ed, Vd, Jd = fb.build([Cd], [od], precision="fp64", want_J=True, stream=stream.cuda_stream)
+    out["accuracy"] = {"dE_xc": abs(Em - Ed), "max_abs_dV_xc": float((Vm[0] - Vd[0]).abs().max()),
+                       "rel_dJ": float((Jm - Jd).abs().max() / Jd.abs().max())}
+    fb.close()
+    return out
 
 
 # ---------------------------------------------------------------- nkx ----
@@ -405,6 +444,8 @@ def run_nkx(args):
         }
         if os.environ.get("NKX_BENCH_NO_CPU") is None and world == 1:
             line["cpu_baseline"] = cpu_baseline(c, Z, funcs, Cm, args.cpu_sample)
+        if world == 1 and args.j_waters > 0 and not args.aux:
+            line["xc_plus_j"] = xc_plus_j(args.j_waters, max(1, min(args.steps, 3)), args.warmup, stream)
         print(json.dumps(line), flush=True)
     fb.close()
     if dist is not None:
