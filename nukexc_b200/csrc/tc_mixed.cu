@@ -229,17 +229,30 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             if (!mbar_wait(&full_bar[st], (step / kStages) & 1, a.err, 4, &abort_flag)) return;
             tc_fence_after();
             const uint32_t base = smem_u32(smem + st * kStageBytes);
+            // products of A digit plane i with B planes j = 0 .. 3-i into
+            // level L = i + j; the A plane stays in the collector buffer for
+            // its run, so shared memory feeds 4 A tiles per 32-byte K slice
+            // instead of 10
 #pragma unroll
             for (int kk = 0; kk < 2; ++kk)
 #pragma unroll
-              for (int L = 0; L < 4; ++L)
+              for (int i = 0; i < 4; ++i) {
+                const uint64_t ad = smem_desc_k64(base + i * (128 * 64) + kk * 32);
 #pragma unroll
-                for (int i = 0; i <= L; ++i) {
-                  const int j = L - i;
-                  const uint64_t ad = smem_desc_k64(base + i * (128 * 64) + kk * 32);
+                for (int j = 0; j <= 3 - i; ++j) {
                   const uint64_t bd = smem_desc_k64(base + kABytes + j * (64 * 64) + kk * 32);
-                  mma_i8(d + L * 64, ad, bd, kIdesc, (k == 0 && kk == 0 && i == 0) ? 0u : 1u);
+                  const uint32_t dt = d + (i + j) * 64;
+                  const uint32_t acc = (k == 0 && kk == 0 && i == 0) ? 0u : 1u;
+                  if (i == 3)
+                    mma_i8_a<CollectorDiscard>(dt, ad, bd, kIdesc, acc);
+                  else if (j == 0)
+                    mma_i8_a<CollectorFill>(dt, ad, bd, kIdesc, acc);
+                  else if (j == 3 - i)
+                    mma_i8_a<CollectorLastUse>(dt, ad, bd, kIdesc, acc);
+                  else
+                    mma_i8_a<CollectorUse>(dt, ad, bd, kIdesc, acc);
                 }
+              }
             mma_commit(&empty_bar[st]);
           }
           mma_commit(&tfull_bar[buf]);

@@ -129,6 +129,31 @@ __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_
       : "memory");
 }
 
+// kind::i8 MMA that keeps its A operand in the tensor core's collector
+// buffer: consecutive MMAs on the same A tile read shared memory once
+// (CollectorFill on the first, CollectorUse in between, CollectorLastUse on
+// the last); CollectorDiscard is the plain form.
+enum CollectorUsage { CollectorDiscard = 0, CollectorFill = 1, CollectorUse = 2, CollectorLastUse = 3 };
+
+template <int U>
+__device__ __forceinline__ void mma_i8_a(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                         uint32_t accumulate) {
+#define NKX_MMA_I8(Q)                                                                                      \
+  asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"                                          \
+               "tcgen05.mma.cta_group::1.kind::i8" Q " [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem), "l"(a_desc), \
+               "l"(b_desc), "r"(idesc), "r"(accumulate)                                                    \
+               : "memory")
+  if constexpr (U == CollectorFill)
+    NKX_MMA_I8(".collector::a::fill");
+  else if constexpr (U == CollectorUse)
+    NKX_MMA_I8(".collector::a::use");
+  else if constexpr (U == CollectorLastUse)
+    NKX_MMA_I8(".collector::a::lastuse");
+  else
+    NKX_MMA_I8("");
+#undef NKX_MMA_I8
+}
+
 // Instruction descriptor of kind::tf32, FP32 accumulator, both operands
 // K-major, M x N.
 __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
