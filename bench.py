@@ -56,6 +56,8 @@ def parse():
                     help="add the grid density-fitted J (aux zeta_k = 0.3*1.8^k up to l = 3) fused into V")
     ap.add_argument("--j-waters", type=int, default=32,
                     help="size of the XC + DF-J comparison reported beside the headline (0: skip)")
+    ap.add_argument("--grad-waters", type=int, default=16,
+                    help="size of the XC nuclear-gradient measurement reported beside the headline (0: skip)")
     ap.add_argument("--workspace-mb", type=int, default=0,
                     help="cap on the per-chunk collocation workspace in MiB (0: automatic); more chunks, same work")
     return ap.parse_args()
@@ -288,6 +290,58 @@ def xc_plus_j(n, steps, warmup, stream):
     return out
 
 
+def xc_gradient_check(n, stream, ngeom=3, ncomp=2, h=1e-4):
+    """XC nuclear gradient (FP64) of (H2O)_n PBE at seeded perturbed geometries
+    (each atom + N(0, 0.05 bohr)): time per gradient and the largest deviation
+    from Richardson-extrapolated central differences of the FP64 E_xc of the
+    GPU build on a few seeded components (grid rebuilt at each displaced
+    geometry, no weight-threshold compaction)."""
+    import torch
+    from nukexc_b200 import api as A
+    from nukexc_b200 import molecules as M
+    c0, Z = M.water_cluster(n, seed=0)
+    funcs0 = M.sto_basis(c0, Z)
+    Cm = M.random_orbitals(len(funcs0), 5 * n, seed=0)
+    occ = np.ones(5 * n)
+    rng = np.random.default_rng(11)
+
+    def builder(c):
+        g = A.make_flat_grid(c, Z, 75, 29, weight_threshold=-1.0, radial="ta")
+        return A.FockBuilder(c, Z, A.make_manual_basis(M.sto_basis(c, Z)), g, func_ids=FUNCS)
+
+    def energy(c):
+        fb = builder(c)
+        E, _, _ = fb.build([Cm], [occ], precision="fp64")
+        fb.close()
+        return E
+
+    times, worst, comps = [], 0.0, []
+    for k in range(ngeom):
+        c = np.asarray(c0, float) + rng.normal(0.0, 0.05, size=np.shape(c0))
+        fb = builder(c)
+        fb.xc_gradient([Cm], [occ])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        G = fb.xc_gradient([Cm], [occ])
+        times.append((time.perf_counter() - t0) * 1e3)
+        fb.close()
+        for _ in range(ncomp):
+            a, j = int(rng.integers(len(Z))), int(rng.integers(3))
+
+            def central(hh):
+                cp, cm = c.copy(), c.copy()
+                cp[a, j] += hh
+                cm[a, j] -= hh
+                return (energy(cp) - energy(cm)) / (2 * hh)
+            fd = (4.0 * central(h / 2) - central(h)) / 3.0
+            worst = max(worst, abs(G[a, j] - fd))
+            comps.append([k, a, j])
+    return {"workload": f"(H2O)_{n} PBE XC nuclear gradient, FP64", "geometries": ngeom,
+            "ms_per_gradient": float(np.median(times)), "fd_components": comps,
+            "max_abs_error_vs_fd": worst, "gate": "<= 1e-5 Eh/bohr",
+            "fd": "Richardson-extrapolated central differences, h = 1e-4 and 5e-5 bohr, FP64 GPU E_xc"}
+
+
 # ---------------------------------------------------------------- nkx ----
 def vgemm_flops(info_pairs_per_batch, nz=1):
     """Algorithmic FLOPs of the V = Phi Z^T contraction: sum_b 2 n_b^2 256."""
@@ -483,6 +537,8 @@ def run_nkx(args):
             line["cpu_baseline"] = cpu_baseline(c, Z, funcs, Cm, args.cpu_sample)
         if world == 1 and args.j_waters > 0 and not args.aux:
             line["xc_plus_j"] = xc_plus_j(args.j_waters, max(1, min(args.steps, 3)), args.warmup, stream)
+        if world == 1 and args.grad_waters > 0:
+            line["xc_gradient"] = xc_gradient_check(args.grad_waters, stream)
         print(json.dumps(line), flush=True)
     fb.close()
     if dist is not None:
