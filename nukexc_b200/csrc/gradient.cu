@@ -430,7 +430,7 @@ static void xc_gradient(Plan &P, int nspin, int nocc, const double *C, const dou
   GradState &G = grad_state(P, nspin, nocc);
   NKX_CUDA(cudaMemsetAsync(P.d_E, 0, sizeof(double), s));
   NKX_CUDA(cudaMemsetAsync(G.F, 0, sizeof(double) * 3 * P.natoms, s));
-  functional_kernel<<<gblk(P.npad, 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.d_w, P.d_rho, P.d_grad, nullptr,
+  functional_kernel<<<gblk(P.npad, 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.npad, P.d_w, P.d_rho, P.d_grad, nullptr,
                                                      P.d_coef, P.d_E, G.edens);
   NKX_LAUNCH_CHECK();
   ++P.launches;

@@ -231,17 +231,18 @@ __global__ void __launch_bounds__(256) density_fp64_kernel(const double *__restr
   }
 }
 
-// Functional on every point: E_xc, and the Z coefficients
+// Functional on points [0, n) of the arrays given (plane stride npad; callers
+// offset the pointers to work on a range): E_xc, and the Z coefficients
 // coef[spin][0][g] = w (1/2 vrho + 1/2 vJ), coef[spin][1..3][g] = w vec
 // (xc_integrals.hpp:506-514 closed shell, :655-664 open shell).  vj (may be
 // null) is the weighted fitted Coulomb potential folded into both spins.
-__global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, const double *__restrict__ w,
+__global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, long n, const double *__restrict__ w,
                                   const double *__restrict__ rho, const double *__restrict__ grad,
                                   const double *__restrict__ vj, double *__restrict__ coef, double *Eacc,
                                   double *__restrict__ edens) {
   const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
   double e = 0.0, fdens = 0.0;
-  if (g < npad) {
+  if (g < n) {
     const double wg = w[g];
     double vr[2] = {0, 0}, vec[2][3] = {{0, 0, 0}, {0, 0, 0}}, gr[2][3] = {{0, 0, 0}, {0, 0, 0}};
     if (gga)
@@ -1093,7 +1094,7 @@ void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool s
   // ---- functional
   T.begin(ST_FUNC, s);
   NKX_CUDA(cudaMemsetAsync(P.d_E, 0, sizeof(double), s));
-  functional_kernel<<<nblk(P.npad, 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.d_w, P.d_rho, P.d_grad,
+  functional_kernel<<<nblk(P.npad, 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.npad, P.d_w, P.d_rho, P.d_grad,
                                                       (needJ && fuse) ? P.d_vj : nullptr, P.d_coef, P.d_E,
                                                       nullptr);
   NKX_LAUNCH_CHECK();

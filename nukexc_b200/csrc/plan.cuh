@@ -131,7 +131,7 @@ void upload_orbitals(Plan &P, int nspin, int nocc, const double *C, const double
 void fp64_density_pass(Plan &P, int nspin, int nocc, cudaStream_t s, StageTimer &T);
 void launch_colloc(Plan &P, const Chunk &c, cudaStream_t s);
 void destroy_grad_state(void *p);
-__global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, const double *__restrict__ w,
+__global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, long n, const double *__restrict__ w,
                                   const double *__restrict__ rho, const double *__restrict__ grad,
                                   const double *__restrict__ vj, double *__restrict__ coef, double *Eacc,
                                   double *__restrict__ edens);

@@ -525,6 +525,96 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
   }
 }
 
+// Pass B, part 1 for builds without J: the same operands as colloc_z_kernel,
+// but phi and grad phi come back from the pass-A digits of the pair instead
+// of a second STO evaluation.  qphT[pair][comp][digit][g][f] holds
+// X = d0 2^24 + d1 2^16 + d2 2^8 + d3 with x = X s_g 2^-30 (s_g the
+// power-of-two scale of point g over the block), so the recovered values
+// differ from the collocation by less than 2^-31 s_g.
+template <bool GRAD, int NZ>
+__global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__restrict__ qphT,
+                                                              const double *__restrict__ sphT,
+                                                              const int *__restrict__ pair_batch, long p0,
+                                                              const double *__restrict__ coef, long npad,
+                                                              double *__restrict__ ws, double *__restrict__ sph,
+                                                              double *__restrict__ szs) {
+  constexpr int NC = GRAD ? 4 : 1;
+  constexpr int nz = NZ, nop = 1 + NZ;
+  __shared__ double red[8][4][128];
+  const long qrel = blockIdx.x;
+  const int b = pair_batch[p0 + qrel];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t T = (size_t)kBatch * kBlockF;
+  double m[nop][4];
+#pragma unroll
+  for (int o = 0; o < nop; ++o)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) m[o][c] = 0.0;
+  double *out = ws + qrel * 4 * T;
+  for (int g = warp; g < kBatch; g += 8) {
+    const long gg = (long)b * kBatch + g;
+    double v[NC][4];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const long pc = qrel * NC + c;
+      const double sc = sphT[pc * 256 + g] * 0x1p-30;
+      uint32_t wd[4];
+#pragma unroll
+      for (int d = 0; d < 4; ++d) wd[d] = reinterpret_cast<const uint32_t *>(qphT + ((pc * 4 + d) * 256 + g) * 128)[lane];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const long long X = (long long)(int8_t)(wd[0] >> (8 * k)) * (1LL << 24) +
+                            (long long)(int8_t)(wd[1] >> (8 * k)) * (1LL << 16) +
+                            (long long)(int8_t)(wd[2] >> (8 * k)) * (1LL << 8) + (long long)(int8_t)(wd[3] >> (8 * k));
+        v[c][k] = (double)X * sc;
+      }
+    }
+    double z[nop][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) z[0][k] = v[0][k];
+#pragma unroll
+    for (int sp = 0; sp < nz; ++sp) {
+      const double *cs = coef + (size_t)sp * 4 * npad;
+      const double c0 = cs[gg];
+      double c1 = 0.0, c2 = 0.0, c3 = 0.0;
+      if (GRAD) {
+        c1 = cs[npad + gg];
+        c2 = cs[2 * npad + gg];
+        c3 = cs[3 * npad + gg];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        z[1 + sp][k] = c0 * v[0][k];
+        if (GRAD) z[1 + sp][k] += c1 * v[NC > 1 ? 1 : 0][k] + c2 * v[NC > 2 ? 2 : 0][k] + c3 * v[NC > 3 ? 3 : 0][k];
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < nop; ++o) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) m[o][c] = fmax(m[o][c], fabs(z[o][c]));
+      double2 *dst = reinterpret_cast<double2 *>(out + o * T + (size_t)g * kBlockF + 4 * lane);
+      dst[0] = make_double2(z[o][0], z[o][1]);
+      dst[1] = make_double2(z[o][2], z[o][3]);
+    }
+  }
+#pragma unroll
+  for (int o = 0; o < nop; ++o)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) red[warp][o][4 * lane + c] = m[o][c];
+  __syncthreads();
+  for (int e = threadIdx.x; e < nop * 128; e += 256) {
+    const int o = e / 128, ff = e % 128;
+    double mm = 0.0;
+    for (int w = 0; w < 8; ++w) mm = fmax(mm, red[w][o][ff]);
+    double sc;
+    inv_pow2_scale(mm, sc);
+    if (o == 0)
+      sph[qrel * 128 + ff] = sc;
+    else
+      szs[(qrel * nz + (o - 1)) * 128 + ff] = sc;
+  }
+}
+
 // Pass B, part 2: digits of the V operands, transposed to
 // qph[pair][digit][f][g] and qz[pair][z][digit][f][g] through a shared
 // tile in slabs of 64 points (rows padded to 68 bytes: conflict-free).
@@ -762,8 +852,9 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     NKX_LAUNCH_CHECK();
     ++P.launches;
   }
-  // ---- pass A: collocation, int8 density contraction, FP64 rho / grad rho
-  for (const Chunk &c : P.chunks) {
+  // pass A of one chunk: collocation -> digits, int8 density contraction,
+  // FP64 rho / grad rho of the chunk's batches
+  auto pass_a = [&](const Chunk &c) {
     const long np = c.p1 - c.p0, nb = c.b1 - c.b0;
     if (np > 0) {
       Tm.begin(ST_COLLOC, s);
@@ -808,31 +899,10 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     NKX_LAUNCH_CHECK();
     ++P.launches;
     Tm.end(s);
-  }
-  // ---- J fit and the functional, in FP64
-  if (needJ) {
-    Tm.begin(ST_COULOMB, s);
-    coulomb_fit(P, nspin, s);
-    Tm.end(s);
-  }
-  Tm.begin(ST_FUNC, s);
-  NKX_CUDA(cudaMemsetAsync(P.d_E, 0, sizeof(double), s));
-  functional_kernel<<<(unsigned)((P.npad + 255) / 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.d_w, P.d_rho,
-                                                                      P.d_grad, (needJ && fuse) ? P.d_vj : nullptr,
-                                                                      P.d_coef, P.d_E, nullptr);
-  NKX_LAUNCH_CHECK();
-  ++P.launches;
-  Tm.end(s);
-  // ---- pass B: quantised Phi and Z, int8 V contraction
-  NKX_CUDA(cudaMemsetAsync(P.d_V, 0, sizeof(double) * nzs * P.nbf_pad * P.nbf_pad, s));
-  for (const Chunk &c : P.chunks) {
+  };
+  // pass B of one chunk after its Phi / Z staging is written: digits, int8 V
+  auto pass_b = [&](const Chunk &c) {
     const long np = c.p1 - c.p0;
-    if (np <= 0) continue;
-    Tm.begin(ST_COLLOC, s);
-    launch_colloc_z(P, M, c, nzs, nspin, s);
-    NKX_LAUNCH_CHECK();
-    ++P.launches;
-    Tm.end(s);
     Tm.begin(ST_ZBUILD, s);
     zquant_kernel<<<(unsigned)np, 256, (size_t)(1 + nzs) * 4 * 128 * 68, s>>>(P.ws_phi, M.sph, M.sz, nzs, M.qph, M.qz);
     NKX_LAUNCH_CHECK();
@@ -859,6 +929,71 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     launch_i8(M, M.m_ph, M.m_z, a, s);
     ++P.launches;
     Tm.end(s);
+  };
+  NKX_CUDA(cudaMemsetAsync(P.d_E, 0, sizeof(double), s));
+  NKX_CUDA(cudaMemsetAsync(P.d_V, 0, sizeof(double) * nzs * P.nbf_pad * P.nbf_pad, s));
+  if (!needJ) {
+    // Without J every point's functional needs only its own batch, so each
+    // chunk goes through both passes while its pass-A digits are resident,
+    // and pass B recovers Phi and grad Phi from them instead of evaluating
+    // the STOs again.
+    for (const Chunk &c : P.chunks) {
+      pass_a(c);
+      const long g0 = c.b0 * kBatch, n = (c.b1 - c.b0) * kBatch;
+      Tm.begin(ST_FUNC, s);
+      functional_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, n, P.d_w + g0,
+                                                                    P.d_rho + g0, P.d_grad + g0, nullptr,
+                                                                    P.d_coef + g0, P.d_E, nullptr);
+      NKX_LAUNCH_CHECK();
+      ++P.launches;
+      Tm.end(s);
+      const long np = c.p1 - c.p0;
+      if (np <= 0) continue;
+      Tm.begin(ST_ZBUILD, s);
+#define NKX_ZD(G, NZ)                                                                                               \
+  z_from_digits_kernel<G, NZ><<<(unsigned)np, 256, 0, s>>>(M.qphT, M.sphT, P.d_pair_batch, c.p0, P.d_coef, P.npad, \
+                                                           P.ws_phi, M.sph, M.sz)
+      if (P.gga) {
+        if (nspin == 1)
+          NKX_ZD(true, 1);
+        else
+          NKX_ZD(true, 2);
+      } else {
+        if (nspin == 1)
+          NKX_ZD(false, 1);
+        else
+          NKX_ZD(false, 2);
+      }
+#undef NKX_ZD
+      NKX_LAUNCH_CHECK();
+      ++P.launches;
+      Tm.end(s);
+      pass_b(c);
+    }
+  } else {
+    for (const Chunk &c : P.chunks) pass_a(c);
+    // ---- J fit and the functional, in FP64
+    Tm.begin(ST_COULOMB, s);
+    coulomb_fit(P, nspin, s);
+    Tm.end(s);
+    Tm.begin(ST_FUNC, s);
+    functional_kernel<<<(unsigned)((P.npad + 255) / 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.npad, P.d_w,
+                                                                        P.d_rho, P.d_grad, fuse ? P.d_vj : nullptr,
+                                                                        P.d_coef, P.d_E, nullptr);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+    Tm.end(s);
+    // ---- pass B: Phi and Z from a second collocation (J needs every point's
+    // density before any Z), digits, int8 V contraction
+    for (const Chunk &c : P.chunks) {
+      if (c.p1 - c.p0 <= 0) continue;
+      Tm.begin(ST_COLLOC, s);
+      launch_colloc_z(P, M, c, nzs, nspin, s);
+      NKX_LAUNCH_CHECK();
+      ++P.launches;
+      Tm.end(s);
+      pass_b(c);
+    }
   }
   int herr = 0;
   NKX_CUDA(cudaMemcpyAsync(&herr, M.err, sizeof(int), cudaMemcpyDeviceToHost, s));
