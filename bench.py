@@ -58,13 +58,21 @@ def parse():
                     help="size of the XC + DF-J comparison reported beside the headline (0: skip)")
     ap.add_argument("--grad-waters", type=int, default=16,
                     help="size of the XC nuclear-gradient measurement reported beside the headline (0: skip)")
+    ap.add_argument("--aggregate", type=int, default=0,
+                    help="instead of water clusters: the C/H/N/O aggregate of this many atoms (1500: ~12000 "
+                         "functions, ~3e7 points), closed shell with nocc = electrons / 2")
     ap.add_argument("--workspace-mb", type=int, default=0,
                     help="cap on the per-chunk collocation workspace in MiB (0: automatic); more chunks, same work")
     return ap.parse_args()
 
 
-def workload(n):
+def workload(n, aggregate=0):
     from nukexc_b200 import molecules as M
+    if aggregate:
+        c, Z = M.aggregate(aggregate, seed=0)
+        funcs = M.aggregate_basis(c, Z)
+        C = M.random_orbitals(len(funcs), sum(Z) // 2, seed=0)
+        return c, Z, funcs, C
     c, Z = M.water_cluster(n, seed=0)
     funcs = M.sto_basis(c, Z)
     C = M.random_orbitals(len(funcs), 5 * n, seed=0)
@@ -72,12 +80,21 @@ def workload(n):
 
 
 def config(args, extra=None):
-    name = f"(H2O)_{args.waters} PBE XC" + (" + DF-J" if getattr(args, "aux", False) else "") + " Fock build"
-    cfg = {"workload": name, "waters": args.waters,
-           "basis": "even-tempered STO zeta_k=0.5*2.2^k, O 6s4p2d, H 4s2p",
-           "grid": "Treutler-Ahlrichs M4 75 x Lebedev 302 per atom, Becke (Laqua clamp), w>1e-15",
-           "batch_points": 256, "screen_tol": 1e-10, "nocc": 5 * args.waters, "occ": 1.0,
-           "l2": "inputs larger than L2 (per-chunk workspace of several GB streamed each step)"}
+    agg = getattr(args, "aggregate", 0)
+    if agg:
+        cfg = {"workload": f"C/H/N/O aggregate, {agg} atoms (3:5:1:1, random packing, d_min 1.0 A) PBE XC Fock build",
+               "atoms": agg,
+               "basis": "even-tempered STO, heavy 3s2p1d zeta_k=1.4*2.4^k, H 2s zeta_k=1.2*2.4^k",
+               "grid": "Treutler-Ahlrichs M4 75 x Lebedev 302 per atom, Becke (Laqua clamp), w>1e-15",
+               "batch_points": 256, "screen_tol": 1e-10, "nocc": "electrons / 2", "occ": 1.0,
+               "l2": "inputs larger than L2 (per-chunk workspace of several GB streamed each step)"}
+    else:
+        name = f"(H2O)_{args.waters} PBE XC" + (" + DF-J" if getattr(args, "aux", False) else "") + " Fock build"
+        cfg = {"workload": name, "waters": args.waters,
+               "basis": "even-tempered STO zeta_k=0.5*2.2^k, O 6s4p2d, H 4s2p",
+               "grid": "Treutler-Ahlrichs M4 75 x Lebedev 302 per atom, Becke (Laqua clamp), w>1e-15",
+               "batch_points": 256, "screen_tol": 1e-10, "nocc": 5 * args.waters, "occ": 1.0,
+               "l2": "inputs larger than L2 (per-chunk workspace of several GB streamed each step)"}
     if extra:
         cfg.update(extra)
     return cfg
@@ -235,7 +252,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    c, Z, funcs, C = workload(args.waters)
+    c, Z, funcs, C = workload(args.waters, args.aggregate)
     npts = max(256, args.cpu_sample)
     for _ in range(args.warmup):
         cpu_baseline(c, Z, funcs, C, 512)
@@ -366,7 +383,7 @@ def run_nkx(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    c, Z, funcs, Cm = workload(args.waters)
+    c, Z, funcs, Cm = workload(args.waters, args.aggregate)
     g = A.make_flat_grid(c, Z, 75, 29, weight_threshold=1e-15, radial="ta")
     # strong scaling: rank r integrates the points of its share of atoms
     sel = S.select_points(g.point_owner, len(Z), rank, world)

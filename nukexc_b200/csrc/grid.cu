@@ -62,14 +62,20 @@ __global__ void becke_kernel(const double *__restrict__ centers, int natoms, con
   const int own = owner[g];
   double norm = 0.0, pown = 0.0;
   if (full) {
+    // with the clamp, factors of atoms j with r_j >= r_i + Rc are 1 (mu <= -1
+    // is clamped) and cells with r_i >= r_min + Rc are 0 (the nearest atom
+    // gives mu >= 1): skipping them is the full loop without its trivial terms
     for (int i = 0; i < natoms; ++i) {
       const double ri = dist3(p, centers + 3 * i);
+      if (clamp && ri >= rmin + Rc) continue;
       double P = 1.0;
       for (int j = 0; j < natoms; ++j) {
         if (j == i) continue;
+        const double rj = dist3(p, centers + 3 * j);
+        if (clamp && rj >= ri + Rc) continue;
         double Rij = dist3(centers + 3 * i, centers + 3 * j);
         if (clamp) Rij = fmin(Rij, Rc);
-        P *= becke_s((ri - dist3(p, centers + 3 * j)) / Rij);
+        P *= becke_s((ri - rj) / Rij);
       }
       if (i == own) pown = P;
       norm += P;

@@ -23,6 +23,7 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <parallel/algorithm>
 #include <cstdint>
 #include <cstring>
 #include <functional>
@@ -665,7 +666,9 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
       lo[d] = std::min(lo[d], xyz[3 * g + d]);
       hi[d] = std::max(hi[d], xyz[3 * g + d]);
     }
-  std::vector<uint64_t> code(npoints);
+  // (code, index) pairs sorted lexicographically: the stable Morton order
+  std::vector<std::pair<uint64_t, long>> key(npoints);
+#pragma omp parallel for schedule(static)
   for (long g = 0; g < npoints; ++g) {
     uint64_t c = 0;
     for (int d = 0; d < 3; ++d) {
@@ -673,11 +676,12 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
       const double u = (xyz[3 * g + d] - lo[d]) / span;
       c |= spread3((uint64_t)std::min(2097151.0, std::max(0.0, u * 2097151.0))) << d;
     }
-    code[g] = c;
+    key[g] = {c, g};
   }
+  __gnu_parallel::sort(key.begin(), key.end());
   P.perm.resize(npoints);
-  std::iota(P.perm.begin(), P.perm.end(), 0L);
-  std::stable_sort(P.perm.begin(), P.perm.end(), [&](long a, long b) { return code[a] < code[b]; });
+  for (long g = 0; g < npoints; ++g) P.perm[g] = key[g].second;
+  std::vector<std::pair<uint64_t, long>>().swap(key);
   std::vector<double> hx(P.npad), hy(P.npad), hz(P.npad), hw(P.npad, 0.0);
   for (long p = 0; p < P.npad; ++p) {
     const long g = P.perm[std::min(p, npoints - 1)];
@@ -765,7 +769,17 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
   // cutoff sphere meets the batch bounding box (octree.hpp:331-366)
   P.h_mask.assign((size_t)P.nbatch * P.mask_words, 0u);
   P.h_pair_off.assign(P.nbatch + 1, 0);
-  std::vector<int> pblk, pbatch;
+  // per block, the box holding every function's cutoff sphere: a block whose
+  // box misses the batch box has no significant function there
+  std::vector<double> blo(3 * (size_t)P.nblk, 1e300), bhi(3 * (size_t)P.nblk, -1e300);
+  for (int f = 0; f < P.nbf; ++f) {
+    const int I = f / kBlockF;
+    for (int d = 0; d < 3; ++d) {
+      blo[3 * I + d] = std::min(blo[3 * I + d], prim->center[3 * f + d] - cut[f]);
+      bhi[3 * I + d] = std::max(bhi[3 * I + d], prim->center[3 * f + d] + cut[f]);
+    }
+  }
+#pragma omp parallel for schedule(dynamic, 64)
   for (long b = 0; b < P.nbatch; ++b) {
     double bl[3] = {1e300, 1e300, 1e300}, bh[3] = {-1e300, -1e300, -1e300};
     for (int g = 0; g < kBatch; ++g) {
@@ -777,6 +791,9 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
       }
     }
     for (int I = 0; I < P.nblk; ++I) {
+      bool near = true;
+      for (int d = 0; d < 3; ++d) near = near && blo[3 * I + d] <= bh[d] && bhi[3 * I + d] >= bl[d];
+      if (!near) continue;
       bool sig = false;
       for (int f = I * kBlockF; f < std::min(P.nbf, (I + 1) * kBlockF) && !sig; ++f) {
         double d2 = 0.0;
@@ -787,12 +804,16 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
         }
         sig = d2 <= cut[f] * cut[f];
       }
-      if (sig) {
-        P.h_mask[b * P.mask_words + I / 32] |= 1u << (I % 32);
+      if (sig) P.h_mask[b * P.mask_words + I / 32] |= 1u << (I % 32);
+    }
+  }
+  std::vector<int> pblk, pbatch;
+  for (long b = 0; b < P.nbatch; ++b) {
+    for (int I = 0; I < P.nblk; ++I)
+      if ((P.h_mask[b * P.mask_words + I / 32] >> (I % 32)) & 1u) {
         pblk.push_back(I);
         pbatch.push_back((int)b);
       }
-    }
     P.h_pair_off[b + 1] = (int)pblk.size();
   }
   P.npairs = (long)pblk.size();
