@@ -696,14 +696,56 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
   // function of rank 32 c + lane, ranks sorted by (l, m): the collocation
   // kernels give lane l of a warp positions 4l .. 4l+3, so the 32 lanes
   // evaluating slot c take the same solid-harmonic branch.  Blocks keep
-  // their function sets, so screening is unchanged.
+  // their function sets.
   auto tab0 = make_sto_table(*prim);
+  // Before that, the functions are grouped by centre (runs of one centre in
+  // the caller's order) and the centres put in Morton order of position, so
+  // the 128-function blocks are compact in space and screening keeps few
+  // blocks per batch even when the caller lists atoms in random order.
+  std::vector<int> order(P.nbf);
+  {
+    struct Run {
+      int first, n;
+      uint64_t code;
+    };
+    std::vector<Run> runs;
+    auto same_centre = [&](int f, int g) {
+      return prim->center[3 * f] == prim->center[3 * g] && prim->center[3 * f + 1] == prim->center[3 * g + 1] &&
+             prim->center[3 * f + 2] == prim->center[3 * g + 2];
+    };
+    for (int f = 0; f < P.nbf; ++f) {
+      if (!runs.empty() && same_centre(runs.back().first, f)) {
+        ++runs.back().n;
+        continue;
+      }
+      runs.push_back(Run{f, 1, 0});
+    }
+    double clo[3] = {1e300, 1e300, 1e300}, chi[3] = {-1e300, -1e300, -1e300};
+    for (const Run &r : runs)
+      for (int d = 0; d < 3; ++d) {
+        clo[d] = std::min(clo[d], prim->center[3 * r.first + d]);
+        chi[d] = std::max(chi[d], prim->center[3 * r.first + d]);
+      }
+    for (Run &r : runs) {
+      uint64_t c = 0;
+      for (int d = 0; d < 3; ++d) {
+        const double span = chi[d] > clo[d] ? chi[d] - clo[d] : 1.0;
+        const double u = (prim->center[3 * r.first + d] - clo[d]) / span;
+        c |= spread3((uint64_t)std::min(2097151.0, std::max(0.0, u * 2097151.0))) << d;
+      }
+      r.code = c;
+    }
+    std::stable_sort(runs.begin(), runs.end(), [](const Run &a, const Run &b) { return a.code < b.code; });
+    int k = 0;
+    for (const Run &r : runs)
+      for (int i = 0; i < r.n; ++i) order[k++] = r.first + i;
+  }
   std::vector<StoFunc> tab(P.nbf_pad);
   P.h_fperm.assign(P.nbf_pad, -1);
   std::vector<int> finv(std::max(1, P.nbf), 0);
   for (int I = 0; I < P.nblk; ++I) {
     std::vector<int> fs;
-    for (int f = I * kBlockF; f < std::min(P.nbf, (I + 1) * kBlockF); ++f) fs.push_back(f);
+    for (int q = I * kBlockF; q < std::min(P.nbf, (I + 1) * kBlockF); ++q) fs.push_back(order[q]);
     std::stable_sort(fs.begin(), fs.end(), [&](int x, int y) {
       return tab0[x].l != tab0[y].l ? tab0[x].l < tab0[y].l : tab0[x].m < tab0[y].m;
     });
@@ -772,8 +814,9 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
   // per block, the box holding every function's cutoff sphere: a block whose
   // box misses the batch box has no significant function there
   std::vector<double> blo(3 * (size_t)P.nblk, 1e300), bhi(3 * (size_t)P.nblk, -1e300);
-  for (int f = 0; f < P.nbf; ++f) {
-    const int I = f / kBlockF;
+  for (int q = 0; q < P.nbf_pad; ++q) {
+    const int f = P.h_fperm[q], I = q / kBlockF;
+    if (f < 0) continue;
     for (int d = 0; d < 3; ++d) {
       blo[3 * I + d] = std::min(blo[3 * I + d], prim->center[3 * f + d] - cut[f]);
       bhi[3 * I + d] = std::max(bhi[3 * I + d], prim->center[3 * f + d] + cut[f]);
@@ -795,7 +838,9 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
       for (int d = 0; d < 3; ++d) near = near && blo[3 * I + d] <= bh[d] && bhi[3 * I + d] >= bl[d];
       if (!near) continue;
       bool sig = false;
-      for (int f = I * kBlockF; f < std::min(P.nbf, (I + 1) * kBlockF) && !sig; ++f) {
+      for (int q = I * kBlockF; q < (I + 1) * kBlockF && !sig; ++q) {
+        const int f = P.h_fperm[q];
+        if (f < 0) continue;
         double d2 = 0.0;
         for (int d = 0; d < 3; ++d) {
           const double c = prim->center[3 * f + d];
