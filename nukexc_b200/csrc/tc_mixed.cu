@@ -17,13 +17,17 @@
 // 2^-30 s_a s_b each) are dropped; everything kept is exact, so unlike FP32
 // tensor-core accumulation the result carries no rounding bias.
 //
-// Roles (320 threads): warp 0 lane 0 issues 3-D TMA loads of the four digit
-// planes of A (128 rows) and B (64 rows), 64 K-bytes per stage, into a
-// 4-stage ring of 48 KB (64-byte swizzle); warp 1 lane 0 issues the MMAs
-// (M = 128, N = 64, K = 32) and owns TMEM (2 buffers x 4 levels x 64
-// columns); warps 2..9 are the epilogue (warp w reads TMEM lanes
-// 32 (w % 4) .. + 31, columns 32 ((w - 2) / 4) .. + 31 of each level) with
-// FP64 accumulators in registers.  All waits are bounded (tc_ptx.cuh).
+// Roles (576 threads): warp 0 lane 0 issues 3-D TMA loads of the four digit
+// planes of A and B (128 rows each), 64 K-bytes per stage, into a 3-stage
+// ring of 64 KB (64-byte swizzle); warp 1 lane 0 issues the MMAs
+// (M = 128, N = 128, K = 32) and owns TMEM (4 levels x 128 columns, the
+// whole 512); warps 2..17 are the epilogue (warp w reads TMEM lanes
+// 32 (w % 4) .. + 31, columns 32 ((w - 2) / 4) .. + 31 of each level, in
+// slices of 8) with FP64 accumulators in registers.  N = 128 because
+// M = 128 x N = 64 int8 MMAs are limited by shared-memory operand bandwidth
+// to about two thirds of the tensor rate; the price is one TMEM buffer, so
+// the epilogue of a group and the MMAs of the next one alternate.  All
+// waits are bounded (tc_ptx.cuh).
 #include <cuda.h>
 
 #include <algorithm>
@@ -36,12 +40,13 @@ namespace nkx {
 
 using namespace tc;
 
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr int kABytes = 4 * 128 * 64;  // four digit planes, 128 rows x 64 B
-constexpr int kBBytes = 4 * 64 * 64;   // four digit planes, 64 rows x 64 B
+constexpr int kBBytes = 4 * 128 * 64;  // four digit planes, 128 rows x 64 B
 constexpr int kStageBytes = kABytes + kBBytes;
-constexpr int kGemmThreads = 320;
-constexpr uint32_t kIdesc = idesc_i8(128, 64);
+constexpr int kGemmThreads = 64 + 512;
+constexpr int kEpiThreads = 512;
+constexpr uint32_t kIdesc = idesc_i8(128, 128);
 constexpr double kTwoM36 = 0x1p-36;
 
 enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1 };
@@ -64,15 +69,15 @@ struct TcArgs {
 };
 
 struct UnitIter {
-  int I = 0, J = 0, zi = 0;        // V: row block, 64-column block, Z plane
+  int I = 0, J = 0, zi = 0;        // V: row block, column block, Z plane
   long bl = 0;                     // density: batch within chunk
-  int h = 0, c = 0, s = 0, t = 0;  // density: point half, comp, spin, 64-orbital tile
+  int h = 0, c = 0, s = 0, t = 0;  // density: point half, comp, spin, 128-orbital tile
   __device__ UnitIter(const TcArgs &a, long u) {
     if (a.mode == TC_MODE_V) {
-      const long n2 = (long)a.nblk * 2 * a.nblk;
+      const long n2 = (long)a.nblk * a.nblk;
       zi = (int)(u / n2);
-      I = (int)((u % n2) / (2 * a.nblk));
-      J = (int)(u % (2 * a.nblk));
+      I = (int)((u % n2) / a.nblk);
+      J = (int)(u % a.nblk);
     } else {
       long r = u;
       t = (int)(r % a.ntile_i);
@@ -106,7 +111,7 @@ __device__ __forceinline__ bool blk_has(const uint32_t *m, int I) { return (m[I 
 template <class Fn>
 __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &it, Fn &&fn) {
   if (a.mode == TC_MODE_V) {
-    const int Jb = it.J >> 1, jh = it.J & 1;
+    const int Jb = it.J;
     for (long b = a.b0; b < a.b1; ++b) {
       const uint32_t *m = a.mask + b * a.mask_words;
       if (!blk_has(m, it.I) || !blk_has(m, Jb)) continue;
@@ -116,7 +121,7 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
       g.qa = qb0 + blk_pos(m, it.I);
       g.qb = qb0 + blk_pos(m, Jb);
       g.blk = 0;
-      const int za = (int)(g.qa * 4), zb = (int)((g.qb * a.nz + it.zi) * 4), yb = 64 * jh;
+      const int za = (int)(g.qa * 4), zb = (int)((g.qb * a.nz + it.zi) * 4), yb = 0;
       fn(g, [=](int k, int &xa, int &ya, int &zA, int &xb, int &yB, int &zB) {
         xa = 64 * k;
         ya = 0;
@@ -136,7 +141,7 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
       g.qb = 0;
       g.blk = a.pair_blk[q];
       const int za = (int)((g.qa * a.ncomp + it.c) * 4), ya = 128 * it.h;
-      const int xb0 = g.blk * 128, yb = 64 * it.t, zb = it.s * 4;
+      const int xb0 = g.blk * 128, yb = 128 * it.t, zb = it.s * 4;
       fn(g, [=](int k, int &xa, int &yA, int &zA, int &xb, int &yB, int &zB) {
         xa = 64 * k;
         yA = ya;
@@ -159,7 +164,7 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
 __global__ void __launch_bounds__(kGemmThreads, 1)
     tc_i8_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs a) {
   extern __shared__ __align__(1024) uint8_t dsmem[];
-  __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar[2], tempty_bar[2], drain_bar;
+  __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar, tempty_bar, drain_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_flag;
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dsmem) + 1023) & ~uintptr_t(1023));
@@ -171,10 +176,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       mbar_init(&full_bar[i], 1);
       mbar_init(&empty_bar[i], 1);
     }
-    for (int i = 0; i < 2; ++i) {
-      mbar_init(&tfull_bar[i], 1);
-      mbar_init(&tempty_bar[i], 256);
-    }
+    mbar_init(&tfull_bar, 1);
+    mbar_init(&tempty_bar, kEpiThreads);
     mbar_init(&drain_bar, 1);
     fence_mbar_init();
     prefetch_tmap(&mapA);
@@ -220,10 +223,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         UnitIter it(a, u);
         for_each_group(a, it, [&](const Group &g, auto) {
           if (abort_flag) return;
-          const uint32_t buf = grp & 1, use = grp >> 1;
-          if (!mbar_wait(&tempty_bar[buf], (use & 1) ^ 1, a.err, 3, &abort_flag)) return;
+          // the single TMEM buffer: wait until the epilogue has read group grp - 1
+          if (!mbar_wait(&tempty_bar, (grp & 1) ^ 1, a.err, 3, &abort_flag)) return;
           tc_fence_after();
-          const uint32_t d = tmem + buf * 256;
+          const uint32_t d = tmem;
           for (int k = 0; k < g.nsteps; ++k, ++step) {
             const int st = step % kStages;
             if (!mbar_wait(&full_bar[st], (step / kStages) & 1, a.err, 4, &abort_flag)) return;
@@ -240,8 +243,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 const uint64_t ad = smem_desc_k64(base + i * (128 * 64) + kk * 32);
 #pragma unroll
                 for (int j = 0; j <= 3 - i; ++j) {
-                  const uint64_t bd = smem_desc_k64(base + kABytes + j * (64 * 64) + kk * 32);
-                  const uint32_t dt = d + (i + j) * 64;
+                  const uint64_t bd = smem_desc_k64(base + kABytes + j * (128 * 64) + kk * 32);
+                  const uint32_t dt = d + (i + j) * 128;
                   const uint32_t acc = (k == 0 && kk == 0 && i == 0) ? 0u : 1u;
                   if (i == 3)
                     mma_i8_a<CollectorDiscard>(dt, ad, bd, kIdesc, acc);
@@ -255,7 +258,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
               }
             mma_commit(&empty_bar[st]);
           }
-          mma_commit(&tfull_bar[buf]);
+          mma_commit(&tfull_bar);
           ++grp;
         });
       }
@@ -265,7 +268,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     }
   } else {
     // ------------------------------------------------------ epilogue
-    const int q = warp & 3, hc = (warp - 2) >> 2;
+    const int q = warp & 3, cq = (warp - 2) >> 2;
     const int row = 32 * q + lane;
     const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
     uint32_t grp = 0;
@@ -277,8 +280,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       bool any = false;
       for_each_group(a, it, [&](const Group &g, auto) {
         if (abort_flag) return;
-        const uint32_t buf = grp & 1, use = grp >> 1;
-        if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag)) return;
+        if (!mbar_wait(&tfull_bar, grp & 1, a.err, 6, &abort_flag)) return;
         tc_fence_after();
         __syncwarp();
         const bool live = g.nsteps > 0;
@@ -288,10 +290,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         if (live) {
           if (a.mode == TC_MODE_V) {
             sa = a.sA[g.qa * 128 + row] * kTwoM36;
-            sb = a.sB + (g.qb * a.nz + it.zi) * 128 + 64 * (it.J & 1) + 32 * hc;
+            sb = a.sB + (g.qb * a.nz + it.zi) * 128 + 32 * cq;
           } else {
             sa = a.sA[(g.qa * a.ncomp + it.c) * 256 + 128 * it.h + row] * kTwoM36;
-            sb = a.sB + ((size_t)it.s * a.nocc_pad + 64 * it.t + 32 * hc) * a.nblk + g.blk;
+            sb = a.sB + ((size_t)it.s * a.nocc_pad + 128 * it.t + 32 * cq) * a.nblk + g.blk;
             sbs = a.nblk;
           }
         }
@@ -299,28 +301,28 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         // |Acc_L| < 2^24 for K <= 256, so |S| < 2^49 converts to FP64 exactly;
         // the product is s_a s_b 2^-36 S (one rounding per group and element)
 #pragma unroll
-        for (int hh = 0; hh < 2; ++hh) {
-          uint32_t v0[16], v1[16], v2[16], v3[16];
-          const uint32_t ta = tmem + lane_addr + buf * 256 + 32 * hc + 16 * hh;
-          tmem_ld16u_async(ta, v0);
-          tmem_ld16u_async(ta + 64, v1);
-          tmem_ld16u_async(ta + 128, v2);
-          tmem_ld16u_async(ta + 192, v3);
-          tmem_wait16(v0);
-          tmem_wait16(v1);
-          tmem_wait16(v2);
-          tmem_wait16(v3);
+        for (int hh = 0; hh < 4; ++hh) {
+          uint32_t v0[8], v1[8], v2[8], v3[8];
+          const uint32_t ta = tmem + lane_addr + 32 * cq + 8 * hh;
+          tmem_ld8u_async(ta, v0);
+          tmem_ld8u_async(ta + 128, v1);
+          tmem_ld8u_async(ta + 256, v2);
+          tmem_ld8u_async(ta + 384, v3);
+          tmem_wait8(v0);
+          tmem_wait8(v1);
+          tmem_wait8(v2);
+          tmem_wait8(v3);
           if (live) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
+            for (int j = 0; j < 8; ++j) {
               const long long S = (long long)(int)v0[j] * (1LL << 24) + (long long)(int)v1[j] * (1LL << 16) +
                                   (long long)(int)v2[j] * (1LL << 8) + (long long)(int)v3[j];
-              acc[16 * hh + j] = fma((double)S, sa * sb[(16 * hh + j) * sbs], acc[16 * hh + j]);
+              acc[8 * hh + j] = fma((double)S, sa * sb[(8 * hh + j) * sbs], acc[8 * hh + j]);
             }
           }
         }
         tc_fence_before();
-        mbar_arrive(&tempty_bar[buf]);
+        mbar_arrive(&tempty_bar);
         ++grp;
         any = any || live;
       });
@@ -329,13 +331,13 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
           double *Vz = a.V + (size_t)it.zi * a.nbf_pad * a.nbf_pad;
           const size_t r = (size_t)it.I * 128 + row;
 #pragma unroll
-          for (int j = 0; j < 32; ++j) Vz[r + ((size_t)it.J * 64 + 32 * hc + j) * a.nbf_pad] += acc[j];
+          for (int j = 0; j < 32; ++j) Vz[r + ((size_t)it.J * 128 + 32 * cq + j) * a.nbf_pad] += acc[j];
         }
       } else {
         const long plane = (it.bl * a.nspin + it.s) * a.ncomp + it.c;
         double *Tp = a.T + plane * (long)a.nocc_pad * 256 + 128 * it.h + row;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) Tp[(size_t)(64 * it.t + 32 * hc + j) * 256] = acc[j];
+        for (int j = 0; j < 32; ++j) Tp[(size_t)(128 * it.t + 32 * cq + j) * 256] = acc[j];
       }
     }
   }
@@ -787,7 +789,7 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     M->err = M->alloc<int>(1);
     M->m_phT = make_map3(M->qphT, 128, 256, M->cap * 4 * 4, 128);
     M->m_ph = make_map3(M->qph, 256, 128, M->cap * 4, 128);
-    M->m_z = make_map3(M->qz, 256, 128, M->cap * 3 * 4, 64);
+    M->m_z = make_map3(M->qz, 256, 128, M->cap * 3 * 4, 128);
     int dev = 0;
     NKX_CUDA(cudaGetDevice(&dev));
     NKX_CUDA(cudaDeviceGetAttribute(&M->nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -796,13 +798,13 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     NKX_CUDA(cudaFuncSetAttribute(zquant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 68));
   }
   MixedState &M = *static_cast<MixedState *>(P.mx_state);
-  const int nocc_pad = ((nocc + 63) / 64) * 64;
+  const int nocc_pad = ((nocc + 127) / 128) * 128;
   if (nocc_pad > M.nocc_pad) {
     M.nocc_pad = nocc_pad;
     M.qct = M.alloc<uint8_t>((size_t)2 * 4 * nocc_pad * P.nbf_pad);
     M.sct = M.alloc<double>((size_t)2 * nocc_pad * P.nblk);
     M.T = M.alloc<double>((size_t)M.nbatch_chunk * 2 * 4 * nocc_pad * 256);
-    M.m_ct = make_map3(M.qct, P.nbf_pad, nocc_pad, 8, 64);
+    M.m_ct = make_map3(M.qct, P.nbf_pad, nocc_pad, 8, 128);
   }
   return M;
 }
@@ -883,7 +885,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.sB = M.sct;
     a.nspin = nspin;
     a.ncomp = nc;
-    a.ntile_i = M.nocc_pad / 64;
+    a.ntile_i = M.nocc_pad / 128;
     a.nocc_pad = M.nocc_pad;
     a.T = M.T;
     a.err = M.err;
@@ -925,7 +927,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.sB = M.sz;
     a.V = P.d_V;
     a.err = M.err;
-    a.nunits = (long)nzs * P.nblk * 2 * P.nblk;
+    a.nunits = (long)nzs * P.nblk * P.nblk;
     launch_i8(M, M.m_ph, M.m_z, a, s);
     ++P.launches;
     Tm.end(s);
