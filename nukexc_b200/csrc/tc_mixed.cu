@@ -17,17 +17,18 @@
 // 2^-30 s_a s_b each) are dropped; everything kept is exact, so unlike FP32
 // tensor-core accumulation the result carries no rounding bias.
 //
-// Roles (576 threads): warp 0 lane 0 issues 3-D TMA loads of the four digit
-// planes of A and B (128 rows each), 64 K-bytes per stage, into a 3-stage
-// ring of 64 KB (64-byte swizzle); warp 1 lane 0 issues the MMAs
-// (M = 128, N = 128, K = 32) and owns TMEM (4 levels x 128 columns, the
-// whole 512); warps 2..17 are the epilogue (warp w reads TMEM lanes
-// 32 (w % 4) .. + 31, columns 32 ((w - 2) / 4) .. + 31 of each level, in
-// slices of 8) with FP64 accumulators in registers.  N = 128 because
-// M = 128 x N = 64 int8 MMAs are limited by shared-memory operand bandwidth
-// to about two thirds of the tensor rate; the price is one TMEM buffer, so
-// the epilogue of a group and the MMAs of the next one alternate.  All
-// waits are bounded (tc_ptx.cuh).
+// Roles: warp 0 lane 0 issues 3-D TMA loads of the four digit planes of A
+// (128 rows) and B (N rows), 64 K-bytes per stage, into a ring of stages
+// (64-byte swizzle); warp 1 lane 0 issues the MMAs (M = 128, N, K = 32) and
+// owns TMEM (all 512 columns: NBUF buffers x 4 levels x N); warps 2.. are
+// the epilogue (warp w reads TMEM lanes 32 (w % 4) .. + 31, columns
+// 32 ((w - 2) / 4) .. + 31 of each level, in slices of 8) with FP64
+// accumulators in registers.  The V contraction uses N = 128 (576 threads,
+// one TMEM buffer): M = 128 x N = 64 int8 MMAs are limited by shared-memory
+// operand bandwidth to about two thirds of the tensor rate.  The density
+// contraction keeps N = 64 (320 threads, two TMEM buffers): its groups are
+// two K steps long, so overlapping the epilogue matters more there, and its
+// orbital dimension pads to 64.  All waits are bounded (tc_ptx.cuh).
 #include <cuda.h>
 
 #include <algorithm>
@@ -40,16 +41,28 @@ namespace nkx {
 
 using namespace tc;
 
-constexpr int kStages = 3;
 constexpr int kABytes = 4 * 128 * 64;  // four digit planes, 128 rows x 64 B
-constexpr int kBBytes = 4 * 128 * 64;  // four digit planes, 128 rows x 64 B
-constexpr int kStageBytes = kABytes + kBBytes;
-constexpr int kGemmThreads = 64 + 512;
-constexpr int kEpiThreads = 512;
-constexpr uint32_t kIdesc = idesc_i8(128, 128);
 constexpr double kTwoM36 = 0x1p-36;
 
 enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1 };
+
+// Shape per mode.  V: N = 128 (one TMEM buffer of 4 levels x 128 columns,
+// 16 epilogue warps, 3 stages of 64 KB).  Density: N = 64 (two buffers of
+// 4 levels x 64 columns so the epilogue of a block overlaps the MMAs of the
+// next, 8 epilogue warps, 4 stages of 48 KB); its groups are only two K steps
+// long and the orbital count pads to 64, not 128.
+template <int MODE>
+struct TcShape {
+  static constexpr int N = MODE == TC_MODE_V ? 128 : 64;
+  static constexpr int NBUF = N == 128 ? 1 : 2;
+  static constexpr int kStages = N == 128 ? 3 : 4;
+  static constexpr int kBBytes = 4 * N * 64;
+  static constexpr int kStageBytes = kABytes + kBBytes;
+  static constexpr int kEpiThreads = 32 * 4 * (N / 32);
+  static constexpr int kThreads = 64 + kEpiThreads;
+  static constexpr uint32_t kIdesc = idesc_i8(128, N);
+  static constexpr int kSmem = kStages * kStageBytes + 1024;
+};
 
 struct TcArgs {
   int mode;
@@ -141,7 +154,7 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
       g.qb = 0;
       g.blk = a.pair_blk[q];
       const int za = (int)((g.qa * a.ncomp + it.c) * 4), ya = 128 * it.h;
-      const int xb0 = g.blk * 128, yb = 128 * it.t, zb = it.s * 4;
+      const int xb0 = g.blk * 128, yb = TcShape<TC_MODE_DENSITY>::N * it.t, zb = it.s * 4;
       fn(g, [=](int k, int &xa, int &yA, int &zA, int &xb, int &yB, int &zB) {
         xa = 64 * k;
         yA = ya;
@@ -161,10 +174,13 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
   }
 }
 
-__global__ void __launch_bounds__(kGemmThreads, 1)
+template <int MODE>
+__global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
     tc_i8_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs a) {
+  using Sh = TcShape<MODE>;
+  constexpr int N = Sh::N, NBUF = Sh::NBUF, kStages = Sh::kStages, kStageBytes = Sh::kStageBytes;
   extern __shared__ __align__(1024) uint8_t dsmem[];
-  __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar, tempty_bar, drain_bar;
+  __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar[NBUF], tempty_bar[NBUF], drain_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_flag;
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dsmem) + 1023) & ~uintptr_t(1023));
@@ -176,8 +192,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       mbar_init(&full_bar[i], 1);
       mbar_init(&empty_bar[i], 1);
     }
-    mbar_init(&tfull_bar, 1);
-    mbar_init(&tempty_bar, kEpiThreads);
+    for (int i = 0; i < NBUF; ++i) {
+      mbar_init(&tfull_bar[i], 1);
+      mbar_init(&tempty_bar[i], Sh::kEpiThreads);
+    }
     mbar_init(&drain_bar, 1);
     fence_mbar_init();
     prefetch_tmap(&mapA);
@@ -223,10 +241,12 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         UnitIter it(a, u);
         for_each_group(a, it, [&](const Group &g, auto) {
           if (abort_flag) return;
-          // the single TMEM buffer: wait until the epilogue has read group grp - 1
-          if (!mbar_wait(&tempty_bar, (grp & 1) ^ 1, a.err, 3, &abort_flag)) return;
+          // TMEM buffer grp % NBUF: wait until the epilogue has read the group
+          // that used it last
+          const uint32_t buf = grp % NBUF, use = grp / NBUF;
+          if (!mbar_wait(&tempty_bar[buf], (use & 1) ^ 1, a.err, 3, &abort_flag)) return;
           tc_fence_after();
-          const uint32_t d = tmem;
+          const uint32_t d = tmem + buf * 4 * N;
           for (int k = 0; k < g.nsteps; ++k, ++step) {
             const int st = step % kStages;
             if (!mbar_wait(&full_bar[st], (step / kStages) & 1, a.err, 4, &abort_flag)) return;
@@ -243,22 +263,22 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 const uint64_t ad = smem_desc_k64(base + i * (128 * 64) + kk * 32);
 #pragma unroll
                 for (int j = 0; j <= 3 - i; ++j) {
-                  const uint64_t bd = smem_desc_k64(base + kABytes + j * (128 * 64) + kk * 32);
-                  const uint32_t dt = d + (i + j) * 128;
+                  const uint64_t bd = smem_desc_k64(base + kABytes + j * (N * 64) + kk * 32);
+                  const uint32_t dt = d + (i + j) * N;
                   const uint32_t acc = (k == 0 && kk == 0 && i == 0) ? 0u : 1u;
                   if (i == 3)
-                    mma_i8_a<CollectorDiscard>(dt, ad, bd, kIdesc, acc);
+                    mma_i8_a<CollectorDiscard>(dt, ad, bd, Sh::kIdesc, acc);
                   else if (j == 0)
-                    mma_i8_a<CollectorFill>(dt, ad, bd, kIdesc, acc);
+                    mma_i8_a<CollectorFill>(dt, ad, bd, Sh::kIdesc, acc);
                   else if (j == 3 - i)
-                    mma_i8_a<CollectorLastUse>(dt, ad, bd, kIdesc, acc);
+                    mma_i8_a<CollectorLastUse>(dt, ad, bd, Sh::kIdesc, acc);
                   else
-                    mma_i8_a<CollectorUse>(dt, ad, bd, kIdesc, acc);
+                    mma_i8_a<CollectorUse>(dt, ad, bd, Sh::kIdesc, acc);
                 }
               }
             mma_commit(&empty_bar[st]);
           }
-          mma_commit(&tfull_bar);
+          mma_commit(&tfull_bar[buf]);
           ++grp;
         });
       }
@@ -280,7 +300,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       bool any = false;
       for_each_group(a, it, [&](const Group &g, auto) {
         if (abort_flag) return;
-        if (!mbar_wait(&tfull_bar, grp & 1, a.err, 6, &abort_flag)) return;
+        const uint32_t buf = grp % NBUF, use = grp / NBUF;
+        if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag)) return;
         tc_fence_after();
         __syncwarp();
         const bool live = g.nsteps > 0;
@@ -293,7 +314,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             sb = a.sB + (g.qb * a.nz + it.zi) * 128 + 32 * cq;
           } else {
             sa = a.sA[(g.qa * a.ncomp + it.c) * 256 + 128 * it.h + row] * kTwoM36;
-            sb = a.sB + ((size_t)it.s * a.nocc_pad + 128 * it.t + 32 * cq) * a.nblk + g.blk;
+            sb = a.sB + ((size_t)it.s * a.nocc_pad + N * it.t + 32 * cq) * a.nblk + g.blk;
             sbs = a.nblk;
           }
         }
@@ -303,11 +324,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 #pragma unroll
         for (int hh = 0; hh < 4; ++hh) {
           uint32_t v0[8], v1[8], v2[8], v3[8];
-          const uint32_t ta = tmem + lane_addr + 32 * cq + 8 * hh;
+          const uint32_t ta = tmem + lane_addr + buf * 4 * N + 32 * cq + 8 * hh;
           tmem_ld8u_async(ta, v0);
-          tmem_ld8u_async(ta + 128, v1);
-          tmem_ld8u_async(ta + 256, v2);
-          tmem_ld8u_async(ta + 384, v3);
+          tmem_ld8u_async(ta + N, v1);
+          tmem_ld8u_async(ta + 2 * N, v2);
+          tmem_ld8u_async(ta + 3 * N, v3);
           tmem_wait8(v0);
           tmem_wait8(v1);
           tmem_wait8(v2);
@@ -322,7 +343,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
           }
         }
         tc_fence_before();
-        mbar_arrive(&tempty_bar);
+        mbar_arrive(&tempty_bar[buf]);
         ++grp;
         any = any || live;
       });
@@ -337,7 +358,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         const long plane = (it.bl * a.nspin + it.s) * a.ncomp + it.c;
         double *Tp = a.T + plane * (long)a.nocc_pad * 256 + 128 * it.h + row;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) Tp[(size_t)(128 * it.t + 32 * cq + j) * 256] = acc[j];
+        for (int j = 0; j < 32; ++j) Tp[(size_t)(N * it.t + 32 * cq + j) * 256] = acc[j];
       }
     }
   }
@@ -793,18 +814,21 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     int dev = 0;
     NKX_CUDA(cudaGetDevice(&dev));
     NKX_CUDA(cudaDeviceGetAttribute(&M->nsm, cudaDevAttrMultiProcessorCount, dev));
-    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kStages * kStageBytes + 1024));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TcShape<TC_MODE_V>::kSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TcShape<TC_MODE_DENSITY>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(zquant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 68));
   }
   MixedState &M = *static_cast<MixedState *>(P.mx_state);
-  const int nocc_pad = ((nocc + 127) / 128) * 128;
+  constexpr int NT = TcShape<TC_MODE_DENSITY>::N;
+  const int nocc_pad = ((nocc + NT - 1) / NT) * NT;
   if (nocc_pad > M.nocc_pad) {
     M.nocc_pad = nocc_pad;
     M.qct = M.alloc<uint8_t>((size_t)2 * 4 * nocc_pad * P.nbf_pad);
     M.sct = M.alloc<double>((size_t)2 * nocc_pad * P.nblk);
     M.T = M.alloc<double>((size_t)M.nbatch_chunk * 2 * 4 * nocc_pad * 256);
-    M.m_ct = make_map3(M.qct, P.nbf_pad, nocc_pad, 8, 128);
+    M.m_ct = make_map3(M.qct, P.nbf_pad, nocc_pad, 8, TcShape<TC_MODE_DENSITY>::N);
   }
   return M;
 }
@@ -812,7 +836,11 @@ static MixedState &mixed_state(Plan &P, int nocc) {
 static void launch_i8(MixedState &M, const CUtensorMap &mA, const CUtensorMap &mB, const TcArgs &a, cudaStream_t s) {
   if (a.nunits <= 0) return;
   const unsigned grid = (unsigned)std::min<long>(a.nunits, M.nsm);
-  tc_i8_kernel<<<grid, kGemmThreads, kStages * kStageBytes + 1024, s>>>(mA, mB, a);
+  if (a.mode == TC_MODE_V)
+    tc_i8_kernel<TC_MODE_V><<<grid, TcShape<TC_MODE_V>::kThreads, TcShape<TC_MODE_V>::kSmem, s>>>(mA, mB, a);
+  else
+    tc_i8_kernel<TC_MODE_DENSITY><<<grid, TcShape<TC_MODE_DENSITY>::kThreads, TcShape<TC_MODE_DENSITY>::kSmem, s>>>(
+        mA, mB, a);
   NKX_LAUNCH_CHECK();
 }
 
@@ -885,7 +913,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.sB = M.sct;
     a.nspin = nspin;
     a.ncomp = nc;
-    a.ntile_i = M.nocc_pad / 128;
+    a.ntile_i = M.nocc_pad / TcShape<TC_MODE_DENSITY>::N;
     a.nocc_pad = M.nocc_pad;
     a.T = M.T;
     a.err = M.err;
