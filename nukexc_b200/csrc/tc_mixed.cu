@@ -321,24 +321,38 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
         // exact integer combine of the four levels, S = sum_L 2^(8 (3 - L)) Acc_L:
         // |Acc_L| < 2^24 for K <= 256, so |S| < 2^49 converts to FP64 exactly;
         // the product is s_a s_b 2^-36 S (one rounding per group and element)
+        // slices of SL columns: 8 for the 320-thread shape, 4 for the
+        // 576-thread one (96 registers a thread)
+        constexpr int SL = N == 128 ? 4 : 8;
 #pragma unroll
-        for (int hh = 0; hh < 4; ++hh) {
-          uint32_t v0[8], v1[8], v2[8], v3[8];
-          const uint32_t ta = tmem + lane_addr + buf * 4 * N + 32 * cq + 8 * hh;
-          tmem_ld8u_async(ta, v0);
-          tmem_ld8u_async(ta + N, v1);
-          tmem_ld8u_async(ta + 2 * N, v2);
-          tmem_ld8u_async(ta + 3 * N, v3);
-          tmem_wait8(v0);
-          tmem_wait8(v1);
-          tmem_wait8(v2);
-          tmem_wait8(v3);
+        for (int hh = 0; hh < 32 / SL; ++hh) {
+          uint32_t v0[SL], v1[SL], v2[SL], v3[SL];
+          const uint32_t ta = tmem + lane_addr + buf * 4 * N + 32 * cq + SL * hh;
+          if constexpr (SL == 8) {
+            tmem_ld8u_async(ta, v0);
+            tmem_ld8u_async(ta + N, v1);
+            tmem_ld8u_async(ta + 2 * N, v2);
+            tmem_ld8u_async(ta + 3 * N, v3);
+            tmem_wait8(v0);
+            tmem_wait8(v1);
+            tmem_wait8(v2);
+            tmem_wait8(v3);
+          } else {
+            tmem_ld4u_async(ta, v0);
+            tmem_ld4u_async(ta + N, v1);
+            tmem_ld4u_async(ta + 2 * N, v2);
+            tmem_ld4u_async(ta + 3 * N, v3);
+            tmem_wait4(v0);
+            tmem_wait4(v1);
+            tmem_wait4(v2);
+            tmem_wait4(v3);
+          }
           if (live) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
+            for (int j = 0; j < SL; ++j) {
               const long long S = (long long)(int)v0[j] * (1LL << 24) + (long long)(int)v1[j] * (1LL << 16) +
                                   (long long)(int)v2[j] * (1LL << 8) + (long long)(int)v3[j];
-              acc[8 * hh + j] = fma((double)S, sa * sb[(8 * hh + j) * sbs], acc[8 * hh + j]);
+              acc[SL * hh + j] = fma((double)S, sa * sb[(SL * hh + j) * sbs], acc[SL * hh + j]);
             }
           }
         }

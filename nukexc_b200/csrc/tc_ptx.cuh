@@ -188,6 +188,20 @@ __device__ __forceinline__ void tmem_ld32u(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// 32 lanes x 4 columns of 32-bit words from TMEM, without waiting; the
+// registers are valid only after tmem_wait4 on the same array
+__device__ __forceinline__ void tmem_ld4u_async(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait4(uint32_t (&r)[4]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3])
+               :
+               : "memory");
+}
+
 // 32 lanes x 8 columns of 32-bit words from TMEM, without waiting; the
 // registers are valid only after tmem_wait8 on the same array
 __device__ __forceinline__ void tmem_ld8u_async(uint32_t taddr, uint32_t (&r)[8]) {
