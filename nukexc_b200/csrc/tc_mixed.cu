@@ -321,6 +321,8 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
         // exact integer combine of the four levels, S = sum_L 2^(8 (3 - L)) Acc_L:
         // |Acc_L| < 2^24 for K <= 256, so |S| < 2^49 converts to FP64 exactly;
         // the product is s_a s_b 2^-36 S (one rounding per group and element)
+        // the warp's 32 column scales, one per lane, handed out by shuffles
+        const double sbl = live ? sb[lane * sbs] : 0.0;
         // slices of SL columns: 8 for the 320-thread shape, 4 for the
         // 576-thread one (96 registers a thread)
         constexpr int SL = N == 128 ? 4 : 8;
@@ -352,7 +354,7 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
             for (int j = 0; j < SL; ++j) {
               const long long S = (long long)(int)v0[j] * (1LL << 24) + (long long)(int)v1[j] * (1LL << 16) +
                                   (long long)(int)v2[j] * (1LL << 8) + (long long)(int)v3[j];
-              acc[SL * hh + j] = fma((double)S, sa * sb[(SL * hh + j) * sbs], acc[SL * hh + j]);
+              acc[SL * hh + j] = fma((double)S, sa * __shfl_sync(0xffffffffu, sbl, SL * hh + j), acc[SL * hh + j]);
             }
           }
         }
