@@ -800,6 +800,35 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
       NKX_CUDA(cudaMemcpy(P.d_owner, ho.data(), sizeof(int) * P.npad, cudaMemcpyHostToDevice));
     }
   }
+  // radial shells of every block (functions sharing centre, zeta and
+  // n - l - 1), for the collocation kernels' shared radial factors; padding
+  // positions (norm 0) point at shell 0
+  {
+    std::vector<StoShell> hsh((size_t)P.nblk * kBlockF);
+    std::vector<int> hns(P.nblk, 0), hfs(P.nbf_pad, 0);
+    for (int I = 0; I < P.nblk; ++I) {
+      int n = 0;
+      StoShell *S = hsh.data() + (size_t)I * kBlockF;
+      for (int q = I * kBlockF; q < (I + 1) * kBlockF; ++q) {
+        if (P.h_fperm[q] < 0) continue;
+        const StoFunc &f = tab[q];
+        int s = 0;
+        while (s < n && !(S[s].cx == f.cx && S[s].cy == f.cy && S[s].cz == f.cz && S[s].zeta == f.zeta &&
+                          S[s].k == f.k))
+          ++s;
+        if (s == n) S[n++] = StoShell{f.cx, f.cy, f.cz, f.zeta, f.k, 0};
+        hfs[q] = s;
+      }
+      if (n == 0) S[n++] = StoShell{tab[I * kBlockF].cx, tab[I * kBlockF].cy, tab[I * kBlockF].cz, 1.0, 0, 0};
+      hns[I] = n;
+    }
+    P.d_bshell = P.alloc<StoShell>(hsh.size());
+    NKX_CUDA(cudaMemcpy(P.d_bshell, hsh.data(), sizeof(StoShell) * hsh.size(), cudaMemcpyHostToDevice));
+    P.d_bnshell = P.alloc<int>(P.nblk);
+    NKX_CUDA(cudaMemcpy(P.d_bnshell, hns.data(), sizeof(int) * P.nblk, cudaMemcpyHostToDevice));
+    P.d_fshell = P.alloc<int>(P.nbf_pad);
+    NKX_CUDA(cudaMemcpy(P.d_fshell, hfs.data(), sizeof(int) * P.nbf_pad, cudaMemcpyHostToDevice));
+  }
   P.d_fperm = P.alloc<int>(P.nbf_pad);
   NKX_CUDA(cudaMemcpy(P.d_fperm, P.h_fperm.data(), sizeof(int) * P.nbf_pad, cudaMemcpyHostToDevice));
   P.d_finv = P.alloc<int>(finv.size());

@@ -33,6 +33,8 @@ struct Plan {
   StoFunc *d_sto = nullptr;  // basis in plan order (see build_plan)
   std::vector<int> h_fperm;  // plan position -> caller function (-1: padding)
   int *d_fperm = nullptr, *d_finv = nullptr;
+  StoShell *d_bshell = nullptr;  // radial shells per block [nblk][128]
+  int *d_bnshell = nullptr, *d_fshell = nullptr;
   // atoms (for the nuclear gradient)
   int natoms = 0;
   std::vector<double> h_centers;

@@ -129,71 +129,84 @@ NKX_HD inline double sto_value_cached(const StoFunc &f, double px, double py, do
   return f.norm * rc.R * solid_harmonic(f.l, f.m, dx, dy, dz);
 }
 
+// A radial shell of a function block: the functions sharing centre, zeta and
+// n - l - 1 share r^(n-l-1) e^(-zeta r) and its derivative.
+struct StoShell {
+  double cx, cy, cz, zeta;
+  int k, pad;
+};
+
 #ifdef __CUDACC__
 // One 128-function block in shared memory, laid out for kernels in which lane
 // l of a warp evaluates functions 4l .. 4l+3: field[c][l] holds function
-// 4l + c, so the 32 reads of one field by a warp are consecutive.  same[c][l]
-// is 1 when function 4l + c shares centre, zeta and n - l - 1 with function
-// 4l + c - 1 (the radial factor is then reused).  Keeping the table here
-// instead of in registers leaves room for the per-point operands.
+// 4l + c, so the 32 reads of one field by a warp are consecutive; sh[c][l]
+// is the function's radial shell.  Per point, the lanes of a warp first
+// evaluate the radial factor of each of the block's nshell shells once
+// (block_radials), then each function combines its shell's factor with its
+// solid harmonic (block_funcs_eval4).
 struct BlockFuncs {
-  double cx[4][32], cy[4][32], cz[4][32], zeta[4][32], norm[4][32];
-  int k[4][32], l[4][32], m[4][32], same[4][32];
+  double norm[4][32];
+  int l[4][32], m[4][32], sh[4][32];
+  double scx[128], scy[128], scz[128], szeta[128];
+  int sk[128];
+  int nshell;
 };
 
-// fill B from functions [I*128, I*128 + 128) of sto; the caller synchronises
-__device__ inline void load_block_funcs(BlockFuncs &B, const StoFunc *__restrict__ sto, int I, int tid, int nthr) {
+// fill B for block I from the plan's tables; the caller synchronises
+__device__ inline void load_block_funcs(BlockFuncs &B, const StoFunc *__restrict__ sto,
+                                        const int *__restrict__ fshell, const StoShell *__restrict__ bshell,
+                                        const int *__restrict__ bnshell, int I, int tid, int nthr) {
   for (int t = tid; t < 128; t += nthr) {
     const int lane = t >> 2, c = t & 3;
-    const StoFunc f = sto[I * 128 + t];
-    B.cx[c][lane] = f.cx;
-    B.cy[c][lane] = f.cy;
-    B.cz[c][lane] = f.cz;
-    B.zeta[c][lane] = f.zeta;
+    const StoFunc &f = sto[I * 128 + t];
     B.norm[c][lane] = f.norm;
-    B.k[c][lane] = f.k;
     B.l[c][lane] = f.l;
     B.m[c][lane] = f.m;
-    int same = 0;
-    if (c > 0) {
-      const StoFunc &g = sto[I * 128 + t - 1];
-      same = (f.cx == g.cx && f.cy == g.cy && f.cz == g.cz && f.zeta == g.zeta && f.k == g.k) ? 1 : 0;
-    }
-    B.same[c][lane] = same;
+    B.sh[c][lane] = fshell[I * 128 + t];
+    const StoShell &h = bshell[I * 128 + t];
+    B.scx[t] = h.cx;
+    B.scy[t] = h.cy;
+    B.scz[t] = h.cz;
+    B.szeta[t] = h.zeta;
+    B.sk[t] = h.k;
+  }
+  if (tid == 0) B.nshell = bnshell[I];
+}
+
+// radial factors of every shell of the block at one point, shared by the
+// warp: R[s] = r^k e^(-zeta r) and, with GRAD, C[s] = (k/r - zeta)/r (0 at r = 0)
+template <bool GRAD>
+__device__ __forceinline__ void block_radials(const BlockFuncs &B, int lane, double x, double y, double z,
+                                              double *__restrict__ R, double *__restrict__ C) {
+  for (int s = lane; s < B.nshell; s += 32) {
+    const double dx = x - B.scx[s], dy = y - B.scy[s], dz = z - B.scz[s];
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const int k = B.sk[s];
+    R[s] = ipow(r, k) * exp(-B.szeta[s] * r);
+    if (GRAD) C[s] = r > 0.0 ? (k / r - B.szeta[s]) / r : 0.0;
   }
 }
 
-// bit c set when function 4 lane + c reuses the radial factor of 4 lane + c - 1
-__device__ inline unsigned block_funcs_same_mask(const BlockFuncs &B, int lane) {
-  return (unsigned)B.same[1][lane] << 1 | (unsigned)B.same[2][lane] << 2 | (unsigned)B.same[3][lane] << 3;
-}
-
-// the four functions of one lane at one point: values v[c] and, with GRAD,
-// gradients gx/gy/gz[c]; same arithmetic as sto_value(_grad)_cached
+// the four functions of one lane at one point from the warp's radial
+// factors: values v[c] and, with GRAD, gradients gx/gy/gz[c]; same arithmetic
+// as sto_value(_grad)
 template <bool GRAD>
-__device__ __forceinline__ void block_funcs_eval4(const BlockFuncs &B, int lane, unsigned same, double x, double y,
-                                                  double z, double v[4], double gx[4], double gy[4], double gz[4]) {
-  double dx = 0, dy = 0, dz = 0, Rr = 0, cRr = 0;
+__device__ __forceinline__ void block_funcs_eval4(const BlockFuncs &B, int lane, double x, double y, double z,
+                                                  const double *__restrict__ Rs, const double *__restrict__ Cs,
+                                                  double v[4], double gx[4], double gy[4], double gz[4]) {
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    if (c == 0 || !((same >> c) & 1)) {
-      dx = x - B.cx[c][lane];
-      dy = y - B.cy[c][lane];
-      dz = z - B.cz[c][lane];
-      const double r = sqrt(dx * dx + dy * dy + dz * dz);
-      const int k = B.k[c][lane];
-      Rr = ipow(r, k) * exp(-B.zeta[c][lane] * r);
-      if (GRAD) cRr = r > 0.0 ? (k / r - B.zeta[c][lane]) / r : 0.0;
-    }
-    const double R = B.norm[c][lane] * Rr;
+    const int s = B.sh[c][lane];
+    const double dx = x - B.scx[s], dy = y - B.scy[s], dz = z - B.scz[s];
+    const double R = B.norm[c][lane] * Rs[s];
     if (GRAD) {
-      double s, sx, sy, sz;
-      solid_harmonic_grad(B.l[c][lane], B.m[c][lane], dx, dy, dz, s, sx, sy, sz);
-      v[c] = R * s;
-      const double cR = cRr * R;
-      gx[c] = R * sx + s * dx * cR;
-      gy[c] = R * sy + s * dy * cR;
-      gz[c] = R * sz + s * dz * cR;
+      double S, sx, sy, sz;
+      solid_harmonic_grad(B.l[c][lane], B.m[c][lane], dx, dy, dz, S, sx, sy, sz);
+      v[c] = R * S;
+      const double cR = Cs[s] * R;
+      gx[c] = R * sx + S * dx * cR;
+      gy[c] = R * sy + S * dy * cR;
+      gz[c] = R * sz + S * dz * cR;
     } else {
       v[c] = R * solid_harmonic(B.l[c][lane], B.m[c][lane], dx, dy, dz);
     }

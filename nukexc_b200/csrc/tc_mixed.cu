@@ -438,7 +438,11 @@ __global__ void quant_ct_kernel(const double *__restrict__ Ct, int nocc, int noc
 // the block is a warp maximum.  qphT[pair][comp][digit][g][f],
 // sphT[pair][comp][g].
 template <bool GRAD>
-__global__ void __launch_bounds__(256) colloc_quantT_kernel(const StoFunc *__restrict__ sto, const double *__restrict__ px,
+__global__ void __launch_bounds__(256) colloc_quantT_kernel(const StoFunc *__restrict__ sto,
+                                                            const int *__restrict__ fshell,
+                                                            const StoShell *__restrict__ bshell,
+                                                            const int *__restrict__ bnshell,
+                                                            const double *__restrict__ px,
                                                             const double *__restrict__ py, const double *__restrict__ pz,
                                                             const int *__restrict__ pair_batch,
                                                             const int *__restrict__ pair_blk, long p0,
@@ -449,18 +453,21 @@ __global__ void __launch_bounds__(256) colloc_quantT_kernel(const StoFunc *__res
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __shared__ double sx[kBatch], sy[kBatch], sz[kBatch];
   __shared__ BlockFuncs B;
+  __shared__ double wR[8][128], wC[8][128];
   for (int g = threadIdx.x; g < kBatch; g += blockDim.x) {
     sx[g] = px[(long)b * kBatch + g];
     sy[g] = py[(long)b * kBatch + g];
     sz[g] = pz[(long)b * kBatch + g];
   }
-  load_block_funcs(B, sto, I, threadIdx.x, blockDim.x);
+  load_block_funcs(B, sto, fshell, bshell, bnshell, I, threadIdx.x, blockDim.x);
   __syncthreads();
   const long qrel = blockIdx.x;
-  const unsigned same = block_funcs_same_mask(B, lane);
   for (int g = warp; g < kBatch; g += 8) {
     double v[4][4];
-    block_funcs_eval4<GRAD>(B, lane, same, sx[g], sy[g], sz[g], v[0], v[1], v[2], v[3]);
+    __syncwarp();
+    block_radials<GRAD>(B, lane, sx[g], sy[g], sz[g], wR[warp], wC[warp]);
+    __syncwarp();
+    block_funcs_eval4<GRAD>(B, lane, sx[g], sy[g], sz[g], wR[warp], wC[warp], v[0], v[1], v[2], v[3]);
 #pragma unroll
     for (int k = 0; k < NC; ++k) {
       const double m = warp_max(fmax(fmax(fabs(v[k][0]), fabs(v[k][1])), fmax(fabs(v[k][2]), fabs(v[k][3]))));
@@ -484,13 +491,17 @@ __global__ void __launch_bounds__(256) colloc_quantT_kernel(const StoFunc *__res
 // the row scale of every (o, f) over the 256 points: sph[pair][f],
 // sz[pair][z][f].
 template <bool GRAD, int NZ>
-__global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restrict__ sto, const double *__restrict__ px,
-                                                       const double *__restrict__ py, const double *__restrict__ pz,
-                                                       const int *__restrict__ pair_batch,
-                                                       const int *__restrict__ pair_blk, long p0,
-                                                       const double *__restrict__ coef, const double *__restrict__ vj,
-                                                       int nspin, long npad, double *__restrict__ ws,
-                                                       double *__restrict__ sph, double *__restrict__ szs) {
+__global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restrict__ sto,
+                                                         const int *__restrict__ fshell,
+                                                         const StoShell *__restrict__ bshell,
+                                                         const int *__restrict__ bnshell,
+                                                         const double *__restrict__ px,
+                                                         const double *__restrict__ py, const double *__restrict__ pz,
+                                                         const int *__restrict__ pair_batch,
+                                                         const int *__restrict__ pair_blk, long p0,
+                                                         const double *__restrict__ coef, const double *__restrict__ vj,
+                                                         int nspin, long npad, double *__restrict__ ws,
+                                                         double *__restrict__ sph, double *__restrict__ szs) {
   __shared__ double red[8][4][128];
   const long p = p0 + blockIdx.x, qrel = blockIdx.x;
   const int b = pair_batch[p], I = pair_blk[p];
@@ -498,9 +509,10 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
   constexpr int nz = NZ, nop = 1 + NZ;
   const size_t T = (size_t)kBatch * kBlockF;
   __shared__ BlockFuncs B;
-  load_block_funcs(B, sto, I, threadIdx.x, blockDim.x);
+  // during the point loop red[w][0] and red[w][1] hold warp w's radial factors
+  double *wR = red[warp][0], *wC = red[warp][1];
+  load_block_funcs(B, sto, fshell, bshell, bnshell, I, threadIdx.x, blockDim.x);
   __syncthreads();
-  const unsigned same = block_funcs_same_mask(B, lane);
   double m[nop][4];
 #pragma unroll
   for (int o = 0; o < nop; ++o)
@@ -527,7 +539,10 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
       }
     }
     double v[nop][4], gx[4], gy[4], gz[4];
-    block_funcs_eval4<GRAD>(B, lane, same, x, y, z, v[0], gx, gy, gz);
+    __syncwarp();
+    block_radials<GRAD>(B, lane, x, y, z, wR, wC);
+    __syncwarp();
+    block_funcs_eval4<GRAD>(B, lane, x, y, z, wR, wC, v[0], gx, gy, gz);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const double val = v[0][c];
@@ -546,6 +561,7 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
       dst[1] = make_double2(v[o][2], v[o][3]);
     }
   }
+  __syncwarp();
 #pragma unroll
   for (int o = 0; o < nop; ++o)
 #pragma unroll
@@ -866,7 +882,7 @@ template <bool GRAD>
 static void launch_colloc_z_g(Plan &P, MixedState &M, const Chunk &c, int nzs, int nspin, cudaStream_t s) {
   const unsigned np = (unsigned)(c.p1 - c.p0);
 #define NKX_CZ(NZ)                                                                                                   \
-  colloc_z_kernel<GRAD, NZ><<<np, 256, 0, s>>>(P.d_sto, P.d_px, P.d_py, P.d_pz, P.d_pair_batch, P.d_pair_blk, c.p0, \
+  colloc_z_kernel<GRAD, NZ><<<np, 256, 0, s>>>(P.d_sto, P.d_fshell, P.d_bshell, P.d_bnshell, P.d_px, P.d_py, P.d_pz, P.d_pair_batch, P.d_pair_blk, c.p0, \
                                                P.d_coef, P.d_vj, nspin, P.npad, P.ws_phi, M.sph, M.sz)
   if (nzs == 1)
     NKX_CZ(1);
@@ -905,10 +921,10 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     if (np > 0) {
       Tm.begin(ST_COLLOC, s);
       if (P.gga)
-        colloc_quantT_kernel<true><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
+        colloc_quantT_kernel<true><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_fshell, P.d_bshell, P.d_bnshell, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
                                                                 P.d_pair_blk, c.p0, M.qphT, M.sphT);
       else
-        colloc_quantT_kernel<false><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
+        colloc_quantT_kernel<false><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_fshell, P.d_bshell, P.d_bnshell, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
                                                                  P.d_pair_blk, c.p0, M.qphT, M.sphT);
       NKX_LAUNCH_CHECK();
       ++P.launches;
