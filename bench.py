@@ -215,12 +215,12 @@ def int8_gemm_peak(torch):
         n = 8192
         a = torch.randint(-128, 128, (n, n), dtype=torch.int8, device="cuda")
         b = torch.randint(-128, 128, (n, n), dtype=torch.int8, device="cuda").t().contiguous().t()
-        for _ in range(2):
+        for _ in range(5):
             torch._int_mm(a, b)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         best = 1e30
-        for _ in range(5):
+        for _ in range(12):
             e0.record()
             torch._int_mm(a, b)
             e1.record()
