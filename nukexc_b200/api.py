@@ -352,8 +352,10 @@ class FockBuilder:
         check(L.lib().nkx_fock_build(self._h, prec, nspin, nocc, pC, po, L.MEM_HOST if host else L.MEM_DEVICE,
                                      1 if fuse_j else 0, C.byref(E), pV, pJ, s))
         if host:
-            Vs = [V[k * nn:(k + 1) * nn].reshape(self.nbf, self.nbf).T.copy() for k in range(nspin)]
-            Jm = J.reshape(self.nbf, self.nbf).T.copy() if J is not None else None
+            # V and J are symmetric, so the column-major buffers read row-major
+            # are the matrices themselves (no transposing copy)
+            Vs = [V[k * nn:(k + 1) * nn].reshape(self.nbf, self.nbf) for k in range(nspin)]
+            Jm = J.reshape(self.nbf, self.nbf) if J is not None else None
         else:
             Vs = [V[k * nn:(k + 1) * nn].view(self.nbf, self.nbf).t() for k in range(nspin)]
             Jm = J.view(self.nbf, self.nbf).t() if J is not None else None
