@@ -205,6 +205,14 @@ NKX_API nkx_status nkx_coulomb_dense(int nbf, int naux, long npts, const double 
                                      const double *d_X, int K, int nocc, const double *d_C, const double *d_occ,
                                      double *d_J, void *stream);
 
+/* compute_core_hamiltonian (nukexc/core_hamiltonian.hpp:133-289) by
+ * quadrature on device points/weights: S = sum_g w phi phi^T,
+ * T = 1/2 sum_g w grad phi . grad phi^T, V = -sum_g w (sum_A Z_A / |r - R_A|) phi phi^T
+ * (nbf x nbf column-major device outputs; mol holds host centres and charges). */
+NKX_API nkx_status nkx_core_hamiltonian_dense(const nkx_basis *basis, const nkx_molecule *mol,
+                                              const double *d_points, const double *d_w, long npts, double *d_S,
+                                              double *d_T, double *d_V, void *stream);
+
 /* compute_half_inverse (nukexc/nukexc_utils.hpp:198-270): X = U s^-1/2 / D
  * of the preconditioned metric, keeping s > thr (symmetric
  * eigendecomposition on the device).  d_X must hold N*N; *K receives the

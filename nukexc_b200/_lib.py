@@ -20,7 +20,7 @@ XC_LDA_X, XC_LDA_C_VWN, XC_GGA_X_PBE, XC_GGA_C_PBE = 1, 7, 101, 130
 
 EXPORTS = [
     "nkx_make_flat_grid", "nkx_becke_partition", "nkx_fill_collocation", "nkx_density_dense",
-    "nkx_xc_dense", "nkx_xc_dense_noalloc", "nkx_xc_eval", "nkx_potential_collocation", "nkx_half_inverse", "nkx_coulomb_dense",
+    "nkx_xc_dense", "nkx_xc_dense_noalloc", "nkx_xc_eval", "nkx_potential_collocation", "nkx_half_inverse", "nkx_coulomb_dense", "nkx_core_hamiltonian_dense",
     "nkx_plan_create", "nkx_plan_get_info", "nkx_fock_build", "nkx_get_last_timing",
     "nkx_plan_last_density", "nkx_plan_batch_blocks", "nkx_plan_destroy", "nkx_last_error", "nkx_xc_gradient",
 ]
@@ -87,6 +87,7 @@ def lib():
             "nkx_potential_collocation": [vp, vp, vp, l_, vp, vp],
             "nkx_half_inverse": [i, vp, d, vp, vp, vp],
             "nkx_coulomb_dense": [i, i, l_, vp, vp, vp, i, i, vp, vp, vp, vp],
+            "nkx_core_hamiltonian_dense": [vp, vp, vp, vp, l_, vp, vp, vp, vp],
             "nkx_plan_create": [vp, vp, vp, l_, vp, vp, vp, vp, vp],
             "nkx_plan_get_info": [vp, vp],
             "nkx_fock_build": [vp, i, i, i, vp, vp, i, i, vp, vp, vp, vp],

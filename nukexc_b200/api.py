@@ -277,6 +277,21 @@ def compute_coulomb(mo_orbitals, mo_coeff, basis_collocation, basis_aux_collocat
     return J
 
 
+def compute_core_hamiltonian(basis, centers, Z, points, weights):
+    """compute_core_hamiltonian (nukexc/core_hamiltonian.hpp:133-289) by
+    quadrature: (S, T, V_nuc, H = T + V_nuc) as nbf x nbf CUDA tensors."""
+    pts = _dev(points).reshape(-1)
+    w = _dev(weights)
+    n = basis.nbf()
+    out = [torch.empty(n * n, dtype=torch.float64, device="cuda") for _ in range(3)]
+    mol, keep = _mol(centers, Z)
+    b = basis.as_c()
+    check(L.lib().nkx_core_hamiltonian_dense(C.byref(b), C.byref(mol), _p(pts), _p(w), w.numel(),
+                                             *[_p(o) for o in out], None))
+    S, T, V = (o.view(n, n).t() for o in out)
+    return S, T, V, T + V
+
+
 # ------------------------------------------------------------------ plan --
 class FockBuilder:
     """The batched grid-integration Fock build behind nkx_plan_* (the hot

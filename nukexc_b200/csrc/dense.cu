@@ -386,6 +386,83 @@ extern "C" nkx_status nkx_coulomb_dense(int nbf, int naux, long npts, const doub
   });
 }
 
+// per chunk point g: ws[g] = w_g, wv[g] = w_g sum_A Z_A / (|r_g - R_A| + 1e-30)
+// (core_hamiltonian.hpp:226-236)
+__global__ void core_weights_kernel(const double *__restrict__ pts, const double *__restrict__ w, long n,
+                                    const double *__restrict__ centers, const double *__restrict__ Zc, int natoms,
+                                    double *__restrict__ wv) {
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  double v = 0.0;
+  for (int a = 0; a < natoms; ++a) {
+    const double dx = pts[3 * g] - centers[3 * a], dy = pts[3 * g + 1] - centers[3 * a + 1],
+                 dz = pts[3 * g + 2] - centers[3 * a + 2];
+    v += Zc[a] / (sqrt(dx * dx + dy * dy + dz * dz) + 1e-30);
+  }
+  wv[g] = w[g] * v;
+}
+// out(mu, g) = in(mu, g) * s[g]
+__global__ void scale_cols_kernel(int nbf, long n, const double *__restrict__ in, const double *__restrict__ s,
+                                  double *__restrict__ out) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e < (long)nbf * n) out[e] = in[e] * s[e / nbf];
+}
+
+extern "C" nkx_status nkx_core_hamiltonian_dense(const nkx_basis *basis, const nkx_molecule *mol,
+                                                 const double *d_points, const double *d_w, long npts, double *d_S,
+                                                 double *d_T, double *d_V, void *stream) {
+  return run_guarded("nkx_core_hamiltonian_dense", [&] {
+    NKX_REQUIRE(basis && basis->nbf > 0 && mol && mol->natoms > 0 && d_points && d_w && npts > 0 && d_S && d_T && d_V,
+                NKX_ERR_ARG, "invalid arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nbf = basis->nbf;
+    auto tab = make_sto_table(*basis);
+    DevBuf<StoFunc> df(tab.size());
+    NKX_CUDA(cudaMemcpyAsync(df.p, tab.data(), sizeof(StoFunc) * tab.size(), cudaMemcpyHostToDevice, s));
+    std::vector<double> zc(mol->natoms);
+    for (int a = 0; a < mol->natoms; ++a) zc[a] = mol->Z[a];
+    DevBuf<double> dc(3 * (size_t)mol->natoms), dz(mol->natoms);
+    NKX_CUDA(cudaMemcpyAsync(dc.p, mol->xyz, sizeof(double) * 3 * mol->natoms, cudaMemcpyHostToDevice, s));
+    NKX_CUDA(cudaMemcpyAsync(dz.p, zc.data(), sizeof(double) * mol->natoms, cudaMemcpyHostToDevice, s));
+    // points in chunks holding 6 nbf x chunk matrices in about 1 GiB
+    const long chunk = std::max<long>(256, std::min<long>(npts, ((long)1 << 27) / (6L * nbf)));
+    DevBuf<double> phi((size_t)nbf * chunk), gx((size_t)nbf * chunk), gy((size_t)nbf * chunk),
+        gz((size_t)nbf * chunk), sc((size_t)nbf * chunk), wv(chunk);
+    NKX_CUDA(cudaMemsetAsync(d_S, 0, sizeof(double) * nbf * nbf, s));
+    NKX_CUDA(cudaMemsetAsync(d_T, 0, sizeof(double) * nbf * nbf, s));
+    NKX_CUDA(cudaMemsetAsync(d_V, 0, sizeof(double) * nbf * nbf, s));
+    cublasHandle_t h;
+    NKX_REQUIRE(cublasCreate(&h) == CUBLAS_STATUS_SUCCESS, NKX_ERR_CUDA, "cublasCreate failed");
+    cublasSetStream(h, s);
+    bool ok = true;
+    const double one = 1.0, half = 0.5, mone = -1.0;
+    for (long g0 = 0; g0 < npts && ok; g0 += chunk) {
+      const long n = std::min(chunk, npts - g0);
+      const long tot = (long)nbf * n;
+      colloc_dense_kernel<<<nblk(tot, 128), 128, 0, s>>>(df.p, nbf, d_points + 3 * g0, n, phi.p, gx.p, gy.p, gz.p);
+      core_weights_kernel<<<nblk(n, 128), 128, 0, s>>>(d_points + 3 * g0, d_w + g0, n, dc.p, dz.p, mol->natoms, wv.p);
+      // S += phi (w phi)^T
+      scale_cols_kernel<<<nblk(tot, 256), 256, 0, s>>>(nbf, n, phi.p, d_w + g0, sc.p);
+      ok = ok && cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, (int)n, &one, phi.p, nbf, sc.p, nbf, &one, d_S,
+                             nbf) == CUBLAS_STATUS_SUCCESS;
+      // V -= phi (w v phi)^T
+      scale_cols_kernel<<<nblk(tot, 256), 256, 0, s>>>(nbf, n, phi.p, wv.p, sc.p);
+      ok = ok && cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, (int)n, &mone, phi.p, nbf, sc.p, nbf, &one, d_V,
+                             nbf) == CUBLAS_STATUS_SUCCESS;
+      // T += 1/2 sum_k g_k (w g_k)^T
+      for (double *gk : {gx.p, gy.p, gz.p}) {
+        scale_cols_kernel<<<nblk(tot, 256), 256, 0, s>>>(nbf, n, gk, d_w + g0, sc.p);
+        ok = ok && cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, (int)n, &half, gk, nbf, sc.p, nbf, &one, d_T,
+                               nbf) == CUBLAS_STATUS_SUCCESS;
+      }
+      ok = ok && cudaGetLastError() == cudaSuccess;
+    }
+    NKX_CUDA(cudaStreamSynchronize(s));
+    cublasDestroy(h);
+    NKX_REQUIRE(ok, NKX_ERR_CUDA, "kernel or cuBLAS failure in nkx_core_hamiltonian_dense");
+  });
+}
+
 extern "C" nkx_status nkx_half_inverse(int N, const double *d_S, double thr, double *d_X, int *K, void *stream) {
   return run_guarded("nkx_half_inverse", [&] {
     NKX_REQUIRE(N > 0 && d_S && d_X && K, NKX_ERR_ARG, "invalid arguments");

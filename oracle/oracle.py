@@ -284,3 +284,20 @@ def coulomb(b, aux, pts, w, C, occ, X=None, S=None):
     if rc != 0:
         raise RuntimeError("oracle Cholesky failed: metric not positive definite")
     return J.reshape(nbf, nbf).T.copy(), c
+
+
+def core_hamiltonian(b, centers, Z, pts, w):
+    """compute_core_hamiltonian (nukexc/core_hamiltonian.hpp:133-289) by
+    quadrature: S = sum w phi phi^T, T = 1/2 sum w grad phi . grad phi^T,
+    V = -sum w (sum_A Z_A / (|r - R_A| + 1e-30)) phi phi^T (the shift of
+    nukexc/nukexc_config.hpp:61).  Returns (S, T, V)."""
+    pts = np.asarray(pts, float)
+    w = np.asarray(w, float)
+    phi, gx, gy, gz = collocation(b, pts, grad=True)
+    v = np.zeros(len(w))
+    for c, z in zip(np.asarray(centers, float), Z):
+        v += float(z) / (np.linalg.norm(pts - c, axis=1) + 1e-30)
+    S = (phi * w) @ phi.T
+    T = 0.5 * ((gx * w) @ gx.T + (gy * w) @ gy.T + (gz * w) @ gz.T)
+    V = -(phi * (w * v)) @ phi.T
+    return S, T, V

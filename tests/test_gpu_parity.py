@@ -286,3 +286,20 @@ def test_golden_coulomb_h1s_dense():
     X = A.compute_half_inverse(S, 1e-4)
     J = A.compute_coulomb(np.ones((1, 1)), np.ones(1), phi, phi_aux, Vw, X)
     assert J[0, 0].item() == pytest.approx(KAT["h1s_coulomb"]["J00"], rel=1e-10)
+
+
+def test_core_hamiltonian_matches_oracle():
+    # nkx_core_hamiltonian_dense vs the oracle's quadrature (water, and the
+    # exact H 1s values S = 1, T = 1/2, V = -1)
+    c, Z, funcs, g = water_case(1, nrad=40, order=17)
+    b, ob = basis_pair(funcs)
+    S, T, V, H = A.compute_core_hamiltonian(b, c, Z, g.quad_points, g.weights)
+    So, To, Vo = O.core_hamiltonian(ob, c, Z, g.quad_points, g.weights)
+    for X, Xo in ((S, So), (T, To), (V, Vo)):
+        assert np.abs(X.cpu().numpy() - Xo).max() < 1e-11 * max(1.0, np.abs(Xo).max())
+    gh = A.make_flat_grid([[0, 0, 0]], [1], 200, 20, radial="becke")
+    bh, _ = h1s()
+    S, T, V, _ = A.compute_core_hamiltonian(bh, [[0, 0, 0]], [1], gh.quad_points, gh.weights)
+    assert S[0, 0].item() == pytest.approx(1.0, rel=1e-10)
+    assert T[0, 0].item() == pytest.approx(0.5, rel=1e-9)
+    assert V[0, 0].item() == pytest.approx(-1.0, rel=1e-9)

@@ -218,3 +218,14 @@ def test_correlation_uniform_gas_values():
         e130, _, _ = O.xc_eval(130, 1, [rho], [0.0])
         assert abs(e7[0] - e130[0]) < 1e-3
         assert abs(e7[0] - ref) < 1.5e-3
+
+
+def test_core_hamiltonian_h1s_exact():
+    # core_hamiltonian.hpp:133-289 by quadrature; H 1s (zeta = 1): S = 1,
+    # T = zeta^2 / 2, V = -Z zeta (exact values, Becke 200 x L20)
+    pts, w, _ = O.make_flat_grid([[0, 0, 0]], [1], 200, 20, scheme="becke")
+    b = O.make_manual_basis([(1, 0, 0, 1.0, 0, 0, 0)])
+    S, T, V = O.core_hamiltonian(b, [[0, 0, 0]], [1], pts, w)
+    assert S[0, 0] == pytest.approx(1.0, rel=1e-10)
+    assert T[0, 0] == pytest.approx(0.5, rel=1e-9)
+    assert V[0, 0] == pytest.approx(-1.0, rel=1e-9)
