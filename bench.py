@@ -63,6 +63,8 @@ def parse():
                          "functions, ~3e7 points), closed shell with nocc = electrons / 2")
     ap.add_argument("--no-fp64", action="store_true",
                     help="skip the same-GPU FP64 comparison build (for very large workloads)")
+    ap.add_argument("--no-scf", action="store_true",
+                    help="skip the water SCF (Slater + VWN5, SCF to 1e-8 Eh) reported beside the headline")
     ap.add_argument("--workspace-mb", type=int, default=0,
                     help="cap on the per-chunk collocation workspace in MiB (0: automatic); more chunks, same work")
     return ap.parse_args()
@@ -362,6 +364,51 @@ def xc_gradient_check(n, stream, ngeom=3, ncomp=2, h=1e-4):
             "fd": "Richardson-extrapolated central differences, h = 1e-4 and 5e-5 bohr, FP64 GPU E_xc"}
 
 
+def scf_water():
+    """Water, Slater + VWN5, TA-M4 75 x Lebedev 302, closed-shell SCF to 1e-8
+    Eh with the stand-in driver: on the GPU in FP64 and mixed precision, and
+    the same SCF with the CPU oracle (the reference's dense algorithm, all
+    host threads)."""
+    from nukexc_b200 import api as A
+    from nukexc_b200 import molecules as M
+    from nukexc_b200 import scf
+    from oracle import oracle as O
+    xc = ("LDA_X", "LDA_C_VWN")
+    c, Z = M.water()
+    funcs = M.sto_basis(c, Z)
+    aux = M.sto_basis(c, Z, {8: [(0, 6), (1, 5), (2, 4), (3, 2)], 1: [(0, 4), (1, 3), (2, 1)]}, alpha=0.8,
+                      beta=2.5)
+    enuc = scf.nuclear_repulsion(c, Z)
+    out = {"workload": "H2O Slater+VWN5 SCF to 1e-8 Eh, TA-M4 75 x Lebedev 302, grid DF-J (91 aux)",
+           "nbf": len(funcs)}
+    g = A.make_flat_grid(c, Z, 75, 29, weight_threshold=1e-15, radial="ta")
+    b = A.make_manual_basis(funcs)
+    fb = A.FockBuilder(c, Z, b, g, aux=A.make_manual_basis(aux), func_ids=xc)
+    S, T, V, H = A.compute_core_hamiltonian(b, c, Z, g.quad_points, g.weights)
+    for prec in ("fp64", "mixed"):
+        r = scf.rks(S.cpu().numpy(), H.cpu().numpy(), scf.gpu_fock(fb, prec), 5, enuc)
+        out[prec] = {"energy": r["energy"], "iterations": r["iterations"], "converged": r["converged"],
+                     "ms_per_iteration": 1e3 * float(np.median(r["seconds_per_iteration"]))}
+    fb.close()
+    pts, w, _ = O.make_flat_grid(c, Z, 75, 29, weight_threshold=1e-15, scheme="ta")
+    ob, oa = O.make_manual_basis(funcs), O.make_manual_basis(aux)
+    So, To, Vo = O.core_hamiltonian(ob, c, Z, pts, w)
+    Sa = O.aux_metric(oa, pts, w)
+
+    def cpu_fock(Cocc):
+        occ = 2.0 * np.ones(Cocc.shape[1])
+        E, Vx = O.xc_build(ob, pts, w, [1, 7], [Cocc], [occ])
+        J, _ = O.coulomb(ob, oa, pts, w, Cocc, occ, S=Sa)
+        return E, Vx[0], J
+    r = scf.rks(So, To + Vo, cpu_fock, 5, enuc)
+    out["cpu_port"] = {"energy": r["energy"], "iterations": r["iterations"], "converged": r["converged"],
+                       "ms_per_iteration": 1e3 * float(np.median(r["seconds_per_iteration"])),
+                       "cores": os.cpu_count()}
+    out["dE_gpu_fp64_vs_cpu"] = abs(out["fp64"]["energy"] - out["cpu_port"]["energy"])
+    out["dE_mixed_vs_fp64"] = abs(out["mixed"]["energy"] - out["fp64"]["energy"])
+    return out
+
+
 # ---------------------------------------------------------------- nkx ----
 def vgemm_flops(info_pairs_per_batch, nz=1):
     """Algorithmic FLOPs of the V = Phi Z^T contraction: sum_b 2 n_b^2 256."""
@@ -566,6 +613,8 @@ def run_nkx(args):
             line["xc_plus_j"] = xc_plus_j(args.j_waters, max(1, min(args.steps, 3)), args.warmup, stream)
         if world == 1 and args.grad_waters > 0:
             line["xc_gradient"] = xc_gradient_check(args.grad_waters, stream)
+        if world == 1 and not args.no_scf:
+            line["scf_water"] = scf_water()
         print(json.dumps(line), flush=True)
     fb.close()
     if dist is not None:
