@@ -49,31 +49,6 @@ NKX_HD inline double inv_int(int k) {
 #endif
 }
 
-// Gamma(n, x) for integer n >= 1: (n-1)! e^-x sum_{k<n} x^k/k!
-NKX_HD inline double upper_gamma_int(int n, double x) {
-  double sum = 1.0, term = 1.0;
-  for (int k = 1; k < n; ++k) {
-    term *= x * (k <= 64 ? inv_int(k) : 1.0 / k);
-    sum += term;
-  }
-  return fact_d(n - 1) * exp(-x) * sum;
-}
-
-// gamma(n, x) for integer n >= 1: ascending series for x < n, else
-// (n-1)! - Gamma(n, x) (nukexc_utils.hpp:169-196)
-NKX_HD inline double lower_gamma_int(int n, double x) {
-  if (x < n) {
-    double sum = n <= 64 ? inv_int(n) : 1.0 / n, term = sum;
-    for (int k = 1; k < 1000; ++k) {
-      term *= x * (n + k <= 64 ? inv_int(n + k) : 1.0 / (n + k));
-      sum += term;
-      if (term < 1e-16 * sum) break;
-    }
-    return exp(n * log(x) - x) * sum;
-  }
-  return fact_d(n - 1) - upper_gamma_int(n, x);
-}
-
 // radial factor I(r) of V_a = C S_lm I(r); shared by the 2l+1 functions of a
 // shell.  One exp(-x) serves both incomplete gammas: Gamma(b, x) =
 // (b-1)! e^-x sum_(k<b) x^k/k!, and gamma(a, x) by its ascending series

@@ -70,8 +70,9 @@ struct TcArgs {
   const int *pair_off, *pair_blk;
   const uint32_t *mask;
   int mask_words, nblk;
-  // V mode
-  int nz, nbf_pad;
+  // V mode; nsplit > 1 splits each output tile's batches over that many
+  // units (interleaved), which then add their tiles atomically
+  int nz, nbf_pad, nsplit;
   const double *sA, *sB;  // row scales: V: sph[q][128], sz[q*nz+z][128]
   double *V;
   // density mode: sA = sphT[q][nc][256], sB = sct[s][i][blk]
@@ -82,12 +83,14 @@ struct TcArgs {
 };
 
 struct UnitIter {
-  int I = 0, J = 0, zi = 0;        // V: row block, column block, Z plane
+  int I = 0, J = 0, zi = 0, sp = 0;  // V: row block, column block, Z plane, batch split
   long bl = 0;                     // density: batch within chunk
   int h = 0, c = 0, s = 0, t = 0;  // density: point half, comp, spin, 128-orbital tile
   __device__ UnitIter(const TcArgs &a, long u) {
     if (a.mode == TC_MODE_V) {
-      const long n2 = (long)a.nblk * a.nblk;
+      const long n2 = (long)a.nblk * a.nblk, n3 = n2 * a.nz;
+      sp = (int)(u / n3);
+      u %= n3;
       zi = (int)(u / n2);
       I = (int)((u % n2) / a.nblk);
       J = (int)(u % a.nblk);
@@ -125,7 +128,7 @@ template <class Fn>
 __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &it, Fn &&fn) {
   if (a.mode == TC_MODE_V) {
     const int Jb = it.J;
-    for (long b = a.b0; b < a.b1; ++b) {
+    for (long b = a.b0 + it.sp; b < a.b1; b += a.nsplit) {
       const uint32_t *m = a.mask + b * a.mask_words;
       if (!blk_has(m, it.I) || !blk_has(m, Jb)) continue;
       const long qb0 = a.pair_off[b] - a.p0;
@@ -367,8 +370,13 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
         if (any) {
           double *Vz = a.V + (size_t)it.zi * a.nbf_pad * a.nbf_pad;
           const size_t r = (size_t)it.I * 128 + row;
+          if (a.nsplit > 1) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) Vz[r + ((size_t)it.J * 128 + 32 * cq + j) * a.nbf_pad] += acc[j];
+            for (int j = 0; j < 32; ++j) atomicAdd(&Vz[r + ((size_t)it.J * 128 + 32 * cq + j) * a.nbf_pad], acc[j]);
+          } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) Vz[r + ((size_t)it.J * 128 + 32 * cq + j) * a.nbf_pad] += acc[j];
+          }
         }
       } else {
         const long plane = (it.bl * a.nspin + it.s) * a.ncomp + it.c;
@@ -987,7 +995,11 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.sB = M.sz;
     a.V = P.d_V;
     a.err = M.err;
-    a.nunits = (long)nzs * P.nblk * P.nblk;
+    // too few output tiles for the SMs: split the chunk's batches
+    const long tiles = (long)nzs * P.nblk * P.nblk;
+    a.nsplit = tiles >= M.nsm ? 1 : (int)std::min<long>({(M.nsm + tiles - 1) / tiles, c.b1 - c.b0, 16L});
+    a.nsplit = std::max(1, a.nsplit);
+    a.nunits = tiles * a.nsplit;
     launch_i8(M, M.m_ph, M.m_z, a, s);
     ++P.launches;
     Tm.end(s);
