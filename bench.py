@@ -312,7 +312,7 @@ def xc_plus_j(n, steps, warmup, stream):
     return out
 
 
-def xc_gradient_check(n, stream, ngeom=3, ncomp=2, h=1e-4):
+def xc_gradient_check(n, stream, ngeom=10, ncomp=1, h=1e-4):
     """XC nuclear gradient (FP64) of (H2O)_n PBE at seeded perturbed geometries
     (each atom + N(0, 0.05 bohr)): time per gradient and the largest deviation
     from Richardson-extrapolated central differences of the FP64 E_xc of the
