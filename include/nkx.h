@@ -243,6 +243,8 @@ NKX_API nkx_status nkx_plan_get_info(const nkx_plan *plan, nkx_plan_info *info);
  * mem selects whether C/occ/V/J are host or device buffers (host buffers
  * are copied inside the call).  With fuse_j != 0 (and nspin 1), J is folded
  * into the XC contraction and V receives V_xc + J (J may then be NULL).
+ * V may be NULL when J is given and fuse_j == 0: J alone is returned
+ * (compute_coulomb and its sparse / tiled variants).
  * E_xc is written to host *E.  The call is synchronous on return. */
 NKX_API nkx_status nkx_fock_build(nkx_plan *plan, int precision, int nspin, int nocc, const double *C,
                                   const double *occ, int mem, int fuse_j, double *E, double *V, double *J,
@@ -268,6 +270,57 @@ NKX_API nkx_status nkx_plan_last_density(const nkx_plan *plan, double *rho, long
 
 /* Number of significant 128-function blocks of every batch (counts[nbatches]). */
 NKX_API nkx_status nkx_plan_batch_blocks(const nkx_plan *plan, int *counts);
+
+/* Replace the plan's functional (the ids and density threshold of
+ * nkx_plan_options) for the following builds: the reference evaluates one
+ * libxc functional per call (compute_lsda_sparse / compute_gga_lsda_sparse,
+ * nukexc/xc_integrals.hpp:263-264, :728-729). */
+NKX_API nkx_status nkx_plan_set_functional(nkx_plan *plan, int nfunc, const int *func_ids, double dens_threshold);
+
+/* Use the caller's half inverse X (naux x K, column-major; mem selects host
+ * or device) for the J fit c = X X^T y of the following builds, as
+ * compute_coulomb_sparse / _tiled take half_inverse_X
+ * (nukexc/coulomb.hpp:117-121, :383-387). */
+NKX_API nkx_status nkx_plan_set_half_inverse(nkx_plan *plan, int K, const double *X, int mem);
+
+/* The plan's grid Coulomb metric (A|B) (naux x naux, symmetrised),
+ * coulomb_overlap_integral_sparse (nukexc/coulomb.hpp:691-813); mem selects
+ * host or device output. */
+NKX_API nkx_status nkx_plan_aux_metric(const nkx_plan *plan, double *S, int mem);
+
+/* Density on the plan's grid in the caller's point order, FP64
+ * (compute_density_sparse, nukexc/density.hpp:97-148, and
+ * compute_density_and_sigma_sparse, :261-328): rho[nspin][npoints],
+ * grad[nspin][3][npoints], sigma[nspin][npoints] = |grad rho_s|^2; any of the
+ * three may be NULL.  With accumulate != 0, rho and grad are added to the
+ * buffers' contents (the reference's contract) and sigma is formed from the
+ * summed gradient.  C / occ / outputs as in nkx_fock_build (mem). */
+NKX_API nkx_status nkx_plan_density(nkx_plan *plan, int nspin, int nocc, const double *C, const double *occ, int mem,
+                                    int accumulate, double *rho, double *grad, double *sigma, void *stream);
+
+/* ------------------------------------------------------ sparse set-up -- */
+
+/* Morton (Z-order) permutation of npoints host points xyz[3*npoints]:
+ * perm[k] = input index of the k-th point (create_bounding_boxes,
+ * nukexc/octree.hpp:70-110; the order the plans use). */
+NKX_API nkx_status nkx_morton_order(long npoints, const double *xyz, long *perm);
+
+/* build_neighbor_list (nukexc/octree.hpp:317-390) on the device: box b is
+ * boxes[6b .. 6b+5] = (min x, y, z, max x, y, z); function f is the sphere
+ * (centers[3f..3f+2], radii[f]).  offsets[nboxes+1] and neighbors[] are the
+ * CSR of the functions meeting each box, ascending within a box.  Two-call
+ * pattern: with neighbors == NULL the offsets are written and *nnz = list
+ * length; then call again with a neighbors buffer of *nnz entries. */
+NKX_API nkx_status nkx_neighbor_list(int nfunc, const double *d_centers, const double *d_radii, long nboxes,
+                                     const double *d_boxes, int *d_offsets, int *d_neighbors, long *nnz,
+                                     void *stream);
+
+/* Grid Coulomb metric (A|B) = (M + M^T)/2, M_AB = sum_g phi_A(g) w_g V_B(g),
+ * of an aux basis on npoints device points d_xyz[3*npoints] with weights
+ * d_w, into d_S (naux x naux, device), FP64
+ * (coulomb_overlap_integral_sparse / _tiled, nukexc/coulomb.hpp:691-958). */
+NKX_API nkx_status nkx_aux_metric(const nkx_basis *aux, long npoints, const double *d_xyz, const double *d_w,
+                                  double *d_S, void *stream);
 
 NKX_API nkx_status nkx_plan_destroy(nkx_plan *plan);
 

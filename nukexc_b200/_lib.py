@@ -23,6 +23,8 @@ EXPORTS = [
     "nkx_xc_dense", "nkx_xc_dense_noalloc", "nkx_xc_eval", "nkx_potential_collocation", "nkx_half_inverse", "nkx_coulomb_dense", "nkx_core_hamiltonian_dense",
     "nkx_plan_create", "nkx_plan_get_info", "nkx_fock_build", "nkx_get_last_timing",
     "nkx_plan_last_density", "nkx_plan_batch_blocks", "nkx_plan_destroy", "nkx_last_error", "nkx_xc_gradient",
+    "nkx_plan_set_functional", "nkx_plan_set_half_inverse", "nkx_plan_aux_metric", "nkx_plan_density",
+    "nkx_morton_order", "nkx_neighbor_list", "nkx_aux_metric",
 ]
 
 
@@ -96,6 +98,13 @@ def lib():
             "nkx_plan_last_density": [vp, vp, vp],
             "nkx_plan_batch_blocks": [vp, vp],
             "nkx_plan_destroy": [vp],
+            "nkx_plan_set_functional": [vp, i, vp, d],
+            "nkx_plan_set_half_inverse": [vp, i, vp, i],
+            "nkx_plan_aux_metric": [vp, vp, i],
+            "nkx_plan_density": [vp, i, i, vp, vp, i, i, vp, vp, vp, vp],
+            "nkx_morton_order": [l_, vp, vp],
+            "nkx_neighbor_list": [i, vp, vp, l_, vp, vp, vp, vp, vp],
+            "nkx_aux_metric": [vp, l_, vp, vp, vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

@@ -340,10 +340,13 @@ class FockBuilder:
         check(L.lib().nkx_get_last_timing(self._h, C.byref(t)))
         return {k: getattr(t, k) for k, _ in L.BuildTiming._fields_}
 
-    def build(self, C_list, occ_list, precision="fp64", want_J=False, fuse_j=False, stream=None):
+    def build(self, C_list, occ_list, precision="fp64", want_J=False, fuse_j=False, stream=None, want_V=True):
         """One Fock build.  C_list/occ_list: one (nbf x nocc, nocc) per spin,
         numpy (host: copied inside the call) or CUDA tensors (device).
-        Returns (E_xc, [V per spin], J or None); with fuse_j, V includes J."""
+        Returns (E_xc, [V per spin], J or None); with fuse_j, V includes J.
+        want_V=False (with want_J) returns J alone: (E_xc, None, J)."""
+        if not want_V and not (want_J and not fuse_j):
+            raise ValueError("want_V=False needs want_J=True and fuse_j=False")
         nspin = len(C_list)
         host = not isinstance(C_list[0], torch.Tensor)
         nocc = C_list[0].shape[1]
@@ -352,21 +355,23 @@ class FockBuilder:
         if host:
             Cc = np.concatenate([np.ascontiguousarray(np.asarray(c, np.float64).T).reshape(-1) for c in C_list])
             oc = np.concatenate([_np(o, np.float64) for o in occ_list])
-            V = np.zeros(nspin * nn)
+            V = np.zeros(nspin * nn) if want_V else None
             J = np.zeros(nn) if want_J and not fuse_j else None
-            pC, po, pV = (a.ctypes.data_as(C.c_void_p) for a in (Cc, oc, V))
-            pJ = J.ctypes.data_as(C.c_void_p) if J is not None else None
+            pC, po, pV, pJ = (a.ctypes.data_as(C.c_void_p) if a is not None else None for a in (Cc, oc, V, J))
         else:
             Cc = torch.cat([c.t().contiguous().reshape(-1) for c in C_list])
             oc = torch.cat([o.reshape(-1) for o in occ_list]).to(torch.float64)
-            V = torch.empty(nspin * nn, dtype=torch.float64, device="cuda")
+            V = torch.empty(nspin * nn, dtype=torch.float64, device="cuda") if want_V else None
             J = torch.empty(nn, dtype=torch.float64, device="cuda") if want_J and not fuse_j else None
             pC, po, pV, pJ = _p(Cc), _p(oc), _p(V), _p(J)
         E = C.c_double(0)
         s = C.c_void_p(stream) if stream else None
         check(L.lib().nkx_fock_build(self._h, prec, nspin, nocc, pC, po, L.MEM_HOST if host else L.MEM_DEVICE,
                                      1 if fuse_j else 0, C.byref(E), pV, pJ, s))
-        if host:
+        if V is None:
+            Vs = None
+            Jm = J.reshape(self.nbf, self.nbf) if host else J.view(self.nbf, self.nbf).t()
+        elif host:
             # V and J are symmetric, so the column-major buffers read row-major
             # are the matrices themselves (no transposing copy)
             Vs = [V[k * nn:(k + 1) * nn].reshape(self.nbf, self.nbf) for k in range(nspin)]
@@ -391,6 +396,47 @@ class FockBuilder:
                                       oc.ctypes.data_as(C.c_void_p), L.MEM_HOST, becke_clamp,
                                       g.ctypes.data_as(C.c_void_p), s))
         return g.reshape(natoms, 3)
+
+    def density(self, C_list, occ_list, grad=False, stream=None):
+        """rho (nspin x npts) on the plan's grid in the caller's point order,
+        FP64 (compute_density_sparse / compute_density_and_sigma_sparse,
+        nukexc/density.hpp:97-148, :261-328; nkx_plan_density).  With grad,
+        also grad rho (nspin x 3 x npts) and sigma = |grad rho|^2 (nspin x npts)."""
+        nspin = len(C_list)
+        nocc = C_list[0].shape[1]
+        n = self.info()["npoints"]
+        Cc = np.concatenate([np.ascontiguousarray(np.asarray(c, np.float64).T).reshape(-1) for c in C_list])
+        oc = np.concatenate([_np(o, np.float64) for o in occ_list])
+        rho = np.zeros(nspin * n)
+        g = np.zeros(3 * nspin * n) if grad else None
+        sg = np.zeros(nspin * n) if grad else None
+        s = C.c_void_p(stream) if stream else None
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p) if a is not None else None  # noqa: E731
+        check(L.lib().nkx_plan_density(self._h, nspin, nocc, ptr(Cc), ptr(oc), L.MEM_HOST, 0, ptr(rho), ptr(g),
+                                       ptr(sg), s))
+        if grad:
+            return rho.reshape(nspin, n), g.reshape(nspin, 3, n), sg.reshape(nspin, n)
+        return rho.reshape(nspin, n)
+
+    def set_functional(self, func_ids, dens_threshold=1e-15):
+        """Evaluate these functionals in the following builds (nkx_plan_set_functional)."""
+        ids = [_FUNC_NAMES.get(f, f) for f in func_ids]
+        arr = (C.c_int * len(ids))(*ids)
+        check(L.lib().nkx_plan_set_functional(self._h, len(ids), arr, dens_threshold))
+
+    def set_half_inverse(self, X):
+        """Fit J with the caller's half inverse X (naux x K): c = X X^T y
+        (compute_coulomb_sparse's half_inverse_X; nkx_plan_set_half_inverse)."""
+        Xa = np.asarray(X, np.float64)
+        assert Xa.shape[0] == self.naux, "X must be naux x K"
+        col = np.ascontiguousarray(Xa.T).reshape(-1)
+        check(L.lib().nkx_plan_set_half_inverse(self._h, Xa.shape[1], col.ctypes.data_as(C.c_void_p), L.MEM_HOST))
+
+    def aux_metric(self):
+        """The plan's symmetrised grid Coulomb metric (A|B), naux x naux."""
+        S = np.zeros(self.naux * self.naux)
+        check(L.lib().nkx_plan_aux_metric(self._h, S.ctypes.data_as(C.c_void_p), L.MEM_HOST))
+        return S.reshape(self.naux, self.naux).T.copy()
 
     def batch_blocks(self):
         """Significant 128-function blocks per batch."""
@@ -419,3 +465,92 @@ class FockBuilder:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------ sparse set-up ----
+def cutoff_radii(basis):
+    """Per function, the largest r with N r^(n-1) e^(-zeta r) >= cutoff_tol
+    (the reference's cutoff radius, nukexc/stobasis.hpp:203-222), by bisection
+    on the decreasing tail beyond the maximum at r = (n-1)/zeta."""
+    from math import lgamma, log
+    out = np.zeros(basis.nbf())
+    lt = log(basis.cutoff_tol)
+    for i, (n, z) in enumerate(zip(basis.n, basis.zeta)):
+        n, z = int(n), float(z)
+        lnN = (n + 0.5) * log(2.0 * z) - 0.5 * lgamma(2.0 * n + 1.0)
+        g = lambda r: lnN + (n - 1) * log(max(r, 1e-300)) - z * r  # noqa: E731
+        lo = (n - 1) / z
+        hi = lo + 1.0
+        while g(hi) > lt:
+            hi *= 2.0
+        for _ in range(200):
+            mid = 0.5 * (lo + hi)
+            if g(mid) > lt:
+                lo = mid
+            else:
+                hi = mid
+        out[i] = hi
+    return out
+
+
+@dataclass
+class NeighborList:
+    """NeighborList (nukexc/octree.hpp:279-285): CSR of the basis functions
+    meeting each box, ascending per box (CUDA int32 tensors)."""
+    neighbors: torch.Tensor
+    offsets: torch.Tensor
+    max_points_per_box: int
+    total_points: int
+
+
+def create_bounding_boxes(grid, max_points_per_bb):
+    """create_bounding_boxes (nukexc/octree.hpp:70-144): permutes
+    grid.quad_points, grid.weights and grid.point_owner in place into Morton
+    order (nkx_morton_order) and returns the bounds of each run of
+    max_points_per_bb consecutive points as a CUDA tensor (nboxes, 2, 3) of
+    (min corner, max corner)."""
+    if max_points_per_bb <= 0:
+        raise ValueError("max_points_per_bb must be positive")
+    pts = _np(grid.quad_points, np.float64).reshape(-1, 3)
+    G = len(pts)
+    perm = np.zeros(G, np.int64)
+    check(L.lib().nkx_morton_order(G, pts.ctypes.data_as(C.c_void_p), perm.ctypes.data_as(C.c_void_p)))
+    sp = pts[perm]  # a copy: pts may be the grid's own array
+    grid.quad_points[...] = sp.reshape(np.shape(grid.quad_points))
+    grid.weights[...] = np.asarray(grid.weights)[perm]
+    if grid.point_owner is not None and len(grid.point_owner) == G:
+        grid.point_owner[...] = np.asarray(grid.point_owner)[perm]
+    starts = np.arange(0, G, max_points_per_bb)
+    boxes = np.stack([np.minimum.reduceat(sp, starts, axis=0), np.maximum.reduceat(sp, starts, axis=0)], 1)
+    return _dev(boxes)
+
+
+def build_neighbor_list(basis, bounding_boxes, max_points_per_box, total_points):
+    """build_neighbor_list (nukexc/octree.hpp:317-390): functions whose
+    cutoff sphere meets each box (nkx_neighbor_list, on the device)."""
+    boxes = _dev(bounding_boxes).reshape(-1, 6)
+    nb = boxes.shape[0]
+    centers = _dev(basis.center)
+    radii = _dev(cutoff_radii(basis))
+    offsets = torch.zeros(nb + 1, dtype=torch.int32, device="cuda")
+    nnz = C.c_long(0)
+    check(L.lib().nkx_neighbor_list(basis.nbf(), _p(centers), _p(radii), nb, _p(boxes), _p(offsets), None,
+                                    C.byref(nnz), None))
+    neighbors = torch.zeros(max(1, nnz.value), dtype=torch.int32, device="cuda")
+    if nnz.value:
+        check(L.lib().nkx_neighbor_list(basis.nbf(), _p(centers), _p(radii), nb, _p(boxes), _p(offsets),
+                                        _p(neighbors), C.byref(nnz), None))
+    return NeighborList(neighbors[:nnz.value], offsets, max_points_per_box, total_points)
+
+
+def coulomb_overlap_integral(basis_aux, points, weights):
+    """Symmetrised grid Coulomb metric (A|B) of an aux basis
+    (coulomb_overlap_integral_sparse / _tiled, nukexc/coulomb.hpp:691-958;
+    nkx_aux_metric), as a CUDA tensor naux x naux."""
+    pts = _dev(points).reshape(-1)
+    w = _dev(weights)
+    na = basis_aux.nbf()
+    S = torch.zeros(na * na, dtype=torch.float64, device="cuda")
+    b = basis_aux.as_c()
+    check(L.lib().nkx_aux_metric(C.byref(b), len(w), _p(pts), _p(w), _p(S), None))
+    return S.view(na, na).t()

@@ -400,6 +400,37 @@ __global__ void __launch_bounds__(256) vgemm_fp64_kernel(const double *__restric
 
 // out(i, j) = Vp(pi, pj) + Vp(pj, pi), p = finv[.] the plan position of
 // caller function i (symmetrise, unpad and undo the plan order)
+// Plan-order density of one spin (blockIdx.y) -> caller order: rho and the
+// gradient are written, or added to the output with accumulate (the
+// "accumulated into" contract of compute_density_and_sigma_sparse,
+// nukexc/density.hpp:257-260); sigma = |grad rho|^2 of the resulting
+// gradient.  Output planes are npts long: rho[s], grad[3 s + d], sigma[s].
+__global__ void density_out_kernel(long npts, long npad, const long *__restrict__ perm, const double *__restrict__ rho,
+                                   const double *__restrict__ grad, int accumulate, double *__restrict__ orho,
+                                   double *__restrict__ ograd, double *__restrict__ osigma) {
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (p >= npts) return;
+  const long g = perm[p];
+  if (orho) {
+    const double v = rho[(size_t)s * npad + p];
+    orho[(size_t)s * npts + g] = accumulate ? orho[(size_t)s * npts + g] + v : v;
+  }
+  if (ograd || osigma) {
+    double sg = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      double v = grad[((size_t)s * 3 + d) * npad + p];
+      if (ograd) {
+        const size_t o = ((size_t)s * 3 + d) * npts + g;
+        if (accumulate) v += ograd[o];
+        ograd[o] = v;
+      }
+      sg += v * v;
+    }
+    if (osigma) osigma[(size_t)s * npts + g] = sg;
+  }
+}
+
 __global__ void symmetrize_unpad_kernel(int n, int npad, const int *__restrict__ finv, const double *__restrict__ Vp,
                                         double *__restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -588,6 +619,13 @@ __global__ void aux_tables_kernel(const StoFunc *__restrict__ sto, const AuxFunc
   vw[e] = aux_potential(aux[a], px[g], py[g], pz[g]) * w[g];
 }
 
+// interleaved points xyz[3n] -> planes x[n], y[n], z[n]
+__global__ void split_points_kernel(long n, const double *__restrict__ xyz, double *__restrict__ soa) {
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  for (int d = 0; d < 3; ++d) soa[(size_t)d * n + g] = xyz[3 * g + d];
+}
+
 __global__ void gather_kernel(int K, const int *__restrict__ piv, const double *__restrict__ y, double *__restrict__ t) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < K) t[i] = y[piv[i]];
@@ -606,6 +644,33 @@ __global__ void sym_half_kernel(int n, double *S) {
   }
 }
 
+// (A|B) = (M + M^T) / 2 with M_AB = sum_g phi_A(g) w_g V_B(g): the grid
+// Coulomb metric of coulomb_overlap_integral(_sparse/_tiled)
+// (nukexc/coulomb.hpp:691-813, :827-958), FP64 GEMMs over point slices of at
+// most 256 MB of tables; S is naux x naux, column-major, on the device.
+static void grid_metric(const StoFunc *d_asto, const AuxFunc *d_aux, int naux, const double *px, const double *py,
+                        const double *pz, const double *w, long n, cublasHandle_t hb, cudaStream_t s, double *S) {
+  const size_t NA = naux;
+  const long slice = std::max<long>(kBatch, std::min<long>(n, (long)((size_t)1 << 28) / (16 * NA)));
+  double *sphi = dalloc<double>(NA * slice), *svw = dalloc<double>(NA * slice);
+  NKX_CUDA(cudaMemsetAsync(S, 0, sizeof(double) * NA * NA, s));
+  for (long g0 = 0; g0 < n; g0 += slice) {
+    const long np = std::min(slice, n - g0);
+    aux_tables_kernel<<<nblk(NA * np, 128), 128, 0, s>>>(d_asto, d_aux, naux, px, py, pz, w, g0, np, sphi, svw);
+    NKX_LAUNCH_CHECK();
+    const double one = 1.0;
+    NKX_REQUIRE(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, naux, naux, (int)np, &one, sphi, naux, svw, naux, &one, S,
+                            naux) == CUBLAS_STATUS_SUCCESS,
+                NKX_ERR_CUDA, "cublasDgemm failed");
+  }
+  dim3 tb(16, 16), gb(nblk(naux, 16), nblk(naux, 16));
+  sym_half_kernel<<<gb, tb, 0, s>>>(naux, S);
+  NKX_LAUNCH_CHECK();
+  NKX_CUDA(cudaStreamSynchronize(s));
+  cudaFree(sphi);
+  cudaFree(svw);
+}
+
 // ========================================================= plan set-up ==
 
 static uint64_t spread3(uint64_t v) {
@@ -616,6 +681,34 @@ static uint64_t spread3(uint64_t v) {
   v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
   v = (v | v << 2) & 0x1249249249249249ULL;
   return v;
+}
+
+// Morton (Z-order) permutation of n points xyz[3n]: 21-bit codes per axis
+// over the points' bounding box, ties kept in input order.  perm[k] is the
+// input index of the k-th point in the order (the space-filling-curve
+// permutation of create_bounding_boxes, nukexc/octree.hpp:85-104).
+static void morton_order(long n, const double *xyz, std::vector<long> &perm) {
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (long g = 0; g < n; ++g)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], xyz[3 * g + d]);
+      hi[d] = std::max(hi[d], xyz[3 * g + d]);
+    }
+  // (code, index) pairs sorted lexicographically: the stable Morton order
+  std::vector<std::pair<uint64_t, long>> key(n);
+#pragma omp parallel for schedule(static)
+  for (long g = 0; g < n; ++g) {
+    uint64_t c = 0;
+    for (int d = 0; d < 3; ++d) {
+      const double span = hi[d] > lo[d] ? hi[d] - lo[d] : 1.0;
+      const double u = (xyz[3 * g + d] - lo[d]) / span;
+      c |= spread3((uint64_t)std::min(2097151.0, std::max(0.0, u * 2097151.0))) << d;
+    }
+    key[g] = {c, g};
+  }
+  __gnu_parallel::sort(key.begin(), key.end());
+  perm.resize(n);
+  for (long g = 0; g < n; ++g) perm[g] = key[g].second;
 }
 
 void destroy_mixed_state(void *p);
@@ -660,28 +753,7 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
   P.npad = P.nbatch * kBatch;
 
   // --- Morton order of the points (create_bounding_boxes, octree.hpp:70-110)
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  for (long g = 0; g < npoints; ++g)
-    for (int d = 0; d < 3; ++d) {
-      lo[d] = std::min(lo[d], xyz[3 * g + d]);
-      hi[d] = std::max(hi[d], xyz[3 * g + d]);
-    }
-  // (code, index) pairs sorted lexicographically: the stable Morton order
-  std::vector<std::pair<uint64_t, long>> key(npoints);
-#pragma omp parallel for schedule(static)
-  for (long g = 0; g < npoints; ++g) {
-    uint64_t c = 0;
-    for (int d = 0; d < 3; ++d) {
-      const double span = hi[d] > lo[d] ? hi[d] - lo[d] : 1.0;
-      const double u = (xyz[3 * g + d] - lo[d]) / span;
-      c |= spread3((uint64_t)std::min(2097151.0, std::max(0.0, u * 2097151.0))) << d;
-    }
-    key[g] = {c, g};
-  }
-  __gnu_parallel::sort(key.begin(), key.end());
-  P.perm.resize(npoints);
-  for (long g = 0; g < npoints; ++g) P.perm[g] = key[g].second;
-  std::vector<std::pair<uint64_t, long>>().swap(key);
+  morton_order(npoints, xyz, P.perm);
   std::vector<double> hx(P.npad), hy(P.npad), hz(P.npad), hw(P.npad, 0.0);
   for (long p = 0; p < P.npad; ++p) {
     const long g = P.perm[std::min(p, npoints - 1)];
@@ -987,26 +1059,7 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
     NKX_REQUIRE(cublasCreate(&hb) == CUBLAS_STATUS_SUCCESS, NKX_ERR_CUDA, "cublasCreate failed");
     P.cublas = hb;
     cublasSetStream(hb, P.stream);
-    // (A|B) = sum_g phi_A(g) Vw_B(g), FP64, in point slices
-    const long slice = std::max<long>(kBatch, std::min<long>(P.npad, (long)((size_t)1 << 28) / (16 * NA)));
-    double *sphi = dalloc<double>(NA * slice), *svw = dalloc<double>(NA * slice);
-    NKX_CUDA(cudaMemsetAsync(P.d_L, 0, sizeof(double) * NA * NA, P.stream));
-    for (long g0 = 0; g0 < P.npad; g0 += slice) {
-      const long np = std::min(slice, P.npad - g0);
-      aux_tables_kernel<<<nblk(NA * np, 128), 128, 0, P.stream>>>(d_asto, P.d_aux, P.naux, P.d_px, P.d_py, P.d_pz,
-                                                                  P.d_w, g0, np, sphi, svw);
-      NKX_LAUNCH_CHECK();
-      const double one = 1.0;
-      NKX_REQUIRE(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, P.naux, P.naux, (int)np, &one, sphi, P.naux, svw, P.naux,
-                              &one, P.d_L, P.naux) == CUBLAS_STATUS_SUCCESS,
-                  NKX_ERR_CUDA, "cublasDgemm failed");
-    }
-    dim3 tb(16, 16), gb(nblk(P.naux, 16), nblk(P.naux, 16));
-    sym_half_kernel<<<gb, tb, 0, P.stream>>>(P.naux, P.d_L);
-    NKX_LAUNCH_CHECK();
-    NKX_CUDA(cudaStreamSynchronize(P.stream));
-    cudaFree(sphi);
-    cudaFree(svw);
+    grid_metric(d_asto, P.d_aux, P.naux, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, hb, P.stream, P.d_L);
     cudaFree(d_asto);
     P.h_metric.resize(NA * NA);
     NKX_CUDA(cudaMemcpy(P.h_metric.data(), P.d_L, sizeof(double) * NA * NA, cudaMemcpyDeviceToHost));
@@ -1252,12 +1305,15 @@ void upload_orbitals(Plan &P, int nspin, int nocc, const double *C, const double
 void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, const double *occ, int mem, int fuse_j,
                 double *E, double *V, double *J, cudaStream_t user) {
   NKX_REQUIRE(nspin == 1 || nspin == 2, NKX_ERR_ARG, "nspin must be 1 or 2");
-  NKX_REQUIRE(nocc > 0 && C && occ && E && (V || (fuse_j && J)), NKX_ERR_ARG, "invalid arguments");
+  NKX_REQUIRE(nocc > 0 && C && occ && E && (V || J), NKX_ERR_ARG, "invalid arguments");
   NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
   NKX_REQUIRE(precision == NKX_PREC_FP64 || precision == NKX_PREC_MIXED, NKX_ERR_ARG, "unknown precision");
   const bool needJ = P.naux > 0 && (J != nullptr || fuse_j);
   NKX_REQUIRE(!(fuse_j && P.naux == 0), NKX_ERR_ARG, "fuse_j needs a plan with an aux basis");
-  NKX_REQUIRE(V != nullptr, NKX_ERR_ARG, "V must be given");
+  // V may be NULL only when J alone is asked for (the exchange-correlation
+  // terms are then formed and dropped)
+  NKX_REQUIRE(V != nullptr || (J != nullptr && !fuse_j && P.naux > 0), NKX_ERR_ARG,
+              "V must be given unless J alone is requested from a plan with an aux basis");
   const bool separateJ = needJ && !fuse_j && J;
   cudaStream_t s = user ? user : P.stream;
   P.launches = 0;
@@ -1288,6 +1344,7 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
   }
   dim3 tb(16, 16), gb(nblk(P.nbf, 16), nblk(P.nbf, 16));
   for (int z = 0; z < nout; ++z) {
+    if (z < nspin && !V) continue;
     double *o = (z < nspin) ? dst + z * nn : (mem == NKX_MEM_DEVICE ? J : dst + nspin * nn);
     symmetrize_unpad_kernel<<<gb, tb, 0, s>>>(P.nbf, P.nbf_pad, P.d_finv, P.d_V + (size_t)z * P.nbf_pad * P.nbf_pad,
                                               o);
@@ -1295,7 +1352,7 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
   }
   NKX_LAUNCH_CHECK();
   if (mem == NKX_MEM_HOST) {
-    NKX_CUDA(cudaMemcpyAsync(V, dst, sizeof(double) * nspin * nn, cudaMemcpyDeviceToHost, s));
+    if (V) NKX_CUDA(cudaMemcpyAsync(V, dst, sizeof(double) * nspin * nn, cudaMemcpyDeviceToHost, s));
     if (separateJ) NKX_CUDA(cudaMemcpyAsync(J, dst + nspin * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
   }
   NKX_CUDA(cudaMemcpyAsync(E, P.d_E, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1389,6 +1446,140 @@ NKX_API nkx_status nkx_plan_batch_blocks(const nkx_plan *plan, int *counts) {
     NKX_REQUIRE(plan && counts, NKX_ERR_ARG, "invalid arguments");
     const Plan &P = *reinterpret_cast<const Plan *>(plan);
     for (long b = 0; b < P.nbatch; ++b) counts[b] = P.h_pair_off[b + 1] - P.h_pair_off[b];
+  });
+}
+
+NKX_API nkx_status nkx_plan_set_functional(nkx_plan *plan, int nfunc, const int *func_ids, double dens_threshold) {
+  return run_guarded("nkx_plan_set_functional", [&] {
+    NKX_REQUIRE(plan && func_ids, NKX_ERR_ARG, "invalid arguments");
+    Plan &P = *reinterpret_cast<Plan *>(plan);
+    nkx_plan_options o{};
+    o.nfunc = nfunc;
+    for (int i = 0; i < 4 && i < nfunc; ++i) o.func_ids[i] = func_ids[i];
+    o.dens_threshold = dens_threshold;
+    const XcSpec x = make_spec(&o);  // validates nfunc and the ids
+    P.xc = x;
+    P.gga = spec_is_gga(x);
+  });
+}
+
+NKX_API nkx_status nkx_plan_set_half_inverse(nkx_plan *plan, int K, const double *X, int mem) {
+  return run_guarded("nkx_plan_set_half_inverse", [&] {
+    NKX_REQUIRE(plan && X, NKX_ERR_ARG, "invalid arguments");
+    Plan &P = *reinterpret_cast<Plan *>(plan);
+    NKX_REQUIRE(P.naux > 0, NKX_ERR_ARG, "the plan has no aux basis");
+    NKX_REQUIRE(K >= 1 && K <= P.naux, NKX_ERR_ARG, "K must be in [1, naux]");
+    NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
+    const size_t NA = P.naux;
+    if (!P.d_X) P.d_X = P.alloc<double>(NA * NA);
+    if (!P.d_t) P.d_t = P.alloc<double>(NA);
+    NKX_CUDA(cudaMemcpy(P.d_X, X, sizeof(double) * NA * K,
+                        mem == NKX_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice));
+    P.K = K;
+    P.svd_mode = true;
+  });
+}
+
+NKX_API nkx_status nkx_plan_aux_metric(const nkx_plan *plan, double *S, int mem) {
+  return run_guarded("nkx_plan_aux_metric", [&] {
+    NKX_REQUIRE(plan && S, NKX_ERR_ARG, "invalid arguments");
+    const Plan &P = *reinterpret_cast<const Plan *>(plan);
+    NKX_REQUIRE(P.naux > 0, NKX_ERR_ARG, "the plan has no aux basis");
+    NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
+    const size_t bytes = sizeof(double) * P.naux * P.naux;
+    if (mem == NKX_MEM_HOST)
+      std::memcpy(S, P.h_metric.data(), bytes);
+    else
+      NKX_CUDA(cudaMemcpy(S, P.h_metric.data(), bytes, cudaMemcpyHostToDevice));
+  });
+}
+
+NKX_API nkx_status nkx_plan_density(nkx_plan *plan, int nspin, int nocc, const double *C, const double *occ, int mem,
+                                    int accumulate, double *rho, double *grad, double *sigma, void *stream) {
+  return run_guarded("nkx_plan_density", [&] {
+    NKX_REQUIRE(plan, NKX_ERR_ARG, "plan is NULL");
+    Plan &P = *reinterpret_cast<Plan *>(plan);
+    NKX_REQUIRE(nspin == 1 || nspin == 2, NKX_ERR_ARG, "nspin must be 1 or 2");
+    NKX_REQUIRE(nocc > 0 && C && occ && (rho || grad || sigma), NKX_ERR_ARG, "invalid arguments");
+    NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
+    cudaStream_t s = stream ? (cudaStream_t)stream : P.stream;
+    const size_t n = (size_t)P.npts;
+    if (!P.d_perm) {
+      P.d_perm = P.alloc<long>(n);
+      NKX_CUDA(cudaMemcpy(P.d_perm, P.perm.data(), sizeof(long) * n, cudaMemcpyHostToDevice));
+    }
+    upload_orbitals(P, nspin, nocc, C, occ, mem, s);
+    // the gradient needs the gradient collocation whatever the functional
+    const bool gga = P.gga;
+    P.gga = grad || sigma;
+    StageTimer T;
+    try {
+      fp64_density_pass(P, nspin, nocc, s, T);
+    } catch (...) {
+      P.gga = gga;
+      throw;
+    }
+    P.gga = gga;
+    // outputs: the caller's device buffers, or device staging for host ones
+    double *orho = rho, *ograd = grad, *osig = sigma;
+    if (mem == NKX_MEM_HOST) {
+      if (!P.d_dens_out) P.d_dens_out = P.alloc<double>(2 * 5 * n);
+      orho = rho ? P.d_dens_out : nullptr;
+      ograd = grad ? P.d_dens_out + 2 * n : nullptr;
+      osig = sigma ? P.d_dens_out + 8 * n : nullptr;
+      if (accumulate && rho)
+        NKX_CUDA(cudaMemcpyAsync(orho, rho, sizeof(double) * nspin * n, cudaMemcpyHostToDevice, s));
+      if (accumulate && grad)
+        NKX_CUDA(cudaMemcpyAsync(ograd, grad, sizeof(double) * 3 * nspin * n, cudaMemcpyHostToDevice, s));
+    }
+    density_out_kernel<<<dim3(nblk((long)n, 256), nspin), 256, 0, s>>>((long)n, P.npad, P.d_perm, P.d_rho, P.d_grad,
+                                                                        accumulate != 0, orho, ograd, osig);
+    NKX_LAUNCH_CHECK();
+    if (mem == NKX_MEM_HOST) {
+      if (rho) NKX_CUDA(cudaMemcpyAsync(rho, orho, sizeof(double) * nspin * n, cudaMemcpyDeviceToHost, s));
+      if (grad) NKX_CUDA(cudaMemcpyAsync(grad, ograd, sizeof(double) * 3 * nspin * n, cudaMemcpyDeviceToHost, s));
+      if (sigma) NKX_CUDA(cudaMemcpyAsync(sigma, osig, sizeof(double) * nspin * n, cudaMemcpyDeviceToHost, s));
+    }
+    NKX_CUDA(cudaStreamSynchronize(s));
+    P.last_nspin = nspin;
+  });
+}
+
+NKX_API nkx_status nkx_morton_order(long npoints, const double *xyz, long *perm) {
+  return run_guarded("nkx_morton_order", [&] {
+    NKX_REQUIRE(npoints > 0 && xyz && perm, NKX_ERR_ARG, "invalid arguments");
+    std::vector<long> p;
+    morton_order(npoints, xyz, p);
+    std::copy(p.begin(), p.end(), perm);
+  });
+}
+
+NKX_API nkx_status nkx_aux_metric(const nkx_basis *aux, long npoints, const double *d_xyz, const double *d_w,
+                                  double *d_S, void *stream) {
+  return run_guarded("nkx_aux_metric", [&] {
+    NKX_REQUIRE(aux && aux->nbf > 0 && npoints > 0 && d_xyz && d_w && d_S, NKX_ERR_ARG, "invalid arguments");
+    for (int i = 0; i < aux->nbf; ++i)
+      NKX_REQUIRE(aux->l[i] >= 0 && aux->l[i] <= 7 && aux->n[i] > aux->l[i] && abs(aux->m[i]) <= aux->l[i] &&
+                      aux->zeta[i] > 0,
+                  NKX_ERR_UNSUPPORTED, "aux function outside n > l, |m| <= l <= 7, zeta > 0");
+    cudaStream_t s = (cudaStream_t)stream;
+    const auto atab = make_aux_table(*aux);
+    const auto astab = make_sto_table(*aux);
+    auto del = [](void *q) { cudaFree(q); };
+    std::unique_ptr<void, decltype(del)> a1(dalloc<AuxFunc>(aux->nbf), del), a2(dalloc<StoFunc>(aux->nbf), del),
+        a3(dalloc<double>(3 * (size_t)npoints), del);
+    AuxFunc *d_aux = static_cast<AuxFunc *>(a1.get());
+    StoFunc *d_asto = static_cast<StoFunc *>(a2.get());
+    double *soa = static_cast<double *>(a3.get());
+    NKX_CUDA(cudaMemcpy(d_aux, atab.data(), sizeof(AuxFunc) * aux->nbf, cudaMemcpyHostToDevice));
+    NKX_CUDA(cudaMemcpy(d_asto, astab.data(), sizeof(StoFunc) * aux->nbf, cudaMemcpyHostToDevice));
+    split_points_kernel<<<nblk(npoints, 256), 256, 0, s>>>(npoints, d_xyz, soa);
+    NKX_LAUNCH_CHECK();
+    cublasHandle_t hb;
+    NKX_REQUIRE(cublasCreate(&hb) == CUBLAS_STATUS_SUCCESS, NKX_ERR_CUDA, "cublasCreate failed");
+    std::unique_ptr<cublasContext, decltype(&cublasDestroy)> hguard(hb, &cublasDestroy);
+    cublasSetStream(hb, s);
+    grid_metric(d_asto, d_aux, aux->nbf, soa, soa + npoints, soa + 2 * npoints, d_w, npoints, hb, s, d_S);
   });
 }
 

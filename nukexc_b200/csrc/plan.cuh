@@ -69,6 +69,9 @@ struct Plan {
   double *d_Ct = nullptr, *d_occ = nullptr, *d_Cin = nullptr;
   // accumulators / outputs
   double *d_V = nullptr, *d_E = nullptr, *d_out = nullptr;
+  // caller-order density outputs (nkx_plan_density)
+  long *d_perm = nullptr;
+  double *d_dens_out = nullptr;
 
   // Coulomb metric
   bool svd_mode = false;

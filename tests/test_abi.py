@@ -41,3 +41,23 @@ def test_error_path_without_gpu():
     st = L.nkx_plan_create(None, None, None, 0, None, None, None, None, None)
     assert st == 1
     assert b"plan pointer" in L.nkx_last_error()
+
+
+def test_morton_order_host_entry():
+    # nkx_morton_order runs on the host: a permutation along which the
+    # interleaved 21-bit codes over the points' bounding box never decrease
+    import numpy as np
+    from nukexc_b200 import _lib
+    rng = np.random.default_rng(5)
+    pts = rng.normal(size=(5000, 3)) * np.array([3.0, 1.0, 0.5])
+    perm = np.zeros(len(pts), np.int64)
+    _lib.check(_lib.lib().nkx_morton_order(len(pts), pts.ctypes.data_as(ctypes.c_void_p),
+                                           perm.ctypes.data_as(ctypes.c_void_p)))
+    assert np.array_equal(np.sort(perm), np.arange(len(pts)))
+    lo, hi = pts.min(0), pts.max(0)
+    q = np.minimum(2097151.0, np.maximum(0.0, (pts - lo) / (hi - lo) * 2097151.0)).astype(np.uint64)
+    code = np.zeros(len(pts), np.uint64)
+    for bit in range(21):
+        for d in range(3):
+            code |= ((q[:, d] >> np.uint64(bit)) & np.uint64(1)) << np.uint64(3 * bit + d)
+    assert np.all(np.diff(code[perm].astype(np.float64)) >= 0)
