@@ -7,7 +7,7 @@
 // (density.hpp:188-255, xc_integrals.hpp:424-726), run on one
 // warp-specialised tcgen05 kernel of kind::i8.  Every operand row r of a
 // tile is scaled by a power of two s_r >= max|row| and rounded to a 31-bit
-// integer written as four balanced base-256 digits (digits4, tc_ptx.cuh).
+// integer written as four balanced base-256 digits (digits_word, tc_ptx.cuh).
 // A contraction over K is then
 //   sum_k a_k b_k = s_a s_b 2^-60 sum_{L=0..3} 2^(8(6-L)) Acc_L,
 //   Acc_L = sum_k sum_{i+j=L} d_i(a_k) d_j(b_k)            (int32, exact)
@@ -402,17 +402,16 @@ __device__ __forceinline__ double warp_max(double v) {
   for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
-__device__ __forceinline__ uint32_t pack4(int8_t a, int8_t b, int8_t c, int8_t d) {
-  return (uint32_t)(uint8_t)a | ((uint32_t)(uint8_t)b << 8) | ((uint32_t)(uint8_t)c << 16) |
-         ((uint32_t)(uint8_t)d << 24);
-}
-// four consecutive values -> four digit planes (one packed word per plane)
+// four consecutive values -> four digit planes (one packed word per plane:
+// w[p] byte k = digit p of value k, p = 0 the leading digit)
 __device__ __forceinline__ void quant4(const double v[4], double inv, uint32_t w[4]) {
-  int8_t d[4][4];
+  const double s30 = inv * 0x1p30;
+  uint32_t b[4], t[4];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) digits4(v[k], inv, d[0][k], d[1][k], d[2][k], d[3][k]);
+  for (int k = 0; k < 4; ++k) b[k] = digits_word(v[k], s30);
+  transpose4(b, t);
 #pragma unroll
-  for (int p = 0; p < 4; ++p) w[p] = pack4(d[p][0], d[p][1], d[p][2], d[p][3]);
+  for (int p = 0; p < 4; ++p) w[p] = t[3 - p];
 }
 
 // Density operand B: orbital rows (spin, i) over each 128-function block.
@@ -621,16 +620,14 @@ __global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__
     for (int c = 0; c < NC; ++c) {
       const long pc = qrel * NC + c;
       const double sc = sphT[pc * 256 + g] * 0x1p-30;
-      uint32_t wd[4];
+      // plane words (leading digit first) -> one packed digit word per value
+      uint32_t wd[4], bw[4];
 #pragma unroll
-      for (int d = 0; d < 4; ++d) wd[d] = reinterpret_cast<const uint32_t *>(qphT + ((pc * 4 + d) * 256 + g) * 128)[lane];
+      for (int d = 0; d < 4; ++d)
+        wd[3 - d] = reinterpret_cast<const uint32_t *>(qphT + ((pc * 4 + d) * 256 + g) * 128)[lane];
+      transpose4(wd, bw);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const long long X = (long long)(int8_t)(wd[0] >> (8 * k)) * (1LL << 24) +
-                            (long long)(int8_t)(wd[1] >> (8 * k)) * (1LL << 16) +
-                            (long long)(int8_t)(wd[2] >> (8 * k)) * (1LL << 8) + (long long)(int8_t)(wd[3] >> (8 * k));
-        v[c][k] = (double)X * sc;
-      }
+      for (int k = 0; k < 4; ++k) v[c][k] = int_to_double(digits_value(bw[k])) * sc;
     }
     double z[nop][4];
 #pragma unroll
@@ -713,12 +710,11 @@ __global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ 
 #pragma unroll
       for (int o = 0; o < 4; ++o) {
         if (o >= nop) break;
-        int8_t d[4][4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) digits4(v[o][r], inv[o], d[0][r], d[1][r], d[2][r], d[3][r]);
+        uint32_t w[4];
+        quant4(v[o], inv[o], w);
         uint32_t *t = reinterpret_cast<uint32_t *>(tile + ((size_t)o * 4 * 128 + f) * 68) + gq;
 #pragma unroll
-        for (int dd = 0; dd < 4; ++dd) t[dd * 128 * 17] = pack4(d[dd][0], d[dd][1], d[dd][2], d[dd][3]);
+        for (int dd = 0; dd < 4; ++dd) t[dd * 128 * 17] = w[dd];
       }
     }
     __syncthreads();

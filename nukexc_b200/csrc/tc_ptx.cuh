@@ -161,24 +161,34 @@ __device__ __forceinline__ void tmem_wait8(uint32_t (&r)[8]) {
                : "memory");
 }
 
-// Exact integer decomposition used by the int8 tensor-core contractions:
-// x / 2^E with 2^E >= max|row| is rounded to a 31-bit integer
-// X = RN(x 2^(30-E)) and written as X = d0 2^24 + d1 2^16 + d2 2^8 + d3 with
-// balanced digits d1..d3 in [-128, 127] and d0 in [-65, 65].
-__device__ __forceinline__ void digits4(double x, double inv_scale, int8_t &d0, int8_t &d1, int8_t &d2, int8_t &d3) {
-  long long X = __double2ll_rn(x * inv_scale * 1073741824.0);
-  long long r;
-  r = ((X + 128) & 255) - 128;
-  d3 = (int8_t)r;
-  X = (X - r) >> 8;
-  r = ((X + 128) & 255) - 128;
-  d2 = (int8_t)r;
-  X = (X - r) >> 8;
-  r = ((X + 128) & 255) - 128;
-  d1 = (int8_t)r;
-  X = (X - r) >> 8;
-  d0 = (int8_t)X;
+// Digits of X = rint(x * 2^30 / s) (|X| <= 2^30, s the row's power-of-two
+// scale; s30 = 2^30 / s) as four balanced base-256 digits d0..d3,
+// X = d0 2^24 + d1 2^16 + d2 2^8 + d3 with d1..d3 in [-128, 127] and d0 in
+// [-64, 64], packed in one
+// word with byte 0 = d3 .. byte 3 = d0.  The rounding is the FP64
+// round-to-nearest-even of x s30 + 1.5 2^52, whose low word is X; the lower
+// three bytes of Y = X + 0x808080 are the digits plus 128 and its top byte is
+// d0, so the packed digits are Y ^ 0x808080.
+__device__ __forceinline__ uint32_t digits_word(double x, double s30) {
+  const int X = __double2loint(fma(x, s30, 0x1.8p52));
+  return (uint32_t)(X + 0x00808080) ^ 0x00808080u;
 }
+// X back from its packed digits
+__device__ __forceinline__ int digits_value(uint32_t w) { return (int)(w ^ 0x00808080u) - 0x00808080; }
+// exact int32 -> FP64 through the FP64 adder: the low word of 2^52 + 2^31 + X
+__device__ __forceinline__ double int_to_double(int X) {
+  return __hiloint2double(0x43300000, X ^ (int)0x80000000) - 0x1.00000800000p52;
+}
+// 4 x 4 byte transpose: t[i] byte j = a[j] byte i
+__device__ __forceinline__ void transpose4(const uint32_t a[4], uint32_t t[4]) {
+  const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), hi01 = __byte_perm(a[0], a[1], 0x7362);
+  const uint32_t lo23 = __byte_perm(a[2], a[3], 0x5140), hi23 = __byte_perm(a[2], a[3], 0x7362);
+  t[0] = __byte_perm(lo01, lo23, 0x5410);
+  t[1] = __byte_perm(lo01, lo23, 0x7632);
+  t[2] = __byte_perm(hi01, hi23, 0x5410);
+  t[3] = __byte_perm(hi01, hi23, 0x7632);
+}
+
 // power-of-two scale 2^E >= m (E from frexp; 1 for m == 0), as its inverse
 __device__ __forceinline__ double inv_pow2_scale(double m, double &scale) {
   if (!(m > 0.0)) {
