@@ -174,7 +174,8 @@ __device__ inline void load_block_funcs(BlockFuncs &B, const StoFunc *__restrict
 }
 
 // radial factors of every shell of the block at one point, shared by the
-// warp: R[s] = r^k e^(-zeta r) and, with GRAD, C[s] = (k/r - zeta)/r (0 at r = 0)
+// warp: R[s] = r^k e^(-zeta r) and, with GRAD, C[s] = (k/r - zeta)/r (0 at r = 0),
+// with one division
 template <bool GRAD>
 __device__ __forceinline__ void block_radials(const BlockFuncs &B, int lane, double x, double y, double z,
                                               double *__restrict__ R, double *__restrict__ C) {
@@ -183,7 +184,10 @@ __device__ __forceinline__ void block_radials(const BlockFuncs &B, int lane, dou
     const double r = sqrt(dx * dx + dy * dy + dz * dz);
     const int k = B.sk[s];
     R[s] = ipow(r, k) * exp(-B.szeta[s] * r);
-    if (GRAD) C[s] = r > 0.0 ? (k / r - B.szeta[s]) / r : 0.0;
+    if (GRAD) {
+      const double ri = 1.0 / r;
+      C[s] = r > 0.0 ? (k * ri - B.szeta[s]) * ri : 0.0;
+    }
   }
 }
 

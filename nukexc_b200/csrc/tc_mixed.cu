@@ -477,9 +477,10 @@ __global__ void __launch_bounds__(256) colloc_quantT_kernel(const StoFunc *__res
     block_funcs_eval4<GRAD>(B, lane, sx[g], sy[g], sz[g], wR[warp], wC[warp], v[0], v[1], v[2], v[3]);
 #pragma unroll
     for (int k = 0; k < NC; ++k) {
-      const double m = warp_max(fmax(fmax(fabs(v[k][0]), fabs(v[k][1])), fmax(fabs(v[k][2]), fabs(v[k][3]))));
+      const unsigned el = max(max(exp_field(v[k][0]), exp_field(v[k][1])), max(exp_field(v[k][2]), exp_field(v[k][3])));
       double s;
-      const double inv = inv_pow2_scale(m, s);
+      const double inv = warp_inv_pow2_scale(
+          el, fmax(fmax(fabs(v[k][0]), fabs(v[k][1])), fmax(fabs(v[k][2]), fabs(v[k][3]))), s);
       uint32_t w[4];
       quant4(v[k], inv, w);
       const long pc = qrel * NC + k;

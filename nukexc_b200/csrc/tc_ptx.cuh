@@ -201,5 +201,24 @@ __device__ __forceinline__ double inv_pow2_scale(double m, double &scale) {
   return ldexp(1.0, -e);
 }
 
+// The same scale for the largest |v| of a warp, from the biased exponents
+// alone: a normal m with exponent field E has frexp exponent E - 1022, so
+// scale = 2^(E - 1022) and its inverse are built from their bits.  Each lane
+// passes the largest exponent field of its values; all-zero or subnormal
+// (E = 0) and huge (E >= 2045) rows take the general path through `m`.
+__device__ __forceinline__ double warp_inv_pow2_scale(unsigned e_lane, double m_lane, double &scale) {
+  const unsigned e = __reduce_max_sync(0xffffffffu, e_lane);
+  if (e == 0u || e >= 2045u) {
+    double m = m_lane;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    return inv_pow2_scale(m, scale);
+  }
+  scale = __hiloint2double((int)((e + 1u) << 20), 0);
+  return __hiloint2double((int)((2045u - e) << 20), 0);
+}
+// exponent field of x (sign ignored)
+__device__ __forceinline__ unsigned exp_field(double x) { return ((unsigned)__double2hiint(x) >> 20) & 0x7ffu; }
+
 }  // namespace tc
 }  // namespace nkx
