@@ -74,7 +74,8 @@ std::vector<AuxFunc> make_aux_table(const nkx_basis &b) {
     f.a = n + l + 2;
     f.b = n - l + 1;
     f.ga_full = fact_d(f.a - 1) / std::pow(f.zeta, f.a);
-    f.zb = 1.0 / std::pow(f.zeta, f.b);
+    f.za = 1.0 / std::pow(f.zeta, f.a);
+    f.ub = fact_d(f.b - 1) / std::pow(f.zeta, f.b);
     f.l = l;
     f.m = b.m[i];
     // smallest x with e^-x x^(a-1)/(a-1)! < 1e-18 beyond the peak at a-1

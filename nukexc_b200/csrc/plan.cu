@@ -520,13 +520,14 @@ __global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const Au
     if (wr == 0.0) continue;
     const double dx = px[g] - G.cx, dy = py[g] - G.cy, dz = pz[g] - G.cz;
     const double rr = sqrt(dx * dx + dy * dy + dz * dz);
+    const double r2l1inv = rr < 1e-12 ? 0.0 : ipow_c<2 * L + 1>(1.0 / rr);
     double S[NM];
     solid_harmonics_all<L>(dx, dy, dz, S);
 #pragma unroll
     for (int q = 0; q < QM; ++q) {
       if (q >= G.n) break;
       const AuxFunc &f = shells[G.first + q].f;
-      const double wI = wr * aux_radial(f, rr);
+      const double wI = wr * aux_radial_r(f, rr, r2l1inv);
 #pragma unroll
       for (int m = 0; m < NM; ++m) acc[q][m] += wI * (f.C * S[m]);
     }
@@ -557,6 +558,7 @@ __device__ __forceinline__ double aux_group_v(const AuxGroup &G, const AuxShell 
   constexpr int NM = 2 * L + 1;
   const double dx = x - G.cx, dy = y - G.cy, dz = z - G.cz;
   const double rr = sqrt(dx * dx + dy * dy + dz * dz);
+  const double r2l1inv = rr < 1e-12 ? 0.0 : ipow_c<2 * L + 1>(1.0 / rr);
   double S[NM];
   solid_harmonics_all<L>(dx, dy, dz, S);
   double s = 0.0;
@@ -565,14 +567,14 @@ __device__ __forceinline__ double aux_group_v(const AuxGroup &G, const AuxShell 
     double a = 0.0;
 #pragma unroll
     for (int m = 0; m < NM; ++m) a += c[sh.first + m] * (sh.f.C * S[m]);
-    if (a != 0.0) s += a * aux_radial(sh.f, rr);
+    if (a != 0.0) s += a * aux_radial_r(sh.f, rr, r2l1inv);
   }
   return s;
 }
 
 // v_g = w_g sum_a c_a V_a(g) over the groups, then the loose shells
 // (coulomb.hpp:90-95)
-__global__ void aux_v_group_kernel(const AuxGroup *__restrict__ groups, int ngroup,
+__global__ void aux_v_group_kernel(const AuxGroup *__restrict__ groups, int4 goff,
                                    const AuxShell *__restrict__ shells, const int *__restrict__ loose, int nloose,
                                    const double *__restrict__ c, const double *__restrict__ px,
                                    const double *__restrict__ py, const double *__restrict__ pz,
@@ -585,15 +587,11 @@ __global__ void aux_v_group_kernel(const AuxGroup *__restrict__ groups, int ngro
   }
   const double x = px[g], y = py[g], z = pz[g];
   double s = 0.0;
-  for (int k = 0; k < ngroup; ++k) {
-    const AuxGroup G = groups[k];
-    switch (G.l) {
-      case 0: s += aux_group_v<0>(G, shells, c, x, y, z); break;
-      case 1: s += aux_group_v<1>(G, shells, c, x, y, z); break;
-      case 2: s += aux_group_v<2>(G, shells, c, x, y, z); break;
-      default: s += aux_group_v<3>(G, shells, c, x, y, z); break;
-    }
-  }
+  // groups sorted by l: [0, goff.x) l = 0, [goff.x, goff.y) l = 1, ...
+  for (int k = 0; k < goff.x; ++k) s += aux_group_v<0>(groups[k], shells, c, x, y, z);
+  for (int k = goff.x; k < goff.y; ++k) s += aux_group_v<1>(groups[k], shells, c, x, y, z);
+  for (int k = goff.y; k < goff.z; ++k) s += aux_group_v<2>(groups[k], shells, c, x, y, z);
+  for (int k = goff.z; k < goff.w; ++k) s += aux_group_v<3>(groups[k], shells, c, x, y, z);
   for (int k = 0; k < nloose; ++k) {
     const AuxShell &sh = shells[loose[k]];
     const AuxFunc &f = sh.f;
@@ -1198,7 +1196,8 @@ void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
       NKX_LAUNCH_CHECK();
       P.launches += 2;
     }
-    aux_v_group_kernel<<<nblk(P.npad, 128), 128, 0, s>>>(P.d_agroup, P.nagroup, P.d_ashell, P.d_loose, P.nloose,
+    const int4 goff = make_int4(P.h_group_off[1], P.h_group_off[2], P.h_group_off[3], P.h_group_off[4]);
+    aux_v_group_kernel<<<nblk(P.npad, 128), 128, 0, s>>>(P.d_agroup, goff, P.d_ashell, P.d_loose, P.nloose,
                                                          P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, P.d_vj);
     NKX_LAUNCH_CHECK();
     ++P.launches;

@@ -18,7 +18,8 @@ struct AuxFunc {
   double zeta;
   double C;        // 4 pi N / (2l+1)
   double ga_full;  // (a-1)! / zeta^a, a = n+l+2  (the r -> infinity limit of gamma(a,.)/zeta^a)
-  double zb;       // 1 / zeta^b, b = n-l+1
+  double za;       // 1 / zeta^a
+  double ub;       // (b-1)! / zeta^b, b = n-l+1 (the r -> 0 limit of Gamma(b,.)/zeta^b)
   double xfar;     // far-field switch on zeta r
   int a, b, l, m;
 };
@@ -55,18 +56,27 @@ NKX_HD inline double inv_int(int k) {
 // x^a e^-x sum_k x^k / (a (a+1) ... (a+k)) for x < a/2 (ratio below 1/2, so
 // a few tens of terms) or as (a-1)! - Gamma(a, x) above, where
 // P(a, x) >= P(a, a/2) keeps the subtraction's relative error near 1e-15.
-NKX_HD inline double aux_radial(const AuxFunc &f, double r) {
-  if (r < 1e-12) return fact_d(f.b - 1) * f.zb;
+// x^N for a compile-time N
+template <int N>
+NKX_HD inline double ipow_c(double x) {
+  double v = 1.0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) v *= x;
+  return v;
+}
+
+// with r^-(2l+1) given, so the shells of one (centre, l) group share it
+NKX_HD inline double aux_radial_r(const AuxFunc &f, double r, double r2l1inv) {
+  if (r < 1e-12) return f.ub;
   const double x = f.zeta * r;
-  const double r2l1 = ipow(r, 2 * f.l + 1);
-  if (x > f.xfar) return f.ga_full / r2l1;
+  if (x > f.xfar) return f.ga_full * r2l1inv;
   const double ex = exp(-x);
   double su = 1.0, t = 1.0;
   for (int k = 1; k < f.b; ++k) {
     t *= x * inv_int(k);
     su += t;
   }
-  const double upper = fact_d(f.b - 1) * ex * su;
+  const double upper = f.ub * ex * su;
   double lower;
   const int a = f.a;
   if (2.0 * x < a) {
@@ -76,16 +86,20 @@ NKX_HD inline double aux_radial(const AuxFunc &f, double r) {
       sum += term;
       if (term < 1e-17 * sum) break;
     }
-    lower = ipow(x, a) * ex * sum;
+    lower = ipow(x, a) * ex * sum * f.za;
   } else {
     double sl = 1.0, tl = 1.0;
     for (int k = 1; k < a; ++k) {
       tl *= x * (k <= 64 ? inv_int(k) : 1.0 / k);
       sl += tl;
     }
-    lower = fact_d(a - 1) * (1.0 - ex * sl);
+    lower = f.ga_full * (1.0 - ex * sl);
   }
-  return lower * (f.ga_full / fact_d(a - 1)) / r2l1 + upper * f.zb;
+  return lower * r2l1inv + upper;
+}
+
+NKX_HD inline double aux_radial(const AuxFunc &f, double r) {
+  return aux_radial_r(f, r, r < 1e-12 ? 0.0 : 1.0 / ipow(r, 2 * f.l + 1));
 }
 
 NKX_HD inline double aux_potential(const AuxFunc &f, double px, double py, double pz) {
