@@ -173,21 +173,46 @@ __device__ inline void load_block_funcs(BlockFuncs &B, const StoFunc *__restrict
   if (tid == 0) B.nshell = bnshell[I];
 }
 
+// e^x for -700 <= x <= 0 (0 below) to about 1e-14 relative, for the
+// mixed-precision collocation, whose values are rounded to 31 bits anyway:
+// Cody-Waite reduction x = n ln2 + t, |t| <= ln2 / 2, with ln 2 split into
+// a double and its remainder (the FMAs form x - n ln2 without cancellation
+// error), e^t by its Taylor polynomial of degree 11 (truncation below
+// (ln2/2)^12 / 12! < 1e-14) and 2^n from the exponent bits.
+__device__ __forceinline__ double exp_neg(double x) {
+  if (x < -700.0) return 0.0;
+  const double n = rint(x * 1.4426950408889634);
+  double t = fma(-n, 0x1.62e42fefa39efp-1, x);
+  t = fma(-n, 0x1.abc9e3b39803fp-56, t);
+  double p = 0x1.ae64567f544e4p-26;  // 1/11!
+  p = fma(p, t, 0x1.27e4fb7789f5cp-22);
+  p = fma(p, t, 0x1.71de3a556c734p-19);
+  p = fma(p, t, 0x1.a01a01a01a01ap-16);
+  p = fma(p, t, 0x1.a01a01a01a01ap-13);
+  p = fma(p, t, 0x1.6c16c16c16c17p-10);
+  p = fma(p, t, 0x1.1111111111111p-7);
+  p = fma(p, t, 0x1.5555555555555p-5);
+  p = fma(p, t, 0x1.5555555555555p-3);
+  p = fma(p, t, 0.5);
+  p = fma(p, t, 1.0);
+  p = fma(p, t, 1.0);
+  return p * __hiloint2double(((int)n + 1023) << 20, 0);
+}
+
 // radial factors of every shell of the block at one point, shared by the
 // warp: R[s] = r^k e^(-zeta r) and, with GRAD, C[s] = (k/r - zeta)/r (0 at r = 0),
-// with one division
+// from 1/r = rsqrt(r^2) (1 ulp) and exp_neg
 template <bool GRAD>
 __device__ __forceinline__ void block_radials(const BlockFuncs &B, int lane, double x, double y, double z,
                                               double *__restrict__ R, double *__restrict__ C) {
   for (int s = lane; s < B.nshell; s += 32) {
     const double dx = x - B.scx[s], dy = y - B.scy[s], dz = z - B.scz[s];
-    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const double ri = r2 > 0.0 ? rsqrt(r2) : 0.0;
+    const double r = r2 * ri;
     const int k = B.sk[s];
-    R[s] = ipow(r, k) * exp(-B.szeta[s] * r);
-    if (GRAD) {
-      const double ri = 1.0 / r;
-      C[s] = r > 0.0 ? (k * ri - B.szeta[s]) * ri : 0.0;
-    }
+    R[s] = ipow(r, k) * exp_neg(-B.szeta[s] * r);
+    if (GRAD) C[s] = (k * ri - B.szeta[s]) * ri;
   }
 }
 
