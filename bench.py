@@ -463,7 +463,8 @@ def run_nkx(args):
     def step(host=False):
         if host:
             E, V, _ = fb.build([Cm], [occ], precision=prec, fuse_j=fuse, stream=stream.cuda_stream)
-            V = torch.as_tensor(V[0], device="cuda")
+            # the all-reduce of several ranks needs V back on the device
+            V = torch.as_tensor(V[0], device="cuda") if dist is not None else V[0]
         else:
             E, V, _ = fb.build([Cd], [od], precision=prec, fuse_j=fuse, stream=stream.cuda_stream)
             V = V[0]

@@ -355,8 +355,8 @@ class FockBuilder:
         if host:
             Cc = np.concatenate([np.ascontiguousarray(np.asarray(c, np.float64).T).reshape(-1) for c in C_list])
             oc = np.concatenate([_np(o, np.float64) for o in occ_list])
-            V = np.zeros(nspin * nn) if want_V else None
-            J = np.zeros(nn) if want_J and not fuse_j else None
+            V = np.empty(nspin * nn) if want_V else None
+            J = np.empty(nn) if want_J and not fuse_j else None
             pC, po, pV, pJ = (a.ctypes.data_as(C.c_void_p) if a is not None else None for a in (Cc, oc, V, J))
         else:
             Cc = torch.cat([c.t().contiguous().reshape(-1) for c in C_list])
