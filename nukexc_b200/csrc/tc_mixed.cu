@@ -44,7 +44,9 @@ using namespace tc;
 constexpr int kABytes = 4 * 128 * 64;  // four digit planes, 128 rows x 64 B
 constexpr double kTwoM36 = 0x1p-36;
 
-enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1 };
+// TC_MODE_GRAD: Y(g, mu) = sum_i T0(g, i) (C occ)(mu, i) over the orbitals
+// (grad rho = 2 sum_mu grad phi_mu Y_mu, ygrad_kernel)
+enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1, TC_MODE_GRAD = 2 };
 
 // Shape per mode.  V: N = 128 (one TMEM buffer of 4 levels x 128 columns,
 // 16 epilogue warps, 3 stages of 64 KB).  Density: N = 64 (two buffers of
@@ -75,9 +77,14 @@ struct TcArgs {
   int nz, nbf_pad, nsplit;
   const double *sA, *sB;  // row scales: V: sph[q][128], sz[q*nz+z][128]
   double *V;
-  // density mode: sA = sphT[q][nc][256], sB = sct[s][i][blk]
-  int nspin, ncomp, ntile_i, nocc_pad;
+  // density mode: sA = sphT[q][ncs][256], sB = sct[s][i][blk]; ncomp
+  // components are contracted, ncs are stored per pair in qphT / sphT
+  int nspin, ncomp, ncs, ntile_i, nocc_pad;
   double *T;
+  // grad mode: sA = st0[(bl, s, h)][128] (T0 row scales), sB = sco[s][mu]
+  // (C occ row scales); output Y[pair][spin][g][mu] (FP64)
+  const int *pair_batch;
+  double *Y;
   long nunits;
   int *err;
 };
@@ -85,6 +92,7 @@ struct TcArgs {
 struct UnitIter {
   int I = 0, J = 0, zi = 0, sp = 0;  // V: row block, column block, Z plane, batch split
   long bl = 0;                     // density: batch within chunk
+  long q = 0;                      // grad: chunk-relative pair
   int h = 0, c = 0, s = 0, t = 0;  // density: point half, comp, spin, 128-orbital tile
   __device__ UnitIter(const TcArgs &a, long u) {
     if (a.mode == TC_MODE_V) {
@@ -94,6 +102,12 @@ struct UnitIter {
       zi = (int)(u / n2);
       I = (int)((u % n2) / a.nblk);
       J = (int)(u % a.nblk);
+    } else if (a.mode == TC_MODE_GRAD) {
+      t = (int)(u % 2);  // 64-function half of the block
+      h = (int)((u / 2) % 2);
+      s = (int)((u / 4) % a.nspin);
+      q = u / (4 * a.nspin);
+      bl = a.pair_batch[a.p0 + q] - a.b0;
     } else {
       long r = u;
       t = (int)(r % a.ntile_i);
@@ -147,6 +161,23 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
         zB = zb;
       });
     }
+  } else if (a.mode == TC_MODE_GRAD) {
+    // one run over all orbitals: A = T0 digits of (batch, spin, half),
+    // B = (C occ) digits of the pair's block
+    Group g;
+    g.nsteps = a.nocc_pad / 64;
+    g.qa = it.q;
+    g.qb = 0;
+    g.blk = a.pair_blk[a.p0 + it.q];
+    const int za = (int)(((it.bl * a.nspin + it.s) * 2 + it.h) * 4), yb = 128 * g.blk + 64 * it.t, zb = it.s * 4;
+    fn(g, [=](int k, int &xa, int &ya, int &zA, int &xb, int &yB, int &zB) {
+      xa = 64 * k;
+      ya = 0;
+      zA = za;
+      xb = 64 * k;
+      yB = yb;
+      zB = zb;
+    });
   } else {
     const long b = a.b0 + it.bl;
     const int q0 = a.pair_off[b], q1 = a.pair_off[b + 1];
@@ -156,7 +187,7 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
       g.qa = q - a.p0;
       g.qb = 0;
       g.blk = a.pair_blk[q];
-      const int za = (int)((g.qa * a.ncomp + it.c) * 4), ya = 128 * it.h;
+      const int za = (int)((g.qa * a.ncs + it.c) * 4), ya = 128 * it.h;
       const int xb0 = g.blk * 128, yb = TcShape<TC_MODE_DENSITY>::N * it.t, zb = it.s * 4;
       fn(g, [=](int k, int &xa, int &yA, int &zA, int &xb, int &yB, int &zB) {
         xa = 64 * k;
@@ -315,8 +346,11 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
           if (a.mode == TC_MODE_V) {
             sa = a.sA[g.qa * 128 + row] * kTwoM36;
             sb = a.sB + (g.qb * a.nz + it.zi) * 128 + 32 * cq;
+          } else if (a.mode == TC_MODE_GRAD) {
+            sa = a.sA[((it.bl * a.nspin + it.s) * 2 + it.h) * 128 + row] * kTwoM36;
+            sb = a.sB + (size_t)it.s * a.nbf_pad + 128 * g.blk + 64 * it.t + 32 * cq;
           } else {
-            sa = a.sA[(g.qa * a.ncomp + it.c) * 256 + 128 * it.h + row] * kTwoM36;
+            sa = a.sA[(g.qa * a.ncs + it.c) * 256 + 128 * it.h + row] * kTwoM36;
             sb = a.sB + ((size_t)it.s * a.nocc_pad + N * it.t + 32 * cq) * a.nblk + g.blk;
             sbs = a.nblk;
           }
@@ -352,7 +386,16 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
             tmem_wait4(v2);
             tmem_wait4(v3);
           }
-          if (live) {
+          if constexpr (MODE == TC_MODE_GRAD) {
+            // Y(g, mu) of the slice's SL functions
+            double *Yp = a.Y + ((it.q * a.nspin + it.s) * 256 + 128 * it.h + row) * 128 + 64 * it.t + 32 * cq + SL * hh;
+#pragma unroll
+            for (int j = 0; j < SL; ++j) {
+              const long long S = (long long)(int)v0[j] * (1LL << 24) + (long long)(int)v1[j] * (1LL << 16) +
+                                  (long long)(int)v2[j] * (1LL << 8) + (long long)(int)v3[j];
+              Yp[j] = (double)S * (sa * __shfl_sync(0xffffffffu, sbl, SL * hh + j));
+            }
+          } else if (live) {
 #pragma unroll
             for (int j = 0; j < SL; ++j) {
               const long long S = (long long)(int)v0[j] * (1LL << 24) + (long long)(int)v1[j] * (1LL << 16) +
@@ -378,6 +421,8 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
             for (int j = 0; j < 32; ++j) Vz[r + ((size_t)it.J * 128 + 32 * cq + j) * a.nbf_pad] += acc[j];
           }
         }
+      } else if (a.mode == TC_MODE_GRAD) {
+        // Y is written slice by slice above
       } else {
         const long plane = (it.bl * a.nspin + it.s) * a.ncomp + it.c;
         double *Tp = a.T + plane * (long)a.nocc_pad * 256 + 128 * it.h + row;
@@ -437,6 +482,110 @@ __global__ void quant_ct_kernel(const double *__restrict__ Ct, int nocc, int noc
   for (int p = 0; p < 4; ++p)
     *reinterpret_cast<uint32_t *>(q + (((size_t)s * 4 + p) * nocc_pad + i) * nbf_pad + f0) = w[p];
   if (lane == 0) sc[((size_t)s * nocc_pad + i) * nblk + blk] = scl;
+}
+
+// 128 operand rows r with K values each, x(r, k) = src[k * kstride + r]
+// (times kmul[k] when given; k >= K read as 0), into four digit planes
+// out[d][r][k] (row stride Kpad bytes, plane stride plane_stride) with one
+// power-of-two scale per row over all K, scale_out[r].  One thread per row;
+// 64 values at a time go through a shared tile so the rows leave as 64-byte
+// segments.
+__device__ __forceinline__ void quant_rows_128(const double *__restrict__ src, long kstride,
+                                               const double *__restrict__ kmul, int K, int Kpad,
+                                               uint8_t *__restrict__ out, size_t plane_stride,
+                                               double *__restrict__ scale_out) {
+  __shared__ uint32_t tile[4][128][17];
+  const int r = threadIdx.x;
+  double m = 0.0;
+  for (int k = 0; k < K; ++k) m = fmax(m, fabs(src[(size_t)k * kstride + r] * (kmul ? kmul[k] : 1.0)));
+  double sc;
+  const double s30 = inv_pow2_scale(m, sc) * 0x1p30;
+  scale_out[r] = sc;
+  for (int k0 = 0; k0 < Kpad; k0 += 64) {
+#pragma unroll 4
+    for (int w = 0; w < 16; ++w) {
+      uint32_t b[4], t[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = k0 + 4 * w + j;
+        const double v = k < K ? src[(size_t)k * kstride + r] * (kmul ? kmul[k] : 1.0) : 0.0;
+        b[j] = digits_word(v, s30);
+      }
+      transpose4(b, t);
+#pragma unroll
+      for (int d = 0; d < 4; ++d) tile[d][r][w] = t[3 - d];
+    }
+    __syncthreads();
+    for (int e = r; e < 4 * 128 * 16; e += 128) {
+      const int d = e >> 11, rr = (e >> 4) & 127, w = e & 15;
+      *reinterpret_cast<uint32_t *>(out + d * plane_stride + (size_t)rr * Kpad + k0 + 4 * w) = tile[d][rr][w];
+    }
+    __syncthreads();
+  }
+}
+
+// Grad-mode operand A: T0(g, i) of every (batch, spin, half) of the chunk as
+// rows g over the orbitals, qt0[(bl, s, h)][digit][g][i], st0[(bl, s, h)][g].
+__global__ void __launch_bounds__(128) quant_t0_kernel(const double *__restrict__ T, int nocc, int nocc_pad,
+                                                        uint8_t *__restrict__ q, double *__restrict__ sc) {
+  const long base = blockIdx.x;  // ((bl * nspin + s) * 2 + h)
+  const long plane = base >> 1;
+  const int h = (int)(base & 1);
+  quant_rows_128(T + plane * (long)nocc_pad * 256 + 128 * h, 256, nullptr, nocc, nocc_pad,
+                 q + base * 4 * 128 * (size_t)nocc_pad, (size_t)128 * nocc_pad, sc + base * 128);
+}
+
+// Grad-mode operand B: (C occ)(mu, i) as rows mu over the orbitals,
+// qco[s][digit][mu][i], sco[s][mu]; block y = spin, x = 128-function block.
+__global__ void __launch_bounds__(128) quant_cocc_kernel(const double *__restrict__ Ct, const double *__restrict__ occ,
+                                                          int nocc, int nocc_pad, int nbf_pad,
+                                                          uint8_t *__restrict__ q, double *__restrict__ sc) {
+  const int s = blockIdx.y, I = blockIdx.x;
+  quant_rows_128(Ct + (size_t)s * nocc * nbf_pad + 128 * I, nbf_pad, occ + (size_t)s * nocc, nocc, nocc_pad,
+                 q + ((size_t)s * 4 * nbf_pad + 128 * I) * nocc_pad, (size_t)nbf_pad * nocc_pad,
+                 sc + (size_t)s * nbf_pad + 128 * I);
+}
+
+// grad rho(g) = 2 sum_mu grad phi(g, mu) Y(g, mu) for the points of one
+// batch (block x of the chunk) and spin (block y), summed over the batch's
+// pairs; grad phi comes back from the pass-A digits (components 1..3).  Warp
+// w takes the points w + 8k, lane l the functions 4l .. 4l+3 of each block.
+__global__ void __launch_bounds__(256) ygrad_kernel(const double *__restrict__ Y, const uint8_t *__restrict__ qphT,
+                                                    const double *__restrict__ sphT,
+                                                    const int *__restrict__ pair_off, long b0, long p0, int nspin,
+                                                    long npad, double *__restrict__ grad) {
+  const long b = b0 + blockIdx.x;
+  const int s = blockIdx.y;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int q0 = pair_off[b], q1 = pair_off[b + 1];
+  for (int g = warp; g < kBatch; g += 8) {
+    double gs[3] = {0.0, 0.0, 0.0};
+    for (int q = q0; q < q1; ++q) {
+      const long qr = q - p0;
+      const double2 *yp = reinterpret_cast<const double2 *>(Y + ((qr * nspin + s) * 256 + g) * 128 + 4 * lane);
+      const double2 ya = yp[0], yb = yp[1];
+      const double y[4] = {ya.x, ya.y, yb.x, yb.y};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const long pc = qr * 4 + 1 + c;
+        uint32_t wd[4], bw[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d)
+          wd[3 - d] = reinterpret_cast<const uint32_t *>(qphT + ((pc * 4 + d) * 256 + g) * 128)[lane];
+        transpose4(wd, bw);
+        const double sc = sphT[pc * 256 + g] * 0x1p-30;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) gs[c] = fma(int_to_double(digits_value(bw[k])) * sc, y[k], gs[c]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double v = gs[c];
+#pragma unroll
+      for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) grad[((size_t)s * 3 + c) * npad + b * kBatch + g] = 2.0 * v;
+    }
+  }
 }
 
 // Pass A, fused: collocation of one (batch, block) pair straight into the
@@ -803,8 +952,11 @@ struct MixedState {
   int nocc_pad = 0, nbatch_chunk = 0, nsm = 148;
   uint8_t *qphT = nullptr, *qph = nullptr, *qz = nullptr, *qct = nullptr;
   double *sphT = nullptr, *sph = nullptr, *sz = nullptr, *sct = nullptr, *T = nullptr;
+  // grad mode: T0 and (C occ) digits with their row scales
+  uint8_t *qt0 = nullptr, *qco = nullptr;
+  double *st0 = nullptr, *sco = nullptr;
   int *err = nullptr;
-  CUtensorMap m_phT, m_ph, m_z, m_ct;
+  CUtensorMap m_phT, m_ph, m_z, m_ct, m_t0, m_co;
   std::vector<void *> bufs;
   ~MixedState() {
     for (void *p : bufs) cudaFree(p);
@@ -855,6 +1007,8 @@ static MixedState &mixed_state(Plan &P, int nocc) {
                                   TcShape<TC_MODE_V>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   TcShape<TC_MODE_DENSITY>::kSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TcShape<TC_MODE_GRAD>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(zquant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 68));
   }
   MixedState &M = *static_cast<MixedState *>(P.mx_state);
@@ -866,6 +1020,12 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     M.sct = M.alloc<double>((size_t)2 * nocc_pad * P.nblk);
     M.T = M.alloc<double>((size_t)M.nbatch_chunk * 2 * 4 * nocc_pad * 256);
     M.m_ct = make_map3(M.qct, P.nbf_pad, nocc_pad, 8, TcShape<TC_MODE_DENSITY>::N);
+    M.qt0 = M.alloc<uint8_t>((size_t)M.nbatch_chunk * 2 * 2 * 4 * 128 * nocc_pad);
+    M.st0 = M.alloc<double>((size_t)M.nbatch_chunk * 2 * 2 * 128);
+    M.qco = M.alloc<uint8_t>((size_t)2 * 4 * P.nbf_pad * nocc_pad);
+    M.sco = M.alloc<double>((size_t)2 * P.nbf_pad);
+    M.m_t0 = make_map3(M.qt0, nocc_pad, 128, (long)M.nbatch_chunk * 2 * 2 * 4, 128);
+    M.m_co = make_map3(M.qco, nocc_pad, P.nbf_pad, 2 * 4, TcShape<TC_MODE_GRAD>::N);
   }
   return M;
 }
@@ -875,6 +1035,9 @@ static void launch_i8(MixedState &M, const CUtensorMap &mA, const CUtensorMap &m
   const unsigned grid = (unsigned)std::min<long>(a.nunits, M.nsm);
   if (a.mode == TC_MODE_V)
     tc_i8_kernel<TC_MODE_V><<<grid, TcShape<TC_MODE_V>::kThreads, TcShape<TC_MODE_V>::kSmem, s>>>(mA, mB, a);
+  else if (a.mode == TC_MODE_GRAD)
+    tc_i8_kernel<TC_MODE_GRAD><<<grid, TcShape<TC_MODE_GRAD>::kThreads, TcShape<TC_MODE_GRAD>::kSmem, s>>>(mA, mB,
+                                                                                                          a);
   else
     tc_i8_kernel<TC_MODE_DENSITY><<<grid, TcShape<TC_MODE_DENSITY>::kThreads, TcShape<TC_MODE_DENSITY>::kSmem, s>>>(
         mA, mB, a);
@@ -919,6 +1082,19 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     NKX_LAUNCH_CHECK();
     ++P.launches;
   }
+  // GGA density gradient through Y = T0 (C occ)^T: grad rho = 2 sum_mu
+  // grad phi_mu Y_mu needs one orbital contraction (T0) and one more over
+  // the orbitals (Y) instead of the three gradient components of T.  It pays
+  // from about 256 orbitals on ((H2O)64, 320 orbitals: 226 vs 232 ms; the
+  // 1500-atom aggregate, 2850: 13.4 vs 24.8 s); with fewer the per-pair Y
+  // traffic dominates.  Above 8192 orbitals the int32 levels could overflow.
+  const bool grad_mode = P.gga && M.nocc_pad >= 256 && M.nocc_pad <= 8192;
+  if (grad_mode) {
+    quant_cocc_kernel<<<dim3((unsigned)P.nblk, nspin), 128, 0, s>>>(P.d_Ct, P.d_occ, nocc, M.nocc_pad, P.nbf_pad,
+                                                                    M.qco, M.sco);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+  }
   // pass A of one chunk: collocation -> digits, int8 density contraction,
   // FP64 rho / grad rho of the chunk's batches
   auto pass_a = [&](const Chunk &c) {
@@ -949,15 +1125,16 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.sA = M.sphT;
     a.sB = M.sct;
     a.nspin = nspin;
-    a.ncomp = nc;
+    a.ncs = nc;
+    a.ncomp = grad_mode ? 1 : nc;
     a.ntile_i = M.nocc_pad / TcShape<TC_MODE_DENSITY>::N;
     a.nocc_pad = M.nocc_pad;
     a.T = M.T;
     a.err = M.err;
-    a.nunits = nb * nspin * 2 * nc * a.ntile_i;
+    a.nunits = nb * nspin * 2 * a.ncomp * a.ntile_i;
     launch_i8(M, M.m_phT, M.m_ct, a, s);
     ++P.launches;
-    if (P.gga)
+    if (P.gga && !grad_mode)
       density_contract_kernel<true><<<dim3((unsigned)nb, nspin), 256, 0, s>>>(M.T, P.d_occ, nocc, M.nocc_pad, nspin,
                                                                               c.b0, P.d_rho, P.d_grad, P.npad);
     else
@@ -965,6 +1142,34 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
                                                                                c.b0, P.d_rho, P.d_grad, P.npad);
     NKX_LAUNCH_CHECK();
     ++P.launches;
+    if (grad_mode && np > 0) {
+      quant_t0_kernel<<<(unsigned)(nb * nspin * 2), 128, 0, s>>>(M.T, nocc, M.nocc_pad, M.qt0, M.st0);
+      NKX_LAUNCH_CHECK();
+      ++P.launches;
+      TcArgs g{};
+      g.mode = TC_MODE_GRAD;
+      g.b0 = c.b0;
+      g.b1 = c.b1;
+      g.p0 = c.p0;
+      g.pair_blk = P.d_pair_blk;
+      g.pair_batch = P.d_pair_batch;
+      g.nblk = P.nblk;
+      g.nbf_pad = P.nbf_pad;
+      g.sA = M.st0;
+      g.sB = M.sco;
+      g.nspin = nspin;
+      g.ncs = nc;
+      g.nocc_pad = M.nocc_pad;
+      g.Y = P.ws_phi;  // free during pass A: the FP64 staging of pass B
+      g.err = M.err;
+      g.nunits = np * nspin * 4;
+      launch_i8(M, M.m_t0, M.m_co, g, s);
+      ++P.launches;
+      ygrad_kernel<<<dim3((unsigned)nb, nspin), 256, 0, s>>>(P.ws_phi, M.qphT, M.sphT, P.d_pair_off, c.b0, c.p0,
+                                                            nspin, P.npad, P.d_grad);
+      NKX_LAUNCH_CHECK();
+      ++P.launches;
+    }
     Tm.end(s);
   };
   // pass B of one chunk after its Phi / Z staging is written: digits, int8 V

@@ -86,3 +86,26 @@ def test_mixed_fused_coulomb_vs_fp64():
     assert np.abs(Jm - J64).max() < 1e-6 * np.abs(J64).max()
     Ef, Vf, _ = fb.build([Cm], [occ], precision="mixed", fuse_j=True)
     assert np.abs(Vf[0] - (V64[0] + J64)).max() < 1e-6 * np.abs(J64).max()
+
+
+def test_mixed_gga_many_orbitals_gradient_path():
+    # 264 and 260 occupied orbitals (padded to 320): the GGA density gradient
+    # goes through Y = T0 (C occ)^T and the grad phi contraction
+    c, Z, funcs, g = case(6, seed=7, nrad=30, order=11)
+    b = A.make_manual_basis(funcs)
+    nbf = len(funcs)
+    assert nbf >= 264
+    C1 = M.random_orbitals(nbf, 264, seed=8)
+    fb = A.FockBuilder(c, Z, b, g)
+    occ = np.linspace(1.0, 0.3, 264)
+    E64, V64, _ = fb.build([C1], [occ], precision="fp64")
+    Em, Vm, _ = fb.build([C1], [occ], precision="mixed")
+    assert abs(Em - E64) < E_TOL
+    assert np.abs(Vm[0] - V64[0]).max() < V_TOL
+    Cb = np.concatenate([M.random_orbitals(nbf, 260, seed=9), np.zeros((nbf, 4))], 1)
+    occ2 = [np.ones(264), np.r_[np.ones(260), np.zeros(4)]]
+    E64, V64, _ = fb.build([C1, Cb], occ2, precision="fp64")
+    Em, Vm, _ = fb.build([C1, Cb], occ2, precision="mixed")
+    assert abs(Em - E64) < E_TOL
+    for s in range(2):
+        assert np.abs(Vm[s] - V64[s]).max() < V_TOL
