@@ -1,10 +1,12 @@
 // Mixed-precision Fock build on the 5th-generation tensor cores (sm_100a):
 // error-free int8 digit contractions with exact int32 accumulation.
 //
-// Both dense contractions of the Fock build,
+// The dense contractions of the Fock build,
 //   density  T_c(g, i) = sum_f PhiT_c(g, f) Ct(i, f)      c = value, d/dx, d/dy, d/dz
 //   V        Vbar(mu, nu) += sum_g Phi(mu, g) Z(nu, g)    per (batch, block) pair
-// (density.hpp:188-255, xc_integrals.hpp:424-726), run on one
+// (density.hpp:188-255, xc_integrals.hpp:424-726) and, for GGA from 256
+// orbitals on, Y(g, mu) = sum_i T_0(g, i) C(mu, i) occ_i in place of the three
+// gradient components of T (grad rho = 2 sum_mu grad phi_mu Y_mu), run on one
 // warp-specialised tcgen05 kernel of kind::i8.  Every operand row r of a
 // tile is scaled by a power of two s_r >= max|row| and rounded to a 31-bit
 // integer written as four balanced base-256 digits (digits_word, tc_ptx.cuh).
@@ -28,7 +30,8 @@
 // operand bandwidth to about two thirds of the tensor rate.  The density
 // contraction keeps N = 64 (320 threads, two TMEM buffers): its groups are
 // two K steps long, so overlapping the epilogue matters more there, and its
-// orbital dimension pads to 64.  All waits are bounded (tc_ptx.cuh).
+// orbital dimension pads to 64; the Y pass uses the same shape over
+// 64-function halves of a block.  All waits are bounded (tc_ptx.cuh).
 #include <cuda.h>
 
 #include <algorithm>
