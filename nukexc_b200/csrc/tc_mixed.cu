@@ -549,10 +549,11 @@ __global__ void __launch_bounds__(128) quant_cocc_kernel(const double *__restric
                  sc + (size_t)s * nbf_pad + 128 * I);
 }
 
-// grad rho(g) = 2 sum_mu grad phi(g, mu) Y(g, mu) for the points of one
-// batch (block x of the chunk) and spin (block y), summed over the batch's
-// pairs; grad phi comes back from the pass-A digits (components 1..3).  Warp
-// w takes the points w + 8k, lane l the functions 4l .. 4l+3 of each block.
+// grad rho(g) = 2 sum_mu grad phi(g, mu) Y(g, mu) for one quarter (block z,
+// 64 points) of one batch (block x of the chunk) and spin (block y), summed
+// over the batch's pairs; grad phi comes back from the pass-A digits
+// (components 1..3).  Warp w takes the points 64 z + w + 8k, lane l the
+// functions 4l .. 4l+3 of each block.
 __global__ void __launch_bounds__(256) ygrad_kernel(const double *__restrict__ Y, const uint8_t *__restrict__ qphT,
                                                     const double *__restrict__ sphT,
                                                     const int *__restrict__ pair_off, long b0, long p0, int nspin,
@@ -561,7 +562,7 @@ __global__ void __launch_bounds__(256) ygrad_kernel(const double *__restrict__ Y
   const int s = blockIdx.y;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int q0 = pair_off[b], q1 = pair_off[b + 1];
-  for (int g = warp; g < kBatch; g += 8) {
+  for (int g = 64 * blockIdx.z + warp; g < 64 * (blockIdx.z + 1); g += 8) {
     double gs[3] = {0.0, 0.0, 0.0};
     for (int q = q0; q < q1; ++q) {
       const long qr = q - p0;
@@ -1168,8 +1169,8 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       g.nunits = np * nspin * 4;
       launch_i8(M, M.m_t0, M.m_co, g, s);
       ++P.launches;
-      ygrad_kernel<<<dim3((unsigned)nb, nspin), 256, 0, s>>>(P.ws_phi, M.qphT, M.sphT, P.d_pair_off, c.b0, c.p0,
-                                                            nspin, P.npad, P.d_grad);
+      ygrad_kernel<<<dim3((unsigned)nb, nspin, 4), 256, 0, s>>>(P.ws_phi, M.qphT, M.sphT, P.d_pair_off, c.b0, c.p0,
+                                                               nspin, P.npad, P.d_grad);
       NKX_LAUNCH_CHECK();
       ++P.launches;
     }
