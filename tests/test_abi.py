@@ -61,3 +61,18 @@ def test_morton_order_host_entry():
         for d in range(3):
             code |= ((q[:, d] >> np.uint64(bit)) & np.uint64(1)) << np.uint64(3 * bit + d)
     assert np.all(np.diff(code[perm].astype(np.float64)) >= 0)
+
+
+def test_api_cutoff_radii_match_oracle():
+    # the Python mirror's cutoff radii (host bisection, used for the
+    # neighbour lists) equal the oracle's restatement of compute_cutoff
+    import sys
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    from nukexc_b200 import api as A
+    funcs = [(n, l, 0, z, 0.0, 0.0, 0.0) for n, l in [(1, 0), (2, 1), (3, 2), (4, 3)] for z in (0.3, 1.0, 7.5)]
+    for tol in (1e-10, 1e-6):
+        ours = A.cutoff_radii(A.make_manual_basis(funcs, cutoff_tol=tol))
+        ref = O.make_manual_basis(funcs, cutoff_tol=tol)["cutoff"]
+        assert np.allclose(ours, ref, rtol=1e-9, atol=0.0)  # both solve ln N + (n-1) ln r - zeta r = ln tol
