@@ -205,6 +205,15 @@ NKX_API nkx_status nkx_coulomb_dense(int nbf, int naux, long npts, const double 
                                      const double *d_X, int K, int nocc, const double *d_C, const double *d_occ,
                                      double *d_J, void *stream);
 
+/* compute_exact_exchange (nukexc/exact_exchange.hpp:57-119), the grid RI-K
+ * of the reference's dense path: T = Phi^T C, and per occupied orbital i
+ * (P|mu i) = sum_g Vw(P, g) phi_mu(g) T_i(g), Y_i = (P|mu i)^T X,
+ * K = sum_i occ_i Y_i Y_i^T.  Same operands as nkx_coulomb_dense (column-major
+ * device arrays; d_K nbf x nbf).  FP64 cuBLAS; nocc * naux * nbf * npts work. */
+NKX_API nkx_status nkx_exchange_dense(int nbf, int naux, long npts, const double *d_phi, const double *d_Vw,
+                                      const double *d_X, int K, int nocc, const double *d_C, const double *d_occ,
+                                      double *d_K, void *stream);
+
 /* compute_core_hamiltonian (nukexc/core_hamiltonian.hpp:133-289) by
  * quadrature on device points/weights: S = sum_g w phi phi^T,
  * T = 1/2 sum_g w grad phi . grad phi^T, V = -sum_g w (sum_A Z_A / |r - R_A|) phi phi^T

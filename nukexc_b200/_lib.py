@@ -24,7 +24,7 @@ EXPORTS = [
     "nkx_plan_create", "nkx_plan_get_info", "nkx_fock_build", "nkx_get_last_timing",
     "nkx_plan_last_density", "nkx_plan_batch_blocks", "nkx_plan_destroy", "nkx_last_error", "nkx_xc_gradient",
     "nkx_plan_set_functional", "nkx_plan_set_half_inverse", "nkx_plan_aux_metric", "nkx_plan_density",
-    "nkx_morton_order", "nkx_neighbor_list", "nkx_aux_metric",
+    "nkx_morton_order", "nkx_neighbor_list", "nkx_aux_metric", "nkx_exchange_dense",
 ]
 
 
@@ -89,6 +89,7 @@ def lib():
             "nkx_potential_collocation": [vp, vp, vp, l_, vp, vp],
             "nkx_half_inverse": [i, vp, d, vp, vp, vp],
             "nkx_coulomb_dense": [i, i, l_, vp, vp, vp, i, i, vp, vp, vp, vp],
+            "nkx_exchange_dense": [i, i, l_, vp, vp, vp, i, i, vp, vp, vp, vp],
             "nkx_core_hamiltonian_dense": [vp, vp, vp, vp, l_, vp, vp, vp, vp],
             "nkx_plan_create": [vp, vp, vp, l_, vp, vp, vp, vp, vp],
             "nkx_plan_get_info": [vp, vp],

@@ -277,6 +277,24 @@ def compute_coulomb(mo_orbitals, mo_coeff, basis_collocation, basis_aux_collocat
     return J
 
 
+def compute_exact_exchange(mo_orbitals, mo_coeff, basis_collocation, basis_aux_collocation,
+                           potential_collocation_scaled, half_inverse_X):
+    """compute_exact_exchange (nukexc/exact_exchange.hpp:57-119), the dense
+    grid RI-K, through nkx_exchange_dense: K = sum_i occ_i Y_i Y_i^T with
+    Y_i = ((Vw (Phi o T_i)^T)^T X) and T = C^T Phi."""
+    nbf, npts = basis_collocation.shape
+    naux, K = half_inverse_X.shape
+    f = _flat_lmat(basis_collocation)
+    Vw = _flat_lmat(potential_collocation_scaled)
+    X = _flat_lmat(half_inverse_X)
+    C_ = _flat_lmat(mo_orbitals)
+    occ = _dev(mo_coeff)
+    Km = torch.empty(nbf * nbf, dtype=torch.float64, device="cuda")
+    check(L.lib().nkx_exchange_dense(nbf, naux, npts, _p(f), _p(Vw), _p(X), K, occ.numel(), _p(C_), _p(occ),
+                                     _p(Km), None))
+    return Km.view(nbf, nbf).t()
+
+
 def compute_core_hamiltonian(basis, centers, Z, points, weights):
     """compute_core_hamiltonian (nukexc/core_hamiltonian.hpp:133-289) by
     quadrature: (S, T, V_nuc, H = T + V_nuc) as nbf x nbf CUDA tensors."""

@@ -386,6 +386,48 @@ extern "C" nkx_status nkx_coulomb_dense(int nbf, int naux, long npts, const doub
   });
 }
 
+// compute_exact_exchange (nukexc/exact_exchange.hpp:57-119), the reference's
+// dense grid RI-K: T = Phi^T C (npts x nocc), then per orbital i
+//   B = Phi o T_i (columns scaled), (P|mu i) = Vw B^T (naux x nbf),
+//   Y = (P|mu i)^T X (nbf x K),  K += occ_i Y Y^T,
+// FP64 cuBLAS GEMMs.  The work is nocc * naux * nbf * npts: small systems.
+extern "C" nkx_status nkx_exchange_dense(int nbf, int naux, long npts, const double *d_phi, const double *d_Vw,
+                                         const double *d_X, int K, int nocc, const double *d_C, const double *d_occ,
+                                         double *d_K, void *stream) {
+  return run_guarded("nkx_exchange_dense", [&] {
+    NKX_REQUIRE(nbf > 0 && naux > 0 && npts > 0 && K > 0 && K <= naux && nocc > 0 && d_phi && d_Vw && d_X && d_C &&
+                    d_occ && d_K,
+                NKX_ERR_ARG, "invalid arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<double> occ(nocc);
+    NKX_CUDA(cudaMemcpyAsync(occ.data(), d_occ, sizeof(double) * nocc, cudaMemcpyDeviceToHost, s));
+    NKX_CUDA(cudaStreamSynchronize(s));
+    DevBuf<double> T((size_t)npts * nocc), B((size_t)nbf * npts), P3((size_t)naux * nbf), Y((size_t)nbf * K);
+    cublasHandle_t h;
+    NKX_REQUIRE(cublasCreate(&h) == CUBLAS_STATUS_SUCCESS, NKX_ERR_CUDA, "cublasCreate failed");
+    cublasSetStream(h, s);
+    const double one = 1.0, zero = 0.0;
+    bool ok = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)npts, nocc, nbf, &one, d_phi, nbf, d_C, nbf, &zero, T.p,
+                          (int)npts) == CUBLAS_STATUS_SUCCESS;
+    ok = ok && cudaMemsetAsync(d_K, 0, sizeof(double) * nbf * nbf, s) == cudaSuccess;
+    for (int i = 0; i < nocc && ok; ++i) {
+      scale_columns_kernel<<<nblk((long)nbf * npts, 256), 256, 0, s>>>(nbf, npts, d_phi, T.p + (size_t)i * npts,
+                                                                        B.p);
+      ok = cudaGetLastError() == cudaSuccess;
+      ok = ok && cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, naux, nbf, (int)npts, &one, d_Vw, naux, B.p, nbf, &zero,
+                             P3.p, naux) == CUBLAS_STATUS_SUCCESS;
+      ok = ok && cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, nbf, K, naux, &one, P3.p, naux, d_X, naux, &zero, Y.p,
+                             nbf) == CUBLAS_STATUS_SUCCESS;
+      const double oi = occ[i];
+      ok = ok && cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, K, &oi, Y.p, nbf, Y.p, nbf, &one, d_K, nbf) ==
+                     CUBLAS_STATUS_SUCCESS;
+    }
+    NKX_CUDA(cudaStreamSynchronize(s));
+    cublasDestroy(h);
+    NKX_REQUIRE(ok, NKX_ERR_CUDA, "cuBLAS call in nkx_exchange_dense failed");
+  });
+}
+
 // per chunk point g: ws[g] = w_g, wv[g] = w_g sum_A Z_A / (|r_g - R_A| + 1e-30)
 // (core_hamiltonian.hpp:226-236)
 __global__ void core_weights_kernel(const double *__restrict__ pts, const double *__restrict__ w, long n,

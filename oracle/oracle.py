@@ -286,6 +286,21 @@ def coulomb(b, aux, pts, w, C, occ, X=None, S=None):
     return J.reshape(nbf, nbf).T.copy(), c
 
 
+def exchange(b, aux, pts, w, C, occ, X):
+    """Grid RI-K of the reference's dense path (nukexc/exact_exchange.hpp:57-119):
+    T = C^T Phi; per orbital i, (P|mu i) = Vw (Phi o T_i)^T, Y_i = (P|mu i)^T X,
+    K = sum_i occ_i Y_i Y_i^T (numpy, small cases)."""
+    phi = collocation(b, pts)
+    vw = potential_collocation(aux, pts, w)
+    T = np.asarray(C).T @ phi
+    K = np.zeros((phi.shape[0], phi.shape[0]))
+    for i in range(T.shape[0]):
+        three = vw @ (phi * T[i]).T
+        Y = three.T @ X
+        K += occ[i] * (Y @ Y.T)
+    return K
+
+
 def core_hamiltonian(b, centers, Z, pts, w):
     """compute_core_hamiltonian (nukexc/core_hamiltonian.hpp:133-289) by
     quadrature: S = sum w phi phi^T, T = 1/2 sum w grad phi . grad phi^T,

@@ -11,6 +11,7 @@
 
 #include "nukexc/coulomb.hpp"
 #include "nukexc/density.hpp"
+#include "nukexc/exact_exchange.hpp"
 #include "nukexc/grid.hpp"
 #include "nukexc/nukexc_utils.hpp"
 #include "nukexc/octree.hpp"
@@ -54,7 +55,7 @@ int main() {
   const int max_points_per_box = 32;
 
   // ---- hydrogen 1s self-repulsion, sparse and tiled (test_hydrogen.cxx:633-686, :914-952)
-  double J_sparse_h1s = 0.0, J_tiled_h1s = 0.0;
+  double J_sparse_h1s = 0.0, J_tiled_h1s = 0.0, K_dense_h1s = 0.0, K_sparse_h1s = 0.0, K_tiled_h1s = 0.0;
   {
     Molecule mol({{0.0, 0.0, 0.0}}, {1u});
     FlatGrid grid = make_flat_grid<BeckeRadial>(mol, 100, 20);
@@ -74,6 +75,17 @@ int main() {
     DeviceView2DLeft X = compute_half_inverse(S, 1e-4);
     J_sparse_h1s = nkx_shim::copy_to_host(compute_coulomb_sparse(space, mo, occ, basis, basis_aux, grid, nl, X))[0];
     J_tiled_h1s = nkx_shim::copy_to_host(compute_coulomb_tiled(space, mo, occ, basis, basis_aux, grid, nl, X))[0];
+    // self-exchange (test_hydrogen.cxx:688-758, :760-822, :954-992)
+    K_sparse_h1s =
+        nkx_shim::copy_to_host(compute_exact_exchange_sparse(space, mo, occ, basis, basis_aux, grid, nl, X))[0];
+    K_tiled_h1s =
+        nkx_shim::copy_to_host(compute_exact_exchange_tiled(space, mo, occ, basis, basis_aux, grid, nl, X))[0];
+    const size_t G = grid.weights.extent(0);
+    DeviceView2DLeft phi("phi", 1, G), phi_aux("phi aux", 5, G), vw("Vw", 5, G);
+    fill_collocation(space, basis, grid.quad_points, phi);
+    fill_collocation(space, basis_aux, grid.quad_points, phi_aux);
+    sto_potential_collocation_scaled(space, basis_aux, grid, vw);
+    K_dense_h1s = nkx_shim::copy_to_host(compute_exact_exchange(space, mo, occ, phi, phi_aux, vw, X))[0];
   }
 
   // ---- H2, two s-STOs per atom (test_hydrogen.cxx:994-1073) plus p functions
@@ -152,6 +164,13 @@ int main() {
   DeviceView2DLeft Jd = compute_coulomb(space, mo, occ, phi, phi_aux, vw, X);
   const double J_sparse_vs_dense = max_abs_diff(nkx_shim::copy_to_host(Js), nkx_shim::copy_to_host(Jd));
   const double J_scale = max_abs(nkx_shim::copy_to_host(Jd));
+  // exchange: tiled(tile=1) vs sparse element-wise (test_hydrogen.cxx:994-1073), sparse vs dense
+  DeviceView2DLeft Ks = compute_exact_exchange_sparse(space, mo, occ, basis, basis_aux, grid, nl, X);
+  DeviceView2DLeft Kt = compute_exact_exchange_tiled(space, mo, occ, basis, basis_aux, grid, nl, X, 1);
+  DeviceView2DLeft Kd = compute_exact_exchange(space, mo, occ, phi, phi_aux, vw, X);
+  const double K_tiled_vs_sparse = max_abs_diff(nkx_shim::copy_to_host(Ks), nkx_shim::copy_to_host(Kt));
+  const double K_sparse_vs_dense = max_abs_diff(nkx_shim::copy_to_host(Ks), nkx_shim::copy_to_host(Kd));
+  const double K_scale = max_abs(nkx_shim::copy_to_host(Kd));
 
   // density: sparse vs dense
   DeviceView1D rho_s = compute_density_sparse(basis, grid, nl, mo, occ);
@@ -209,9 +228,12 @@ int main() {
       "\"J_sparse_vs_dense\": %.3e, \"J_scale\": %.6g, \"rho_sparse_vs_dense\": %.3e, "
       "\"grad_sparse_vs_dense\": %.3e, \"sigma_sparse_vs_dense\": %.3e, \"sigma_scale\": %.6g, "
       "\"rho_accumulated\": %.3e, \"xc_dE\": %.3e, \"xc_dV\": %.3e, \"E_lda_x\": %.12g, \"E_vwn\": %.12g, "
-      "\"E_pbe_x\": %.12g, \"E_pbe_c\": %.12g, \"family_checked\": %d}\n",
+      "\"E_pbe_x\": %.12g, \"E_pbe_c\": %.12g, \"family_checked\": %d, \"K_dense_h1s\": %.17g, "
+      "\"K_sparse_h1s\": %.17g, \"K_tiled_h1s\": %.17g, \"K_tiled_vs_sparse\": %.3e, \"K_sparse_vs_dense\": %.3e, "
+      "\"K_scale\": %.6g}\n",
       J_sparse_h1s, J_tiled_h1s, boxes_ok, weights_permuted, nl_ok, nb.size(), metric_tiled_vs_sparse,
       J_tiled_vs_sparse, J_sparse_vs_dense, J_scale, rho_sparse_vs_dense, grad_sparse_vs_dense, sigma_sparse_vs_dense,
-      sigma_scale, rho_accumulated, xc_dE, xc_dV, xc_E[0], xc_E[1], xc_E[2], xc_E[3], family_checked);
+      sigma_scale, rho_accumulated, xc_dE, xc_dV, xc_E[0], xc_E[1], xc_E[2], xc_E[3], family_checked, K_dense_h1s,
+      K_sparse_h1s, K_tiled_h1s, K_tiled_vs_sparse, K_sparse_vs_dense, K_scale);
   return 0;
 }

@@ -303,3 +303,35 @@ def test_core_hamiltonian_matches_oracle():
     assert S[0, 0].item() == pytest.approx(1.0, rel=1e-10)
     assert T[0, 0].item() == pytest.approx(0.5, rel=1e-9)
     assert V[0, 0].item() == pytest.approx(-1.0, rel=1e-9)
+
+
+def test_golden_exchange_h1s_dense():
+    # tests/test_hydrogen.cxx:688-758: K_00 = 5/8
+    c, Z = np.zeros((1, 3)), np.array([1])
+    g = A.make_flat_grid(c, Z, 100, 20, radial="becke")
+    b = A.make_manual_basis([(1, 0, 0, 1.0, 0, 0, 0)])
+    aux = A.make_manual_basis([(1, 0, 0, z, 0, 0, 0) for z in (0.5, 1.0, 2.0, 3.0, 4.0)])
+    phi = A.fill_collocation(b, g.quad_points)
+    phia = A.fill_collocation(aux, g.quad_points)
+    vw = A.sto_potential_collocation_scaled(aux, g.quad_points, g.weights)
+    S = (phia @ vw.t() + vw @ phia.t()) / 2
+    X = A.compute_half_inverse(S, KAT["h1s_exchange"]["half_inverse_thr"])
+    K = A.compute_exact_exchange(np.ones((1, 1)), np.ones(1), phi, phia, vw, X)
+    assert float(K[0, 0]) == pytest.approx(KAT["h1s_exchange"]["K00"], rel=KAT["h1s_exchange"]["rel"])
+
+
+def test_exchange_matches_oracle_water():
+    c, Z, funcs, g = water_case(1, nrad=30, order=11)
+    b, ob = basis_pair(funcs)
+    aux, oaux = basis_pair(small_aux(c, Z))
+    Cm = M.random_orbitals(len(funcs), 5, seed=12)
+    occ = np.linspace(2.0, 1.0, 5)
+    S = O.aux_metric(oaux, g.quad_points, g.weights)
+    X = O.half_inverse(S, 1e-6)
+    phi = A.fill_collocation(b, g.quad_points)
+    phia = A.fill_collocation(aux, g.quad_points)
+    vw = A.sto_potential_collocation_scaled(aux, g.quad_points, g.weights)
+    K = A.compute_exact_exchange(Cm, occ, phi, phia, vw, X).cpu().numpy()
+    Ko = O.exchange(ob, oaux, g.quad_points, g.weights, Cm, occ, X)
+    assert np.abs(K - Ko).max() < 1e-10 * np.abs(Ko).max()
+    assert np.abs(K - K.T).max() < 1e-12 * np.abs(Ko).max()

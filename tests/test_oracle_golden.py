@@ -122,6 +122,16 @@ def test_h1s_coulomb_self_repulsion(use_cholesky):
     assert J[0, 0] == pytest.approx(KAT["h1s_coulomb"]["J00"], rel=KAT["h1s_coulomb"]["rel"])
 
 
+def test_h1s_exchange_self_exchange():
+    # tests/test_hydrogen.cxx:688-758: K_00 = 5/8 for the one occupied orbital
+    pts, w, _ = O.make_flat_grid([[0, 0, 0]], [1], 100, 20, scheme="becke")
+    b = O.make_manual_basis([(1, 0, 0, 1.0, 0, 0, 0)])
+    aux = O.make_manual_basis([(1, 0, 0, z, 0, 0, 0) for z in (0.5, 1.0, 2.0, 3.0, 4.0)])
+    X = O.half_inverse(O.aux_metric(aux, pts, w), KAT["h1s_exchange"]["half_inverse_thr"])
+    K = O.exchange(b, aux, pts, w, np.ones((1, 1)), np.ones(1), X)
+    assert K[0, 0] == pytest.approx(KAT["h1s_exchange"]["K00"], rel=KAT["h1s_exchange"]["rel"])
+
+
 def test_becke_one_half_original():
     # tests/test_partition.cxx:140-195: unclamped Becke, symmetric points -> 0.5
     centers = np.array([[-1.0, 0, 0], [1.0, 0, 0]])

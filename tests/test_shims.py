@@ -88,3 +88,8 @@ def test_sparse_shims_match_reference_and_dense(tmp_path):
     assert out["xc_dV"] <= 1e-9
     assert out["E_lda_x"] < 0 and out["E_pbe_x"] < out["E_lda_x"] and out["E_pbe_c"] < 0
     assert out["family_checked"] == 1
+    # RI-K self-exchange 5/8, dense / sparse / tiled (test_hydrogen.cxx:688-758, :760-822, :954-992)
+    for key in ("K_dense_h1s", "K_sparse_h1s", "K_tiled_h1s"):
+        assert out[key] == pytest.approx(KAT["h1s_exchange"]["K00"], rel=KAT["h1s_exchange"]["rel"])
+    assert out["K_tiled_vs_sparse"] <= 1e-9
+    assert out["K_sparse_vs_dense"] <= 1e-12 * max(1.0, out["K_scale"])
