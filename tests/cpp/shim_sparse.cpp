@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <vector>
 
+#include "nukexc/core_hamiltonian.hpp"
 #include "nukexc/coulomb.hpp"
 #include "nukexc/density.hpp"
 #include "nukexc/exact_exchange.hpp"
@@ -56,6 +57,7 @@ int main() {
 
   // ---- hydrogen 1s self-repulsion, sparse and tiled (test_hydrogen.cxx:633-686, :914-952)
   double J_sparse_h1s = 0.0, J_tiled_h1s = 0.0, K_dense_h1s = 0.0, K_sparse_h1s = 0.0, K_tiled_h1s = 0.0;
+  double S00 = 0.0, T00 = 0.0, V00 = 0.0, H00 = 0.0, coreH_screened_diff = 0.0;
   {
     Molecule mol({{0.0, 0.0, 0.0}}, {1u});
     FlatGrid grid = make_flat_grid<BeckeRadial>(mol, 100, 20);
@@ -86,6 +88,18 @@ int main() {
     fill_collocation(space, basis_aux, grid.quad_points, phi_aux);
     sto_potential_collocation_scaled(space, basis_aux, grid, vw);
     K_dense_h1s = nkx_shim::copy_to_host(compute_exact_exchange(space, mo, occ, phi, phi_aux, vw, X))[0];
+    // core Hamiltonian of H 1s by quadrature: S = 1, T = 1/2, V = -1
+    CoreHamiltonianResult h = compute_core_hamiltonian(basis, grid);
+    S00 = nkx_shim::copy_to_host(h.overlap)[0];
+    T00 = nkx_shim::copy_to_host(h.kinetic)[0];
+    V00 = nkx_shim::copy_to_host(h.nuclear)[0];
+    H00 = nkx_shim::copy_to_host(h.hamiltonian)[0];
+    const CoreHamiltonianResult hs[4] = {compute_core_hamiltonian_screened(basis, grid, nl),
+                                         compute_core_hamiltonian_screened_scratch(basis, grid, nl),
+                                         compute_core_hamiltonian_screened_tiled(basis, grid, nl),
+                                         compute_core_hamiltonian_screened_sparse(basis, grid, nl)};
+    for (const CoreHamiltonianResult &x : hs)
+      coreH_screened_diff = std::max(coreH_screened_diff, std::fabs(nkx_shim::copy_to_host(x.hamiltonian)[0] - H00));
   }
 
   // ---- H2, two s-STOs per atom (test_hydrogen.cxx:994-1073) plus p functions
@@ -230,10 +244,12 @@ int main() {
       "\"rho_accumulated\": %.3e, \"xc_dE\": %.3e, \"xc_dV\": %.3e, \"E_lda_x\": %.12g, \"E_vwn\": %.12g, "
       "\"E_pbe_x\": %.12g, \"E_pbe_c\": %.12g, \"family_checked\": %d, \"K_dense_h1s\": %.17g, "
       "\"K_sparse_h1s\": %.17g, \"K_tiled_h1s\": %.17g, \"K_tiled_vs_sparse\": %.3e, \"K_sparse_vs_dense\": %.3e, "
-      "\"K_scale\": %.6g}\n",
+      "\"K_scale\": %.6g, \"S00\": %.17g, \"T00\": %.17g, \"V00\": %.17g, \"H00\": %.17g, "
+      "\"coreH_screened_diff\": %.3e}\n",
       J_sparse_h1s, J_tiled_h1s, boxes_ok, weights_permuted, nl_ok, nb.size(), metric_tiled_vs_sparse,
       J_tiled_vs_sparse, J_sparse_vs_dense, J_scale, rho_sparse_vs_dense, grad_sparse_vs_dense, sigma_sparse_vs_dense,
       sigma_scale, rho_accumulated, xc_dE, xc_dV, xc_E[0], xc_E[1], xc_E[2], xc_E[3], family_checked, K_dense_h1s,
-      K_sparse_h1s, K_tiled_h1s, K_tiled_vs_sparse, K_sparse_vs_dense, K_scale);
+      K_sparse_h1s, K_tiled_h1s, K_tiled_vs_sparse, K_sparse_vs_dense, K_scale, S00, T00, V00, H00,
+      coreH_screened_diff);
   return 0;
 }

@@ -93,3 +93,10 @@ def test_sparse_shims_match_reference_and_dense(tmp_path):
         assert out[key] == pytest.approx(KAT["h1s_exchange"]["K00"], rel=KAT["h1s_exchange"]["rel"])
     assert out["K_tiled_vs_sparse"] <= 1e-9
     assert out["K_sparse_vs_dense"] <= 1e-12 * max(1.0, out["K_scale"])
+    # core Hamiltonian of H 1s (S = 1, T = 1/2, V = -1 analytically), and the
+    # screened variants equal to it (test_integration.cxx:83-311 asks 1e-6)
+    assert out["S00"] == pytest.approx(1.0, abs=1e-8)
+    assert out["T00"] == pytest.approx(0.5, abs=1e-6)
+    assert out["V00"] == pytest.approx(-1.0, abs=1e-6)
+    assert out["H00"] == pytest.approx(out["T00"] + out["V00"], abs=1e-14)
+    assert out["coreH_screened_diff"] <= 1e-6
