@@ -1,4 +1,5 @@
-// Drop-in replacement of nukexc/density.hpp: compute_density (:150-186) and
+// Drop-in replacement of nukexc/density.hpp: compute_density (:150-186, and the
+// (basis, grid) overload :55-95) and
 // compute_density_and_sigma (:188-255) over nkx_density_dense, and their
 // sparse variants compute_density_sparse (:97-148) and
 // compute_density_and_sigma_sparse (:261-328) over the neighbour list's plan
@@ -25,6 +26,16 @@ V1 compute_density_t(const V2 collocation_values, const V2 mo_orbitals, const V1
 inline DeviceView1D compute_density(const DeviceView2DLeft collocation_values, const DeviceView2DLeft mo_orbitals,
                                     const DeviceView1D mo_coeff) {
   return compute_density_t<DeviceView2DLeft, DeviceView1D>(collocation_values, mo_orbitals, mo_coeff);
+}
+
+// rho on the grid from the basis (density.hpp:55-95): the collocation is
+// formed on the grid's points first
+inline DeviceView1D compute_density(const STOBasisSet basis, const FlatGrid grid, const DeviceView2DLeft mo_orbitals,
+                                    const DeviceView1D mo_coeff) {
+  ExecSpace space;
+  DeviceView2DLeft phi("collocation", basis.nbf(), grid.weights.extent(0));
+  fill_collocation(space, basis, grid.quad_points, phi);
+  return compute_density(phi, mo_orbitals, mo_coeff);
 }
 
 // rho, the three gradient components and sigma = |grad rho|^2, written into

@@ -189,7 +189,9 @@ int main() {
   // density: sparse vs dense
   DeviceView1D rho_s = compute_density_sparse(basis, grid, nl, mo, occ);
   DeviceView1D rho_d = compute_density(phi, mo, occ);
-  const double rho_sparse_vs_dense = max_abs_diff(nkx_shim::copy_to_host(rho_s), nkx_shim::copy_to_host(rho_d));
+  const double rho_sparse_vs_dense = std::max(
+      max_abs_diff(nkx_shim::copy_to_host(rho_s), nkx_shim::copy_to_host(rho_d)),
+      max_abs_diff(nkx_shim::copy_to_host(compute_density(basis, grid, mo, occ)), nkx_shim::copy_to_host(rho_d)));
   DeviceView1D r2("rho", G0), ax("gx", G0), ay("gy", G0), az("gz", G0), sg("sigma", G0);
   compute_density_and_sigma_sparse(basis, grid, nl, mo, occ, r2, ax, ay, az, sg);
   DeviceView1D r3("rho", G0), bx("gx", G0), by("gy", G0), bz("gz", G0), sd("sigma", G0);
