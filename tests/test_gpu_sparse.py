@@ -124,3 +124,21 @@ def test_set_functional_equals_new_plan():
     assert E == pytest.approx(Er, rel=1e-14)
     assert np.abs(V[0] - Vr[0]).max() <= 1e-14 * np.abs(Vr[0]).max()
     assert abs(El - Er) > 1e-3
+
+
+def test_neighbor_list_screening_regression():
+    # tests/test_neighborlist.cxx:50-140 on a synthetic stand-in: 8-point
+    # boxes, basis cutoff 1e-6; the CSR offsets are non-decreasing and a
+    # (H2O)16 cluster screens away well over 30 % of the box x function pairs
+    c, Z = M.water_cluster(16, 4)
+    funcs = M.sto_basis(c, Z)
+    g = A.make_flat_grid(c, Z, 30, 29, weight_threshold=1e-15, radial="ta")
+    b = A.make_manual_basis(funcs, cutoff_tol=1e-6)
+    bb = A.create_bounding_boxes(g, 8)
+    nl = A.build_neighbor_list(b, bb, 8, len(g.weights))
+    off = nl.offsets.cpu().numpy()
+    assert np.all(np.diff(off) >= 0)
+    dense = (len(off) - 1) * b.nbf()
+    screened = int(off[-1])
+    assert screened < dense
+    assert 1.0 - screened / dense > 0.3
