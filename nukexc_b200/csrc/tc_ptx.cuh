@@ -1,5 +1,5 @@
 // Thin inline-PTX layer for the sm_100a tensor-core kernels: mbarriers,
-// TMA tile loads (no cluster multicast), tcgen05 MMA / TMEM.  Every wait is
+// TMA tile loads into the CTA's own shared memory, tcgen05 MMA / TMEM.  Every wait is
 // bounded: after kWaitLimitNs of global time it raises an error flag and
 // returns false, so no kernel can spin forever.
 #pragma once
