@@ -806,6 +806,7 @@ __global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__
     for (int o = 0; o < nop; ++o) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) m[o][c] = fmax(m[o][c], fabs(z[o][c]));
+      if (o == 0) continue;  // zquant takes phi from the digits again
       double2 *dst = reinterpret_cast<double2 *>(out + o * T + (size_t)g * kBlockF + 4 * lane);
       dst[0] = make_double2(z[o][0], z[o][1]);
       dst[1] = make_double2(z[o][2], z[o][3]);
@@ -834,7 +835,8 @@ __global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__
 // tile in slabs of 64 points (rows padded to 68 bytes: conflict-free).
 __global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ ws, const double *__restrict__ sph,
                                                      const double *__restrict__ szs, int nz, uint8_t *__restrict__ qph,
-                                                     uint8_t *__restrict__ qz) {
+                                                     uint8_t *__restrict__ qz, const uint8_t *__restrict__ qphT,
+                                                     const double *__restrict__ sphT, int ncs) {
   extern __shared__ __align__(16) uint8_t tile[];  // [(1 + nz)][4][128][68]
   const long q = blockIdx.x;
   const size_t T = (size_t)kBatch * kBlockF;
@@ -858,6 +860,20 @@ __global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ 
 #pragma unroll
       for (int o = 0; o < 4; ++o) {
         if (o >= nop) break;
+        if (o == 0 && qphT) {
+          // phi straight from the pass-A digits of the pair (value component):
+          // X from the four digit bytes, x = X s_g 2^-30
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int g = g0 + 4 * gq + r;
+            int X = 0;
+#pragma unroll
+            for (int d = 0; d < 4; ++d)
+              X = X * 256 + (int)(int8_t)qphT[(((size_t)q * ncs * 4 + d) * 256 + g) * 128 + f];
+            v[0][r] = int_to_double(X) * (sphT[(size_t)q * ncs * 256 + g] * 0x1p-30);
+          }
+          continue;
+        }
 #pragma unroll
         for (int r = 0; r < 4; ++r) v[o][r] = src[o * T + (size_t)(g0 + 4 * gq + r) * kBlockF + f];
       }
@@ -1177,10 +1193,13 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     Tm.end(s);
   };
   // pass B of one chunk after its Phi / Z staging is written: digits, int8 V
-  auto pass_b = [&](const Chunk &c) {
+  // (phi_digits: pass B of the streamed build, whose Phi comes back from the
+  // pass-A digits instead of the FP64 staging)
+  auto pass_b = [&](const Chunk &c, bool phi_digits) {
     const long np = c.p1 - c.p0;
     Tm.begin(ST_ZBUILD, s);
-    zquant_kernel<<<(unsigned)np, 256, (size_t)(1 + nzs) * 4 * 128 * 68, s>>>(P.ws_phi, M.sph, M.sz, nzs, M.qph, M.qz);
+    zquant_kernel<<<(unsigned)np, 256, (size_t)(1 + nzs) * 4 * 128 * 68, s>>>(
+        P.ws_phi, M.sph, M.sz, nzs, M.qph, M.qz, phi_digits ? M.qphT : nullptr, M.sphT, nc);
     NKX_LAUNCH_CHECK();
     ++P.launches;
     Tm.end(s);
@@ -1248,7 +1267,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       NKX_LAUNCH_CHECK();
       ++P.launches;
       Tm.end(s);
-      pass_b(c);
+      pass_b(c, true);
     }
   } else {
     for (const Chunk &c : P.chunks) pass_a(c);
@@ -1272,7 +1291,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       NKX_LAUNCH_CHECK();
       ++P.launches;
       Tm.end(s);
-      pass_b(c);
+      pass_b(c, false);
     }
   }
   int herr = 0;
