@@ -1106,7 +1106,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
   // grad phi_mu Y_mu needs one orbital contraction (T0) and one more over
   // the orbitals (Y) instead of the three gradient components of T.  It pays
   // from about 256 orbitals on ((H2O)64, 320 orbitals: 226 vs 232 ms; the
-  // 1500-atom aggregate, 2850: 13.4 vs 24.8 s); with fewer the per-pair Y
+  // 1500-atom aggregate, 2850: 12.2 vs 24.8 s); with fewer the per-pair Y
   // traffic dominates.  Above 8192 orbitals the int32 levels could overflow.
   const bool grad_mode = P.gga && M.nocc_pad >= 256 && M.nocc_pad <= 8192;
   if (grad_mode) {
