@@ -39,9 +39,11 @@ enum {
 };
 
 /* Precision of the dense contractions (the density and the V = Phi Z^T
- * contraction).  FP64: plain FP64 kernels.  MIXED: tcgen05 tensor-core
- * TF32 products of split operands (hi + lo) with FP32 accumulation per grid
- * batch and FP64 accumulation across batches. */
+ * contraction).  FP64: plain FP64 kernels.  MIXED: every operand row is
+ * scaled by a power of two and rounded to a 31-bit integer held as four
+ * int8 digits; the products run as tcgen05 kind::i8 tensor-core MMAs with
+ * exact int32 accumulation per grid batch, combined in FP64 across batches
+ * (relative error about 1e-9 of the row maxima). */
 enum { NKX_PREC_FP64 = 0, NKX_PREC_MIXED = 1 };
 
 /* Radial quadratures (IntegratorXX Becke / TreutlerAhlrichs, nukexc/grid.hpp:172-305) */
@@ -53,6 +55,8 @@ enum { NKX_SIZING_UNIFORM = 0, NKX_SIZING_PYSCF = 1 };
 enum {
   NKX_XC_LDA_X = 1,
   NKX_XC_LDA_C_VWN = 7, /* VWN5 */
+  NKX_XC_LDA_C_PW = 12,     /* Perdew-Wang 92, published constants */
+  NKX_XC_LDA_C_PW_MOD = 13, /* Perdew-Wang 92, constants as used inside PBE correlation */
   NKX_XC_GGA_X_PBE = 101,
   NKX_XC_GGA_C_PBE = 130
 };
@@ -166,18 +170,24 @@ NKX_API nkx_status nkx_xc_dense(int nbf, long npts, const double *d_phi, const d
                                 int nocc, const double *d_C, const double *d_occ, const nkx_plan_options *opts,
                                 double *E, double *d_V, void *stream);
 
-/* The dense XC build of nkx_xc_dense for callers that cannot allocate device
- * memory (for example while a CUDA graph is being captured, or under a fixed
- * memory budget handed over at start-up).  No counterpart in the reference.
- * Same arguments and results as nkx_xc_dense; it calls no cudaMalloc/cudaFree
- * and no allocating library routine.  Its scratch is one fixed array of
- * NKX_NOALLOC_SCRATCH_DOUBLES doubles (32 MiB) in the library's device
- * memory, held by every GPU that loads the library until exit; problems with
+/* The dense XC build of nkx_xc_dense for callers that must not allocate
+ * device memory: host programs that give (almost) all GPU memory to their
+ * own pool allocator at start-up, where a library cudaMalloc would fail or
+ * fragment the pool, and latency-critical loops that cannot take the
+ * device-wide synchronisation of cudaMalloc / cudaFree.  No counterpart in
+ * the reference.  Same arguments and results as nkx_xc_dense; it calls no
+ * cudaMalloc, cudaFree or allocating library routine.  Its scratch is one
+ * fixed array of NKX_NOALLOC_SCRATCH_DOUBLES doubles (32 MiB) in the
+ * library's device memory, held by every GPU that loads the library until
+ * the process exits; problems with
  * 32 + pad(nspin*npts) + pad(3*nspin*npts) + pad(nspin*nbf*npts) > that
- * (pad = round up to 32) are rejected with NKX_ERR_ARG.  The first call on a
- * device looks up the array's address (cudaGetSymbolAddress) and should come
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU race and must be serialised by the caller. */
+ * (pad = round up to 32; about nspin*npts*(nbf+4)) are rejected with
+ * NKX_ERR_ARG before any work is launched.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) and should come before
+ * any stream capture; the library must not be used across a
+ * cudaDeviceReset.  All calls share the array and each clears what must
+ * start at zero: calls that overlap on the GPU race on it and must be
+ * serialised by the caller. */
 #define NKX_NOALLOC_SCRATCH_DOUBLES (4u << 20)
 NKX_API nkx_status nkx_xc_dense_noalloc(int nbf, long npts, const double *d_phi, const double *d_gx,
                                         const double *d_gy, const double *d_gz, const double *d_w, int nspin,
@@ -291,6 +301,18 @@ NKX_API nkx_status nkx_plan_set_functional(nkx_plan *plan, int nfunc, const int 
  * compute_coulomb_sparse / _tiled take half_inverse_X
  * (nukexc/coulomb.hpp:117-121, :383-387). */
 NKX_API nkx_status nkx_plan_set_half_inverse(nkx_plan *plan, int K, const double *X, int mem);
+
+/* Limit, in nanoseconds, of the device-side waits of the plan's tensor-core
+ * kernels that may be abandoned (0 restores the default of 2 s).  When such a
+ * wait runs out, the kernel stops issuing work, waits for the copies and MMAs
+ * it has already issued (those drain waits keep a fixed 2 s limit), frees its
+ * tensor memory and returns; the build then fails with NKX_ERR_TIMEOUT and
+ * the plan stays usable for the next build.  stall != 0 exists to test that
+ * path: each tensor-core kernel of the following mixed builds first waits on
+ * a barrier that nothing completes, so it gives up after `ns`; stall = 0
+ * restores normal builds.  No counterpart in the reference (its kernels have
+ * no device waits). */
+NKX_API nkx_status nkx_plan_set_wait_limit(nkx_plan *plan, unsigned long long ns, int stall);
 
 /* The plan's grid Coulomb metric (A|B) (naux x naux, symmetrised),
  * coulomb_overlap_integral_sparse (nukexc/coulomb.hpp:691-813); mem selects

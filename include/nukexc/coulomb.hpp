@@ -3,7 +3,8 @@
 // (basis_aux_collocation is used, as in the reference, only for N_aux); the
 // sparse and tiled variants compute_coulomb_sparse (:117-368) and
 // compute_coulomb_tiled (:383-689) over the neighbour list's plan with the
-// caller's half inverse X (nkx_plan_set_half_inverse + nkx_fock_build, FP64);
+// caller's half inverse X (nkx_plan_set_half_inverse + nkx_fock_build, in
+// the precision chosen by set_precision / NKX_PRECISION, FP64 by default);
 // and the grid Coulomb metric coulomb_overlap_integral_sparse (:691-813) /
 // _tiled (:827-958) over nkx_aux_metric.  The tile size of the tiled
 // variants is a performance parameter of the reference's kernels; here it is
@@ -44,7 +45,7 @@ DeviceView2DLeft coulomb_plan(const Space &space, const DeviceView2DLeft &mo_orb
                   where);
   DeviceView2DLeft J("Coulomb matrix", nbf, nbf);
   double E = 0.0;
-  nkx_shim::check(nkx_fock_build(p, NKX_PREC_FP64, 1, (int)mo_orbitals.extent(1), mo_orbitals.data(), mo_coeff.data(),
+  nkx_shim::check(nkx_fock_build(p, precision(), 1, (int)mo_orbitals.extent(1), mo_orbitals.data(), mo_coeff.data(),
                                  NKX_MEM_DEVICE, 0, &E, nullptr, J.data(), stream_of(space)),
                   where);
   return J;

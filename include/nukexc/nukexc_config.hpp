@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <cstdlib>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -121,9 +122,36 @@ using DeviceArray = nkx_shim::View<T>;
 inline cudaStream_t stream_of(const ExecSpace &s) { return s.stream; }
 #endif
 
+// Precision of the plan-based drop-ins (the *_sparse / *_tiled XC and J
+// functions, which run the batched Fock build of nkx_fock_build).
+// NKX_PREC_FP64 (the default) computes like the reference; NKX_PREC_MIXED
+// runs the contractions on the B200 tensor cores as exact int8-digit
+// products (about 1e-9 relative to the operands' row maxima; within
+// |dE_xc| <= 1e-6 Eh and max|dV_xc| <= 1e-7 of FP64).  The first use reads
+// the environment variable NKX_PRECISION ("mixed" or "fp64"), so an
+// unmodified driver compiled against these headers can switch without a code
+// change; set_precision() overrides it.  The dense functions (compute_lda ...
+// on collocation matrices) are always FP64.
+namespace shim_detail {
+inline int &precision_slot() {
+  static int p = [] {
+    const char *e = std::getenv("NKX_PRECISION");
+    return (e && (std::string(e) == "mixed" || std::string(e) == "MIXED")) ? (int)NKX_PREC_MIXED
+                                                                            : (int)NKX_PREC_FP64;
+  }();
+  return p;
+}
+}  // namespace shim_detail
+inline void set_precision(int precision) {
+  if (precision != NKX_PREC_FP64 && precision != NKX_PREC_MIXED)
+    throw std::runtime_error("set_precision: NKX_PREC_FP64 or NKX_PREC_MIXED expected");
+  shim_detail::precision_slot() = precision;
+}
+inline int precision() { return shim_detail::precision_slot(); }
+
 // libxc's xc_func_type identifies the functional by info->number; any type
-// with that member works here (the ids LDA_X 1, LDA_C_VWN 7, GGA_X_PBE 101,
-// GGA_C_PBE 130 are supported)
+// with that member works here (the ids LDA_X 1, LDA_C_VWN 7, LDA_C_PW 12,
+// LDA_C_PW_MOD 13, GGA_X_PBE 101, GGA_C_PBE 130 are supported)
 template <class F>
 int functional_id(const F &func) {
   return func.info->number;

@@ -3,7 +3,8 @@
 // compute_lsda (:168-261), compute_gga (:424-541) and compute_gga_lsda
 // (:543-726) over nkx_xc_dense, and the sparse variants compute_lsda_sparse
 // (:263-422) and compute_gga_lsda_sparse (:728-977) over the neighbour list's
-// plan (nkx_plan_set_functional + nkx_fock_build, FP64).  As in the
+// plan (nkx_plan_set_functional + nkx_fock_build, in the precision chosen by
+// set_precision / NKX_PRECISION, FP64 by default).  As in the
 // reference, one call evaluates one functional (`func`, identified by libxc's
 // info->number); the returned potential is the full symmetrised
 // N_bf x N_bf matrix and the energy is sum_g w_g rho_g exc_g.  Functional
@@ -128,7 +129,7 @@ inline XC_result_polarized polarized(const DeviceView2DLeft &phi, const double *
   return split_potential(E, V, nbf);
 }
 
-// polarised XC through the neighbour list's plan (FP64)
+// polarised XC through the neighbour list's plan (precision())
 inline XC_result_polarized polarized_sparse(const STOBasisSet &basis, const FlatGrid &grid, const NeighborList &nl,
                                             const DeviceView2DLeft &Ca, const DeviceView1D &oa,
                                             const DeviceView2DLeft &Cb, const DeviceView1D &ob, int id) {
@@ -139,7 +140,7 @@ inline XC_result_polarized polarized_sparse(const STOBasisSet &basis, const Flat
   SpinStack st(Ca, oa, Cb, ob);
   DeviceView1D V("stacked potentials", 2 * nbf * nbf);
   double E = 0.0;
-  nkx_shim::check(nkx_fock_build(p, NKX_PREC_FP64, 2, (int)st.nocc, st.C.data(), st.occ.data(), NKX_MEM_DEVICE, 0,
+  nkx_shim::check(nkx_fock_build(p, precision(), 2, (int)st.nocc, st.C.data(), st.occ.data(), NKX_MEM_DEVICE, 0,
                                  &E, V.data(), nullptr, nullptr),
                   "compute_xc_sparse");
   return split_potential(E, V, nbf);

@@ -17,6 +17,7 @@ RADIAL_BECKE, RADIAL_TA = 0, 1
 SIZING_UNIFORM, SIZING_PYSCF = 0, 1
 MEM_DEVICE, MEM_HOST = 0, 1
 XC_LDA_X, XC_LDA_C_VWN, XC_GGA_X_PBE, XC_GGA_C_PBE = 1, 7, 101, 130
+XC_LDA_C_PW, XC_LDA_C_PW_MOD = 12, 13
 
 EXPORTS = [
     "nkx_make_flat_grid", "nkx_becke_partition", "nkx_fill_collocation", "nkx_density_dense",
@@ -24,7 +25,7 @@ EXPORTS = [
     "nkx_plan_create", "nkx_plan_get_info", "nkx_fock_build", "nkx_get_last_timing",
     "nkx_plan_last_density", "nkx_plan_batch_blocks", "nkx_plan_destroy", "nkx_last_error", "nkx_xc_gradient",
     "nkx_plan_set_functional", "nkx_plan_set_half_inverse", "nkx_plan_aux_metric", "nkx_plan_density",
-    "nkx_morton_order", "nkx_neighbor_list", "nkx_aux_metric", "nkx_exchange_dense",
+    "nkx_morton_order", "nkx_neighbor_list", "nkx_aux_metric", "nkx_exchange_dense", "nkx_plan_set_wait_limit",
 ]
 
 
@@ -101,6 +102,7 @@ def lib():
             "nkx_plan_destroy": [vp],
             "nkx_plan_set_functional": [vp, i, vp, d],
             "nkx_plan_set_half_inverse": [vp, i, vp, i],
+            "nkx_plan_set_wait_limit": [vp, C.c_ulonglong, i],
             "nkx_plan_aux_metric": [vp, vp, i],
             "nkx_plan_density": [vp, i, i, vp, vp, i, i, vp, vp, vp, vp],
             "nkx_morton_order": [l_, vp, vp],

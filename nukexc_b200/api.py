@@ -18,7 +18,7 @@ import torch
 from . import _lib as L
 from ._lib import check
 
-_FUNC_NAMES = {"LDA_X": 1, "LDA_C_VWN": 7, "GGA_X_PBE": 101, "GGA_C_PBE": 130}
+_FUNC_NAMES = {"LDA_X": 1, "LDA_C_VWN": 7, "LDA_C_PW": 12, "LDA_C_PW_MOD": 13, "GGA_X_PBE": 101, "GGA_C_PBE": 130}
 
 
 def _dev(x, dtype=torch.float64):
@@ -435,6 +435,12 @@ class FockBuilder:
         if grad:
             return rho.reshape(nspin, n), g.reshape(nspin, 3, n), sg.reshape(nspin, n)
         return rho.reshape(nspin, n)
+
+    def set_wait_limit(self, ns=0, stall=False):
+        """Limit of the tensor-core kernels' device waits in ns (0: default,
+        2 s); stall=True makes the following mixed builds give up after it
+        (a test of the NKX_ERR_TIMEOUT path; nkx_plan_set_wait_limit)."""
+        check(L.lib().nkx_plan_set_wait_limit(self._h, int(ns), 1 if stall else 0))
 
     def set_functional(self, func_ids, dens_threshold=1e-15):
         """Evaluate these functionals in the following builds (nkx_plan_set_functional)."""

@@ -7,6 +7,7 @@
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
+#include <algorithm>
 #include <functional>
 #include <vector>
 
@@ -172,32 +173,69 @@ __global__ void xc_z_dense_kernel(XcSpec s, bool gga, int nbf, long npts, int ns
   if ((threadIdx.x & 31) == 0) atomicAdd(Eacc, e);
 }
 
-// Vbar(i,j) = sum_g A(i,g) B(j,g); A, B column-major n x npts.  16x16 tiles.
-__global__ void nt_gemm_dense_kernel(int n, long npts, const double *A, const double *B, double *V) {
-  __shared__ double As[16][17], Bs[16][17];
-  const int i = blockIdx.y * 16 + threadIdx.y, j = blockIdx.x * 16 + threadIdx.x;
-  double acc = 0.0;
-  for (long g0 = 0; g0 < npts; g0 += 16) {
-    const long ga = g0 + threadIdx.x;
-    const int ia = blockIdx.y * 16 + threadIdx.y, jb = blockIdx.x * 16 + threadIdx.y;
-    As[threadIdx.y][threadIdx.x] = (ia < n && ga < npts) ? A[(size_t)ia + (size_t)ga * n] : 0.0;
-    Bs[threadIdx.y][threadIdx.x] = (jb < n && ga < npts) ? B[(size_t)jb + (size_t)ga * n] : 0.0;
+// V += Vbar + Vbar^T with Vbar(i,j) = sum_g A(i,g) B(j,g); A, B column-major
+// n x npts (xc_integrals.hpp:148-153 forms Vbar by DGEMM and then adds its
+// transpose).  n is small (the basis) and npts large, so the point range is
+// split over blockIdx.z: each block forms a 64 x 64 tile over its slice of
+// points in registers (4 x 4 per thread, 16-point steps through shared
+// memory) and adds it to V(i,j) and V(j,i) atomically.  V must be zero on
+// entry.
+constexpr int kGemmTile = 64, kGemmK = 16;
+__global__ void __launch_bounds__(256) nt_gemm_sym_kernel(int n, long npts, long kslice, const double *__restrict__ A,
+                                                          const double *__restrict__ B, double *V) {
+  __shared__ double As[kGemmK][kGemmTile + 1], Bs[kGemmK][kGemmTile + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int i0 = blockIdx.y * kGemmTile, j0 = blockIdx.x * kGemmTile;
+  const long g_lo = blockIdx.z * kslice, g_hi = min(npts, g_lo + kslice);
+  double acc[4][4] = {};
+  for (long g0 = g_lo; g0 < g_hi; g0 += kGemmK) {
+    // 64 rows x 16 points of A and of B: thread t loads rows t % 64, points
+    // t / 64 + 4 e (coalesced along the rows)
+    for (int e = 0; e < 4; ++e) {
+      const int r = threadIdx.x & 63, k = (threadIdx.x >> 6) + 4 * e;
+      const long g = g0 + k;
+      const bool gin = g < g_hi;
+      As[k][r] = (gin && i0 + r < n) ? A[(size_t)(i0 + r) + (size_t)g * n] : 0.0;
+      Bs[k][r] = (gin && j0 + r < n) ? B[(size_t)(j0 + r) + (size_t)g * n] : 0.0;
+    }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < 16; ++k) acc += As[threadIdx.y][k] * Bs[threadIdx.x][k];
+    for (int k = 0; k < kGemmK; ++k) {
+      double a[4], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        a[r] = As[k][tx + 16 * r];
+        b[r] = Bs[k][ty + 16 * r];
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+    }
     __syncthreads();
   }
-  if (i < n && j < n) V[(size_t)i + (size_t)j * n] = acc;
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * c;
+      if (i < n && j < n) {
+        atomicAdd(&V[(size_t)i + (size_t)j * n], acc[r][c]);
+        atomicAdd(&V[(size_t)j + (size_t)i * n], acc[r][c]);
+      }
+    }
 }
 
-// V = Vbar + Vbar^T in place (xc_integrals.hpp:148-153)
-__global__ void symmetrize_kernel(int n, double *V) {
-  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && j < n && i <= j) {
-    const double v = V[(size_t)i + (size_t)j * n] + V[(size_t)j + (size_t)i * n];
-    V[(size_t)i + (size_t)j * n] = v;
-    V[(size_t)j + (size_t)i * n] = v;
-  }
+// Launch of nt_gemm_sym_kernel for one n x n output (zeroed here): enough
+// point slices to give every SM a couple of blocks.
+static void launch_nt_gemm_sym(int n, long npts, const double *A, const double *B, double *V, cudaStream_t s) {
+  NKX_CUDA(cudaMemsetAsync(V, 0, sizeof(double) * n * n, s));
+  const int nt = (n + kGemmTile - 1) / kGemmTile;
+  const long want = std::max<long>(1, (2L * 148 + (long)nt * nt - 1) / ((long)nt * nt));
+  const long nsl = std::max<long>(1, std::min<long>(want, (npts + 255) / 256));
+  const long kslice = ((npts + nsl - 1) / nsl + kGemmK - 1) / kGemmK * kGemmK;
+  const long nz = (npts + kslice - 1) / kslice;
+  nt_gemm_sym_kernel<<<dim3(nt, nt, (unsigned)nz), 256, 0, s>>>(n, npts, kslice, A, B, V);
 }
 
 __global__ void potential_dense_kernel(const AuxFunc *__restrict__ f, int naux, const double *__restrict__ pts,
@@ -318,12 +356,8 @@ extern "C" nkx_status nkx_xc_dense(int nbf, long npts, const double *d_phi, cons
     xc_z_dense_kernel<<<nblk(npts, 128), 128, 0, s>>>(sp, gga, nbf, npts, nspin, d_phi, d_gx, d_gy, d_gz, d_w,
                                                      rho.p, grad.p, Z.p, Ed.p);
     NKX_LAUNCH_CHECK();
-    dim3 tb(16, 16), gb(nblk(nbf, 16), nblk(nbf, 16));
-    for (int sp_i = 0; sp_i < nspin; ++sp_i) {
-      double *Vs = d_V + (size_t)sp_i * nbf * nbf;
-      nt_gemm_dense_kernel<<<gb, tb, 0, s>>>(nbf, npts, d_phi, Z.p + (size_t)sp_i * nbf * npts, Vs);
-      symmetrize_kernel<<<gb, tb, 0, s>>>(nbf, Vs);
-    }
+    for (int sp_i = 0; sp_i < nspin; ++sp_i)
+      launch_nt_gemm_sym(nbf, npts, d_phi, Z.p + (size_t)sp_i * nbf * npts, d_V + (size_t)sp_i * nbf * nbf, s);
     NKX_LAUNCH_CHECK();
     NKX_CUDA(cudaMemcpyAsync(E, Ed.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     NKX_CUDA(cudaStreamSynchronize(s));
@@ -550,18 +584,29 @@ extern "C" nkx_status nkx_half_inverse(int N, const double *d_S, double thr, dou
 }
 
 // ---------------------------------------------------------------------------
-// nkx_xc_dense_noalloc: the dense XC build for callers that cannot allocate
-// device memory -- code running while a CUDA graph is being captured, a host
-// that hands the library a fixed memory budget up front, or a process whose
-// allocator must not see cudaMalloc/cudaFree after start-up.  The scratch
-// (per-point density and gradient, the Z matrix, the energy accumulator)
-// lives in one file-scope __device__ array of kNoAllocScratchDoubles doubles
-// (32 MiB) that every GPU loading the library keeps until process exit.
-// Its device address is looked up once per device with
-// cudaGetSymbolAddress on the first call made with that device current; that
-// first call should therefore happen before any stream capture.  All calls
-// share the array: calls whose work overlaps on the GPU (different streams,
-// or host threads) race on it and must be serialised by the caller.
+// nkx_xc_dense_noalloc: the dense XC build of nkx_xc_dense for callers that
+// must not allocate device memory.  Some host programs hand (almost) all of
+// the GPU's memory to their own pool allocator when they start, so a
+// cudaMalloc from a library would fail or fragment that pool; others run the
+// Fock build inside a latency-critical loop where cudaMalloc / cudaFree,
+// which synchronise the whole device, are not acceptable.  This entry point
+// keeps its scratch (energy accumulator, per-point density and gradient, the
+// Z matrix) in one file-scope __device__ array of kNoAllocScratchDoubles
+// doubles (32 MiB), which every GPU that loads the library holds until the
+// process exits, and it calls no cudaMalloc, cudaFree or allocating library
+// routine.
+//
+// In host code the array's name is only a host-side stand-in, never a device
+// address, so the first call made on a device (with that device current)
+// looks the address up with cudaGetSymbolAddress and remembers it for that
+// device; that first call should come before any stream capture.  The
+// remembered address belongs to the device's current context: the library
+// must not be used across a cudaDeviceReset.  Every call shares the array and
+// finds the previous call's contents there, so everything that must start at
+// zero is cleared by the call itself; calls whose work overlaps on the GPU
+// (other streams, other host threads) race on the array and must be
+// serialised by the caller.  Problems that need more scratch than the array
+// holds are rejected with NKX_ERR_ARG before anything is launched.
 // ---------------------------------------------------------------------------
 #include <mutex>
 
@@ -598,14 +643,19 @@ extern "C" nkx_status nkx_xc_dense_noalloc(int nbf, long npts, const double *d_p
     const XcSpec sp = make_spec(opts);
     const bool gga = spec_is_gga(sp);
     NKX_REQUIRE(!gga || (d_gx && d_gy && d_gz), NKX_ERR_ARG, "GGA needs collocation gradients");
-    // layout in doubles, each piece 256-byte aligned: E | rho | grad | Z
+    // layout in doubles, each piece 256-byte aligned: E | rho | grad | Z.
+    // npts is bounded first, so the products below cannot wrap around.
+    const size_t per_point = (size_t)nspin * ((size_t)nbf + 4);
+    const std::string too_large =
+        "problem too large for the fixed 32 MiB scratch: needs about nspin*npts*(nbf+4) doubles <= 4194304";
+    NKX_REQUIRE((size_t)npts <= kNoAllocScratchDoubles / per_point, NKX_ERR_ARG,
+                too_large + " (nspin " + std::to_string(nspin) + ", npts " + std::to_string(npts) + ", nbf " +
+                    std::to_string(nbf) + ")");
     auto up = [](size_t n) { return (n + 31) & ~(size_t)31; };
     const size_t nE = 32, nrho = up((size_t)nspin * npts), ngrad = up((size_t)nspin * 3 * npts);
     const size_t nZ = up((size_t)nspin * nbf * npts);
     const size_t need = nE + nrho + ngrad + nZ;
-    NKX_REQUIRE(need <= kNoAllocScratchDoubles, NKX_ERR_ARG,
-                "problem too large for the fixed 32 MiB scratch: needs nspin*npts*(nbf+4) doubles <= 4194304 (" +
-                    std::to_string(need) + " requested)");
+    NKX_REQUIRE(need <= kNoAllocScratchDoubles, NKX_ERR_ARG, too_large + " (" + std::to_string(need) + " requested)");
     double *base = noalloc_scratch_address();
     double *Ed = base, *rho = base + nE, *grad = rho + nrho, *Z = grad + ngrad;
     cudaStream_t s = (cudaStream_t)stream;
@@ -619,12 +669,8 @@ extern "C" nkx_status nkx_xc_dense_noalloc(int nbf, long npts, const double *d_p
     xc_z_dense_kernel<<<nblk(npts, 128), 128, 0, s>>>(sp, gga, nbf, npts, nspin, d_phi, d_gx, d_gy, d_gz, d_w,
                                                      rho, grad, Z, Ed);
     NKX_LAUNCH_CHECK();
-    dim3 tb(16, 16), gb(nblk(nbf, 16), nblk(nbf, 16));
-    for (int sp_i = 0; sp_i < nspin; ++sp_i) {
-      double *Vs = d_V + (size_t)sp_i * nbf * nbf;
-      nt_gemm_dense_kernel<<<gb, tb, 0, s>>>(nbf, npts, d_phi, Z + (size_t)sp_i * nbf * npts, Vs);
-      symmetrize_kernel<<<gb, tb, 0, s>>>(nbf, Vs);
-    }
+    for (int sp_i = 0; sp_i < nspin; ++sp_i)
+      launch_nt_gemm_sym(nbf, npts, d_phi, Z + (size_t)sp_i * nbf * npts, d_V + (size_t)sp_i * nbf * nbf, s);
     NKX_LAUNCH_CHECK();
     NKX_CUDA(cudaMemcpyAsync(E, Ed, sizeof(double), cudaMemcpyDeviceToHost, s));
     NKX_CUDA(cudaStreamSynchronize(s));

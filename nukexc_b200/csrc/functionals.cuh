@@ -196,16 +196,27 @@ NKX_HD inline T pw92_g(const T &rs, double A, double a1, double b1, double b2, d
   return -2.0 * A * (1.0 + a1 * rs) * dlog(1.0 + 1.0 / den);
 }
 
+// Perdew-Wang 92 correlation energy per particle (Phys. Rev. B 45, 13244).
+// mod = false: the published constants (A = 0.031091, 0.015545, 0.016887,
+// f''(0) = 1.709921; libxc's LDA_C_PW); mod = true: the constants carried to
+// more digits that PBE correlation uses (libxc's LDA_C_PW_MOD).
 template <class T>
-NKX_HD inline T eps_pw92(const T &rs, const T &zeta, const T &opz, const T &omz) {
-  const T gP = pw92_g(rs, 0.0310907, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294);
-  const T gF = pw92_g(rs, 0.01554535, 0.20548, 14.1189, 6.1977, 3.3662, 0.62517);
-  const T gA = pw92_g(rs, 0.0168869, 0.11125, 10.357, 3.6231, 0.88026, 0.49671);
-  const double fz20 = 1.709920934161365617563962776245;
+NKX_HD inline T eps_pw92(const T &rs, const T &zeta, const T &opz, const T &omz, bool mod = true) {
+  const T gP = pw92_g(rs, mod ? 0.0310907 : 0.031091, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294);
+  const T gF = pw92_g(rs, mod ? 0.01554535 : 0.015545, 0.20548, 14.1189, 6.1977, 3.3662, 0.62517);
+  const T gA = pw92_g(rs, mod ? 0.0168869 : 0.016887, 0.11125, 10.357, 3.6231, 0.88026, 0.49671);
+  const double fz20 = mod ? 1.709920934161365617563962776245 : 1.709921;
   const T fz = fzeta(opz, omz);
   const T z2 = zeta * zeta;
   const T z4 = z2 * z2;
   return gP - gA * fz * (1.0 / fz20) * (1.0 - z4) + (gF - gP) * fz * z4;
+}
+
+template <class T>
+NKX_HD inline T f_pw92(const T &ra, const T &rb, bool mod) {
+  const T rho = ra + rb;
+  const T rs = dpow(3.0 / (4.0 * kPi * rho), 1.0 / 3.0);
+  return rho * eps_pw92(rs, (ra - rb) / rho, 2.0 * ra / rho, 2.0 * rb / rho, mod);
 }
 
 template <class T>
@@ -244,7 +255,8 @@ NKX_HD inline T f_pbe_c(const T &ra, const T &rb, const T &sigma) {
 
 NKX_HD inline bool func_is_gga(int id) { return id == NKX_XC_GGA_X_PBE || id == NKX_XC_GGA_C_PBE; }
 NKX_HD inline bool func_supported(int id) {
-  return id == NKX_XC_LDA_X || id == NKX_XC_LDA_C_VWN || id == NKX_XC_GGA_X_PBE || id == NKX_XC_GGA_C_PBE;
+  return id == NKX_XC_LDA_X || id == NKX_XC_LDA_C_VWN || id == NKX_XC_LDA_C_PW || id == NKX_XC_LDA_C_PW_MOD ||
+         id == NKX_XC_GGA_X_PBE || id == NKX_XC_GGA_C_PBE;
 }
 
 template <int N>
@@ -253,6 +265,8 @@ NKX_HD inline Dual<N> f_total(int id, const Dual<N> &ra, const Dual<N> &rb, cons
   switch (id) {
     case NKX_XC_LDA_X: return f_lda_x(ra, rb);
     case NKX_XC_LDA_C_VWN: return f_vwn5(ra, rb);
+    case NKX_XC_LDA_C_PW: return f_pw92(ra, rb, false);
+    case NKX_XC_LDA_C_PW_MOD: return f_pw92(ra, rb, true);
     case NKX_XC_GGA_X_PBE: return f_pbe_x(ra, rb, saa, sbb);
     case NKX_XC_GGA_C_PBE: return f_pbe_c(ra, rb, saa + 2.0 * sab + sbb);
     default: return dconst<N>(0.0);

@@ -425,6 +425,7 @@ static void xc_gradient(Plan &P, int nspin, int nocc, const double *C, const dou
   NKX_REQUIRE(P.all_funcs_on_atoms, NKX_ERR_ARG, "the gradient needs every basis function centred on an atom");
   P.launches = 0;
   StageTimer Tm;
+  NKX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int) * 2, s));
   upload_orbitals(P, nspin, nocc, C, occ, mem, s);
   fp64_density_pass(P, nspin, nocc, s, Tm);
   GradState &G = grad_state(P, nspin, nocc);
@@ -469,7 +470,10 @@ static void xc_gradient(Plan &P, int nspin, int nocc, const double *C, const dou
   NKX_LAUNCH_CHECK();
   P.launches += 2;
   NKX_CUDA(cudaMemcpyAsync(grad, G.F, fs_bytes, cudaMemcpyDeviceToHost, s));
+  int status[2] = {0, 0};
+  NKX_CUDA(cudaMemcpyAsync(status, P.d_status, sizeof(status), cudaMemcpyDeviceToHost, s));
   NKX_CUDA(cudaStreamSynchronize(s));
+  NKX_REQUIRE(status[1] == 0, NKX_ERR_NUMERIC, "non-finite value in the orbitals or occupations");
 }
 
 }  // namespace nkx

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <parallel/algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <functional>
@@ -442,14 +443,21 @@ __global__ void symmetrize_unpad_kernel(int n, int npad, const int *__restrict__
 
 // C (nbf x nocc column-major, per spin) -> Ct[spin][i][p] = C(fperm[p], i)
 // in plan order, zero at padding positions (fperm < 0)
-__global__ void pack_orbitals_kernel(const double *__restrict__ C, const int *__restrict__ fperm, int nbf, int nocc,
-                                     int nspin, int nbf_pad, double *__restrict__ Ct) {
+// Orbitals into plan order; a non-finite coefficient or occupation raises
+// nonfinite[0] (the build then returns NKX_ERR_NUMERIC).
+__global__ void pack_orbitals_kernel(const double *__restrict__ C, const double *__restrict__ occ,
+                                     const int *__restrict__ fperm, int nbf, int nocc, int nspin, int nbf_pad,
+                                     double *__restrict__ Ct, int *nonfinite) {
   const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long tot = (long)nspin * nocc * nbf_pad;
   if (e >= tot) return;
   const int f = fperm[e % nbf_pad];
   const long si = e / nbf_pad;
-  Ct[e] = f >= 0 ? C[si * nbf + f] : 0.0;
+  const double c = f >= 0 ? C[si * nbf + f] : 0.0;
+  Ct[e] = c;
+  bool bad = !isfinite(c);
+  if (e < (long)nspin * nocc) bad = bad || !isfinite(occ[e]);
+  if (bad) atomicOr(nonfinite, 1);
 }
 
 // y_a += sum over a slice of points of w_g rho_g V_a(g) for the functions of
@@ -1015,6 +1023,8 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
   P.d_vj = P.alloc<double>(P.npad);
   P.d_V = P.alloc<double>(3 * (size_t)P.nbf_pad * P.nbf_pad);
   P.d_E = P.alloc<double>(1);
+  P.d_status = P.alloc<int>(2);
+  NKX_CUDA(cudaMemset(P.d_status, 0, sizeof(int) * 2));
   NKX_CUDA(cudaMemset(P.d_rho, 0, sizeof(double) * 2 * P.npad));
   NKX_CUDA(cudaMemset(P.d_grad, 0, sizeof(double) * 6 * P.npad));
 
@@ -1295,8 +1305,8 @@ void upload_orbitals(Plan &P, int nspin, int nocc, const double *C, const double
   } else {
     NKX_CUDA(cudaMemcpyAsync(P.d_occ, occ, sizeof(double) * nspin * nocc, cudaMemcpyDeviceToDevice, s));
   }
-  pack_orbitals_kernel<<<nblk((long)nspin * nocc * P.nbf_pad, 256), 256, 0, s>>>(Cd, P.d_fperm, P.nbf, nocc, nspin,
-                                                                                  P.nbf_pad, P.d_Ct);
+  pack_orbitals_kernel<<<nblk((long)nspin * nocc * P.nbf_pad, 256), 256, 0, s>>>(
+      Cd, P.d_occ, P.d_fperm, P.nbf, nocc, nspin, P.nbf_pad, P.d_Ct, P.d_status + 1);
   NKX_LAUNCH_CHECK();
   ++P.launches;
 }
@@ -1321,6 +1331,7 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
   NKX_CUDA(cudaEventCreate(&t0));
   NKX_CUDA(cudaEventCreate(&t1));
   NKX_CUDA(cudaEventRecord(t0, s));
+  NKX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int) * 2, s));
 
   upload_orbitals(P, nspin, nocc, C, occ, mem, s);
 
@@ -1355,6 +1366,8 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
     if (separateJ) NKX_CUDA(cudaMemcpyAsync(J, dst + nspin * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
   }
   NKX_CUDA(cudaMemcpyAsync(E, P.d_E, sizeof(double), cudaMemcpyDeviceToHost, s));
+  int status[2] = {0, 0};
+  NKX_CUDA(cudaMemcpyAsync(status, P.d_status, sizeof(status), cudaMemcpyDeviceToHost, s));
   NKX_CUDA(cudaEventRecord(t1, s));
   NKX_CUDA(cudaStreamSynchronize(s));
   float st[6];
@@ -1370,6 +1383,10 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   P.last_nspin = nspin;
+  NKX_REQUIRE(status[0] == 0, NKX_ERR_TIMEOUT,
+              "a tensor-core kernel wait gave up (wait code " + std::to_string(status[0]) + "); outputs are invalid");
+  NKX_REQUIRE(status[1] == 0 && std::isfinite(*E), NKX_ERR_NUMERIC,
+              "non-finite value in the orbitals, occupations, grid or an operand of the build; outputs are invalid");
 }
 
 }  // namespace nkx
@@ -1479,6 +1496,15 @@ NKX_API nkx_status nkx_plan_set_half_inverse(nkx_plan *plan, int K, const double
   });
 }
 
+NKX_API nkx_status nkx_plan_set_wait_limit(nkx_plan *plan, unsigned long long ns, int stall) {
+  return run_guarded("nkx_plan_set_wait_limit", [&] {
+    NKX_REQUIRE(plan, NKX_ERR_ARG, "plan is NULL");
+    Plan &P = *reinterpret_cast<Plan *>(plan);
+    P.wait_ns = ns ? ns : 2000000000ull;
+    P.stall_test = stall != 0;
+  });
+}
+
 NKX_API nkx_status nkx_plan_aux_metric(const nkx_plan *plan, double *S, int mem) {
   return run_guarded("nkx_plan_aux_metric", [&] {
     NKX_REQUIRE(plan && S, NKX_ERR_ARG, "invalid arguments");
@@ -1507,6 +1533,7 @@ NKX_API nkx_status nkx_plan_density(nkx_plan *plan, int nspin, int nocc, const d
       P.d_perm = P.alloc<long>(n);
       NKX_CUDA(cudaMemcpy(P.d_perm, P.perm.data(), sizeof(long) * n, cudaMemcpyHostToDevice));
     }
+    NKX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int) * 2, s));
     upload_orbitals(P, nspin, nocc, C, occ, mem, s);
     // the gradient needs the gradient collocation whatever the functional
     const bool gga = P.gga;
@@ -1539,8 +1566,11 @@ NKX_API nkx_status nkx_plan_density(nkx_plan *plan, int nspin, int nocc, const d
       if (grad) NKX_CUDA(cudaMemcpyAsync(grad, ograd, sizeof(double) * 3 * nspin * n, cudaMemcpyDeviceToHost, s));
       if (sigma) NKX_CUDA(cudaMemcpyAsync(sigma, osig, sizeof(double) * nspin * n, cudaMemcpyDeviceToHost, s));
     }
+    int status[2] = {0, 0};
+    NKX_CUDA(cudaMemcpyAsync(status, P.d_status, sizeof(status), cudaMemcpyDeviceToHost, s));
     NKX_CUDA(cudaStreamSynchronize(s));
     P.last_nspin = nspin;
+    NKX_REQUIRE(status[1] == 0, NKX_ERR_NUMERIC, "non-finite value in the orbitals or occupations");
   });
 }
 

@@ -86,6 +86,13 @@ struct Plan {
   float *mx_phi = nullptr, *mx_a = nullptr, *mx_b = nullptr, *mx_c = nullptr;
   void *mx_state = nullptr;
 
+  // build status words, zeroed by every build: [0] code of the first
+  // tensor-core wait that gave up, [1] non-finite input or operand seen
+  int *d_status = nullptr;
+  // limit of the device waits that may be abandoned (nkx_plan_set_wait_limit)
+  unsigned long long wait_ns = 2000000000ull;
+  int stall_test = 0;  // tests of the error path: tensor-core kernels wait on a barrier nothing completes
+
   nkx_build_timing last{};
   int launches = 0;
   int last_nspin = 1;

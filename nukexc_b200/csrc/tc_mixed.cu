@@ -89,7 +89,13 @@ struct TcArgs {
   const int *pair_batch;
   double *Y;
   long nunits;
+  // err[0]: code of the first wait that gave up (0: none); waits that can
+  // be abandoned give up after wait_ns, the drain waits after kDrainLimitNs
   int *err;
+  unsigned long long wait_ns;
+  // stall != 0 (tests of the error path): the MMA issuer first waits on a
+  // barrier that nothing completes, so the kernel gives up after wait_ns
+  int stall;
 };
 
 struct UnitIter {
@@ -217,7 +223,7 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
   using Sh = TcShape<MODE>;
   constexpr int N = Sh::N, NBUF = Sh::NBUF, kStages = Sh::kStages, kStageBytes = Sh::kStageBytes;
   extern __shared__ __align__(1024) uint8_t dsmem[];
-  __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar[NBUF], tempty_bar[NBUF], drain_bar;
+  __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar[NBUF], tempty_bar[NBUF], drain_bar, stall_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_flag;
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dsmem) + 1023) & ~uintptr_t(1023));
@@ -234,6 +240,7 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
       mbar_init(&tempty_bar[i], Sh::kEpiThreads);
     }
     mbar_init(&drain_bar, 1);
+    mbar_init(&stall_bar, 1);
     fence_mbar_init();
     prefetch_tmap(&mapA);
     prefetch_tmap(&mapB);
@@ -256,7 +263,7 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
         for_each_group(a, it, [&](const Group &g, auto coords) {
           for (int k = 0; k < g.nsteps && !abort_flag; ++k, ++step) {
             const int st = step % kStages;
-            if (!mbar_wait(&empty_bar[st], ((step / kStages) & 1) ^ 1, a.err, 1, &abort_flag)) return;
+            if (!mbar_wait(&empty_bar[st], ((step / kStages) & 1) ^ 1, a.err, 1, &abort_flag, a.wait_ns)) return;
             int xa, ya, za, xb, yb, zb;
             coords(k, xa, ya, za, xb, yb, zb);
             uint8_t *base = smem + st * kStageBytes;
@@ -268,12 +275,13 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
       }
       volatile int keep_waiting = 0;
       for (uint32_t k = (step > kStages ? step - kStages : 0); k < step; ++k)
-        mbar_wait(&full_bar[k % kStages], (k / kStages) & 1, a.err, 2, &keep_waiting);
+        mbar_wait(&full_bar[k % kStages], (k / kStages) & 1, a.err, 2, &keep_waiting, kDrainLimitNs);
     }
   } else if (warp == 1) {
     // ------------------------------------------------------ MMA issuer
     if (lane == 0) {
       uint32_t step = 0, grp = 0;
+      if (a.stall) mbar_wait(&stall_bar, 0, a.err, 7, &abort_flag, a.wait_ns);
       for (long u = blockIdx.x; u < a.nunits && !abort_flag; u += gridDim.x) {
         UnitIter it(a, u);
         for_each_group(a, it, [&](const Group &g, auto) {
@@ -281,12 +289,12 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
           // TMEM buffer grp % NBUF: wait until the epilogue has read the group
           // that used it last
           const uint32_t buf = grp % NBUF, use = grp / NBUF;
-          if (!mbar_wait(&tempty_bar[buf], (use & 1) ^ 1, a.err, 3, &abort_flag)) return;
+          if (!mbar_wait(&tempty_bar[buf], (use & 1) ^ 1, a.err, 3, &abort_flag, a.wait_ns)) return;
           tc_fence_after();
           const uint32_t d = tmem + buf * 4 * N;
           for (int k = 0; k < g.nsteps; ++k, ++step) {
             const int st = step % kStages;
-            if (!mbar_wait(&full_bar[st], (step / kStages) & 1, a.err, 4, &abort_flag)) return;
+            if (!mbar_wait(&full_bar[st], (step / kStages) & 1, a.err, 4, &abort_flag, a.wait_ns)) return;
             tc_fence_after();
             const uint32_t base = smem_u32(smem + st * kStageBytes);
             // products of A digit plane i with B planes j = 0 .. 3-i into
@@ -321,7 +329,7 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
       }
       volatile int keep_waiting = 0;
       mma_commit(&drain_bar);
-      mbar_wait(&drain_bar, 0, a.err, 5, &keep_waiting);
+      mbar_wait(&drain_bar, 0, a.err, 5, &keep_waiting, kDrainLimitNs);
     }
   } else {
     // ------------------------------------------------------ epilogue
@@ -338,7 +346,7 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
       for_each_group(a, it, [&](const Group &g, auto) {
         if (abort_flag) return;
         const uint32_t buf = grp % NBUF, use = grp / NBUF;
-        if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag)) return;
+        if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag, a.wait_ns)) return;
         tc_fence_after();
         __syncwarp();
         const bool live = g.nsteps > 0;
@@ -450,6 +458,14 @@ __device__ __forceinline__ double warp_max(double v) {
   for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
+// A non-finite operand value (exponent field 0x7ff) would still become
+// finite digits and a silently wrong product, so every quantiser reports one
+// in *flag (the plan's numeric status word) and the build returns
+// NKX_ERR_NUMERIC.  Called by all lanes of a warp.
+__device__ __forceinline__ void report_nonfinite(bool bad, int *flag) {
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
 // four consecutive values -> four digit planes (one packed word per plane:
 // w[p] byte k = digit p of value k, p = 0 the leading digit)
 __device__ __forceinline__ void quant4(const double v[4], double inv, uint32_t w[4]) {
@@ -465,7 +481,7 @@ __device__ __forceinline__ void quant4(const double v[4], double inv, uint32_t w
 // Density operand B: orbital rows (spin, i) over each 128-function block.
 // qct[spin][digit][i][f], sct[spin][i][blk]; rows i >= nocc are zero.
 __global__ void quant_ct_kernel(const double *__restrict__ Ct, int nocc, int nocc_pad, int nspin, int nbf_pad,
-                                int nblk, uint8_t *__restrict__ q, double *__restrict__ sc) {
+                                int nblk, uint8_t *__restrict__ q, double *__restrict__ sc, int *nonfinite) {
   const long r = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (r >= (long)nspin * nocc_pad * nblk) return;
@@ -476,6 +492,8 @@ __global__ void quant_ct_kernel(const double *__restrict__ Ct, int nocc, int noc
   double v[4] = {0, 0, 0, 0};
   if (i < nocc)
     for (int k = 0; k < 4; ++k) v[k] = Ct[((size_t)s * nocc + i) * nbf_pad + f0 + k];
+  report_nonfinite(max(max(exp_field(v[0]), exp_field(v[1])), max(exp_field(v[2]), exp_field(v[3]))) == 0x7ffu,
+                   nonfinite);
   const double m = warp_max(fmax(fmax(fabs(v[0]), fabs(v[1])), fmax(fabs(v[2]), fabs(v[3]))));
   double scl;
   const double inv = inv_pow2_scale(m, scl);
@@ -606,7 +624,8 @@ __global__ void __launch_bounds__(256) colloc_quantT_kernel(const StoFunc *__res
                                                             const double *__restrict__ py, const double *__restrict__ pz,
                                                             const int *__restrict__ pair_batch,
                                                             const int *__restrict__ pair_blk, long p0,
-                                                            uint8_t *__restrict__ q, double *__restrict__ sc) {
+                                                            uint8_t *__restrict__ q, double *__restrict__ sc,
+                                                            int *nonfinite) {
   constexpr int NC = GRAD ? 4 : 1;
   const long p = p0 + blockIdx.x;
   const int b = pair_batch[p], I = pair_blk[p];
@@ -631,6 +650,7 @@ __global__ void __launch_bounds__(256) colloc_quantT_kernel(const StoFunc *__res
 #pragma unroll
     for (int k = 0; k < NC; ++k) {
       const unsigned el = max(max(exp_field(v[k][0]), exp_field(v[k][1])), max(exp_field(v[k][2]), exp_field(v[k][3])));
+      report_nonfinite(el == 0x7ffu, nonfinite);
       double s;
       const double inv = warp_inv_pow2_scale(
           el, fmax(fmax(fabs(v[k][0]), fabs(v[k][1])), fmax(fabs(v[k][2]), fabs(v[k][3]))), s);
@@ -662,7 +682,8 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
                                                          const int *__restrict__ pair_blk, long p0,
                                                          const double *__restrict__ coef, const double *__restrict__ vj,
                                                          int nspin, long npad, double *__restrict__ ws,
-                                                         double *__restrict__ sph, double *__restrict__ szs) {
+                                                         double *__restrict__ sph, double *__restrict__ szs,
+                                                         int *nonfinite) {
   __shared__ double red[8][4][128];
   const long p = p0 + blockIdx.x, qrel = blockIdx.x;
   const int b = pair_batch[p], I = pair_blk[p];
@@ -680,6 +701,7 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
 #pragma unroll
     for (int c = 0; c < 4; ++c) m[o][c] = 0.0;
   double *out = ws + qrel * 4 * T;
+  unsigned efield = 0;  // largest exponent field of the operand values (0x7ff: non-finite)
   for (int g = warp; g < kBatch; g += 8) {
     const long gg = (long)b * kBatch + g;
     const double x = px[gg], y = py[gg], z = pz[gg];
@@ -716,12 +738,16 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
 #pragma unroll
     for (int o = 0; o < nop; ++o) {
 #pragma unroll
-      for (int c = 0; c < 4; ++c) m[o][c] = fmax(m[o][c], fabs(v[o][c]));
+      for (int c = 0; c < 4; ++c) {
+        m[o][c] = fmax(m[o][c], fabs(v[o][c]));
+        efield = max(efield, exp_field(v[o][c]));
+      }
       double2 *dst = reinterpret_cast<double2 *>(out + o * T + (size_t)g * kBlockF + 4 * lane);
       dst[0] = make_double2(v[o][0], v[o][1]);
       dst[1] = make_double2(v[o][2], v[o][3]);
     }
   }
+  report_nonfinite(efield == 0x7ffu, nonfinite);
   __syncwarp();
 #pragma unroll
   for (int o = 0; o < nop; ++o)
@@ -743,7 +769,10 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
 
 // Pass B, part 1 for builds without J: the same operands as colloc_z_kernel,
 // but phi and grad phi come back from the pass-A digits of the pair instead
-// of a second STO evaluation.  qphT[pair][comp][digit][g][f] holds
+// of a second STO evaluation.  Only the Z planes are staged: the phi plane
+// (o = 0) is left unwritten, so this kernel must be followed by
+// zquant_kernel with the pass-A digits given (pass_b(c, true)), which takes
+// phi from those digits.  qphT[pair][comp][digit][g][f] holds
 // X = d0 2^24 + d1 2^16 + d2 2^8 + d3 with x = X s_g 2^-30 (s_g the
 // power-of-two scale of point g over the block), so the recovered values
 // differ from the collocation by less than 2^-31 s_g.
@@ -753,7 +782,7 @@ __global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__
                                                               const int *__restrict__ pair_batch, long p0,
                                                               const double *__restrict__ coef, long npad,
                                                               double *__restrict__ ws, double *__restrict__ sph,
-                                                              double *__restrict__ szs) {
+                                                              double *__restrict__ szs, int *nonfinite) {
   constexpr int NC = GRAD ? 4 : 1;
   constexpr int nz = NZ, nop = 1 + NZ;
   __shared__ double red[8][4][128];
@@ -767,6 +796,7 @@ __global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__
 #pragma unroll
     for (int c = 0; c < 4; ++c) m[o][c] = 0.0;
   double *out = ws + qrel * 4 * T;
+  unsigned efield = 0;  // largest exponent field of the Z values (0x7ff: non-finite)
   for (int g = warp; g < kBatch; g += 8) {
     const long gg = (long)b * kBatch + g;
     double v[NC][4];
@@ -805,13 +835,17 @@ __global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__
 #pragma unroll
     for (int o = 0; o < nop; ++o) {
 #pragma unroll
-      for (int c = 0; c < 4; ++c) m[o][c] = fmax(m[o][c], fabs(z[o][c]));
+      for (int c = 0; c < 4; ++c) {
+        m[o][c] = fmax(m[o][c], fabs(z[o][c]));
+        efield = max(efield, exp_field(z[o][c]));
+      }
       if (o == 0) continue;  // zquant takes phi from the digits again
       double2 *dst = reinterpret_cast<double2 *>(out + o * T + (size_t)g * kBlockF + 4 * lane);
       dst[0] = make_double2(z[o][0], z[o][1]);
       dst[1] = make_double2(z[o][2], z[o][3]);
     }
   }
+  report_nonfinite(efield == 0x7ffu, nonfinite);
 #pragma unroll
   for (int o = 0; o < nop; ++o)
 #pragma unroll
@@ -975,7 +1009,6 @@ struct MixedState {
   // grad mode: T0 and (C occ) digits with their row scales
   uint8_t *qt0 = nullptr, *qco = nullptr;
   double *st0 = nullptr, *sco = nullptr;
-  int *err = nullptr;
   CUtensorMap m_phT, m_ph, m_z, m_ct, m_t0, m_co;
   std::vector<void *> bufs;
   ~MixedState() {
@@ -1016,7 +1049,6 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     M->sph = M->alloc<double>(M->cap * 128);
     M->qz = M->alloc<uint8_t>(M->cap * 3 * 4 * tile);
     M->sz = M->alloc<double>(M->cap * 3 * 128);
-    M->err = M->alloc<int>(1);
     M->m_phT = make_map3(M->qphT, 128, 256, M->cap * 4 * 4, 128);
     M->m_ph = make_map3(M->qph, 256, 128, M->cap * 4, 128);
     M->m_z = make_map3(M->qz, 256, 128, M->cap * 3 * 4, 128);
@@ -1071,7 +1103,7 @@ static void launch_colloc_z_g(Plan &P, MixedState &M, const Chunk &c, int nzs, i
   const unsigned np = (unsigned)(c.p1 - c.p0);
 #define NKX_CZ(NZ)                                                                                                   \
   colloc_z_kernel<GRAD, NZ><<<np, 256, 0, s>>>(P.d_sto, P.d_fshell, P.d_bshell, P.d_bnshell, P.d_px, P.d_py, P.d_pz, P.d_pair_batch, P.d_pair_blk, c.p0, \
-                                               P.d_coef, P.d_vj, nspin, P.npad, P.ws_phi, M.sph, M.sz)
+                                               P.d_coef, P.d_vj, nspin, P.npad, P.ws_phi, M.sph, M.sz, P.d_status + 1)
   if (nzs == 1)
     NKX_CZ(1);
   else if (nzs == 2)
@@ -1094,11 +1126,10 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
   const int nc = P.gga ? 4 : 1;
   const int nzs = nspin + (separateJ ? 1 : 0);
   NKX_REQUIRE(nzs <= 3, NKX_ERR_ARG, "too many Z planes");
-  NKX_CUDA(cudaMemsetAsync(M.err, 0, sizeof(int), s));
   {
     const long rows = (long)nspin * M.nocc_pad * P.nblk;
     quant_ct_kernel<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(P.d_Ct, nocc, M.nocc_pad, nspin, P.nbf_pad,
-                                                                         P.nblk, M.qct, M.sct);
+                                                                         P.nblk, M.qct, M.sct, P.d_status + 1);
     NKX_LAUNCH_CHECK();
     ++P.launches;
   }
@@ -1123,10 +1154,10 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       Tm.begin(ST_COLLOC, s);
       if (P.gga)
         colloc_quantT_kernel<true><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_fshell, P.d_bshell, P.d_bnshell, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
-                                                                P.d_pair_blk, c.p0, M.qphT, M.sphT);
+                                                                P.d_pair_blk, c.p0, M.qphT, M.sphT, P.d_status + 1);
       else
         colloc_quantT_kernel<false><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_fshell, P.d_bshell, P.d_bnshell, P.d_px, P.d_py, P.d_pz, P.d_pair_batch,
-                                                                 P.d_pair_blk, c.p0, M.qphT, M.sphT);
+                                                                 P.d_pair_blk, c.p0, M.qphT, M.sphT, P.d_status + 1);
       NKX_LAUNCH_CHECK();
       ++P.launches;
       Tm.end(s);
@@ -1150,7 +1181,9 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.ntile_i = M.nocc_pad / TcShape<TC_MODE_DENSITY>::N;
     a.nocc_pad = M.nocc_pad;
     a.T = M.T;
-    a.err = M.err;
+    a.err = P.d_status;
+    a.wait_ns = P.wait_ns;
+    a.stall = P.stall_test;
     a.nunits = nb * nspin * 2 * a.ncomp * a.ntile_i;
     launch_i8(M, M.m_phT, M.m_ct, a, s);
     ++P.launches;
@@ -1181,7 +1214,9 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       g.ncs = nc;
       g.nocc_pad = M.nocc_pad;
       g.Y = P.ws_phi;  // free during pass A: the FP64 staging of pass B
-      g.err = M.err;
+      g.err = P.d_status;
+      g.wait_ns = P.wait_ns;
+      g.stall = P.stall_test;
       g.nunits = np * nspin * 4;
       launch_i8(M, M.m_t0, M.m_co, g, s);
       ++P.launches;
@@ -1219,7 +1254,9 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.sA = M.sph;
     a.sB = M.sz;
     a.V = P.d_V;
-    a.err = M.err;
+    a.err = P.d_status;
+    a.wait_ns = P.wait_ns;
+    a.stall = P.stall_test;
     // too few output tiles for the SMs: split the chunk's batches
     const long tiles = (long)nzs * P.nblk * P.nblk;
     a.nsplit = tiles >= M.nsm ? 1 : (int)std::min<long>({(M.nsm + tiles - 1) / tiles, c.b1 - c.b0, 16L});
@@ -1251,7 +1288,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       Tm.begin(ST_ZBUILD, s);
 #define NKX_ZD(G, NZ)                                                                                               \
   z_from_digits_kernel<G, NZ><<<(unsigned)np, 256, 0, s>>>(M.qphT, M.sphT, P.d_pair_batch, c.p0, P.d_coef, P.npad, \
-                                                           P.ws_phi, M.sph, M.sz)
+                                                           P.ws_phi, M.sph, M.sz, P.d_status + 1)
       if (P.gga) {
         if (nspin == 1)
           NKX_ZD(true, 1);
@@ -1294,10 +1331,6 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       pass_b(c, false);
     }
   }
-  int herr = 0;
-  NKX_CUDA(cudaMemcpyAsync(&herr, M.err, sizeof(int), cudaMemcpyDeviceToHost, s));
-  NKX_CUDA(cudaStreamSynchronize(s));
-  NKX_REQUIRE(herr == 0, NKX_ERR_TIMEOUT, "tensor-core kernel wait timed out (code " + std::to_string(herr) + ")");
 }
 
 void destroy_mixed_state(void *p) { delete static_cast<MixedState *>(p); }

@@ -1,6 +1,6 @@
 // Thin inline-PTX layer for the sm_100a tensor-core kernels: mbarriers,
 // TMA tile loads into the CTA's own shared memory, tcgen05 MMA / TMEM.  Every wait is
-// bounded: after kWaitLimitNs of global time it raises an error flag and
+// bounded: after its limit of global time it raises an error flag and
 // returns false, so no kernel can spin forever.
 #pragma once
 
@@ -10,7 +10,11 @@
 namespace nkx {
 namespace tc {
 
-constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
+// Default limit of the waits that can be abandoned (a plan may shorten it),
+// and the fixed limit of the drain waits at the end of a kernel, which only
+// wait for TMA copies and MMAs that were already issued.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;   // 2 s
+constexpr unsigned long long kDrainLimitNs = 2000000000ull;  // 2 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -44,16 +48,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait for the phase with the given parity to complete.  On timeout
-// records `code` in *err and returns false.
+// (limit_ns of global time) records `code` in *err, raises *abort_flag and
+// returns false; it also returns false once another thread raised the flag.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code,
-                                          volatile int *abort_flag) {
+                                          volatile int *abort_flag, unsigned long long limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = globaltimer();
   for (uint32_t it = 1;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 255u) == 0) {
       if (*abort_flag) return false;
-      if (globaltimer() - t0 > kWaitLimitNs) {
+      if (globaltimer() - t0 > limit_ns) {
         atomicCAS(err, 0, code);
         *abort_flag = 1;
         return false;

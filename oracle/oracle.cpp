@@ -188,20 +188,30 @@ cplx f_vwn5(cplx ra, cplx rb) {
   return rho * (eP + eA * fz / fpp0 * (1.0 - z4) + (eF - eP) * fz * z4);
 }
 
-// Perdew-Wang 92 correlation energy per particle (modified constants)
+// Perdew-Wang 92 correlation energy per particle (Phys. Rev. B 45, 13244
+// (1992), eqs. 8-10 and Table I); mod: the more precise constants of
+// libxc's LDA_C_PW_MOD, used inside PBE correlation; otherwise the published
+// ones (libxc's LDA_C_PW, the reference driver's default correlation
+// lda_c_pw, tests/standalone.cxx:88, standalone_helpers.hpp:191-192)
 cplx pw92_g(cplx rs, double A, double a1, double b1, double b2, double b3, double b4) {
   const cplx srs = std::sqrt(rs);
   const cplx den = 2.0 * A * (b1 * srs + b2 * rs + b3 * rs * srs + b4 * rs * rs);
   return -2.0 * A * (1.0 + a1 * rs) * std::log(1.0 + 1.0 / den);
 }
-cplx eps_pw92(cplx rs, cplx zeta, cplx opz, cplx omz) {
-  const cplx gP = pw92_g(rs, 0.0310907, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294);
-  const cplx gF = pw92_g(rs, 0.01554535, 0.20548, 14.1189, 6.1977, 3.3662, 0.62517);
-  const cplx gA = pw92_g(rs, 0.0168869, 0.11125, 10.357, 3.6231, 0.88026, 0.49671);
-  const double fz20 = 1.709920934161365617563962776245;
+cplx eps_pw92(cplx rs, cplx zeta, cplx opz, cplx omz, bool mod = true) {
+  const cplx gP = pw92_g(rs, mod ? 0.0310907 : 0.031091, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294);
+  const cplx gF = pw92_g(rs, mod ? 0.01554535 : 0.015545, 0.20548, 14.1189, 6.1977, 3.3662, 0.62517);
+  const cplx gA = pw92_g(rs, mod ? 0.0168869 : 0.016887, 0.11125, 10.357, 3.6231, 0.88026, 0.49671);
+  const double fz20 = mod ? 1.709920934161365617563962776245 : 1.709921;
   const cplx fz = fzeta(opz, omz);
   const cplx z4 = zeta * zeta * zeta * zeta;
   return gP - gA * fz / fz20 * (1.0 - z4) + (gF - gP) * fz * z4;
+}
+
+cplx f_pw92(cplx ra, cplx rb, bool mod) {
+  const cplx rho = ra + rb;
+  const cplx rs = cbrt_c(3.0 / (4.0 * kPi * rho));
+  return rho * eps_pw92(rs, (ra - rb) / rho, 2.0 * ra / rho, 2.0 * rb / rho, mod);
 }
 
 // PBE exchange, unpolarised form per volume of a closed-shell density n
@@ -242,6 +252,8 @@ cplx f_total(int id, const cplx in[5]) {
   switch (id) {
     case 1: return f_lda_x(in[0], in[1]);
     case 7: return f_vwn5(in[0], in[1]);
+    case 12: return f_pw92(in[0], in[1], false);
+    case 13: return f_pw92(in[0], in[1], true);
     case 101: return f_pbe_x(in[0], in[1], in[2], in[4]);
     case 130: return f_pbe_c(in[0], in[1], in[2] + 2.0 * in[3] + in[4]);
     default: throw std::runtime_error("oracle: unsupported functional id");

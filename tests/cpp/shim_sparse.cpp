@@ -213,23 +213,37 @@ int main() {
   DeviceView1D occ_a = vec({1.0, 1.0});
   const XcInfo lda_x{1}, vwn{7}, pbe_x{101}, pbe_c{130};
   const XcInfo *ids[4] = {&lda_x, &vwn, &pbe_x, &pbe_c};
-  double xc_dE = 0.0, xc_dV = 0.0, xc_E[4];
+  double xc_dE = 0.0, xc_dV = 0.0, xc_E[4], mixed_dE = 0.0, mixed_dV = 0.0;
   for (int k = 0; k < 4; ++k) {
     XcFunc f{ids[k]};
-    XC_result_polarized s, d;
+    XC_result_polarized s, d, m;
     if (k < 2) {
       s = compute_lsda_sparse(basis, grid, nl, mo, occ_a, mo_b, occ_b, f);
       d = compute_lsda(phi, grid.weights, mo, occ_a, mo_b, occ_b, f);
+      set_precision(NKX_PREC_MIXED);
+      m = compute_lsda_sparse(basis, grid, nl, mo, occ_a, mo_b, occ_b, f);
     } else {
       s = compute_gga_lsda_sparse(basis, grid, nl, mo, occ_a, mo_b, occ_b, f);
       d = compute_gga_lsda(phi, gx, gy, gz, grid.weights, mo, occ_a, mo_b, occ_b, f);
+      set_precision(NKX_PREC_MIXED);
+      m = compute_gga_lsda_sparse(basis, grid, nl, mo, occ_a, mo_b, occ_b, f);
     }
+    set_precision(NKX_PREC_FP64);
+    // the tensor-core path selected by set_precision, against the FP64 sparse result
+    mixed_dE = std::max(mixed_dE, std::fabs(m.energy - s.energy));
+    mixed_dV = std::max({mixed_dV,
+                         max_abs_diff(nkx_shim::copy_to_host(m.potential_alpha), nkx_shim::copy_to_host(s.potential_alpha)),
+                         max_abs_diff(nkx_shim::copy_to_host(m.potential_beta), nkx_shim::copy_to_host(s.potential_beta))});
     xc_E[k] = s.energy;
     xc_dE = std::max(xc_dE, std::fabs(s.energy - d.energy));
     xc_dV = std::max({xc_dV,
                       max_abs_diff(nkx_shim::copy_to_host(s.potential_alpha), nkx_shim::copy_to_host(d.potential_alpha)),
                       max_abs_diff(nkx_shim::copy_to_host(s.potential_beta), nkx_shim::copy_to_host(d.potential_beta))});
   }
+  set_precision(NKX_PREC_MIXED);
+  DeviceView2DLeft Jm = compute_coulomb_sparse(space, mo, occ, basis, basis_aux, grid, nl, X);
+  set_precision(NKX_PREC_FP64);
+  const double J_mixed_vs_fp64 = max_abs_diff(nkx_shim::copy_to_host(Jm), nkx_shim::copy_to_host(Js));
   int family_checked = 0;
   try {
     XcFunc f{&pbe_x};
@@ -247,11 +261,11 @@ int main() {
       "\"E_pbe_x\": %.12g, \"E_pbe_c\": %.12g, \"family_checked\": %d, \"K_dense_h1s\": %.17g, "
       "\"K_sparse_h1s\": %.17g, \"K_tiled_h1s\": %.17g, \"K_tiled_vs_sparse\": %.3e, \"K_sparse_vs_dense\": %.3e, "
       "\"K_scale\": %.6g, \"S00\": %.17g, \"T00\": %.17g, \"V00\": %.17g, \"H00\": %.17g, "
-      "\"coreH_screened_diff\": %.3e}\n",
+      "\"coreH_screened_diff\": %.3e, \"mixed_dE\": %.3e, \"mixed_dV\": %.3e, \"J_mixed_vs_fp64\": %.3e}\n",
       J_sparse_h1s, J_tiled_h1s, boxes_ok, weights_permuted, nl_ok, nb.size(), metric_tiled_vs_sparse,
       J_tiled_vs_sparse, J_sparse_vs_dense, J_scale, rho_sparse_vs_dense, grad_sparse_vs_dense, sigma_sparse_vs_dense,
       sigma_scale, rho_accumulated, xc_dE, xc_dV, xc_E[0], xc_E[1], xc_E[2], xc_E[3], family_checked, K_dense_h1s,
       K_sparse_h1s, K_tiled_h1s, K_tiled_vs_sparse, K_sparse_vs_dense, K_scale, S00, T00, V00, H00,
-      coreH_screened_diff);
+      coreH_screened_diff, mixed_dE, mixed_dV, J_mixed_vs_fp64);
   return 0;
 }

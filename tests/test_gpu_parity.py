@@ -121,8 +121,11 @@ def test_becke_screening_exact_on_cluster():
 
 
 def test_collocation_matches_oracle():
+    # every l the device supports (l <= 7), values and gradients; the
+    # oracle's harmonics are pinned to the reference's definition for l <= 7
+    # in test_oracle_golden.py
     funcs = [(l + 1 + k, l, m, 0.7 + 0.9 * k, 0.1 * l, -0.2, 0.3 * k)
-             for l in range(0, 5) for m in range(-l, l + 1) for k in range(2)]
+             for l in range(0, 8) for m in range(-l, l + 1) for k in range(2)]
     b, ob = basis_pair(funcs)
     pts = np.random.default_rng(1).normal(scale=1.5, size=(500, 3))
     d = [x.cpu().numpy() for x in A.fill_grad_collocation(b, pts)]
@@ -131,7 +134,7 @@ def test_collocation_matches_oracle():
         np.testing.assert_allclose(x, y, rtol=1e-12, atol=1e-14 * np.abs(y).max())
 
 
-@pytest.mark.parametrize("fid", [1, 7, 101, 130])
+@pytest.mark.parametrize("fid", [1, 7, 12, 13, 101, 130])
 @pytest.mark.parametrize("nspin", [1, 2])
 def test_functionals_match_oracle(fid, nspin):
     rng = np.random.default_rng(fid + nspin)

@@ -100,3 +100,7 @@ def test_sparse_shims_match_reference_and_dense(tmp_path):
     assert out["V00"] == pytest.approx(-1.0, abs=1e-6)
     assert out["H00"] == pytest.approx(out["T00"] + out["V00"], abs=1e-14)
     assert out["coreH_screened_diff"] <= 1e-6
+    # set_precision(NKX_PREC_MIXED) moves the sparse XC and J onto the
+    # tensor-core build: within the mixed scheme's gate of the FP64 results
+    assert out["mixed_dE"] <= 1e-6 and out["mixed_dV"] <= 1e-7
+    assert out["J_mixed_vs_fp64"] <= 1e-7 * max(1.0, out["J_scale"])
