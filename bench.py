@@ -65,6 +65,10 @@ def parse():
                     help="skip the same-GPU FP64 comparison build (for very large workloads)")
     ap.add_argument("--no-scf", action="store_true",
                     help="skip the water SCF (Slater + VWN5, SCF to 1e-8 Eh) reported beside the headline")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the plan's default kernel choices")
+    ap.add_argument("--aggregate-gate", type=int, default=1500,
+                    help="also time and gate the mixed vs FP64 build of the C/H/N/O aggregate of this many atoms "
+                         "beside the headline (0: skip)")
     ap.add_argument("--workspace-mb", type=int, default=0,
                     help="cap on the per-chunk collocation workspace in MiB (0: automatic); more chunks, same work")
     return ap.parse_args()
@@ -369,6 +373,52 @@ def xc_gradient_check(n, stream, ngeom=10, ncomp=1, h=1e-4):
             "fd": "Richardson-extrapolated central differences, h = 1e-4 and 5e-5 bohr, FP64 GPU E_xc"}
 
 
+def aggregate_gate(natoms, stream):
+    """Survey configuration 5: the seeded C/H/N/O aggregate (3:5:1:1, random
+    packing in a sphere, d_min 1.0 A, ~12000 STO functions, ~3e7 points),
+    PBE, nocc = electrons / 2: one warm-up and one timed mixed build, one
+    timed FP64 build of the same plan, and the accuracy gate of the mixed
+    build against it (|dE_xc| <= 1e-6 Eh, max|dV| <= 1e-7), all on the device
+    (CUDA events on the launching stream)."""
+    import torch
+    from nukexc_b200 import api as A
+    c, Z, funcs, Cm = workload(0, natoms)
+    t0 = time.perf_counter()
+    g = A.make_flat_grid(c, Z, 75, 29, weight_threshold=1e-15, radial="ta")
+    fb = A.FockBuilder(c, Z, A.make_manual_basis(funcs), g, func_ids=FUNCS)
+    setup = time.perf_counter() - t0
+    info = fb.info()
+    Cd = torch.as_tensor(Cm, device="cuda")
+    od = torch.ones(Cm.shape[1], dtype=torch.float64, device="cuda")
+    out = {"workload": f"C/H/N/O aggregate, {natoms} atoms, PBE XC Fock build", "npoints": int(info["npoints"]),
+           "nbf": len(funcs), "nocc": int(Cm.shape[1]), "npairs": int(info["npairs"]), "setup_s": setup}
+
+    def timed(prec):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        E, V, _ = fb.build([Cd], [od], precision=prec, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return E, V[0], e0.elapsed_time(e1), fb.timing()
+
+    fb.build([Cd], [od], precision="mixed", stream=stream.cuda_stream)  # warm-up
+    Em, Vm, ms_m, tm = timed("mixed")
+    Vm = Vm.clone()
+    Ed, Vd, ms_d, td = timed("fp64")
+    out.update({"mixed_ms_per_build": ms_m, "mixed_points_per_s": info["npoints"] / (ms_m * 1e-3),
+                "mixed_stage_ms": {k: v for k, v in tm.items() if k.endswith("_ms")},
+                "launches_per_mixed_build": tm["launches"], "nchunks": int(fb.info()["nchunks"]),
+                "fp64_ms_per_build": ms_d, "fp64_stage_ms": {k: v for k, v in td.items() if k.endswith("_ms")},
+                "mixed_speedup": ms_d / ms_m,
+                "accuracy": {"dE_xc": abs(Em - Ed), "max_abs_dV": float((Vm - Vd).abs().max()), "E_xc_fp64": Ed,
+                             "gate": "dE<=1e-6 Eh, max|dV|<=1e-7"}})
+    fb.close()
+    del Vm, Vd
+    torch.cuda.empty_cache()
+    return out
+
+
 def scf_water():
     """Water, Slater + VWN5, TA-M4 75 x Lebedev 302, closed-shell SCF to 1e-8
     Eh with the stand-in driver: on the GPU in FP64 and mixed precision, and
@@ -440,16 +490,20 @@ def run_nkx(args):
 
     c, Z, funcs, Cm = workload(args.waters, args.aggregate)
     g = A.make_flat_grid(c, Z, 75, 29, weight_threshold=1e-15, radial="ta")
-    # strong scaling: rank r integrates the points of its share of atoms
-    sel = S.select_points(g.point_owner, len(Z), rank, world)
-    pts, w = g.quad_points[sel], g.weights[sel]
     b = A.make_manual_basis(funcs)
+    # strong scaling: rank r integrates a Morton-contiguous, cost-balanced
+    # range of the grid's 256-point batches
+    if world > 1:
+        sel = S.balanced_split(g.quad_points, b.center, A.cutoff_radii(b), Cm.shape[1], world)[rank]
+    else:
+        sel = np.arange(len(g.weights))
+    pts, w = g.quad_points[sel], g.weights[sel]
     t0 = time.perf_counter()
-    if args.aux and world > 1:
-        raise SystemExit("--aux: the fitted J needs the all-reduced y before the solve; run it on one GPU")
     aux = A.make_manual_basis(M.aux_basis(c, Z)) if args.aux else None
     fb = A.FockBuilder(c, Z, b, (pts, w), aux=aux, func_ids=FUNCS, workspace_bytes=args.workspace_mb << 20)
     fuse = bool(args.aux)
+    if aux is not None and dist is not None:
+        S.shard_metric(fb, dist)  # the whole grid's (A|B), once per geometry
     setup_s = time.perf_counter() - t0
     info = fb.info()
     nbf = len(funcs)
@@ -464,8 +518,23 @@ def run_nkx(args):
             prec = "mixed"
         except Exception:
             prec = "fp64"
+    tuning = None
+    if prec == "mixed" and not args.no_autotune:
+        # the plan's autotuner picks the MMA widths, the Y path and the chunk
+        # size by timing whole builds (untimed setup)
+        t0 = time.perf_counter()
+        tuning = fb.autotune([Cd], [od], stream=stream.cuda_stream)
+        tuning["seconds"] = time.perf_counter() - t0
+        info = fb.info()
 
     def step(host=False):
+        if fuse and dist is not None:
+            # J on a sharded grid: density, all-reduce of the fit vector y,
+            # then the rest of the build; E and V all-reduced inside
+            Cs, os_ = ([Cm], [occ]) if host else ([Cd], [od])
+            E, _, _ = S.sharded_build(fb, Cs, os_, dist, precision=prec, want_J=False, fuse_j=True,
+                                      stream=stream.cuda_stream)
+            return E
         if host:
             E, V, _ = fb.build([Cm], [occ], precision=prec, fuse_j=fuse, stream=stream.cuda_stream)
             # the all-reduce of several ranks needs V back on the device
@@ -599,8 +668,11 @@ def run_nkx(args):
             "data": "synthetic",
             "config": config(args, {"precision": prec, "npoints": total_pts, "nbf": nbf,
                                     "nbatches": info["nbatches"], "npairs": info["npairs"],
-                                    "nchunks": info["nchunks"], "plan_setup_s": setup_s,
-                                    "parallelism": f"grid split by atoms over {world} GPU(s)"}),
+                                    "nchunks": info["nchunks"], "plan_setup_s": setup_s, "autotune": tuning,
+                                    "parallelism": (f"grid split into {world} Morton-contiguous, cost-balanced batch "
+                                                    f"ranges, one GPU each; all-reduce of E, V"
+                                                    + (" and of the J fit vector y" if fuse else "")
+                                                    if world > 1 else "one GPU")}),
             "stage_ms_per_step": {k: v / args.steps for k, v in stage.items() if k.endswith("_ms")},
             "roofline": {"bound": "tensor", "kernel": "vgemm (V = Phi Z^T)", "achieved": ach, "peak": peak,
                          "unit": unit, "frac": ach / peak,
@@ -631,6 +703,8 @@ def run_nkx(args):
             line["xc_gradient"] = xc_gradient_check(args.grad_waters, stream)
         if world == 1 and not args.no_scf:
             line["scf_water"] = scf_water()
+        if world == 1 and args.aggregate_gate > 0 and not args.aggregate:
+            line["aggregate_gate"] = aggregate_gate(args.aggregate_gate, stream)
         print(json.dumps(line), flush=True)
     fb.close()
     if dist is not None:

@@ -269,6 +269,62 @@ NKX_API nkx_status nkx_fock_build(nkx_plan *plan, int precision, int nspin, int 
                                   const double *occ, int mem, int fuse_j, double *E, double *V, double *J,
                                   void *stream);
 
+/* Two-phase Fock build for a grid sharded over ranks (one process per GPU,
+ * one plan per rank made from the points that rank integrates).  The grid
+ * RI-J fit (nukexc/coulomb.hpp:84-95) needs the whole grid's fit vector
+ * y = Vw rho before any potential, so the build is split around that
+ * exchange, which the caller performs (e.g. ncclAllReduce on `stream`):
+ *   phase 1: C and occ in (as nkx_fock_build), the density pass, and this
+ *            rank's share of y (naux doubles) written to y;
+ *   caller:  y_total = sum of y over the ranks;
+ *   phase 2: y_total in; c = (A|B)^-1 y_total with the plan's metric (set it
+ *            to the all-reduced full-grid metric with nkx_plan_set_metric),
+ *            the functional, V and J on this rank's points.  E, V, J as in
+ *            nkx_fock_build are this rank's partial sums, to be all-reduced.
+ * Phase 2 must follow phase 1 on the same plan; it reuses phase 1's
+ * precision, spin count and orbitals.  y and the outputs follow `mem`.
+ * No counterpart in the reference (a single device). */
+NKX_API nkx_status nkx_fock_build_phase1(nkx_plan *plan, int precision, int nspin, int nocc, const double *C,
+                                         const double *occ, int mem, double *y, void *stream);
+NKX_API nkx_status nkx_fock_build_phase2(nkx_plan *plan, const double *y, int mem, int fuse_j, double *E, double *V,
+                                         double *J, void *stream);
+
+/* Replace the plan's Coulomb metric (A|B) (naux x naux, symmetric,
+ * column-major; mem: host or device) and factor it again the way the plan
+ * was created (pivoted Cholesky, or the half inverse when metric_svd_thr > 0;
+ * a half inverse set with nkx_plan_set_half_inverse is dropped).  For a
+ * sharded grid this is the sum over ranks of nkx_plan_aux_metric. */
+NKX_API nkx_status nkx_plan_set_metric(nkx_plan *plan, const double *S, int mem);
+
+/* Choices of the mixed-precision build that nkx_plan_autotune measures. */
+typedef struct {
+  int v_n;            /* tcgen05 MMA width N of the V contraction: 128 or 64 */
+  int dens_n;         /* MMA width of the density contraction: 64 or 128 */
+  int ypath;          /* GGA density gradient through Y = T0 (C occ)^T: -1 auto (from 256 orbitals), 0, 1 */
+  long chunk_pairs;   /* (batch, block) pairs per streamed chunk */
+  int from_cache;     /* out: 1 when the choices came from the cache file */
+  int trials;         /* out: builds timed */
+  float default_ms;   /* out: build time with the choices the plan had before */
+  float best_ms;      /* out: build time with the chosen ones */
+} nkx_tuning;
+
+/* Autotuner of the mixed-precision build (no counterpart in the reference:
+ * its kernels take fixed launch shapes).  With the caller's orbitals (as
+ * nkx_fock_build, XC only), it times whole builds (CUDA events) and keeps, one
+ * knob at a time with the others at their best so far: the Y path (GGA), the
+ * density MMA width, the V MMA width, and the chunk size (x1, x2, x4 of the
+ * current one while device memory allows).  With cache_path != NULL a file of
+ * earlier results keyed by the device and the problem's shape (functions,
+ * blocks, pairs, points, orbitals, spins, GGA) is read first -- a hit applies
+ * its choices without timing -- and the new result is appended.  *out (may be
+ * NULL) receives the choices and timings.  The plan keeps the choices for
+ * all later mixed builds. */
+NKX_API nkx_status nkx_plan_autotune(nkx_plan *plan, int nspin, int nocc, const double *C, const double *occ, int mem,
+                                     const char *cache_path, nkx_tuning *out, void *stream);
+NKX_API nkx_status nkx_plan_get_tuning(const nkx_plan *plan, nkx_tuning *out);
+/* Apply choices (for example a stored autotune result); chunk_pairs <= 0 keeps the chunking. */
+NKX_API nkx_status nkx_plan_set_tuning(nkx_plan *plan, const nkx_tuning *t);
+
 /* XC nuclear gradient at fixed orbitals, FP64 (no counterpart in the
  * reference): grad[3*natoms] (host, Eh/bohr) = dE_xc/dR of
  * E_xc = sum_g w_g f(rho(r_g)) with every grid point moving with its owner

@@ -26,6 +26,8 @@ EXPORTS = [
     "nkx_plan_last_density", "nkx_plan_batch_blocks", "nkx_plan_destroy", "nkx_last_error", "nkx_xc_gradient",
     "nkx_plan_set_functional", "nkx_plan_set_half_inverse", "nkx_plan_aux_metric", "nkx_plan_density",
     "nkx_morton_order", "nkx_neighbor_list", "nkx_aux_metric", "nkx_exchange_dense", "nkx_plan_set_wait_limit",
+    "nkx_fock_build_phase1", "nkx_fock_build_phase2", "nkx_plan_set_metric",
+    "nkx_plan_autotune", "nkx_plan_get_tuning", "nkx_plan_set_tuning",
 ]
 
 
@@ -62,6 +64,11 @@ class BuildTiming(C.Structure):
                 ("total_ms", C.c_float), ("launches", C.c_int)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("v_n", C.c_int), ("dens_n", C.c_int), ("ypath", C.c_int), ("chunk_pairs", C.c_long),
+                ("from_cache", C.c_int), ("trials", C.c_int), ("default_ms", C.c_float), ("best_ms", C.c_float)]
+
+
 class NkxError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"nkx status {code}: {msg}")
@@ -95,6 +102,12 @@ def lib():
             "nkx_plan_create": [vp, vp, vp, l_, vp, vp, vp, vp, vp],
             "nkx_plan_get_info": [vp, vp],
             "nkx_fock_build": [vp, i, i, i, vp, vp, i, i, vp, vp, vp, vp],
+            "nkx_fock_build_phase1": [vp, i, i, i, vp, vp, i, vp, vp],
+            "nkx_fock_build_phase2": [vp, vp, i, i, vp, vp, vp, vp],
+            "nkx_plan_set_metric": [vp, vp, i],
+            "nkx_plan_autotune": [vp, i, i, vp, vp, i, C.c_char_p, vp, vp],
+            "nkx_plan_get_tuning": [vp, vp],
+            "nkx_plan_set_tuning": [vp, vp],
             "nkx_xc_gradient": [vp, i, i, vp, vp, i, d, vp, vp],
             "nkx_get_last_timing": [vp, vp],
             "nkx_plan_last_density": [vp, vp, vp],

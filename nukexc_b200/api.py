@@ -462,6 +462,97 @@ class FockBuilder:
         check(L.lib().nkx_plan_aux_metric(self._h, S.ctypes.data_as(C.c_void_p), L.MEM_HOST))
         return S.reshape(self.naux, self.naux).T.copy()
 
+    def autotune(self, C_list, occ_list, cache_path=None, stream=None):
+        """Time the mixed build's knobs on these orbitals and keep the fastest
+        (nkx_plan_autotune); returns the choices and timings as a dict."""
+        nspin = len(C_list)
+        host = not isinstance(C_list[0], torch.Tensor)
+        nocc = C_list[0].shape[1]
+        if host:
+            Cc = np.concatenate([np.ascontiguousarray(np.asarray(c, np.float64).T).reshape(-1) for c in C_list])
+            oc = np.concatenate([_np(o, np.float64) for o in occ_list])
+            pC, po = Cc.ctypes.data_as(C.c_void_p), oc.ctypes.data_as(C.c_void_p)
+        else:
+            Cc = torch.cat([c.t().contiguous().reshape(-1) for c in C_list])
+            oc = torch.cat([o.reshape(-1) for o in occ_list]).to(torch.float64)
+            pC, po = _p(Cc), _p(oc)
+        t = L.Tuning()
+        s = C.c_void_p(stream) if stream else None
+        check(L.lib().nkx_plan_autotune(self._h, nspin, nocc, pC, po, L.MEM_HOST if host else L.MEM_DEVICE,
+                                        cache_path.encode() if cache_path else None, C.byref(t), s))
+        return {k: getattr(t, k) for k, _ in L.Tuning._fields_}
+
+    def tuning(self):
+        t = L.Tuning()
+        check(L.lib().nkx_plan_get_tuning(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in L.Tuning._fields_ if k in ("v_n", "dens_n", "ypath", "chunk_pairs")}
+
+    def set_tuning(self, v_n=128, dens_n=64, ypath=-1, chunk_pairs=0):
+        t = L.Tuning(v_n, dens_n, ypath, chunk_pairs, 0, 0, 0.0, 0.0)
+        check(L.lib().nkx_plan_set_tuning(self._h, C.byref(t)))
+
+    def set_metric(self, S):
+        """Replace the plan's Coulomb metric (A|B) (naux x naux) and factor it
+        again (nkx_plan_set_metric); for a sharded grid, the sum over ranks of
+        aux_metric()."""
+        Sa = np.asarray(S, np.float64)
+        assert Sa.shape == (self.naux, self.naux), "S must be naux x naux"
+        col = np.ascontiguousarray(Sa.T).reshape(-1)
+        check(L.lib().nkx_plan_set_metric(self._h, col.ctypes.data_as(C.c_void_p), L.MEM_HOST))
+
+    def build_phase1(self, C_list, occ_list, precision="fp64", stream=None):
+        """First half of a build on a sharded grid (nkx_fock_build_phase1):
+        the density pass and this plan's share of the J fit vector y
+        (naux; numpy for host orbitals, a CUDA tensor for device ones)."""
+        nspin = len(C_list)
+        host = not isinstance(C_list[0], torch.Tensor)
+        nocc = C_list[0].shape[1]
+        prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
+        if host:
+            Cc = np.concatenate([np.ascontiguousarray(np.asarray(c, np.float64).T).reshape(-1) for c in C_list])
+            oc = np.concatenate([_np(o, np.float64) for o in occ_list])
+            y = np.empty(self.naux)
+            pC, po, py = (a.ctypes.data_as(C.c_void_p) for a in (Cc, oc, y))
+        else:
+            Cc = torch.cat([c.t().contiguous().reshape(-1) for c in C_list])
+            oc = torch.cat([o.reshape(-1) for o in occ_list]).to(torch.float64)
+            y = torch.empty(self.naux, dtype=torch.float64, device="cuda")
+            pC, po, py = _p(Cc), _p(oc), _p(y)
+        s = C.c_void_p(stream) if stream else None
+        check(L.lib().nkx_fock_build_phase1(self._h, prec, nspin, nocc, pC, po, L.MEM_HOST if host else L.MEM_DEVICE,
+                                            py, s))
+        self._phase_nspin = nspin
+        return y
+
+    def build_phase2(self, y_total, want_J=False, fuse_j=False, stream=None):
+        """Second half (nkx_fock_build_phase2) with the fit vector summed over
+        the ranks; returns this plan's partial (E_xc, [V per spin], J or None)
+        like build(); host or device outputs follow y_total."""
+        nspin = self._phase_nspin
+        host = not isinstance(y_total, torch.Tensor)
+        nn = self.nbf * self.nbf
+        if host:
+            yv = _np(y_total, np.float64)
+            V = np.empty(nspin * nn)
+            J = np.empty(nn) if want_J and not fuse_j else None
+            py, pV, pJ = (a.ctypes.data_as(C.c_void_p) if a is not None else None for a in (yv, V, J))
+        else:
+            yv = y_total.to(torch.float64).contiguous()
+            V = torch.empty(nspin * nn, dtype=torch.float64, device="cuda")
+            J = torch.empty(nn, dtype=torch.float64, device="cuda") if want_J and not fuse_j else None
+            py, pV, pJ = _p(yv), _p(V), _p(J)
+        E = C.c_double(0)
+        s = C.c_void_p(stream) if stream else None
+        check(L.lib().nkx_fock_build_phase2(self._h, py, L.MEM_HOST if host else L.MEM_DEVICE, 1 if fuse_j else 0,
+                                            C.byref(E), pV, pJ, s))
+        if host:
+            Vs = [V[k * nn:(k + 1) * nn].reshape(self.nbf, self.nbf) for k in range(nspin)]
+            Jm = J.reshape(self.nbf, self.nbf) if J is not None else None
+        else:
+            Vs = [V[k * nn:(k + 1) * nn].view(self.nbf, self.nbf).t() for k in range(nspin)]
+            Jm = J.view(self.nbf, self.nbf).t() if J is not None else None
+        return E.value, Vs, Jm
+
     def batch_blocks(self):
         """Significant 128-function blocks per batch."""
         n = self.info()["nbatches"]

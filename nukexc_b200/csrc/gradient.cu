@@ -284,26 +284,14 @@ __device__ __forceinline__ void becke_s_ds(double mu, double &s, double &ds) {
   ds = -0.5 * (1.5 - 1.5 * p2 * p2) * (1.5 - 1.5 * p1 * p1) * (1.5 - 1.5 * mu * mu);
 }
 
-__device__ __forceinline__ double cell_P(const double *__restrict__ C, int natoms, const double r[3], int i,
-                                         double clamp) {
-  const double ri = sqrt((r[0] - C[3 * i]) * (r[0] - C[3 * i]) + (r[1] - C[3 * i + 1]) * (r[1] - C[3 * i + 1]) +
-                         (r[2] - C[3 * i + 2]) * (r[2] - C[3 * i + 2]));
-  double P = 1.0;
-  for (int j = 0; j < natoms && P != 0.0; ++j) {
-    if (j == i) continue;
-    const double dx = C[3 * i] - C[3 * j], dy = C[3 * i + 1] - C[3 * j + 1], dz = C[3 * i + 2] - C[3 * j + 2];
-    double Rij = sqrt(dx * dx + dy * dy + dz * dz);
-    if (clamp > 0.0) Rij = fmin(Rij, clamp);
-    const double rj = sqrt((r[0] - C[3 * j]) * (r[0] - C[3 * j]) + (r[1] - C[3 * j + 1]) * (r[1] - C[3 * j + 1]) +
-                           (r[2] - C[3 * j + 2]) * (r[2] - C[3 * j + 2]));
-    double mu = (ri - rj) / Rij;
-    mu = mu > 1.0 ? 1.0 : (mu < -1.0 ? -1.0 : mu);
-    double s, ds;
-    becke_s_ds(mu, s, ds);
-    P *= s;
-  }
-  return P;
-}
+// Atoms that can contribute at a point: with the Laqua clamp Rc, a cell i
+// with r_i >= r_min + Rc has P_i = 0 exactly (the nearest atom gives
+// mu >= 1), and a factor j with r_j >= r_i + Rc is exactly 1 with s' = 0
+// (mu <= -1), so every non-trivial cell, factor and derivative term involves
+// only atoms with r < r_min + 2 Rc -- the same exact screening as
+// becke_kernel.  Without the clamp, or when more than kGradList atoms are that
+// close, the loops run over all atoms.
+constexpr int kGradList = 192;
 
 __global__ void becke_grad_kernel(const double *__restrict__ C, int natoms, const double *__restrict__ px,
                                   const double *__restrict__ py, const double *__restrict__ pz,
@@ -320,23 +308,66 @@ __global__ void becke_grad_kernel(const double *__restrict__ C, int natoms, cons
   if (g < npad && w[g] != 0.0 && edens[g] != 0.0) {
     const double r[3] = {px[g], py[g], pz[g]};
     const int o = owner[g];
+    auto dist = [&](int a) {
+      const double dx = r[0] - C[3 * a], dy = r[1] - C[3 * a + 1], dz = r[2] - C[3 * a + 2];
+      return sqrt(dx * dx + dy * dy + dz * dz);
+    };
+    int list[kGradList];
+    int nl = 0;
+    bool full = !(clamp > 0.0);
+    double rmin = 1e300;
+    if (!full) {
+      for (int a = 0; a < natoms; ++a) rmin = fmin(rmin, dist(a));
+      for (int a = 0; a < natoms; ++a)
+        if (dist(a) < rmin + 2.0 * clamp) {
+          if (nl == kGradList) {
+            full = true;
+            break;
+          }
+          list[nl++] = a;
+        }
+    }
+    const int n = full ? natoms : nl;
+    auto atom = [&](int k) { return full ? k : list[k]; };
+    // P_i over the candidate set (factors of the other atoms are exactly 1)
+    auto cellP = [&](int i) {
+      const double ri = dist(i);
+      if (!full && ri >= rmin + clamp) return 0.0;
+      double P = 1.0;
+      for (int c = 0; c < n && P != 0.0; ++c) {
+        const int j = atom(c);
+        if (j == i) continue;
+        const double dx = C[3 * i] - C[3 * j], dy = C[3 * i + 1] - C[3 * j + 1], dz = C[3 * i + 2] - C[3 * j + 2];
+        double Rij = sqrt(dx * dx + dy * dy + dz * dz);
+        if (clamp > 0.0) Rij = fmin(Rij, clamp);
+        double mu = (ri - dist(j)) / Rij;
+        mu = mu > 1.0 ? 1.0 : (mu < -1.0 ? -1.0 : mu);
+        double sv, dsv;
+        becke_s_ds(mu, sv, dsv);
+        P *= sv;
+      }
+      return P;
+    };
     double Z = 0.0, Po = 0.0;
-    for (int i = 0; i < natoms; ++i) {
-      const double P = cell_P(C, natoms, r, i, clamp);
+    for (int c = 0; c < n; ++c) {
+      const int i = atom(c);
+      const double P = cellP(i);
       Z += P;
       if (i == o) Po = P;
     }
     if (Po > 0.0 && Z > 0.0) {
       const double Q = Po / Z, a = w[g] / Q, fa = edens[g] * a;
-      for (int i = 0; i < natoms; ++i) {
-        const double Pi = (i == o) ? Po : cell_P(C, natoms, r, i, clamp);
+      for (int ci = 0; ci < n; ++ci) {
+        const int i = atom(ci);
+        const double Pi = (i == o) ? Po : cellP(i);
         const double kappa = Q * ((i == o ? 1.0 : 0.0) - Pi / Z);
         if (kappa == 0.0) continue;
         double ui[3] = {r[0] - C[3 * i], r[1] - C[3 * i + 1], r[2] - C[3 * i + 2]};
         const double ri = sqrt(ui[0] * ui[0] + ui[1] * ui[1] + ui[2] * ui[2]);
         if (!(ri > 0.0)) continue;
         for (int k = 0; k < 3; ++k) ui[k] /= ri;
-        for (int j = 0; j < natoms; ++j) {
+        for (int cj = 0; cj < n; ++cj) {
+          const int j = atom(cj);
           if (j == i) continue;
           double e[3] = {C[3 * i] - C[3 * j], C[3 * i + 1] - C[3 * j + 1], C[3 * i + 2] - C[3 * j + 2]};
           const double dij = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
@@ -347,10 +378,10 @@ __global__ void becke_grad_kernel(const double *__restrict__ C, int natoms, cons
           if (!(rj > 0.0)) continue;
           const double mu = (ri - rj) / Rij;
           if (!(mu > -1.0 && mu < 1.0)) continue;  // clamped: s' = 0
-          double s, ds;
-          becke_s_ds(mu, s, ds);
-          if (!(s > 0.0)) continue;
-          const double lam = fa * kappa * ds / s / Rij;
+          double sv, ds;
+          becke_s_ds(mu, sv, ds);
+          if (!(sv > 0.0)) continue;
+          const double lam = fa * kappa * ds / sv / Rij;
           for (int k = 0; k < 3; ++k) {
             uj[k] /= rj;
             const double ek = clamped ? 0.0 : mu * e[k] / dij;

@@ -124,113 +124,155 @@ __global__ void __launch_bounds__(256) colloc_fp64_kernel(const StoFunc *__restr
   }
 }
 
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Density of one 64-point tile of one batch for one spin, FP64.
-// T(g,i) = sum_f PhiT(g,f) Ct(i,f) over the batch's significant blocks (and
+// T(g,i) = sum_f PhiT(g,f) C(f,i) over the batch's significant blocks (and
 // the three gradient components), then rho = sum_i occ_i T^2 and
 // grad rho = 2 sum_i occ_i T grad T (density.hpp:188-255).  Thread (ty, tx)
 // owns points g = ty + 16a (a < 4) and orbitals i = tx + 16c (c < 4) of the
-// current 64-orbital tile.
+// CTA's 64-orbital tile.  The orbital tile is the fastest index of the grid,
+// so the CTAs of one 64-point slab run together and its PhiT rows come from
+// L2 after the first (at 2850 orbitals a slab serves 45 tiles); each CTA adds
+// its tile's share of rho and grad rho atomically (they are zeroed by the
+// caller).  A K step is 16 functions of one block: the
+// PhiT rows (16 contiguous functions per component and point) and the rows
+// of the function-major orbitals Cf (64 contiguous orbitals per function)
+// stream into shared memory with 16-byte cp.async copies through a ring of
+// kDStages stages while the previous steps are multiplied.
+constexpr int kDKs = 16, kDStages = 3;
 template <bool GRAD>
-__global__ void __launch_bounds__(256) density_fp64_kernel(const double *__restrict__ phiT, const double *__restrict__ Ct,
-                                                           const double *__restrict__ occ, int nocc, int nbf_pad,
-                                                           const int *__restrict__ pair_off,
+constexpr int kDStageDoubles = (GRAD ? 4 : 1) * 64 * kDKs + kDKs * 64;
+template <bool GRAD>
+constexpr int kDSmemBytes = kDStages * kDStageDoubles<GRAD> * 8;
+
+template <bool GRAD>
+__global__ void __launch_bounds__(256) density_fp64_kernel(const double *__restrict__ phiT, const double *__restrict__ Cf,
+                                                           const double *__restrict__ occ, int nocc, int nocc_pad,
+                                                           int nbf_pad, const int *__restrict__ pair_off,
                                                            const int *__restrict__ pair_blk, long b0, long p0,
                                                            double *__restrict__ rho, double *__restrict__ grad,
                                                            long npad) {
   constexpr int NC = GRAD ? 4 : 1;
-  constexpr int KS = 16;
-  __shared__ double Ps[NC][KS][64 + 1];
-  __shared__ double Cs[KS][64 + 1];
+  constexpr int SD = kDStageDoubles<GRAD>;
+  extern __shared__ __align__(16) double dsm[];  // [stage][Ps: NC x 64 points x 16 | Cs: 16 x 64 orbitals]
   const int spin = blockIdx.y;
-  const long b = b0 + blockIdx.x / 4;
-  const int g0 = (blockIdx.x % 4) * 64;
+  const int ntile = nocc_pad / 64;
+  const int i0 = (blockIdx.x % ntile) * 64;
+  const long bq = blockIdx.x / ntile;
+  const long b = b0 + bq / 4;
+  const int g0 = (int)(bq % 4) * 64;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const double *C = Ct + (size_t)spin * nocc * nbf_pad;
+  const double *C = Cf + (size_t)spin * nbf_pad * nocc_pad;
   const double *oc = occ + (size_t)spin * nocc;
   const int q0 = pair_off[b], q1 = pair_off[b + 1];
   const size_t tile = (size_t)kBatch * kBlockF;
-  double racc[4][4];
+  const int total = (q1 - q0) * (kBlockF / kDKs);  // K steps of the orbital tile
+  if (total == 0) return;  // no significant function: nothing to add
+  auto issue = [&](int t, int st) {
+    if (t < total) {
+      const int r = t;
+      const int q = q0 + r / (kBlockF / kDKs), f0 = (r % (kBlockF / kDKs)) * kDKs;
+      const double *P = phiT + (size_t)(q - p0) * NC * tile + (size_t)g0 * kBlockF + f0;
+      double *Ps = dsm + st * SD, *Cs = Ps + NC * 64 * kDKs;
+      for (int e = threadIdx.x; e < NC * 64 * (kDKs / 2); e += 256) {
+        const int row = e / (kDKs / 2), part = e % (kDKs / 2);  // row = (comp, point)
+        cp_async16(Ps + row * kDKs + 2 * part, P + (size_t)(row / 64) * tile + (size_t)(row % 64) * kBlockF + 2 * part);
+      }
+      const double *Cr = C + (size_t)(pair_blk[q] * kBlockF + f0) * nocc_pad + i0;
+      for (int e = threadIdx.x; e < kDKs * 32; e += 256) {
+        const int k = e / 32, part = e % 32;
+        cp_async16(Cs + k * 64 + 2 * part, Cr + (size_t)k * nocc_pad + 2 * part);
+      }
+    }
+    cp_async_commit();
+  };
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int st = 0; st < kDStages - 1; ++st) issue(st, st);
+  double acc[NC][4][4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) racc[a][k] = 0.0;
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[c][a][j] = 0.0;
+  for (int t = 0; t < total; ++t) {
+    cp_async_wait<kDStages - 2>();
+    __syncthreads();  // step t is visible; the stage refilled below was read in step t - 1
+    issue(t + kDStages - 1, (t + kDStages - 1) % kDStages);
+    const double *Ps = dsm + (t % kDStages) * SD, *Cs = Ps + NC * 64 * kDKs;
+#pragma unroll
+    for (int k = 0; k < kDKs; ++k) {
+      double bv[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Cs[k * 64 + tx + 16 * j];
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          const double av = Ps[(c * 64 + ty + 16 * a) * kDKs + k];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[c][a][j] = fma(av, bv[j], acc[c][a][j]);
+        }
+    }
+    if (t == total - 1) {
+      // contract over this orbital tile
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        double sm[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int i = i0 + tx + 16 * j;
+          const double o = i < nocc ? oc[i] : 0.0;
+          const double tv = acc[0][a][j];
+          sm[0] += o * tv * tv;
+          if (GRAD) {
+            sm[1] += o * tv * acc[NC > 1 ? 1 : 0][a][j];
+            sm[2] += o * tv * acc[NC > 2 ? 2 : 0][a][j];
+            sm[3] += o * tv * acc[NC > 3 ? 3 : 0][a][j];
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+          for (int off = 8; off; off >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
+        if (tx == 0) {
+          const long g = b * kBatch + g0 + ty + 16 * a;
+          atomicAdd(&rho[(size_t)spin * npad + g], sm[0]);
+          if (GRAD) {
+            atomicAdd(&grad[((size_t)spin * 3 + 0) * npad + g], 2.0 * sm[1]);
+            atomicAdd(&grad[((size_t)spin * 3 + 1) * npad + g], 2.0 * sm[2]);
+            atomicAdd(&grad[((size_t)spin * 3 + 2) * npad + g], 2.0 * sm[3]);
+          }
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
 
-  for (int i0 = 0; i0 < nocc; i0 += 64) {
-    double acc[NC][4][4];
-#pragma unroll
-    for (int c = 0; c < NC; ++c)
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[c][a][j] = 0.0;
-    for (int q = q0; q < q1; ++q) {
-      const int I = pair_blk[q];
-      const double *P = phiT + (size_t)(q - p0) * NC * tile;
-      for (int f0 = 0; f0 < kBlockF; f0 += KS) {
-        // stage PhiT(g0..g0+63, f0..f0+15) of each comp and Ct(i0..i0+63, f0..)
-        for (int e = threadIdx.x; e < NC * 64 * KS; e += 256) {
-          const int c = e / (64 * KS), r = (e / KS) % 64, k = e % KS;
-          Ps[c][k][r] = P[c * tile + (size_t)(g0 + r) * kBlockF + f0 + k];
-        }
-        for (int e = threadIdx.x; e < 64 * KS; e += 256) {
-          const int r = e / KS, k = e % KS;
-          const int i = i0 + r;
-          Cs[k][r] = i < nocc ? C[(size_t)i * nbf_pad + I * kBlockF + f0 + k] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < KS; ++k) {
-          double bv[4];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) bv[j] = Cs[k][tx + 16 * j];
-#pragma unroll
-          for (int c = 0; c < NC; ++c)
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-              const double av = Ps[c][k][ty + 16 * a];
-#pragma unroll
-              for (int j = 0; j < 4; ++j) acc[c][a][j] += av * bv[j];
-            }
-        }
-        __syncthreads();
-      }
-    }
-    // contract over this orbital tile
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      double s[4] = {0, 0, 0, 0};
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int i = i0 + tx + 16 * j;
-        const double o = i < nocc ? oc[i] : 0.0;
-        const double t = acc[0][a][j];
-        s[0] += o * t * t;
-        if (GRAD) {
-          s[1] += o * t * acc[NC > 1 ? 1 : 0][a][j];
-          s[2] += o * t * acc[NC > 2 ? 2 : 0][a][j];
-          s[3] += o * t * acc[NC > 3 ? 3 : 0][a][j];
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-#pragma unroll
-        for (int off = 8; off; off >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], off);
-        racc[a][k] += s[k];
-      }
-    }
+// Orbitals in function-major order for density_fp64_kernel:
+// Cf[spin][f][i] = Ct[spin][i][f], orbitals padded to nocc_pad with zeros.
+__global__ void transpose_orbitals_kernel(const double *__restrict__ Ct, int nocc, int nocc_pad, int nbf_pad,
+                                          double *__restrict__ Cf) {
+  __shared__ double t[32][33];
+  const int spin = blockIdx.z;
+  const int f0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r;
+    t[r][threadIdx.x] = i < nocc ? Ct[((size_t)spin * nocc + i) * nbf_pad + f0 + threadIdx.x] : 0.0;
   }
-  if (tx == 0) {
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const long g = b * kBatch + g0 + ty + 16 * a;
-      rho[(size_t)spin * npad + g] = racc[a][0];
-      if (GRAD) {
-        grad[((size_t)spin * 3 + 0) * npad + g] = 2.0 * racc[a][1];
-        grad[((size_t)spin * 3 + 1) * npad + g] = 2.0 * racc[a][2];
-        grad[((size_t)spin * 3 + 2) * npad + g] = 2.0 * racc[a][3];
-      }
-    }
-  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y)
+    Cf[((size_t)spin * nbf_pad + f0 + r) * nocc_pad + i0 + threadIdx.x] = t[threadIdx.x][r];
 }
 
 // Functional on points [0, n) of the arrays given (plane stride npad; callers
@@ -337,58 +379,88 @@ __device__ __forceinline__ int block_pos(const uint32_t *m, int I) {
 }
 __device__ __forceinline__ bool block_has(const uint32_t *m, int I) { return (m[I >> 5] >> (I & 31)) & 1u; }
 
-// Vbar(I,J) tile += sum over the chunk's batches b with I, J significant of
-// PhiT_bI^T ZT_bJ, FP64.  One CTA per (I, J, z) tile of 128 x 128; thread
-// (ty, tx) owns rows ty + 16i, cols tx + 16j; K slabs of 16 points staged in
-// shared memory straight from the [g][f] layout.
+// V contraction of the FP64 build: Vbar(I, J) += sum_b PhiT_b,I^T Z_b,J over
+// the chunk's batches b where blocks I and J are both significant
+// (xc_integrals.hpp:677-706), one 128 x 128 output tile per CTA (8 x 8 per
+// thread).  The operand rows of a pair, PhiT[g][f] and Z^T[g][f], are 1 KB
+// rows of 128 functions per point, so each 16-point K step of both operands
+// (32 KB) streams into shared memory with 16-byte cp.async copies through a
+// ring of kVStages stages while the previous steps are multiplied.
+constexpr int kVKs = 16, kVStages = 4;
+constexpr int kVStageDoubles = 2 * kVKs * kBlockF;
+constexpr int kVSmemBytes = kVStages * kVStageDoubles * 8;
+
+// next K step of a V unit: step k of batch b, batches without both blocks skipped
+__device__ __forceinline__ void vstep_next(const uint32_t *__restrict__ mask, int mask_words, long b1, int I, int J,
+                                           long &b, int &k) {
+  if (++k < kBatch / kVKs) return;
+  k = 0;
+  for (++b; b < b1; ++b) {
+    const uint32_t *m = mask + b * mask_words;
+    if (block_has(m, I) && block_has(m, J)) return;
+  }
+}
+
 __global__ void __launch_bounds__(256) vgemm_fp64_kernel(const double *__restrict__ phiT, const double *__restrict__ zT,
                                                          int phi_stride_tiles, int nz, const int *__restrict__ pair_off,
                                                          const uint32_t *__restrict__ mask, int mask_words, long b0,
                                                          long b1, long p0, int nbf_pad, double *__restrict__ V) {
-  constexpr int KS = 16;
-  __shared__ double As[KS][128];
-  __shared__ double Bs[KS][128];
+  extern __shared__ __align__(16) double vsm[];  // [stage][A | B][kVKs][128]
   const int J = blockIdx.x, I = blockIdx.y, zi = blockIdx.z;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const size_t tile = (size_t)kBatch * kBlockF;
+  // first step: the first batch with both blocks significant
+  long lb = b0 - 1;
+  int lk = kBatch / kVKs - 1;
+  vstep_next(mask, mask_words, b1, I, J, lb, lk);
+  if (lb >= b1) return;
+  long cb = lb;
+  int ck = lk;
+  // issue the copies of step (lb, lk) into stage st; returns false past the end
+  auto issue = [&](int st) {
+    if (lb < b1) {
+      const uint32_t *m = mask + lb * mask_words;
+      const long qb = pair_off[lb] - p0;
+      const double *A = phiT + (size_t)(qb + block_pos(m, I)) * phi_stride_tiles * tile + (size_t)lk * kVKs * kBlockF;
+      const double *B = zT + ((size_t)(qb + block_pos(m, J)) * nz + zi) * tile + (size_t)lk * kVKs * kBlockF;
+      double *dA = vsm + st * kVStageDoubles, *dB = dA + kVKs * kBlockF;
+#pragma unroll
+      for (int r = 0; r < (kVKs * kBlockF / 2) / 256; ++r) {
+        const int e = 2 * (threadIdx.x + 256 * r);
+        cp_async16(dA + e, A + e);
+        cp_async16(dB + e, B + e);
+      }
+      vstep_next(mask, mask_words, b1, I, J, lb, lk);
+    }
+    cp_async_commit();  // an empty group past the end keeps the group count uniform
+  };
+#pragma unroll
+  for (int st = 0; st < kVStages - 1; ++st) issue(st);
   double acc[8][8];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
-  bool any = false;
-  for (long b = b0; b < b1; ++b) {
-    const uint32_t *m = mask + b * mask_words;
-    if (!block_has(m, I) || !block_has(m, J)) continue;
-    any = true;
-    const long qb = pair_off[b] - p0;
-    const double *A = phiT + (size_t)(qb + block_pos(m, I)) * phi_stride_tiles * tile;
-    const double *B = zT + ((size_t)(qb + block_pos(m, J)) * nz + zi) * tile;
-    for (int g0 = 0; g0 < kBatch; g0 += KS) {
+  for (int it = 0; cb < b1; ++it) {
+    cp_async_wait<kVStages - 2>();
+    __syncthreads();  // step it is visible; the stage refilled below was read in step it - 1
+    issue((it + kVStages - 1) % kVStages);
+    const double *As = vsm + (it % kVStages) * kVStageDoubles, *Bs = As + kVKs * kBlockF;
 #pragma unroll
-      for (int r = 0; r < (KS * 128) / 256; ++r) {
-        const int e = threadIdx.x + 256 * r;
-        const int k = e >> 7, f = e & 127;
-        As[k][f] = A[(size_t)(g0 + k) * kBlockF + f];
-        Bs[k][f] = B[(size_t)(g0 + k) * kBlockF + f];
-      }
-      __syncthreads();
+    for (int k = 0; k < kVKs; ++k) {
+      double a[8], bb[8];
 #pragma unroll
-      for (int k = 0; k < KS; ++k) {
-        double a[8], bb[8];
+      for (int i = 0; i < 8; ++i) a[i] = As[k * kBlockF + ty + 16 * i];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) a[i] = As[k][ty + 16 * i];
+      for (int j = 0; j < 8; ++j) bb[j] = Bs[k * kBlockF + tx + 16 * j];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) bb[j] = Bs[k][tx + 16 * j];
+      for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
-#pragma unroll
-          for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * bb[j];
-      }
-      __syncthreads();
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
     }
+    vstep_next(mask, mask_words, b1, I, J, cb, ck);
   }
-  if (!any) return;
+  cp_async_wait<0>();
   double *Vz = V + (size_t)zi * nbf_pad * nbf_pad;
 #pragma unroll
   for (int i = 0; i < 8; ++i)
@@ -736,6 +808,118 @@ T *Plan::alloc(size_t n) {
   return p;
 }
 
+// Factor of the Coulomb metric held in P.h_metric (naux x naux, column-major,
+// symmetrised): the reference's preconditioned half inverse when the plan
+// was created with metric_svd_thr > 0, else a pivoted Cholesky of the
+// Jacobi-preconditioned metric.  Used at plan creation and by
+// nkx_plan_set_metric (the full-grid metric of a grid sharded over ranks).
+static void factor_metric(Plan &P) {
+  const size_t NA = P.naux;
+  NKX_CUDA(cudaMemcpy(P.d_L, P.h_metric.data(), sizeof(double) * NA * NA, cudaMemcpyHostToDevice));
+  if (P.svd_mode) {
+    // the reference's preconditioned half inverse: c = X X^T y
+    int K = 0;
+    NKX_REQUIRE(nkx_half_inverse(P.naux, P.d_L, P.metric_svd_thr, P.d_X, &K, P.stream) == NKX_OK,
+                NKX_ERR_NUMERIC, "half inverse of the metric failed");
+    P.K = K;
+    P.metric_min_diag = 0.0;
+  } else {
+    // Pivoted Cholesky of the Jacobi-preconditioned metric A = D^-1 S D^-1:
+    // the grid-integrated (A|B) of an even-tempered aux set is indefinite
+    // at the 1e-4 level (diffuse functions reach past the grid), so aux
+    // functions whose remaining diagonal falls below kMetricTol are
+    // dropped (their fit coefficient is 0) and the kept block is factorised.
+    const double kMetricTol = 1e-5;
+    std::vector<double> D(NA), A(NA * NA);
+    for (size_t i = 0; i < NA; ++i) D[i] = std::sqrt(P.h_metric[i + i * NA]);
+    for (size_t j = 0; j < NA; ++j)
+      for (size_t i = 0; i < NA; ++i) A[i * NA + j] = P.h_metric[i + j * NA] / (D[i] * D[j]);
+    std::vector<double> Lr(NA * NA, 0.0), d(NA);  // row-major rows of L
+    std::vector<char> used(NA, 0);
+    for (size_t i = 0; i < NA; ++i) d[i] = A[i * NA + i];
+    std::vector<int> piv;
+    for (size_t k = 0; k < NA; ++k) {
+      long p = -1;
+      double best = kMetricTol;
+      for (size_t i = 0; i < NA; ++i)
+        if (!used[i] && d[i] >= best) {
+          best = d[i];
+          p = (long)i;
+        }
+      if (p < 0) break;
+      used[p] = 1;
+      piv.push_back((int)p);
+      const double sq = std::sqrt(d[p]);
+      const double *lp = &Lr[(size_t)p * NA];
+#pragma omp parallel for schedule(static)
+      for (long i = 0; i < (long)NA; ++i) {
+        if (used[i] && i != p) continue;
+        const double *li = &Lr[(size_t)i * NA];
+        double acc = A[(size_t)i * NA + p];
+        for (size_t c = 0; c < k; ++c) acc -= li[c] * lp[c];
+        const double v = acc / sq;
+        Lr[(size_t)i * NA + k] = v;
+        if (i != p) d[i] -= v * v;
+      }
+    }
+    const int K = (int)piv.size();
+    NKX_REQUIRE(K > 0, NKX_ERR_NUMERIC, "aux metric (A|B) has no positive pivot");
+    // F = D_sel L_sel, lower triangular K x K in pivot order, column-major
+    std::vector<double> F((size_t)K * K, 0.0);
+    double mn = 1e300;
+    for (int a = 0; a < K; ++a)
+      for (int c = 0; c <= a; ++c) F[a + (size_t)c * K] = D[piv[a]] * Lr[(size_t)piv[a] * NA + c];
+    for (int a = 0; a < K; ++a) mn = std::min(mn, F[a + (size_t)a * K] / D[piv[a]]);
+    P.K = K;
+    P.h_piv = piv;
+    NKX_CUDA(cudaMemcpy(P.d_L, F.data(), sizeof(double) * K * K, cudaMemcpyHostToDevice));
+    NKX_CUDA(cudaMemcpy(P.d_piv, piv.data(), sizeof(int) * K, cudaMemcpyHostToDevice));
+    P.metric_min_diag = mn;
+  }
+}
+
+void Plan::release(void *p) {
+  if (!p) return;
+  cudaFree(p);
+  allocs.erase(std::remove(allocs.begin(), allocs.end(), p), allocs.end());
+}
+
+// Device bytes a chunk needs per (batch, block) pair: the FP64 staging of
+// four 256 x 128 planes (1 MB) plus the mixed build's int8 digits (1 MB), or
+// the FP64 build's three Z planes (0.75 MB).  The default workspace is
+// kDefaultWorkspace or a third of the free memory, whichever is smaller.
+constexpr size_t kPairBytes = (size_t)2 << 20;
+constexpr size_t kDefaultWorkspace = (size_t)24 << 30;
+
+// Chunks of consecutive batches holding at most maxp (batch, block) pairs,
+// and the chunk-sized staging: the FP64 planes now; the FP64 build's Z
+// planes and the mixed build's digits when a build first needs them.
+void plan_chunks(Plan &P, long maxp) {
+  P.chunks.clear();
+  P.max_chunk_pairs = 0;
+  long b = 0;
+  while (b < P.nbatch) {
+    Chunk c;
+    c.b0 = b;
+    c.p0 = P.h_pair_off[b];
+    while (b < P.nbatch && (P.h_pair_off[b + 1] - c.p0 <= maxp || b == c.b0)) ++b;
+    c.b1 = b;
+    c.p1 = P.h_pair_off[b];
+    P.max_chunk_pairs = std::max(P.max_chunk_pairs, c.p1 - c.p0);
+    P.chunks.push_back(c);
+  }
+  P.chunk_pair_limit = maxp;
+  const size_t tile = (size_t)kBatch * kBlockF;
+  P.release(P.ws_phi);
+  P.release(P.ws_z);
+  P.ws_z = nullptr;
+  if (P.mx_state) {
+    destroy_mixed_state(P.mx_state);
+    P.mx_state = nullptr;
+  }
+  P.ws_phi = P.alloc<double>(std::max<long>(1, P.max_chunk_pairs) * 4 * tile);
+}
+
 static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, const nkx_basis *aux, long npoints,
                        const double *xyz, const double *w, const int *owner, const nkx_plan_options *opts) {
   NKX_REQUIRE(prim && prim->nbf > 0 && npoints > 0 && xyz && w && opts, NKX_ERR_ARG, "invalid arguments");
@@ -993,28 +1177,13 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
   }
 
   // --- chunks of batches sized by the workspace
-  const size_t tile = (size_t)kBatch * kBlockF;
-  const size_t per_pair = tile * sizeof(double) * (4 + 3);  // PhiT (4) + Z (up to 3: a, b, J)
   size_t ws = opts->workspace_bytes;
   if (ws == 0) {
     size_t fr = 0, tot = 0;
     NKX_CUDA(cudaMemGetInfo(&fr, &tot));
-    ws = std::min<size_t>((size_t)12 << 30, fr / 3);
+    ws = std::min<size_t>(kDefaultWorkspace, fr / 3);
   }
-  long maxp = std::max<long>(1, (long)(ws / per_pair));
-  long b = 0;
-  while (b < P.nbatch) {
-    Chunk c;
-    c.b0 = b;
-    c.p0 = P.h_pair_off[b];
-    while (b < P.nbatch && (P.h_pair_off[b + 1] - c.p0 <= maxp || b == c.b0)) ++b;
-    c.b1 = b;
-    c.p1 = P.h_pair_off[b];
-    P.max_chunk_pairs = std::max(P.max_chunk_pairs, c.p1 - c.p0);
-    P.chunks.push_back(c);
-  }
-  P.ws_phi = P.alloc<double>(std::max<long>(1, P.max_chunk_pairs) * 4 * tile);
-  P.ws_z = P.alloc<double>(std::max<long>(1, P.max_chunk_pairs) * 3 * tile);
+  plan_chunks(P, std::max<long>(1, (long)(ws / kPairBytes)));
 
   // per-point arrays (two spins)
   P.d_rho = P.alloc<double>(2 * P.npad);
@@ -1075,71 +1244,12 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
     NKX_REQUIRE(cusolverDnCreate(&hs) == CUSOLVER_STATUS_SUCCESS, NKX_ERR_CUDA, "cusolverDnCreate failed");
     P.cusolver = hs;
     cusolverDnSetStream(hs, P.stream);
-    if (opts->metric_svd_thr > 0) {
-      // the reference's preconditioned half inverse: c = X X^T y
-      P.svd_mode = true;
-      P.d_X = P.alloc<double>(NA * NA);
-      P.d_t = P.alloc<double>(NA);
-      int K = 0;
-      NKX_REQUIRE(nkx_half_inverse(P.naux, P.d_L, opts->metric_svd_thr, P.d_X, &K, P.stream) == NKX_OK,
-                  NKX_ERR_NUMERIC, "half inverse of the metric failed");
-      P.K = K;
-      P.metric_min_diag = 0.0;
-    } else {
-      // Pivoted Cholesky of the Jacobi-preconditioned metric A = D^-1 S D^-1:
-      // the grid-integrated (A|B) of an even-tempered aux set is indefinite
-      // at the 1e-4 level (diffuse functions reach past the grid), so aux
-      // functions whose remaining diagonal falls below kMetricTol are
-      // dropped (their fit coefficient is 0) and the kept block is factorised.
-      const double kMetricTol = 1e-5;
-      std::vector<double> D(NA), A(NA * NA);
-      for (size_t i = 0; i < NA; ++i) D[i] = std::sqrt(P.h_metric[i + i * NA]);
-      for (size_t j = 0; j < NA; ++j)
-        for (size_t i = 0; i < NA; ++i) A[i * NA + j] = P.h_metric[i + j * NA] / (D[i] * D[j]);
-      std::vector<double> Lr(NA * NA, 0.0), d(NA);  // row-major rows of L
-      std::vector<char> used(NA, 0);
-      for (size_t i = 0; i < NA; ++i) d[i] = A[i * NA + i];
-      std::vector<int> piv;
-      for (size_t k = 0; k < NA; ++k) {
-        long p = -1;
-        double best = kMetricTol;
-        for (size_t i = 0; i < NA; ++i)
-          if (!used[i] && d[i] >= best) {
-            best = d[i];
-            p = (long)i;
-          }
-        if (p < 0) break;
-        used[p] = 1;
-        piv.push_back((int)p);
-        const double sq = std::sqrt(d[p]);
-        const double *lp = &Lr[(size_t)p * NA];
-#pragma omp parallel for schedule(static)
-        for (long i = 0; i < (long)NA; ++i) {
-          if (used[i] && i != p) continue;
-          const double *li = &Lr[(size_t)i * NA];
-          double acc = A[(size_t)i * NA + p];
-          for (size_t c = 0; c < k; ++c) acc -= li[c] * lp[c];
-          const double v = acc / sq;
-          Lr[(size_t)i * NA + k] = v;
-          if (i != p) d[i] -= v * v;
-        }
-      }
-      const int K = (int)piv.size();
-      NKX_REQUIRE(K > 0, NKX_ERR_NUMERIC, "aux metric (A|B) has no positive pivot");
-      // F = D_sel L_sel, lower triangular K x K in pivot order, column-major
-      std::vector<double> F((size_t)K * K, 0.0);
-      double mn = 1e300;
-      for (int a = 0; a < K; ++a)
-        for (int c = 0; c <= a; ++c) F[a + (size_t)c * K] = D[piv[a]] * Lr[(size_t)piv[a] * NA + c];
-      for (int a = 0; a < K; ++a) mn = std::min(mn, F[a + (size_t)a * K] / D[piv[a]]);
-      P.K = K;
-      P.h_piv = piv;
-      NKX_CUDA(cudaMemcpy(P.d_L, F.data(), sizeof(double) * K * K, cudaMemcpyHostToDevice));
-      P.d_piv = P.alloc<int>(K);
-      NKX_CUDA(cudaMemcpy(P.d_piv, piv.data(), sizeof(int) * K, cudaMemcpyHostToDevice));
-      P.d_t = P.alloc<double>(NA);
-      P.metric_min_diag = mn;
-    }
+    P.svd_mode = opts->metric_svd_thr > 0;
+    P.metric_svd_thr = opts->metric_svd_thr;
+    P.d_X = P.svd_mode ? P.alloc<double>(NA * NA) : nullptr;
+    P.d_t = P.alloc<double>(NA);
+    P.d_piv = P.alloc<int>(NA);
+    factor_metric(P);
   }
   NKX_CUDA(cudaStreamSynchronize(P.stream));
 }
@@ -1159,9 +1269,11 @@ void launch_colloc(Plan &P, const Chunk &c, cudaStream_t s) {
   ++P.launches;
 }
 
-// y = (Vw rho_total), c = (A|B)^-1 y (pivoted Cholesky or half inverse),
-// v_g = w_g sum_a c_a V_a(g)  (coulomb.hpp:84-95)
-void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
+// The grid RI-J fit (coulomb.hpp:84-95) in two steps, so that a grid
+// sharded over ranks can sum y between them: coulomb_y forms this plan's
+// y = Vw rho_total over its points; coulomb_solve solves c = (A|B)^-1 y
+// (pivoted Cholesky or half inverse) and forms v_g = w_g sum_a c_a V_a(g).
+void coulomb_y(Plan &P, int nspin, cudaStream_t s) {
     NKX_CUDA(cudaMemsetAsync(P.d_y, 0, sizeof(double) * P.naux, s));
     const long nsl = std::max<long>(1, std::min<long>(64, (P.npad + 4095) / 4096));
     const long slice = (P.npad + nsl - 1) / nsl;
@@ -1185,6 +1297,9 @@ void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
       NKX_LAUNCH_CHECK();
       ++P.launches;
     }
+}
+
+void coulomb_solve(Plan &P, cudaStream_t s) {
     if (P.svd_mode) {
       const double one = 1.0, zero = 0.0;
       cublasHandle_t hb = (cublasHandle_t)P.cublas;
@@ -1213,8 +1328,29 @@ void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
     ++P.launches;
 }
 
+void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
+  coulomb_y(P, nspin, s);
+  coulomb_solve(P, s);
+}
+
 // FP64 pass A: collocation + density of every chunk into d_rho / d_grad
 void fp64_density_pass(Plan &P, int nspin, int nocc, cudaStream_t s, StageTimer &T) {
+  const int nocc_pad = (nocc + 63) / 64 * 64;
+  if ((size_t)nocc_pad * P.nbf_pad * 2 > P.cf_cap) {
+    P.cf_cap = (size_t)nocc_pad * P.nbf_pad * 2;
+    P.d_Cf = P.alloc<double>(P.cf_cap);
+  }
+  transpose_orbitals_kernel<<<dim3(P.nbf_pad / 32, nocc_pad / 32, nspin), dim3(32, 8), 0, s>>>(P.d_Ct, nocc, nocc_pad,
+                                                                                             P.nbf_pad, P.d_Cf);
+  NKX_LAUNCH_CHECK();
+  ++P.launches;
+  NKX_CUDA(cudaFuncSetAttribute(density_fp64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kDSmemBytes<true>));
+  NKX_CUDA(cudaFuncSetAttribute(density_fp64_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kDSmemBytes<false>));
+  // the density kernels add their orbital tiles' shares
+  NKX_CUDA(cudaMemsetAsync(P.d_rho, 0, sizeof(double) * nspin * P.npad, s));
+  if (P.gga) NKX_CUDA(cudaMemsetAsync(P.d_grad, 0, sizeof(double) * 3 * nspin * P.npad, s));
   for (const Chunk &c : P.chunks) {
     const long nb = c.b1 - c.b0;
     if (c.p1 - c.p0 > 0) {
@@ -1223,12 +1359,12 @@ void fp64_density_pass(Plan &P, int nspin, int nocc, cudaStream_t s, StageTimer 
       T.end(s);
     }
     T.begin(ST_DENSITY, s);
-    dim3 grid((unsigned)(nb * 4), nspin);
+    dim3 grid((unsigned)(nb * 4 * (nocc_pad / 64)), nspin);
     if (P.gga)
-      density_fp64_kernel<true><<<grid, 256, 0, s>>>(P.ws_phi, P.d_Ct, P.d_occ, nocc, P.nbf_pad, P.d_pair_off,
+      density_fp64_kernel<true><<<grid, 256, kDSmemBytes<true>, s>>>(P.ws_phi, P.d_Cf, P.d_occ, nocc, nocc_pad, P.nbf_pad, P.d_pair_off,
                                                      P.d_pair_blk, c.b0, c.p0, P.d_rho, P.d_grad, P.npad);
     else
-      density_fp64_kernel<false><<<grid, 256, 0, s>>>(P.ws_phi, P.d_Ct, P.d_occ, nocc, P.nbf_pad, P.d_pair_off,
+      density_fp64_kernel<false><<<grid, 256, kDSmemBytes<false>, s>>>(P.ws_phi, P.d_Cf, P.d_occ, nocc, nocc_pad, P.nbf_pad, P.d_pair_off,
                                                       P.d_pair_blk, c.b0, c.p0, P.d_rho, P.d_grad, P.npad);
     NKX_LAUNCH_CHECK();
     ++P.launches;
@@ -1237,15 +1373,25 @@ void fp64_density_pass(Plan &P, int nspin, int nocc, cudaStream_t s, StageTimer 
 }
 
 void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
-                     StageTimer &T) {
+                     StageTimer &T, int phase) {
   const bool multi = P.chunks.size() > 1;
   const int nzs = nspin + (separateJ ? 1 : 0);
-  // ---- pass A: collocation + density
-  fp64_density_pass(P, nspin, nocc, s, T);
+  if (!P.ws_z) P.ws_z = P.alloc<double>(std::max<long>(1, P.max_chunk_pairs) * 3 * (size_t)kBatch * kBlockF);
+  NKX_CUDA(cudaFuncSetAttribute(vgemm_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kVSmemBytes));
+  if (phase != 2) {
+    // ---- pass A: collocation + density, and this plan's share of the J fit vector
+    fp64_density_pass(P, nspin, nocc, s, T);
+    if (needJ) {
+      T.begin(ST_COULOMB, s);
+      coulomb_y(P, nspin, s);
+      T.end(s);
+    }
+    if (phase == 1) return;
+  }
   // ---- J: fit coefficients and fitted potential
   if (needJ) {
     T.begin(ST_COULOMB, s);
-    coulomb_fit(P, nspin, s);
+    coulomb_solve(P, s);
     T.end(s);
   }
   // ---- functional
@@ -1279,7 +1425,7 @@ void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool s
     ++P.launches;
     T.end(s);
     T.begin(ST_VGEMM, s);
-    vgemm_fp64_kernel<<<dim3(P.nblk, P.nblk, nzs), 256, 0, s>>>(P.ws_phi, P.ws_z, P.gga ? 4 : 1, nzs, P.d_pair_off,
+    vgemm_fp64_kernel<<<dim3(P.nblk, P.nblk, nzs), 256, kVSmemBytes, s>>>(P.ws_phi, P.ws_z, P.gga ? 4 : 1, nzs, P.d_pair_off,
                                                                 P.d_mask, P.mask_words, c.b0, c.b1, c.p0, P.nbf_pad,
                                                                 P.d_V);
     NKX_LAUNCH_CHECK();
@@ -1311,17 +1457,32 @@ void upload_orbitals(Plan &P, int nspin, int nocc, const double *C, const double
   ++P.launches;
 }
 
+// One Fock build (phase 0), or one half of a build whose grid is sharded
+// over ranks: phase 1 uploads the orbitals, runs the density pass and writes
+// this plan's share of the J fit vector y to `y` (naux doubles, host or
+// device by `mem`); the caller sums y over the ranks; phase 2 takes the
+// summed y (same memory kind) and finishes the build (fit, functional, V and
+// J on this plan's points).  Phase 2 needs a phase 1 of the same
+// precision, spin count and orbitals on this plan immediately before it.
 void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, const double *occ, int mem, int fuse_j,
-                double *E, double *V, double *J, cudaStream_t user) {
+                double *E, double *V, double *J, cudaStream_t user, int phase, double *y) {
+  if (phase == 2) {
+    NKX_REQUIRE(P.phase1_done, NKX_ERR_ARG, "phase 2 of a sharded build needs phase 1 on this plan first");
+    precision = P.phase1_precision;
+    nspin = P.phase1_nspin;
+    nocc = P.phase1_nocc;
+  }
   NKX_REQUIRE(nspin == 1 || nspin == 2, NKX_ERR_ARG, "nspin must be 1 or 2");
-  NKX_REQUIRE(nocc > 0 && C && occ && E && (V || J), NKX_ERR_ARG, "invalid arguments");
+  NKX_REQUIRE(phase == 2 || (nocc > 0 && C && occ), NKX_ERR_ARG, "invalid orbitals");
+  NKX_REQUIRE(phase == 1 || (E && (V || J)), NKX_ERR_ARG, "invalid outputs");
+  NKX_REQUIRE(phase == 0 || (y && P.naux > 0), NKX_ERR_ARG, "a sharded build needs y and a plan with an aux basis");
   NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
   NKX_REQUIRE(precision == NKX_PREC_FP64 || precision == NKX_PREC_MIXED, NKX_ERR_ARG, "unknown precision");
-  const bool needJ = P.naux > 0 && (J != nullptr || fuse_j);
+  const bool needJ = P.naux > 0 && (J != nullptr || fuse_j || phase != 0);
   NKX_REQUIRE(!(fuse_j && P.naux == 0), NKX_ERR_ARG, "fuse_j needs a plan with an aux basis");
   // V may be NULL only when J alone is asked for (the exchange-correlation
   // terms are then formed and dropped)
-  NKX_REQUIRE(V != nullptr || (J != nullptr && !fuse_j && P.naux > 0), NKX_ERR_ARG,
+  NKX_REQUIRE(phase == 1 || V != nullptr || (J != nullptr && !fuse_j && P.naux > 0), NKX_ERR_ARG,
               "V must be given unless J alone is requested from a plan with an aux basis");
   const bool separateJ = needJ && !fuse_j && J;
   cudaStream_t s = user ? user : P.stream;
@@ -1331,15 +1492,38 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
   NKX_CUDA(cudaEventCreate(&t0));
   NKX_CUDA(cudaEventCreate(&t1));
   NKX_CUDA(cudaEventRecord(t0, s));
-  NKX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int) * 2, s));
+  P.phase1_done = false;
+  if (phase == 2) {
+    NKX_CUDA(cudaMemcpyAsync(P.d_y, y, sizeof(double) * P.naux,
+                             mem == NKX_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+  } else {
+    NKX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int) * 2, s));
+    upload_orbitals(P, nspin, nocc, C, occ, mem, s);
+  }
 
-  upload_orbitals(P, nspin, nocc, C, occ, mem, s);
+  const bool mixed = precision == NKX_PREC_MIXED && mixed_available(P);
+  NKX_REQUIRE(mixed || precision == NKX_PREC_FP64, NKX_ERR_UNSUPPORTED, "mixed precision path unavailable");
+  if (mixed)
+    fock_build_mixed(P, nspin, nocc, needJ, fuse_j != 0, separateJ, s, T, phase);
+  else
+    fock_build_fp64(P, nspin, nocc, needJ, fuse_j != 0, separateJ, s, T, phase);
 
-  if (precision == NKX_PREC_MIXED && mixed_available(P))
-    fock_build_mixed(P, nspin, nocc, needJ, fuse_j != 0, separateJ, s, T);
-  else {
-    NKX_REQUIRE(precision == NKX_PREC_FP64, NKX_ERR_UNSUPPORTED, "mixed precision path unavailable");
-    fock_build_fp64(P, nspin, nocc, needJ, fuse_j != 0, separateJ, s, T);
+  if (phase == 1) {
+    NKX_CUDA(cudaMemcpyAsync(y, P.d_y, sizeof(double) * P.naux,
+                             mem == NKX_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+    int status[2] = {0, 0};
+    NKX_CUDA(cudaMemcpyAsync(status, P.d_status, sizeof(status), cudaMemcpyDeviceToHost, s));
+    NKX_CUDA(cudaEventRecord(t1, s));
+    NKX_CUDA(cudaStreamSynchronize(s));
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    NKX_REQUIRE(status[0] == 0, NKX_ERR_TIMEOUT, "a tensor-core kernel wait gave up in phase 1");
+    NKX_REQUIRE(status[1] == 0, NKX_ERR_NUMERIC, "non-finite value in the orbitals, occupations or an operand");
+    P.phase1_done = true;
+    P.phase1_precision = precision;
+    P.phase1_nspin = nspin;
+    P.phase1_nocc = nocc;
+    return;
   }
 
   // symmetrise + unpad into the output (device) or a staging buffer (host)
@@ -1431,6 +1615,45 @@ NKX_API nkx_status nkx_fock_build(nkx_plan *plan, int precision, int nspin, int 
     NKX_REQUIRE(plan, NKX_ERR_ARG, "plan is NULL");
     Plan &P = *reinterpret_cast<Plan *>(plan);
     fock_build(P, precision, nspin, nocc, C, occ, mem, fuse_j, E, V, J, (cudaStream_t)stream);
+  });
+}
+
+NKX_API nkx_status nkx_fock_build_phase1(nkx_plan *plan, int precision, int nspin, int nocc, const double *C,
+                                         const double *occ, int mem, double *y, void *stream) {
+  return run_guarded("nkx_fock_build_phase1", [&] {
+    NKX_REQUIRE(plan, NKX_ERR_ARG, "plan is NULL");
+    Plan &P = *reinterpret_cast<Plan *>(plan);
+    fock_build(P, precision, nspin, nocc, C, occ, mem, 0, nullptr, nullptr, nullptr, (cudaStream_t)stream, 1, y);
+  });
+}
+
+NKX_API nkx_status nkx_fock_build_phase2(nkx_plan *plan, const double *y, int mem, int fuse_j, double *E, double *V,
+                                         double *J, void *stream) {
+  return run_guarded("nkx_fock_build_phase2", [&] {
+    NKX_REQUIRE(plan, NKX_ERR_ARG, "plan is NULL");
+    Plan &P = *reinterpret_cast<Plan *>(plan);
+    fock_build(P, 0, 0, 0, nullptr, nullptr, mem, fuse_j, E, V, J, (cudaStream_t)stream, 2, const_cast<double *>(y));
+  });
+}
+
+NKX_API nkx_status nkx_plan_set_metric(nkx_plan *plan, const double *S, int mem) {
+  return run_guarded("nkx_plan_set_metric", [&] {
+    NKX_REQUIRE(plan && S, NKX_ERR_ARG, "invalid arguments");
+    Plan &P = *reinterpret_cast<Plan *>(plan);
+    NKX_REQUIRE(P.naux > 0, NKX_ERR_ARG, "the plan has no aux basis");
+    NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
+    const size_t NA = P.naux;
+    P.h_metric.resize(NA * NA);
+    NKX_CUDA(cudaMemcpy(P.h_metric.data(), S, sizeof(double) * NA * NA,
+                        mem == NKX_MEM_HOST ? cudaMemcpyHostToHost : cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < NA; ++i)
+      NKX_REQUIRE(std::isfinite(P.h_metric[i + i * NA]) && P.h_metric[i + i * NA] > 0, NKX_ERR_NUMERIC,
+                  "metric diagonal must be positive and finite");
+    // the mode chosen at plan creation (a caller's half inverse is replaced)
+    P.svd_mode = P.metric_svd_thr > 0;
+    if (P.svd_mode && !P.d_X) P.d_X = P.alloc<double>(NA * NA);
+    factor_metric(P);
+    NKX_CUDA(cudaStreamSynchronize(P.stream));
   });
 }
 

@@ -14,6 +14,14 @@ struct Chunk {
   long p0 = 0, p1 = 0;  // (batch, block) pair range
 };
 
+// Choices of the mixed-precision build that the autotuner (nkx_plan_autotune)
+// measures; the defaults are what it found best on (H2O)_64.
+struct Tuning {
+  int v_n = 128;   // tcgen05 MMA width N of the V contraction (128 or 64)
+  int dens_n = 64; // MMA width of the density contraction (64 or 128)
+  int ypath = -1;  // GGA density gradient through Y = T0 (C occ)^T: -1 from 256 orbitals, 0 off, 1 on
+};
+
 struct Plan {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -58,7 +66,8 @@ struct Plan {
   uint32_t *d_mask = nullptr;
 
   std::vector<Chunk> chunks;
-  long max_chunk_pairs = 0;
+  long max_chunk_pairs = 0, chunk_pair_limit = 0;
+  Tuning tune;
   double *ws_phi = nullptr;  // PhiT tiles of a chunk: [pair][comp][g][f]
   double *ws_z = nullptr;    // Z^T tiles of a chunk:  [pair][z][g][f]
 
@@ -67,6 +76,8 @@ struct Plan {
   // orbitals
   int nocc_cap = 0;
   double *d_Ct = nullptr, *d_occ = nullptr, *d_Cin = nullptr;
+  double *d_Cf = nullptr;  // function-major orbitals of the FP64 density pass
+  size_t cf_cap = 0;
   // accumulators / outputs
   double *d_V = nullptr, *d_E = nullptr, *d_out = nullptr;
   // caller-order density outputs (nkx_plan_density)
@@ -75,6 +86,7 @@ struct Plan {
 
   // Coulomb metric
   bool svd_mode = false;
+  double metric_svd_thr = 0.0;
   int K = 0, lwork = 0;
   double *d_L = nullptr, *d_X = nullptr, *d_t = nullptr, *d_y = nullptr, *d_c = nullptr, *d_work = nullptr;
   int *d_info = nullptr, *d_piv = nullptr;
@@ -92,6 +104,9 @@ struct Plan {
   // limit of the device waits that may be abandoned (nkx_plan_set_wait_limit)
   unsigned long long wait_ns = 2000000000ull;
   int stall_test = 0;  // tests of the error path: tensor-core kernels wait on a barrier nothing completes
+  // state kept between the two phases of a sharded build
+  bool phase1_done = false;
+  int phase1_precision = 0, phase1_nspin = 1, phase1_nocc = 0;
 
   nkx_build_timing last{};
   int launches = 0;
@@ -100,7 +115,14 @@ struct Plan {
   ~Plan();
   template <class T>
   T *alloc(size_t n);
+  void release(void *p);  // frees one allocation made with alloc
 };
+
+void plan_chunks(Plan &P, long max_pairs);
+// one Fock build, or phase 1 / 2 of a build on a sharded grid (plan.cu)
+void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, const double *occ, int mem, int fuse_j,
+                double *E, double *V, double *J, cudaStream_t user, int phase = 0, double *y = nullptr);
+void destroy_mixed_state(void *p);
 
 // Accumulates CUDA-event time per build stage.
 struct StageTimer {
@@ -148,6 +170,8 @@ __global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, long
                                   const double *__restrict__ vj, double *__restrict__ coef, double *Eacc,
                                   double *__restrict__ edens);
 void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
-                      StageTimer &T);
+                      StageTimer &T, int phase);
+void coulomb_y(Plan &P, int nspin, cudaStream_t s);
+void coulomb_solve(Plan &P, cudaStream_t s);
 
 }  // namespace nkx

@@ -51,14 +51,17 @@ constexpr double kTwoM36 = 0x1p-36;
 // (grad rho = 2 sum_mu grad phi_mu Y_mu, ygrad_kernel)
 enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1, TC_MODE_GRAD = 2 };
 
-// Shape per mode.  V: N = 128 (one TMEM buffer of 4 levels x 128 columns,
-// 16 epilogue warps, 3 stages of 64 KB).  Density: N = 64 (two buffers of
-// 4 levels x 64 columns so the epilogue of a block overlaps the MMAs of the
-// next, 8 epilogue warps, 4 stages of 48 KB); its groups are only two K steps
-// long and the orbital count pads to 64, not 128.
-template <int MODE>
+// Shape by the MMA width N.  N = 128: one TMEM buffer of 4 levels x 128
+// columns, 16 epilogue warps, 3 stages of 64 KB.  N = 64: two buffers of
+// 4 levels x 64 columns, so the epilogue of one group overlaps the MMAs of
+// the next, 8 epilogue warps, 4 stages of 48 KB.  Any contraction can run
+// either shape (the V unit then covers a 128 x N part of its output tile,
+// the density unit an N-orbital tile); the Y pass runs N = 64.  The plan's
+// tuning (nkx_plan_autotune) picks the shape per contraction; the defaults
+// are N = 128 for V and N = 64 for the density.
+template <int N_>
 struct TcShape {
-  static constexpr int N = MODE == TC_MODE_V ? 128 : 64;
+  static constexpr int N = N_;
   static constexpr int NBUF = N == 128 ? 1 : 2;
   static constexpr int kStages = N == 128 ? 3 : 4;
   static constexpr int kBBytes = 4 * N * 64;
@@ -96,21 +99,26 @@ struct TcArgs {
   // stall != 0 (tests of the error path): the MMA issuer first waits on a
   // barrier that nothing completes, so the kernel gives up after wait_ns
   int stall;
+  int nt;  // MMA width N of the launched kernel (V: 128 / nt units per output tile)
 };
 
 struct UnitIter {
-  int I = 0, J = 0, zi = 0, sp = 0;  // V: row block, column block, Z plane, batch split
+  int I = 0, J = 0, zi = 0, sp = 0, hc = 0;  // V: row block, column block, Z plane, batch split, column part
   long bl = 0;                     // density: batch within chunk
   long q = 0;                      // grad: chunk-relative pair
   int h = 0, c = 0, s = 0, t = 0;  // density: point half, comp, spin, 128-orbital tile
-  __device__ UnitIter(const TcArgs &a, long u) {
+  // nh: column parts of a 128-function block in a V unit (128 / N, a
+  // compile-time constant at the kernel's call sites)
+  __device__ UnitIter(const TcArgs &a, long u, int nh) {
     if (a.mode == TC_MODE_V) {
-      const long n2 = (long)a.nblk * a.nblk, n3 = n2 * a.nz;
+      const long n2 = (long)a.nblk * a.nblk * nh, n3 = n2 * a.nz;
       sp = (int)(u / n3);
       u %= n3;
       zi = (int)(u / n2);
-      I = (int)((u % n2) / a.nblk);
-      J = (int)(u % a.nblk);
+      u %= n2;
+      I = (int)(u / ((long)a.nblk * nh));
+      J = (int)((u / nh) % a.nblk);
+      hc = (int)(u % nh);
     } else if (a.mode == TC_MODE_GRAD) {
       t = (int)(u % 2);  // 64-function half of the block
       h = (int)((u / 2) % 2);
@@ -160,7 +168,7 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
       g.qa = qb0 + blk_pos(m, it.I);
       g.qb = qb0 + blk_pos(m, Jb);
       g.blk = 0;
-      const int za = (int)(g.qa * 4), zb = (int)((g.qb * a.nz + it.zi) * 4), yb = 0;
+      const int za = (int)(g.qa * 4), zb = (int)((g.qb * a.nz + it.zi) * 4), yb = a.nt * it.hc;
       fn(g, [=](int k, int &xa, int &ya, int &zA, int &xb, int &yB, int &zB) {
         xa = 64 * k;
         ya = 0;
@@ -197,7 +205,7 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
       g.qb = 0;
       g.blk = a.pair_blk[q];
       const int za = (int)((g.qa * a.ncs + it.c) * 4), ya = 128 * it.h;
-      const int xb0 = g.blk * 128, yb = TcShape<TC_MODE_DENSITY>::N * it.t, zb = it.s * 4;
+      const int xb0 = g.blk * 128, yb = a.nt * it.t, zb = it.s * 4;
       fn(g, [=](int k, int &xa, int &yA, int &zA, int &xb, int &yB, int &zB) {
         xa = 64 * k;
         yA = ya;
@@ -217,10 +225,10 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
   }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
+template <int MODE, int NW>
+__global__ void __launch_bounds__(TcShape<NW>::kThreads, 1)
     tc_i8_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs a) {
-  using Sh = TcShape<MODE>;
+  using Sh = TcShape<NW>;
   constexpr int N = Sh::N, NBUF = Sh::NBUF, kStages = Sh::kStages, kStageBytes = Sh::kStageBytes;
   extern __shared__ __align__(1024) uint8_t dsmem[];
   __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar[NBUF], tempty_bar[NBUF], drain_bar, stall_bar;
@@ -259,7 +267,7 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
     if (lane == 0) {
       uint32_t step = 0;
       for (long u = blockIdx.x; u < a.nunits && !abort_flag; u += gridDim.x) {
-        UnitIter it(a, u);
+        UnitIter it(a, u, kBlockF / N);
         for_each_group(a, it, [&](const Group &g, auto coords) {
           for (int k = 0; k < g.nsteps && !abort_flag; ++k, ++step) {
             const int st = step % kStages;
@@ -283,7 +291,7 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
       uint32_t step = 0, grp = 0;
       if (a.stall) mbar_wait(&stall_bar, 0, a.err, 7, &abort_flag, a.wait_ns);
       for (long u = blockIdx.x; u < a.nunits && !abort_flag; u += gridDim.x) {
-        UnitIter it(a, u);
+        UnitIter it(a, u, kBlockF / N);
         for_each_group(a, it, [&](const Group &g, auto) {
           if (abort_flag) return;
           // TMEM buffer grp % NBUF: wait until the epilogue has read the group
@@ -338,7 +346,7 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
     const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
     uint32_t grp = 0;
     for (long u = blockIdx.x; u < a.nunits && !abort_flag; u += gridDim.x) {
-      UnitIter it(a, u);
+      UnitIter it(a, u, kBlockF / N);
       double acc[32];
 #pragma unroll
       for (int j = 0; j < 32; ++j) acc[j] = 0.0;
@@ -356,7 +364,7 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
         if (live) {
           if (a.mode == TC_MODE_V) {
             sa = a.sA[g.qa * 128 + row] * kTwoM36;
-            sb = a.sB + (g.qb * a.nz + it.zi) * 128 + 32 * cq;
+            sb = a.sB + (g.qb * a.nz + it.zi) * 128 + N * it.hc + 32 * cq;
           } else if (a.mode == TC_MODE_GRAD) {
             sa = a.sA[((it.bl * a.nspin + it.s) * 2 + it.h) * 128 + row] * kTwoM36;
             sb = a.sB + (size_t)it.s * a.nbf_pad + 128 * g.blk + 64 * it.t + 32 * cq;
@@ -426,10 +434,11 @@ __global__ void __launch_bounds__(TcShape<MODE>::kThreads, 1)
           const size_t r = (size_t)it.I * 128 + row;
           if (a.nsplit > 1) {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) atomicAdd(&Vz[r + ((size_t)it.J * 128 + 32 * cq + j) * a.nbf_pad], acc[j]);
+            for (int j = 0; j < 32; ++j)
+              atomicAdd(&Vz[r + ((size_t)it.J * 128 + N * it.hc + 32 * cq + j) * a.nbf_pad], acc[j]);
           } else {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) Vz[r + ((size_t)it.J * 128 + 32 * cq + j) * a.nbf_pad] += acc[j];
+            for (int j = 0; j < 32; ++j) Vz[r + ((size_t)it.J * 128 + N * it.hc + 32 * cq + j) * a.nbf_pad] += acc[j];
           }
         }
       } else if (a.mode == TC_MODE_GRAD) {
@@ -1009,10 +1018,40 @@ struct MixedState {
   // grad mode: T0 and (C occ) digits with their row scales
   uint8_t *qt0 = nullptr, *qco = nullptr;
   double *st0 = nullptr, *sco = nullptr;
-  CUtensorMap m_phT, m_ph, m_z, m_ct, m_t0, m_co;
+  // B operand maps by box width: Z with 128- and 64-row boxes (V at N = 128 / 64),
+  // Ct with 64- and 128-row boxes (density at N = 64 / 128)
+  CUtensorMap m_phT, m_ph, m_z, m_z64, m_ct, m_ct128, m_t0, m_co;
   std::vector<void *> bufs;
+  size_t T_cap = 0, qt0_cap = 0;  // doubles of T, bytes of qt0 (grown on demand)
   ~MixedState() {
     for (void *p : bufs) cudaFree(p);
+    cudaFree(T);
+    cudaFree(qt0);
+  }
+  // T: the chunk's FP64 density tiles, nbatch x nspin x ncomp planes of
+  // nocc_pad x 256 (one component on the Y path); qt0: their T0 digits
+  void ensure_T(size_t doubles) {
+    if (doubles <= T_cap) return;
+    cudaFree(T);
+    T = nullptr;
+    T_cap = 0;
+    if (cudaMalloc(&T, doubles * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error{NKX_ERR_ALLOC, "density tile allocation of " + std::to_string(doubles * 8) + " bytes failed"};
+    }
+    T_cap = doubles;
+  }
+  void ensure_qt0(size_t bytes, long rows_planes, int nocc_pad_) {
+    if (bytes <= qt0_cap) return;
+    cudaFree(qt0);
+    qt0 = nullptr;
+    qt0_cap = 0;
+    if (cudaMalloc(&qt0, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error{NKX_ERR_ALLOC, "T0 digit allocation of " + std::to_string(bytes) + " bytes failed"};
+    }
+    qt0_cap = bytes;
+    m_t0 = make_map3(qt0, nocc_pad_, 128, rows_planes, 128);
   }
   template <class X>
   X *alloc(size_t n) {
@@ -1052,51 +1091,62 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     M->m_phT = make_map3(M->qphT, 128, 256, M->cap * 4 * 4, 128);
     M->m_ph = make_map3(M->qph, 256, 128, M->cap * 4, 128);
     M->m_z = make_map3(M->qz, 256, 128, M->cap * 3 * 4, 128);
+    M->m_z64 = make_map3(M->qz, 256, 128, M->cap * 3 * 4, 64);
     int dev = 0;
     NKX_CUDA(cudaGetDevice(&dev));
     NKX_CUDA(cudaDeviceGetAttribute(&M->nsm, cudaDevAttrMultiProcessorCount, dev));
-    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  TcShape<TC_MODE_V>::kSmem));
-    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_DENSITY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  TcShape<TC_MODE_DENSITY>::kSmem));
-    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  TcShape<TC_MODE_GRAD>::kSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_V, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TcShape<128>::kSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_V, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TcShape<64>::kSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_DENSITY, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TcShape<64>::kSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_DENSITY, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TcShape<128>::kSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_GRAD, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TcShape<64>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(zquant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 68));
   }
   MixedState &M = *static_cast<MixedState *>(P.mx_state);
-  constexpr int NT = TcShape<TC_MODE_DENSITY>::N;
-  const int nocc_pad = ((nocc + NT - 1) / NT) * NT;
+  // orbitals pad to 128 so that either density tile width divides them
+  const int nocc_pad = ((nocc + 127) / 128) * 128;
   if (nocc_pad > M.nocc_pad) {
     M.nocc_pad = nocc_pad;
     M.qct = M.alloc<uint8_t>((size_t)2 * 4 * nocc_pad * P.nbf_pad);
     M.sct = M.alloc<double>((size_t)2 * nocc_pad * P.nblk);
-    M.T = M.alloc<double>((size_t)M.nbatch_chunk * 2 * 4 * nocc_pad * 256);
-    M.m_ct = make_map3(M.qct, P.nbf_pad, nocc_pad, 8, TcShape<TC_MODE_DENSITY>::N);
-    M.qt0 = M.alloc<uint8_t>((size_t)M.nbatch_chunk * 2 * 2 * 4 * 128 * nocc_pad);
+    M.T_cap = M.qt0_cap = 0;  // regrown for the new orbital padding
+    M.m_ct = make_map3(M.qct, P.nbf_pad, nocc_pad, 8, 64);
+    M.m_ct128 = make_map3(M.qct, P.nbf_pad, nocc_pad, 8, 128);
     M.st0 = M.alloc<double>((size_t)M.nbatch_chunk * 2 * 2 * 128);
     M.qco = M.alloc<uint8_t>((size_t)2 * 4 * P.nbf_pad * nocc_pad);
     M.sco = M.alloc<double>((size_t)2 * P.nbf_pad);
-    M.m_t0 = make_map3(M.qt0, nocc_pad, 128, (long)M.nbatch_chunk * 2 * 2 * 4, 128);
-    M.m_co = make_map3(M.qco, nocc_pad, P.nbf_pad, 2 * 4, TcShape<TC_MODE_GRAD>::N);
+    M.m_co = make_map3(M.qco, nocc_pad, P.nbf_pad, 2 * 4, 64);
   }
   return M;
 }
 
+template <int MODE, int NW>
+static void launch_i8_shape(const CUtensorMap &mA, const CUtensorMap &mB, const TcArgs &a, unsigned grid,
+                            cudaStream_t s) {
+  tc_i8_kernel<MODE, NW><<<grid, TcShape<NW>::kThreads, TcShape<NW>::kSmem, s>>>(mA, mB, a);
+}
+
+// one persistent CTA per SM (or per unit when there are fewer)
 static void launch_i8(MixedState &M, const CUtensorMap &mA, const CUtensorMap &mB, const TcArgs &a, cudaStream_t s) {
   if (a.nunits <= 0) return;
   const unsigned grid = (unsigned)std::min<long>(a.nunits, M.nsm);
+  NKX_REQUIRE(a.nt == 64 || a.nt == 128, NKX_ERR_ARG, "tensor-core width must be 64 or 128");
+  NKX_REQUIRE(a.mode != TC_MODE_GRAD || a.nt == 64, NKX_ERR_ARG, "the Y pass runs N = 64");
   if (a.mode == TC_MODE_V)
-    tc_i8_kernel<TC_MODE_V><<<grid, TcShape<TC_MODE_V>::kThreads, TcShape<TC_MODE_V>::kSmem, s>>>(mA, mB, a);
+    a.nt == 128 ? launch_i8_shape<TC_MODE_V, 128>(mA, mB, a, grid, s) : launch_i8_shape<TC_MODE_V, 64>(mA, mB, a, grid, s);
   else if (a.mode == TC_MODE_GRAD)
-    tc_i8_kernel<TC_MODE_GRAD><<<grid, TcShape<TC_MODE_GRAD>::kThreads, TcShape<TC_MODE_GRAD>::kSmem, s>>>(mA, mB,
-                                                                                                          a);
+    launch_i8_shape<TC_MODE_GRAD, 64>(mA, mB, a, grid, s);
   else
-    tc_i8_kernel<TC_MODE_DENSITY><<<grid, TcShape<TC_MODE_DENSITY>::kThreads, TcShape<TC_MODE_DENSITY>::kSmem, s>>>(
-        mA, mB, a);
+    a.nt == 128 ? launch_i8_shape<TC_MODE_DENSITY, 128>(mA, mB, a, grid, s)
+                : launch_i8_shape<TC_MODE_DENSITY, 64>(mA, mB, a, grid, s);
   NKX_LAUNCH_CHECK();
 }
 
-void coulomb_fit(Plan &P, int nspin, cudaStream_t s);
 
 template <bool GRAD>
 static void launch_colloc_z_g(Plan &P, MixedState &M, const Chunk &c, int nzs, int nspin, cudaStream_t s) {
@@ -1121,12 +1171,23 @@ static void launch_colloc_z(Plan &P, MixedState &M, const Chunk &c, int nzs, int
 }
 
 void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
-                      StageTimer &Tm) {
+                      StageTimer &Tm, int phase) {
   MixedState &M = mixed_state(P, nocc);
   const int nc = P.gga ? 4 : 1;
   const int nzs = nspin + (separateJ ? 1 : 0);
   NKX_REQUIRE(nzs <= 3, NKX_ERR_ARG, "too many Z planes");
-  {
+  NKX_REQUIRE(phase == 0 || needJ, NKX_ERR_ARG, "a sharded (two-phase) build needs J");
+  // Y path for the GGA density gradient (see below): the plan's tuning, or
+  // by default from 256 orbitals on
+  const bool y_ok = P.gga && M.nocc_pad <= 8192;
+  const bool grad_mode = y_ok && (P.tune.ypath >= 0 ? P.tune.ypath != 0 : M.nocc_pad >= 256);
+  if (phase != 2) {
+    M.ensure_T((size_t)M.nbatch_chunk * nspin * (grad_mode ? 1 : nc) * M.nocc_pad * 256);
+    if (grad_mode)
+      M.ensure_qt0((size_t)M.nbatch_chunk * nspin * 2 * 4 * 128 * M.nocc_pad, (long)M.nbatch_chunk * nspin * 2 * 4,
+                   M.nocc_pad);
+  }
+  if (phase != 2) {
     const long rows = (long)nspin * M.nocc_pad * P.nblk;
     quant_ct_kernel<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(P.d_Ct, nocc, M.nocc_pad, nspin, P.nbf_pad,
                                                                          P.nblk, M.qct, M.sct, P.d_status + 1);
@@ -1139,8 +1200,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
   // from about 256 orbitals on ((H2O)64, 320 orbitals: 226 vs 232 ms; the
   // 1500-atom aggregate, 2850: 12.2 vs 24.8 s); with fewer the per-pair Y
   // traffic dominates.  Above 8192 orbitals the int32 levels could overflow.
-  const bool grad_mode = P.gga && M.nocc_pad >= 256 && M.nocc_pad <= 8192;
-  if (grad_mode) {
+  if (grad_mode && phase != 2) {
     quant_cocc_kernel<<<dim3((unsigned)P.nblk, nspin), 128, 0, s>>>(P.d_Ct, P.d_occ, nocc, M.nocc_pad, P.nbf_pad,
                                                                     M.qco, M.sco);
     NKX_LAUNCH_CHECK();
@@ -1178,14 +1238,15 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.nspin = nspin;
     a.ncs = nc;
     a.ncomp = grad_mode ? 1 : nc;
-    a.ntile_i = M.nocc_pad / TcShape<TC_MODE_DENSITY>::N;
+    a.nt = P.tune.dens_n;
+    a.ntile_i = (nocc + a.nt - 1) / a.nt;
     a.nocc_pad = M.nocc_pad;
     a.T = M.T;
     a.err = P.d_status;
     a.wait_ns = P.wait_ns;
     a.stall = P.stall_test;
     a.nunits = nb * nspin * 2 * a.ncomp * a.ntile_i;
-    launch_i8(M, M.m_phT, M.m_ct, a, s);
+    launch_i8(M, M.m_phT, a.nt == 128 ? M.m_ct128 : M.m_ct, a, s);
     ++P.launches;
     if (P.gga && !grad_mode)
       density_contract_kernel<true><<<dim3((unsigned)nb, nspin), 256, 0, s>>>(M.T, P.d_occ, nocc, M.nocc_pad, nspin,
@@ -1218,6 +1279,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       g.wait_ns = P.wait_ns;
       g.stall = P.stall_test;
       g.nunits = np * nspin * 4;
+      g.nt = 64;
       launch_i8(M, M.m_t0, M.m_co, g, s);
       ++P.launches;
       ygrad_kernel<<<dim3((unsigned)nb, nspin, 4), 256, 0, s>>>(P.ws_phi, M.qphT, M.sphT, P.d_pair_off, c.b0, c.p0,
@@ -1259,10 +1321,12 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.stall = P.stall_test;
     // too few output tiles for the SMs: split the chunk's batches
     const long tiles = (long)nzs * P.nblk * P.nblk;
-    a.nsplit = tiles >= M.nsm ? 1 : (int)std::min<long>({(M.nsm + tiles - 1) / tiles, c.b1 - c.b0, 16L});
+    a.nt = P.tune.v_n;
+    const long parts = tiles * (kBlockF / a.nt);
+    a.nsplit = parts >= M.nsm ? 1 : (int)std::min<long>({(M.nsm + parts - 1) / parts, c.b1 - c.b0, 16L});
     a.nsplit = std::max(1, a.nsplit);
-    a.nunits = tiles * a.nsplit;
-    launch_i8(M, M.m_ph, M.m_z, a, s);
+    a.nunits = parts * a.nsplit;
+    launch_i8(M, M.m_ph, a.nt == 128 ? M.m_z : M.m_z64, a, s);
     ++P.launches;
     Tm.end(s);
   };
@@ -1307,10 +1371,17 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       pass_b(c, true);
     }
   } else {
-    for (const Chunk &c : P.chunks) pass_a(c);
+    if (phase != 2) {
+      for (const Chunk &c : P.chunks) pass_a(c);
+      // this plan's share of the J fit vector
+      Tm.begin(ST_COULOMB, s);
+      coulomb_y(P, nspin, s);
+      Tm.end(s);
+      if (phase == 1) return;
+    }
     // ---- J fit and the functional, in FP64
     Tm.begin(ST_COULOMB, s);
-    coulomb_fit(P, nspin, s);
+    coulomb_solve(P, s);
     Tm.end(s);
     Tm.begin(ST_FUNC, s);
     functional_kernel<<<(unsigned)((P.npad + 255) / 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.npad, P.d_w,

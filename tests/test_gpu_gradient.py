@@ -101,3 +101,73 @@ def test_cluster_gradient_translation_invariance_and_fd_spot_check():
     for a, k in ((0, 2), (4, 0)):
         fd = fd_component(cc, Z, a, k, [101, 130], [Cm], [occ])
         assert abs(Ga[a, k] - fd) < 1e-8
+
+
+# ------------------------------------------- autograd wrapper (test only) ----
+class XcEnergy(torch.autograd.Function):
+    """E_xc(R) of a fixed set of orbitals as a differentiable function of the
+    nuclear coordinates R (natoms x 3, bohr, FP64): forward rebuilds the grid
+    (points moving with their owner atoms, Becke weights, no compaction), the
+    basis centres and the plan at R and returns the FP64 E_xc of the GPU build;
+    backward returns grad_output * dE_xc/dR from nkx_xc_gradient.  It lives in
+    the test harness only: the library's interface is the C ABI."""
+
+    @staticmethod
+    def forward(ctx, R, Z, func_ids, C_list, occ_list, clamp):
+        c = R.detach().cpu().numpy()
+        g = A.make_flat_grid(c, Z, NRAD, ORDER, weight_threshold=-1.0, radial="ta", becke_clamp=clamp)
+        fb = A.FockBuilder(c, Z, A.make_manual_basis(funcs_at(c, Z)), g, func_ids=func_ids)
+        E, _, _ = fb.build(C_list, occ_list, precision="fp64")
+        G = fb.xc_gradient(C_list, occ_list, becke_clamp=clamp)
+        fb.close()
+        ctx.save_for_backward(torch.as_tensor(G, dtype=R.dtype))
+        return torch.tensor(E, dtype=R.dtype)
+
+    @staticmethod
+    def backward(ctx, gE):
+        (G,) = ctx.saved_tensors
+        return gE * G, None, None, None, None, None
+
+
+def test_autograd_wrapper_gradcheck_water():
+    # torch.autograd.gradcheck: central differences of the wrapped FP64 E_xc
+    # (eps 1e-4 bohr) against backward() for all nine coordinates
+    c, Z = M.water()
+    c = np.asarray(c) + np.random.default_rng(8).normal(0, 0.05, size=np.shape(c))
+    Cm = M.random_orbitals(len(funcs_at(c, Z)), 5, seed=9)
+    occ = 2.0 * np.ones(5)
+    R = torch.tensor(c, dtype=torch.float64, requires_grad=True)
+    f = lambda x: XcEnergy.apply(x, Z, ("GGA_X_PBE", "GGA_C_PBE"), [Cm], [occ], 5.0)  # noqa: E731
+    assert torch.autograd.gradcheck(f, (R,), eps=1e-4, atol=1e-7, rtol=1e-6)
+    E = f(R)
+    E.backward()
+    assert torch.abs(R.grad.sum(0)).max() < 1e-9  # translation invariance
+
+
+def test_screened_becke_gradient_short_clamp_cluster():
+    # a short Laqua clamp (2 bohr) on (H2O)4 makes the per-point candidate
+    # list of the Becke-weight term drop most atoms (r >= r_min + 2 Rc); the
+    # analytic gradient still equals Richardson central differences of the
+    # GPU E_xc built on grids with the same clamp
+    c, Z = M.water_cluster(4, seed=10)
+    c = np.asarray(c, float)
+    Cm = M.random_orbitals(len(funcs_at(c, Z)), 20, seed=11)
+    occ = 2.0 * np.ones(20)
+    xc = ("GGA_X_PBE", "GGA_C_PBE")
+    R = torch.tensor(c, dtype=torch.float64, requires_grad=True)
+    E = XcEnergy.apply(R, Z, xc, [Cm], [occ], 2.0)
+    E.backward()
+    G = R.grad.numpy()
+    assert np.abs(G.sum(0)).max() < 1e-8
+
+    def energy(cc):
+        return float(XcEnergy.apply(torch.tensor(cc), Z, xc, [Cm], [occ], 2.0))
+
+    for a, k in ((1, 0), (6, 2), (11, 1)):
+        def central(h):
+            cp, cm = c.copy(), c.copy()
+            cp[a, k] += h
+            cm[a, k] -= h
+            return (energy(cp) - energy(cm)) / (2 * h)
+        fd = (4.0 * central(H / 2) - central(H)) / 3.0
+        assert abs(G[a, k] - fd) < 1e-8, (a, k, G[a, k], fd)
