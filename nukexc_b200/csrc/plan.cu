@@ -540,8 +540,9 @@ __global__ void aux_y_shell_kernel(const AuxShell *__restrict__ shells, const in
                                    const double *__restrict__ px, const double *__restrict__ py,
                                    const double *__restrict__ pz, const double *__restrict__ w,
                                    const double *__restrict__ rho, int nspin, long npad, long slice,
-                                   double *__restrict__ y) {
-  const AuxShell sh = shells[list[blockIdx.x]];
+                                   const float *__restrict__ rtab, double *__restrict__ y) {
+  const int shell = list[blockIdx.x];
+  const AuxShell sh = shells[shell];
   const AuxFunc &f = sh.f;
   const long g0 = blockIdx.y * slice, g1 = min(npad, g0 + slice);
   double acc[15];
@@ -553,7 +554,8 @@ __global__ void aux_y_shell_kernel(const AuxShell *__restrict__ shells, const in
     const double wr = w[g] * r;
     if (wr == 0.0) continue;
     const double dx = px[g] - f.cx, dy = py[g] - f.cy, dz = pz[g] - f.cz;
-    const double wI = wr * aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz));
+    const double wI =
+        wr * (rtab ? (double)rtab[(size_t)shell * npad + g] : aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz)));
 #pragma unroll
     for (int k = 0; k < 15; ++k)
       if (k < sh.nm) acc[k] += wI * (f.C * solid_harmonic(f.l, f.m + k, dx, dy, dz));
@@ -579,12 +581,29 @@ __global__ void aux_y_shell_kernel(const AuxShell *__restrict__ shells, const in
 // y over the functions of one (centre, l) group of complete shells: per
 // point one distance, one set of 2L+1 solid harmonics, then the radial factor
 // of each shell (coulomb.hpp:84-85).
+// FP32 table of the aux shells' radial factors R(shell, g) = I(|r_g - A|)
+// (the factor aux_radial evaluates; V_a = C S_lm R), one row of npad points
+// per shell.  It depends on the geometry only, so the mixed-precision build
+// computes it once per plan and both J passes read it instead of
+// re-evaluating the incomplete gamma functions: the grid RI-J's 3-index
+// contractions in mixed precision (FP32 operands, FP64 accumulation).
+__global__ void aux_rtab_kernel(const AuxShell *__restrict__ shells, int nshell, const double *__restrict__ px,
+                                const double *__restrict__ py, const double *__restrict__ pz, long npad,
+                                float *__restrict__ rtab) {
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int sh = blockIdx.y;
+  if (g >= npad || sh >= nshell) return;
+  const AuxFunc &f = shells[sh].f;
+  const double dx = px[g] - f.cx, dy = py[g] - f.cy, dz = pz[g] - f.cz;
+  rtab[(size_t)sh * npad + g] = (float)aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz));
+}
+
 template <int L>
 __global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const AuxShell *__restrict__ shells,
                                    const double *__restrict__ px, const double *__restrict__ py,
                                    const double *__restrict__ pz, const double *__restrict__ w,
                                    const double *__restrict__ rho, int nspin, long npad, long slice,
-                                   double *__restrict__ y) {
+                                   const float *__restrict__ rtab, double *__restrict__ y) {
   constexpr int NM = 2 * L + 1, QM = aux_group_max(L);
   const AuxGroup G = groups[blockIdx.x];
   const long g0 = blockIdx.y * slice, g1 = min(npad, g0 + slice);
@@ -607,7 +626,8 @@ __global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const Au
     for (int q = 0; q < QM; ++q) {
       if (q >= G.n) break;
       const AuxFunc &f = shells[G.first + q].f;
-      const double wI = wr * aux_radial_r(f, rr, r2l1inv);
+      const double wI =
+          wr * (rtab ? (double)rtab[(size_t)(G.first + q) * npad + g] : aux_radial_r(f, rr, r2l1inv));
 #pragma unroll
       for (int m = 0; m < NM; ++m) acc[q][m] += wI * (f.C * S[m]);
     }
@@ -634,7 +654,8 @@ __global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const Au
 
 template <int L>
 __device__ __forceinline__ double aux_group_v(const AuxGroup &G, const AuxShell *__restrict__ shells,
-                                              const double *__restrict__ c, double x, double y, double z) {
+                                              const double *__restrict__ c, double x, double y, double z,
+                                              const float *__restrict__ rtab, long npad, long g) {
   constexpr int NM = 2 * L + 1;
   const double dx = x - G.cx, dy = y - G.cy, dz = z - G.cz;
   const double rr = sqrt(dx * dx + dy * dy + dz * dz);
@@ -647,7 +668,8 @@ __device__ __forceinline__ double aux_group_v(const AuxGroup &G, const AuxShell 
     double a = 0.0;
 #pragma unroll
     for (int m = 0; m < NM; ++m) a += c[sh.first + m] * (sh.f.C * S[m]);
-    if (a != 0.0) s += a * aux_radial_r(sh.f, rr, r2l1inv);
+    if (a != 0.0)
+      s += a * (rtab ? (double)rtab[(size_t)(G.first + q) * npad + g] : aux_radial_r(sh.f, rr, r2l1inv));
   }
   return s;
 }
@@ -658,7 +680,8 @@ __global__ void aux_v_group_kernel(const AuxGroup *__restrict__ groups, int4 gof
                                    const AuxShell *__restrict__ shells, const int *__restrict__ loose, int nloose,
                                    const double *__restrict__ c, const double *__restrict__ px,
                                    const double *__restrict__ py, const double *__restrict__ pz,
-                                   const double *__restrict__ w, long npad, double *__restrict__ v) {
+                                   const double *__restrict__ w, long npad, const float *__restrict__ rtab,
+                                   double *__restrict__ v) {
   const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (g >= npad) return;
   if (w[g] == 0.0) {
@@ -668,17 +691,18 @@ __global__ void aux_v_group_kernel(const AuxGroup *__restrict__ groups, int4 gof
   const double x = px[g], y = py[g], z = pz[g];
   double s = 0.0;
   // groups sorted by l: [0, goff.x) l = 0, [goff.x, goff.y) l = 1, ...
-  for (int k = 0; k < goff.x; ++k) s += aux_group_v<0>(groups[k], shells, c, x, y, z);
-  for (int k = goff.x; k < goff.y; ++k) s += aux_group_v<1>(groups[k], shells, c, x, y, z);
-  for (int k = goff.y; k < goff.z; ++k) s += aux_group_v<2>(groups[k], shells, c, x, y, z);
-  for (int k = goff.z; k < goff.w; ++k) s += aux_group_v<3>(groups[k], shells, c, x, y, z);
+  for (int k = 0; k < goff.x; ++k) s += aux_group_v<0>(groups[k], shells, c, x, y, z, rtab, npad, g);
+  for (int k = goff.x; k < goff.y; ++k) s += aux_group_v<1>(groups[k], shells, c, x, y, z, rtab, npad, g);
+  for (int k = goff.y; k < goff.z; ++k) s += aux_group_v<2>(groups[k], shells, c, x, y, z, rtab, npad, g);
+  for (int k = goff.z; k < goff.w; ++k) s += aux_group_v<3>(groups[k], shells, c, x, y, z, rtab, npad, g);
   for (int k = 0; k < nloose; ++k) {
     const AuxShell &sh = shells[loose[k]];
     const AuxFunc &f = sh.f;
     const double dx = x - f.cx, dy = y - f.cy, dz = z - f.cz;
     double a = 0.0;
     for (int m = 0; m < sh.nm; ++m) a += c[sh.first + m] * (f.C * solid_harmonic(f.l, f.m + m, dx, dy, dz));
-    if (a != 0.0) s += a * aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz));
+    if (a != 0.0)
+      s += a * (rtab ? (double)rtab[(size_t)loose[k] * npad + g] : aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz)));
   }
   v[g] = s * w[g];
 }
@@ -1273,7 +1297,35 @@ void launch_colloc(Plan &P, const Chunk &c, cudaStream_t s) {
 // sharded over ranks can sum y between them: coulomb_y forms this plan's
 // y = Vw rho_total over its points; coulomb_solve solves c = (A|B)^-1 y
 // (pivoted Cholesky or half inverse) and forms v_g = w_g sum_a c_a V_a(g).
-void coulomb_y(Plan &P, int nspin, cudaStream_t s) {
+// The FP64 build evaluates the potentials' radial factors; the mixed build
+// reads them from the plan's FP32 table when it fits (coulomb_table).
+// The FP32 radial-factor table of the mixed build (aux_rtab_kernel), made on
+// first use when it fits in a quarter of the free device memory (and
+// kRtabMaxBytes); otherwise the J passes evaluate the factors as FP64 does.
+constexpr size_t kRtabMaxBytes = (size_t)32 << 30;
+static const float *coulomb_table(Plan &P, bool mixed, cudaStream_t s) {
+  if (!mixed || P.rtab_failed) return nullptr;
+  if (!P.d_rtab) {
+    const size_t bytes = (size_t)P.nashell * P.npad * sizeof(float);
+    size_t fr = 0, tot = 0;
+    NKX_CUDA(cudaMemGetInfo(&fr, &tot));
+    if (bytes > kRtabMaxBytes || bytes > fr / 4 || cudaMalloc(&P.d_rtab, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      P.d_rtab = nullptr;
+      P.rtab_failed = true;
+      return nullptr;
+    }
+    P.allocs.push_back(P.d_rtab);
+    aux_rtab_kernel<<<dim3(nblk(P.npad, 256), (unsigned)P.nashell), 256, 0, s>>>(P.d_ashell, P.nashell, P.d_px, P.d_py,
+                                                                                P.d_pz, P.npad, P.d_rtab);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+  }
+  return P.d_rtab;
+}
+
+void coulomb_y(Plan &P, int nspin, cudaStream_t s, bool mixed) {
+    const float *rtab = coulomb_table(P, mixed, s);
     NKX_CUDA(cudaMemsetAsync(P.d_y, 0, sizeof(double) * P.naux, s));
     const long nsl = std::max<long>(1, std::min<long>(64, (P.npad + 4095) / 4096));
     const long slice = (P.npad + nsl - 1) / nsl;
@@ -1283,23 +1335,25 @@ void coulomb_y(Plan &P, int nspin, cudaStream_t s) {
       const AuxGroup *gp = P.d_agroup + P.h_group_off[L];
       const dim3 gy((unsigned)n, (unsigned)nsl);
       switch (L) {
-        case 0: aux_y_group_kernel<0><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, P.d_y); break;
-        case 1: aux_y_group_kernel<1><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, P.d_y); break;
-        case 2: aux_y_group_kernel<2><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, P.d_y); break;
-        default: aux_y_group_kernel<3><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, P.d_y); break;
+        case 0: aux_y_group_kernel<0><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y); break;
+        case 1: aux_y_group_kernel<1><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y); break;
+        case 2: aux_y_group_kernel<2><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y); break;
+        default: aux_y_group_kernel<3><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y); break;
       }
       NKX_LAUNCH_CHECK();
       ++P.launches;
     }
     if (P.nloose > 0) {
       aux_y_shell_kernel<<<dim3(P.nloose, (unsigned)nsl), 256, 0, s>>>(P.d_ashell, P.d_loose, P.d_px, P.d_py, P.d_pz,
-                                                                      P.d_w, P.d_rho, nspin, P.npad, slice, P.d_y);
+                                                                      P.d_w, P.d_rho, nspin, P.npad, slice, rtab,
+                                                                      P.d_y);
       NKX_LAUNCH_CHECK();
       ++P.launches;
     }
 }
 
-void coulomb_solve(Plan &P, cudaStream_t s) {
+void coulomb_solve(Plan &P, cudaStream_t s, bool mixed) {
+    const float *rtab = coulomb_table(P, mixed, s);
     if (P.svd_mode) {
       const double one = 1.0, zero = 0.0;
       cublasHandle_t hb = (cublasHandle_t)P.cublas;
@@ -1323,14 +1377,9 @@ void coulomb_solve(Plan &P, cudaStream_t s) {
     }
     const int4 goff = make_int4(P.h_group_off[1], P.h_group_off[2], P.h_group_off[3], P.h_group_off[4]);
     aux_v_group_kernel<<<nblk(P.npad, 128), 128, 0, s>>>(P.d_agroup, goff, P.d_ashell, P.d_loose, P.nloose,
-                                                         P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, P.d_vj);
+                                                         P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, rtab, P.d_vj);
     NKX_LAUNCH_CHECK();
     ++P.launches;
-}
-
-void coulomb_fit(Plan &P, int nspin, cudaStream_t s) {
-  coulomb_y(P, nspin, s);
-  coulomb_solve(P, s);
 }
 
 // FP64 pass A: collocation + density of every chunk into d_rho / d_grad
@@ -1383,7 +1432,7 @@ void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool s
     fp64_density_pass(P, nspin, nocc, s, T);
     if (needJ) {
       T.begin(ST_COULOMB, s);
-      coulomb_y(P, nspin, s);
+      coulomb_y(P, nspin, s, false);
       T.end(s);
     }
     if (phase == 1) return;
@@ -1391,7 +1440,7 @@ void fock_build_fp64(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool s
   // ---- J: fit coefficients and fitted potential
   if (needJ) {
     T.begin(ST_COULOMB, s);
-    coulomb_solve(P, s);
+    coulomb_solve(P, s, false);
     T.end(s);
   }
   // ---- functional

@@ -58,6 +58,8 @@ struct Plan {
   int nagroup = 0, nloose = 0;
   std::vector<int> h_group_off;  // groups of l = L at [off[L], off[L+1])
   int *d_loose = nullptr;        // shells outside the groups
+  float *d_rtab = nullptr;       // FP32 radial factors [shell][point] of the mixed build's J
+  bool rtab_failed = false;      // the table did not fit: the mixed J evaluates the factors
 
   // screening: pairs of (batch, significant function block), CSR by batch
   std::vector<int> h_pair_off;
@@ -171,7 +173,8 @@ __global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, long
                                   double *__restrict__ edens);
 void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
                       StageTimer &T, int phase);
-void coulomb_y(Plan &P, int nspin, cudaStream_t s);
-void coulomb_solve(Plan &P, cudaStream_t s);
+// mixed: read the aux radial factors from the plan's FP32 table (made on first use)
+void coulomb_y(Plan &P, int nspin, cudaStream_t s, bool mixed);
+void coulomb_solve(Plan &P, cudaStream_t s, bool mixed);
 
 }  // namespace nkx

@@ -1375,13 +1375,13 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       for (const Chunk &c : P.chunks) pass_a(c);
       // this plan's share of the J fit vector
       Tm.begin(ST_COULOMB, s);
-      coulomb_y(P, nspin, s);
+      coulomb_y(P, nspin, s, true);
       Tm.end(s);
       if (phase == 1) return;
     }
     // ---- J fit and the functional, in FP64
     Tm.begin(ST_COULOMB, s);
-    coulomb_solve(P, s);
+    coulomb_solve(P, s, true);
     Tm.end(s);
     Tm.begin(ST_FUNC, s);
     functional_kernel<<<(unsigned)((P.npad + 255) / 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.npad, P.d_w,
