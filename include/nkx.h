@@ -232,6 +232,16 @@ NKX_API nkx_status nkx_core_hamiltonian_dense(const nkx_basis *basis, const nkx_
                                               const double *d_points, const double *d_w, long npts, double *d_S,
                                               double *d_T, double *d_V, void *stream);
 
+/* The quadrature core Hamiltonian of nkx_core_hamiltonian_dense over a plan's
+ * screened batches: only (batch, 128-function block) pairs with the block
+ * significant are integrated, as the reference's screened variants do
+ * (compute_core_hamiltonian_screened / _scratch / _tiled / _sparse,
+ * nukexc/core_hamiltonian.hpp:320-1155).  FP64.  S, T, V (nbf x nbf,
+ * column-major; mem: host or device buffers); mol holds host centres and
+ * charges. */
+NKX_API nkx_status nkx_plan_core_hamiltonian(nkx_plan *plan, const nkx_molecule *mol, double *S, double *T, double *V,
+                                             int mem, void *stream);
+
 /* compute_half_inverse (nukexc/nukexc_utils.hpp:198-270): X = U s^-1/2 / D
  * of the preconditioned metric, keeping s > thr (symmetric
  * eigendecomposition on the device).  d_X must hold N*N; *K receives the

@@ -27,7 +27,7 @@ EXPORTS = [
     "nkx_plan_set_functional", "nkx_plan_set_half_inverse", "nkx_plan_aux_metric", "nkx_plan_density",
     "nkx_morton_order", "nkx_neighbor_list", "nkx_aux_metric", "nkx_exchange_dense", "nkx_plan_set_wait_limit",
     "nkx_fock_build_phase1", "nkx_fock_build_phase2", "nkx_plan_set_metric",
-    "nkx_plan_autotune", "nkx_plan_get_tuning", "nkx_plan_set_tuning",
+    "nkx_plan_autotune", "nkx_plan_get_tuning", "nkx_plan_set_tuning", "nkx_plan_core_hamiltonian",
 ]
 
 
@@ -107,6 +107,7 @@ def lib():
             "nkx_plan_set_metric": [vp, vp, i],
             "nkx_plan_autotune": [vp, i, i, vp, vp, i, C.c_char_p, vp, vp],
             "nkx_plan_get_tuning": [vp, vp],
+            "nkx_plan_core_hamiltonian": [vp, vp, vp, vp, vp, i, vp],
             "nkx_plan_set_tuning": [vp, vp],
             "nkx_xc_gradient": [vp, i, i, vp, vp, i, d, vp, vp],
             "nkx_get_last_timing": [vp, vp],

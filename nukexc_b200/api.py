@@ -491,6 +491,18 @@ class FockBuilder:
         t = L.Tuning(v_n, dens_n, ypath, chunk_pairs, 0, 0, 0.0, 0.0)
         check(L.lib().nkx_plan_set_tuning(self._h, C.byref(t)))
 
+    def core_hamiltonian(self, centers, Z):
+        """S, T, V_n by quadrature over the plan's screened batches (the
+        reference's compute_core_hamiltonian_screened family;
+        nkx_plan_core_hamiltonian), FP64 numpy matrices."""
+        mol, keep = _mol(centers, Z)
+        n = self.nbf * self.nbf
+        S, T, V = np.empty(n), np.empty(n), np.empty(n)
+        check(L.lib().nkx_plan_core_hamiltonian(self._h, C.byref(mol), S.ctypes.data_as(C.c_void_p),
+                                                T.ctypes.data_as(C.c_void_p), V.ctypes.data_as(C.c_void_p),
+                                                L.MEM_HOST, None))
+        return tuple(M.reshape(self.nbf, self.nbf) for M in (S, T, V))
+
     def set_metric(self, S):
         """Replace the plan's Coulomb metric (A|B) (naux x naux) and factor it
         again (nkx_plan_set_metric); for a sharded grid, the sum over ranks of

@@ -402,7 +402,7 @@ __device__ __forceinline__ void vstep_next(const uint32_t *__restrict__ mask, in
 }
 
 __global__ void __launch_bounds__(256) vgemm_fp64_kernel(const double *__restrict__ phiT, const double *__restrict__ zT,
-                                                         int phi_stride_tiles, int nz, const int *__restrict__ pair_off,
+                                                         int phi_stride_tiles, int z_stride, const int *__restrict__ pair_off,
                                                          const uint32_t *__restrict__ mask, int mask_words, long b0,
                                                          long b1, long p0, int nbf_pad, double *__restrict__ V) {
   extern __shared__ __align__(16) double vsm[];  // [stage][A | B][kVKs][128]
@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(256) vgemm_fp64_kernel(const double *__restric
       const uint32_t *m = mask + lb * mask_words;
       const long qb = pair_off[lb] - p0;
       const double *A = phiT + (size_t)(qb + block_pos(m, I)) * phi_stride_tiles * tile + (size_t)lk * kVKs * kBlockF;
-      const double *B = zT + ((size_t)(qb + block_pos(m, J)) * nz + zi) * tile + (size_t)lk * kVKs * kBlockF;
+      const double *B = zT + ((size_t)(qb + block_pos(m, J)) * z_stride + zi) * tile + (size_t)lk * kVKs * kBlockF;
       double *dA = vsm + st * kVStageDoubles, *dB = dA + kVKs * kBlockF;
 #pragma unroll
       for (int r = 0; r < (kVKs * kBlockF / 2) / 256; ++r) {
@@ -555,10 +555,10 @@ __global__ void aux_y_shell_kernel(const AuxShell *__restrict__ shells, const in
     if (wr == 0.0) continue;
     const double dx = px[g] - f.cx, dy = py[g] - f.cy, dz = pz[g] - f.cz;
     const double wI =
-        wr * (rtab ? (double)rtab[(size_t)shell * npad + g] : aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz)));
+        wr * (rtab ? (double)rtab[(size_t)shell * npad + g] : f.C * aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz)));
 #pragma unroll
     for (int k = 0; k < 15; ++k)
-      if (k < sh.nm) acc[k] += wI * (f.C * solid_harmonic(f.l, f.m + k, dx, dy, dz));
+      if (k < sh.nm) acc[k] += wI * solid_harmonic(f.l, f.m + k, dx, dy, dz);
   }
   __shared__ double red[32];
   for (int k = 0; k < sh.nm; ++k) {
@@ -581,9 +581,9 @@ __global__ void aux_y_shell_kernel(const AuxShell *__restrict__ shells, const in
 // y over the functions of one (centre, l) group of complete shells: per
 // point one distance, one set of 2L+1 solid harmonics, then the radial factor
 // of each shell (coulomb.hpp:84-85).
-// FP32 table of the aux shells' radial factors R(shell, g) = I(|r_g - A|)
-// (the factor aux_radial evaluates; V_a = C S_lm R), one row of npad points
-// per shell.  It depends on the geometry only, so the mixed-precision build
+// FP32 table of the aux shells' scaled radial factors C R(shell, g), with
+// R = I(|r_g - A|) the factor aux_radial evaluates (V_a = C S_lm R), one row
+// of npad points per shell.  It depends on the geometry only, so the mixed-precision build
 // computes it once per plan and both J passes read it instead of
 // re-evaluating the incomplete gamma functions: the grid RI-J's 3-index
 // contractions in mixed precision (FP32 operands, FP64 accumulation).
@@ -595,10 +595,12 @@ __global__ void aux_rtab_kernel(const AuxShell *__restrict__ shells, int nshell,
   if (g >= npad || sh >= nshell) return;
   const AuxFunc &f = shells[sh].f;
   const double dx = px[g] - f.cx, dy = py[g] - f.cy, dz = pz[g] - f.cz;
-  rtab[(size_t)sh * npad + g] = (float)aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz));
+  rtab[(size_t)sh * npad + g] = (float)(f.C * aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz)));
 }
 
-template <int L>
+// TAB: C R from the mixed build's table (no distance powers or radial
+// factors evaluated here)
+template <int L, bool TAB>
 __global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const AuxShell *__restrict__ shells,
                                    const double *__restrict__ px, const double *__restrict__ py,
                                    const double *__restrict__ pz, const double *__restrict__ w,
@@ -612,24 +614,34 @@ __global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const Au
   for (int q = 0; q < QM; ++q)
 #pragma unroll
     for (int m = 0; m < NM; ++m) acc[q][m] = 0.0;
+  const float *tab = TAB ? rtab + (size_t)G.first * npad : nullptr;
   for (long g = g0 + threadIdx.x; g < g1; g += blockDim.x) {
     double r = rho[g];
     if (nspin == 2) r += rho[npad + g];
     const double wr = w[g] * r;
     if (wr == 0.0) continue;
     const double dx = px[g] - G.cx, dy = py[g] - G.cy, dz = pz[g] - G.cz;
-    const double rr = sqrt(dx * dx + dy * dy + dz * dz);
-    const double r2l1inv = rr < 1e-12 ? 0.0 : ipow_c<2 * L + 1>(1.0 / rr);
     double S[NM];
     solid_harmonics_all<L>(dx, dy, dz, S);
+    if constexpr (TAB) {
 #pragma unroll
-    for (int q = 0; q < QM; ++q) {
-      if (q >= G.n) break;
-      const AuxFunc &f = shells[G.first + q].f;
-      const double wI =
-          wr * (rtab ? (double)rtab[(size_t)(G.first + q) * npad + g] : aux_radial_r(f, rr, r2l1inv));
+      for (int q = 0; q < QM; ++q) {
+        if (q >= G.n) break;
+        const double wI = wr * (double)tab[(size_t)q * npad + g];
 #pragma unroll
-      for (int m = 0; m < NM; ++m) acc[q][m] += wI * (f.C * S[m]);
+        for (int m = 0; m < NM; ++m) acc[q][m] = fma(wI, S[m], acc[q][m]);
+      }
+    } else {
+      const double rr = sqrt(dx * dx + dy * dy + dz * dz);
+      const double r2l1inv = rr < 1e-12 ? 0.0 : ipow_c<2 * L + 1>(1.0 / rr);
+#pragma unroll
+      for (int q = 0; q < QM; ++q) {
+        if (q >= G.n) break;
+        const AuxFunc &f = shells[G.first + q].f;
+        const double wI = wr * (f.C * aux_radial_r(f, rr, r2l1inv));
+#pragma unroll
+        for (int m = 0; m < NM; ++m) acc[q][m] = fma(wI, S[m], acc[q][m]);
+      }
     }
   }
   __shared__ double red[32];
@@ -652,30 +664,40 @@ __global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const Au
   }
 }
 
-template <int L>
+template <int L, bool TAB>
 __device__ __forceinline__ double aux_group_v(const AuxGroup &G, const AuxShell *__restrict__ shells,
                                               const double *__restrict__ c, double x, double y, double z,
                                               const float *__restrict__ rtab, long npad, long g) {
   constexpr int NM = 2 * L + 1;
   const double dx = x - G.cx, dy = y - G.cy, dz = z - G.cz;
-  const double rr = sqrt(dx * dx + dy * dy + dz * dz);
-  const double r2l1inv = rr < 1e-12 ? 0.0 : ipow_c<2 * L + 1>(1.0 / rr);
   double S[NM];
   solid_harmonics_all<L>(dx, dy, dz, S);
   double s = 0.0;
-  for (int q = 0; q < G.n; ++q) {
-    const AuxShell &sh = shells[G.first + q];
-    double a = 0.0;
+  if constexpr (TAB) {
+    for (int q = 0; q < G.n; ++q) {
+      const int f0 = shells[G.first + q].first;
+      double a = 0.0;
 #pragma unroll
-    for (int m = 0; m < NM; ++m) a += c[sh.first + m] * (sh.f.C * S[m]);
-    if (a != 0.0)
-      s += a * (rtab ? (double)rtab[(size_t)(G.first + q) * npad + g] : aux_radial_r(sh.f, rr, r2l1inv));
+      for (int m = 0; m < NM; ++m) a = fma(c[f0 + m], S[m], a);
+      s = fma(a, (double)rtab[(size_t)(G.first + q) * npad + g], s);
+    }
+  } else {
+    const double rr = sqrt(dx * dx + dy * dy + dz * dz);
+    const double r2l1inv = rr < 1e-12 ? 0.0 : ipow_c<2 * L + 1>(1.0 / rr);
+    for (int q = 0; q < G.n; ++q) {
+      const AuxShell &sh = shells[G.first + q];
+      double a = 0.0;
+#pragma unroll
+      for (int m = 0; m < NM; ++m) a += c[sh.first + m] * (sh.f.C * S[m]);
+      if (a != 0.0) s += a * aux_radial_r(sh.f, rr, r2l1inv);
+    }
   }
   return s;
 }
 
 // v_g = w_g sum_a c_a V_a(g) over the groups, then the loose shells
 // (coulomb.hpp:90-95)
+template <bool TAB>
 __global__ void aux_v_group_kernel(const AuxGroup *__restrict__ groups, int4 goff,
                                    const AuxShell *__restrict__ shells, const int *__restrict__ loose, int nloose,
                                    const double *__restrict__ c, const double *__restrict__ px,
@@ -691,18 +713,18 @@ __global__ void aux_v_group_kernel(const AuxGroup *__restrict__ groups, int4 gof
   const double x = px[g], y = py[g], z = pz[g];
   double s = 0.0;
   // groups sorted by l: [0, goff.x) l = 0, [goff.x, goff.y) l = 1, ...
-  for (int k = 0; k < goff.x; ++k) s += aux_group_v<0>(groups[k], shells, c, x, y, z, rtab, npad, g);
-  for (int k = goff.x; k < goff.y; ++k) s += aux_group_v<1>(groups[k], shells, c, x, y, z, rtab, npad, g);
-  for (int k = goff.y; k < goff.z; ++k) s += aux_group_v<2>(groups[k], shells, c, x, y, z, rtab, npad, g);
-  for (int k = goff.z; k < goff.w; ++k) s += aux_group_v<3>(groups[k], shells, c, x, y, z, rtab, npad, g);
+  for (int k = 0; k < goff.x; ++k) s += aux_group_v<0, TAB>(groups[k], shells, c, x, y, z, rtab, npad, g);
+  for (int k = goff.x; k < goff.y; ++k) s += aux_group_v<1, TAB>(groups[k], shells, c, x, y, z, rtab, npad, g);
+  for (int k = goff.y; k < goff.z; ++k) s += aux_group_v<2, TAB>(groups[k], shells, c, x, y, z, rtab, npad, g);
+  for (int k = goff.z; k < goff.w; ++k) s += aux_group_v<3, TAB>(groups[k], shells, c, x, y, z, rtab, npad, g);
   for (int k = 0; k < nloose; ++k) {
     const AuxShell &sh = shells[loose[k]];
     const AuxFunc &f = sh.f;
     const double dx = x - f.cx, dy = y - f.cy, dz = z - f.cz;
     double a = 0.0;
-    for (int m = 0; m < sh.nm; ++m) a += c[sh.first + m] * (f.C * solid_harmonic(f.l, f.m + m, dx, dy, dz));
+    for (int m = 0; m < sh.nm; ++m) a += c[sh.first + m] * solid_harmonic(f.l, f.m + m, dx, dy, dz);
     if (a != 0.0)
-      s += a * (rtab ? (double)rtab[(size_t)loose[k] * npad + g] : aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz)));
+      s += a * (TAB ? (double)rtab[(size_t)loose[k] * npad + g] : f.C * aux_radial(f, sqrt(dx * dx + dy * dy + dz * dz)));
   }
   v[g] = s * w[g];
 }
@@ -1056,6 +1078,7 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
     P.h_centers.assign(mol->xyz, mol->xyz + 3 * (size_t)mol->natoms);
     P.d_centers = P.alloc<double>(3 * (size_t)P.natoms);
     NKX_CUDA(cudaMemcpy(P.d_centers, P.h_centers.data(), sizeof(double) * 3 * P.natoms, cudaMemcpyHostToDevice));
+
     std::vector<int> fatom(P.nbf_pad, 0);
     P.all_funcs_on_atoms = true;
     for (int q = 0; q < P.nbf_pad; ++q) {
@@ -1278,6 +1301,50 @@ static void build_plan(Plan &P, const nkx_molecule *mol, const nkx_basis *prim, 
   NKX_CUDA(cudaStreamSynchronize(P.stream));
 }
 
+// ------------------------------------------------- core Hamiltonian ----
+// w_g v_n(g) = w_g sum_A Z_A / (|r_g - R_A| + 1e-30), the nuclear attraction
+// weight of core_hamiltonian.hpp:133-289 (V_n = -sum_g w v_n phi phi^T)
+__global__ void core_vne_kernel(const double *__restrict__ px, const double *__restrict__ py,
+                                const double *__restrict__ pz, const double *__restrict__ w, long npad,
+                                const double *__restrict__ centers, const double *__restrict__ charges, int natoms,
+                                double *__restrict__ wv) {
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (g >= npad) return;
+  double v = 0.0;
+  if (w[g] != 0.0)
+    for (int a = 0; a < natoms; ++a) {
+      const double dx = px[g] - centers[3 * a], dy = py[g] - centers[3 * a + 1], dz = pz[g] - centers[3 * a + 2];
+      v += charges[a] / (sqrt(dx * dx + dy * dy + dz * dz) + 1e-30);
+    }
+  wv[g] = w[g] * v;
+}
+
+// Z planes of the core Hamiltonian for the pairs of one chunk, Z^T[pair][3][g][f]
+// from PhiT[pair][4][g][f]: round 0: plane 0 = 1/2 w phi (S), plane 1 =
+// -1/2 w v_n phi (V_n); round 1: plane k = 1/4 w d_k phi (T, k = x, y, z), so
+// that Vbar + Vbar^T of each contraction is the matrix itself.
+__global__ void core_z_kernel(const double *__restrict__ phiT, const double *__restrict__ w,
+                              const double *__restrict__ wv, const int *__restrict__ pair_batch, long p0, int round,
+                              double *__restrict__ zT) {
+  const size_t tile = (size_t)kBatch * kBlockF;
+  const long q = blockIdx.x;
+  const long b = pair_batch[p0 + q];
+  const double *P = phiT + (size_t)q * 4 * tile;
+  double *Z = zT + (size_t)q * 3 * tile;
+  for (int e = threadIdx.x; e < (int)tile; e += blockDim.x) {
+    const long g = b * kBatch + e / kBlockF;
+    if (round == 0) {
+      Z[e] = 0.5 * w[g] * P[e];
+      Z[tile + e] = -0.5 * wv[g] * P[e];
+    } else {
+      const double h = 0.25 * w[g];
+      Z[e] = h * P[tile + e];
+      Z[2 * tile + e] = h * P[3 * tile + e];
+      Z[tile + e] = h * P[2 * tile + e];
+    }
+  }
+}
+
 // ========================================================= Fock build ===
 
 void launch_colloc(Plan &P, const Chunk &c, cudaStream_t s) {
@@ -1335,10 +1402,30 @@ void coulomb_y(Plan &P, int nspin, cudaStream_t s, bool mixed) {
       const AuxGroup *gp = P.d_agroup + P.h_group_off[L];
       const dim3 gy((unsigned)n, (unsigned)nsl);
       switch (L) {
-        case 0: aux_y_group_kernel<0><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y); break;
-        case 1: aux_y_group_kernel<1><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y); break;
-        case 2: aux_y_group_kernel<2><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y); break;
-        default: aux_y_group_kernel<3><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y); break;
+        case 0:
+          if (rtab)
+            aux_y_group_kernel<0, true><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y);
+          else
+            aux_y_group_kernel<0, false><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y);
+          break;
+        case 1:
+          if (rtab)
+            aux_y_group_kernel<1, true><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y);
+          else
+            aux_y_group_kernel<1, false><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y);
+          break;
+        case 2:
+          if (rtab)
+            aux_y_group_kernel<2, true><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y);
+          else
+            aux_y_group_kernel<2, false><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y);
+          break;
+        default:
+          if (rtab)
+            aux_y_group_kernel<3, true><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y);
+          else
+            aux_y_group_kernel<3, false><<<gy, 256, 0, s>>>(gp, P.d_ashell, P.d_px, P.d_py, P.d_pz, P.d_w, P.d_rho, nspin, P.npad, slice, rtab, P.d_y);
+          break;
       }
       NKX_LAUNCH_CHECK();
       ++P.launches;
@@ -1376,8 +1463,14 @@ void coulomb_solve(Plan &P, cudaStream_t s, bool mixed) {
       P.launches += 2;
     }
     const int4 goff = make_int4(P.h_group_off[1], P.h_group_off[2], P.h_group_off[3], P.h_group_off[4]);
-    aux_v_group_kernel<<<nblk(P.npad, 128), 128, 0, s>>>(P.d_agroup, goff, P.d_ashell, P.d_loose, P.nloose,
-                                                         P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, rtab, P.d_vj);
+    if (rtab)
+      aux_v_group_kernel<true><<<nblk(P.npad, 128), 128, 0, s>>>(P.d_agroup, goff, P.d_ashell, P.d_loose, P.nloose,
+                                                                 P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, rtab,
+                                                                 P.d_vj);
+    else
+      aux_v_group_kernel<false><<<nblk(P.npad, 128), 128, 0, s>>>(P.d_agroup, goff, P.d_ashell, P.d_loose, P.nloose,
+                                                                  P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, rtab,
+                                                                  P.d_vj);
     NKX_LAUNCH_CHECK();
     ++P.launches;
 }
@@ -1843,6 +1936,74 @@ NKX_API nkx_status nkx_plan_density(nkx_plan *plan, int nspin, int nocc, const d
     NKX_CUDA(cudaStreamSynchronize(s));
     P.last_nspin = nspin;
     NKX_REQUIRE(status[1] == 0, NKX_ERR_NUMERIC, "non-finite value in the orbitals or occupations");
+  });
+}
+
+NKX_API nkx_status nkx_plan_core_hamiltonian(nkx_plan *plan, const nkx_molecule *mol, double *S, double *T,
+                                             double *V, int mem, void *stream) {
+  return run_guarded("nkx_plan_core_hamiltonian", [&] {
+    NKX_REQUIRE(plan && mol && mol->natoms > 0 && mol->xyz && mol->Z && S && T && V, NKX_ERR_ARG,
+                "invalid arguments");
+    NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
+    Plan &P = *reinterpret_cast<Plan *>(plan);
+    cudaStream_t s = stream ? (cudaStream_t)stream : P.stream;
+    const size_t tile = (size_t)kBatch * kBlockF, nn = (size_t)P.nbf_pad * P.nbf_pad;
+    std::vector<double> zc(mol->natoms);
+    for (int a = 0; a < mol->natoms; ++a) zc[a] = mol->Z[a];
+    double *dc = P.alloc<double>(3 * (size_t)mol->natoms), *dz = P.alloc<double>(mol->natoms);
+    NKX_CUDA(cudaMemcpyAsync(dc, mol->xyz, sizeof(double) * 3 * mol->natoms, cudaMemcpyHostToDevice, s));
+    NKX_CUDA(cudaMemcpyAsync(dz, zc.data(), sizeof(double) * mol->natoms, cudaMemcpyHostToDevice, s));
+    if (!P.ws_z) P.ws_z = P.alloc<double>(std::max<long>(1, P.max_chunk_pairs) * 3 * tile);
+    NKX_CUDA(cudaFuncSetAttribute(vgemm_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kVSmemBytes));
+    core_vne_kernel<<<nblk(P.npad, 256), 256, 0, s>>>(P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, dc, dz, mol->natoms,
+                                                     P.d_vj);
+    NKX_LAUNCH_CHECK();
+    NKX_CUDA(cudaMemsetAsync(P.d_V, 0, sizeof(double) * 3 * nn, s));
+    // the collocation with gradients whatever the plan's functional
+    const bool gga = P.gga;
+    P.gga = true;
+    try {
+      for (const Chunk &c : P.chunks) {
+        const long np = c.p1 - c.p0;
+        if (np <= 0) continue;
+        launch_colloc(P, c, s);
+        // S (plane 0) and V_n (plane 1)
+        core_z_kernel<<<(unsigned)np, 256, 0, s>>>(P.ws_phi, P.d_w, P.d_vj, P.d_pair_batch, c.p0, 0, P.ws_z);
+        vgemm_fp64_kernel<<<dim3(P.nblk, P.nblk, 2), 256, kVSmemBytes, s>>>(
+            P.ws_phi, P.ws_z, 4, 3, P.d_pair_off, P.d_mask, P.mask_words, c.b0, c.b1, c.p0, P.nbf_pad, P.d_V);
+        // T (plane 2): the three gradient components into one output
+        core_z_kernel<<<(unsigned)np, 256, 0, s>>>(P.ws_phi, P.d_w, P.d_vj, P.d_pair_batch, c.p0, 1, P.ws_z);
+        for (int k = 0; k < 3; ++k)
+          vgemm_fp64_kernel<<<dim3(P.nblk, P.nblk, 1), 256, kVSmemBytes, s>>>(
+              P.ws_phi + (size_t)(k + 1) * tile, P.ws_z + (size_t)k * tile, 4, 3, P.d_pair_off, P.d_mask,
+              P.mask_words, c.b0, c.b1, c.p0, P.nbf_pad, P.d_V + 2 * nn);
+        NKX_LAUNCH_CHECK();
+      }
+    } catch (...) {
+      P.gga = gga;
+      throw;
+    }
+    P.gga = gga;
+    const size_t nb = (size_t)P.nbf * P.nbf;
+    double *out = nullptr;
+    if (mem == NKX_MEM_HOST) {
+      if (!P.d_out) P.d_out = P.alloc<double>(3 * nb);
+      out = P.d_out;
+    }
+    double *dst[3] = {mem == NKX_MEM_HOST ? out : S, mem == NKX_MEM_HOST ? out + nb : V,
+                      mem == NKX_MEM_HOST ? out + 2 * nb : T};
+    dim3 tb(16, 16), gb(nblk(P.nbf, 16), nblk(P.nbf, 16));
+    for (int z = 0; z < 3; ++z)
+      symmetrize_unpad_kernel<<<gb, tb, 0, s>>>(P.nbf, P.nbf_pad, P.d_finv, P.d_V + z * nn, dst[z]);
+    NKX_LAUNCH_CHECK();
+    if (mem == NKX_MEM_HOST) {
+      NKX_CUDA(cudaMemcpyAsync(S, dst[0], sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+      NKX_CUDA(cudaMemcpyAsync(V, dst[1], sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+      NKX_CUDA(cudaMemcpyAsync(T, dst[2], sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+    }
+    NKX_CUDA(cudaStreamSynchronize(s));
+    P.release(dc);
+    P.release(dz);
   });
 }
 

@@ -102,6 +102,18 @@ struct TcArgs {
   int nt;  // MMA width N of the launched kernel (V: 128 / nt units per output tile)
 };
 
+// S = 2^24 L0 + 2^16 L1 + 2^8 L2 + L3 of four int32 accumulator levels,
+// exact: the integer sum (|S| < 2^49) is formed in int64 and converted by
+// adding the bit pattern of 1.5 2^52 (the sum is then the FP64 number
+// 1.5 2^52 + S, exact below 2^51) and subtracting 1.5 2^52 in FP64.  Measured
+// on B200: 16.7 values per clock and SM against 11.8 for an int64 -> FP64
+// conversion instruction and 14.8 for four int32 conversions and FMAs.
+__device__ __forceinline__ double level_sum(uint32_t l0, uint32_t l1, uint32_t l2, uint32_t l3) {
+  const long long S = (long long)(int)l0 * (1LL << 24) + (long long)(int)l1 * (1LL << 16) +
+                      (long long)(int)l2 * (1LL << 8) + (long long)(int)l3;
+  return __longlong_as_double(S + 0x4338000000000000LL) - 0x1.8p52;
+}
+
 struct UnitIter {
   int I = 0, J = 0, zi = 0, sp = 0, hc = 0;  // V: row block, column block, Z plane, batch split, column part
   long bl = 0;                     // density: batch within chunk
@@ -374,9 +386,9 @@ __global__ void __launch_bounds__(TcShape<NW>::kThreads, 1)
             sbs = a.nblk;
           }
         }
-        // exact integer combine of the four levels, S = sum_L 2^(8 (3 - L)) Acc_L:
-        // |Acc_L| < 2^24 for K <= 256, so |S| < 2^49 converts to FP64 exactly;
-        // the product is s_a s_b 2^-36 S (one rounding per group and element)
+        // exact combine of the four levels, S = sum_L 2^(8 (3 - L)) Acc_L:
+        // |Acc_L| < 2^24 for K <= 256, so |S| < 2^49 (level_sum); the product
+        // is s_a s_b 2^-36 S (one rounding per group and element)
         // the warp's 32 column scales, one per lane, handed out by shuffles
         const double sbl = live ? sb[lane * sbs] : 0.0;
         // slices of SL columns: 8 for the 320-thread shape, 4 for the
@@ -410,16 +422,14 @@ __global__ void __launch_bounds__(TcShape<NW>::kThreads, 1)
             double *Yp = a.Y + ((it.q * a.nspin + it.s) * 256 + 128 * it.h + row) * 128 + 64 * it.t + 32 * cq + SL * hh;
 #pragma unroll
             for (int j = 0; j < SL; ++j) {
-              const long long S = (long long)(int)v0[j] * (1LL << 24) + (long long)(int)v1[j] * (1LL << 16) +
-                                  (long long)(int)v2[j] * (1LL << 8) + (long long)(int)v3[j];
-              Yp[j] = (double)S * (sa * __shfl_sync(0xffffffffu, sbl, SL * hh + j));
+              const double S = level_sum(v0[j], v1[j], v2[j], v3[j]);
+              Yp[j] = S * (sa * __shfl_sync(0xffffffffu, sbl, SL * hh + j));
             }
           } else if (live) {
 #pragma unroll
             for (int j = 0; j < SL; ++j) {
-              const long long S = (long long)(int)v0[j] * (1LL << 24) + (long long)(int)v1[j] * (1LL << 16) +
-                                  (long long)(int)v2[j] * (1LL << 8) + (long long)(int)v3[j];
-              acc[SL * hh + j] = fma((double)S, sa * __shfl_sync(0xffffffffu, sbl, SL * hh + j), acc[SL * hh + j]);
+              const double S = level_sum(v0[j], v1[j], v2[j], v3[j]);
+              acc[SL * hh + j] = fma(S, sa * __shfl_sync(0xffffffffu, sbl, SL * hh + j), acc[SL * hh + j]);
             }
           }
         }

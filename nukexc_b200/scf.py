@@ -81,3 +81,67 @@ def gpu_fock(fb, precision="fp64"):
                            want_J=True)
         return E, np.asarray(V[0]), np.asarray(J)
     return fock
+
+
+def rks_device(S, H, fb, nocc, e_nuc, precision="fp64", conv=1e-8, maxiter=60, ndiis=8):
+    """The closed-shell SCF of `rks` with every matrix on the GPU: S, H, the
+    orbitals, the density and the Fock matrices stay in device memory
+    (torch, FP64), the Fock builds take and return device buffers
+    (nkx_fock_build with NKX_MEM_DEVICE), and the generalised eigenproblem is
+    solved in the orthogonal basis X = S^-1/2 (symmetric orthogonalisation).
+    Only the energy and the convergence test cross to the host each
+    iteration -- the glue of the reference's driver (tests/standalone.cxx:590-646,
+    :815-846) copies C and the matrices between Armadillo and the device
+    every iteration instead.  fb is a FockBuilder with an aux basis."""
+    import torch
+
+    dev = "cuda"
+    S = torch.as_tensor(S, dtype=torch.float64, device=dev).contiguous()
+    H = torch.as_tensor(H, dtype=torch.float64, device=dev).contiguous()
+    s, U = torch.linalg.eigh(S)
+    X = U @ torch.diag(s.rsqrt()) @ U.t()
+
+    def orbitals(F):
+        e, Cp = torch.linalg.eigh(X.t() @ F @ X)
+        return e, (X @ Cp)[:, :nocc].contiguous()
+
+    eps, Cocc = orbitals(H)
+    occ = torch.full((nocc,), 2.0, dtype=torch.float64, device=dev)
+    focks, errs, energies, times = [], [], [], []
+    E_old = None
+    converged = False
+    for it in range(maxiter):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        E_xc, V, J = fb.build([Cocc], [occ], precision=precision, want_J=True)
+        P = 2.0 * Cocc @ Cocc.t()
+        F = H + J + V[0]
+        E = float((P * H).sum() + 0.5 * (P * J).sum()) + E_xc + e_nuc
+        err = F @ P @ S - S @ P @ F
+        focks.append(F)
+        errs.append(err)
+        focks, errs = focks[-ndiis:], errs[-ndiis:]
+        if len(focks) > 1:
+            n = len(focks)
+            B = -torch.ones((n + 1, n + 1), dtype=torch.float64, device=dev)
+            B[n, n] = 0.0
+            for i in range(n):
+                for j in range(n):
+                    B[i, j] = (errs[i] * errs[j]).sum()
+            rhs = torch.zeros(n + 1, dtype=torch.float64, device=dev)
+            rhs[n] = -1.0
+            try:
+                coef = torch.linalg.solve(B, rhs)[:n]
+                F = sum(c * f for c, f in zip(coef, focks))
+            except RuntimeError:
+                pass
+        eps, Cocc = orbitals(F)
+        err_max = float(err.abs().max())
+        times.append(time.perf_counter() - t0)
+        energies.append(E)
+        if E_old is not None and abs(E - E_old) < conv and err_max < 1e-5:
+            converged = True
+            break
+        E_old = E
+    return {"energy": energies[-1], "energies": energies, "iterations": len(energies), "converged": converged,
+            "seconds_per_iteration": times, "C_occ": Cocc, "orbital_energies": eps}

@@ -1,5 +1,6 @@
-"""The tensor-core (tcgen05 TF32x3) Fock build against the FP64 CUDA path and
-the CPU oracle.  Accuracy gates: |dE_xc| <= 1e-6 Eh and max|dV_xc| <= 1e-7
+"""The mixed-precision Fock build (exact int8-digit contractions on the
+tcgen05 tensor cores, kind::i8 with int32 accumulation and an FP64 combine)
+against the FP64 CUDA path and the CPU oracle.  Accuracy gates: |dE_xc| <= 1e-6 Eh and max|dV_xc| <= 1e-7
 (the mixed-precision target), tighter where the systems are small."""
 import numpy as np
 import pytest

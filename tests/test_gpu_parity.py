@@ -338,3 +338,24 @@ def test_exchange_matches_oracle_water():
     Ko = O.exchange(ob, oaux, g.quad_points, g.weights, Cm, occ, X)
     assert np.abs(K - Ko).max() < 1e-10 * np.abs(Ko).max()
     assert np.abs(K - K.T).max() < 1e-12 * np.abs(Ko).max()
+
+
+def test_core_hamiltonian_screened_plan_matches_dense():
+    # nkx_plan_core_hamiltonian integrates only the significant (batch,
+    # block) pairs of the plan; on (H2O)4 (two function blocks, some pairs
+    # screened out) it equals the dense quadrature up to what the 1e-10
+    # cutoff drops (the reference asks 1e-6 of its screened variants,
+    # tests/test_integration.cxx:83-311)
+    c, Z, funcs, g = water_case(4, seed=3, nrad=30, order=11)
+    b, ob = basis_pair(funcs)
+    fb = A.FockBuilder(c, Z, b, g, func_ids=("LDA_X",))
+    assert fb.info()["npairs"] < fb.info()["nbatches"] * fb.info()["nblocks"]  # screening active
+    S, T, V = fb.core_hamiltonian(c, Z)
+    Sd, Td, Vd, _ = A.compute_core_hamiltonian(b, c, Z, g.quad_points, g.weights)
+    for X, Xd in ((S, Sd), (T, Td), (V, Vd)):
+        Xd = Xd.cpu().numpy()
+        assert np.abs(X - X.T).max() <= 1e-14 * np.abs(Xd).max()
+        assert np.abs(X - Xd).max() <= 1e-8 * max(1.0, np.abs(Xd).max())
+    So, To, Vo = O.core_hamiltonian(ob, c, Z, g.quad_points, g.weights)
+    assert np.abs(S - So).max() <= 1e-8 and np.abs(T - To).max() <= 1e-8 * np.abs(To).max()
+    fb.close()

@@ -72,3 +72,20 @@ def test_water_lda_scf_mixed_precision_converges_to_fp64():
     rmx = gpu_scf("mixed")
     assert rmx["converged"]
     assert abs(rmx["energy"] - r64["energy"]) < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_water_lda_scf_device_resident_matches_host_loop(precision):
+    # the same SCF with S, H, C, P, F on the GPU and device-buffer Fock
+    # builds (scf.rks_device): the same energy as the host loop
+    c, Z, funcs, aux = water_setup()
+    g = A.make_flat_grid(c, Z, 75, 29, weight_threshold=1e-15, radial="ta")
+    b = A.make_manual_basis(funcs)
+    fb = A.FockBuilder(c, Z, b, g, aux=A.make_manual_basis(aux), func_ids=XC)
+    S, T, V, H = A.compute_core_hamiltonian(b, c, Z, g.quad_points, g.weights)
+    enuc = scf.nuclear_repulsion(c, Z)
+    rd = scf.rks_device(S, H, fb, 5, enuc, precision=precision)
+    rh = scf.rks(S.cpu().numpy(), H.cpu().numpy(), scf.gpu_fock(fb, precision), 5, enuc)
+    assert rd["converged"] and rh["converged"]
+    assert abs(rd["energy"] - rh["energy"]) < (1e-9 if precision == "fp64" else 1e-6)
+    fb.close()
