@@ -444,6 +444,17 @@ def scf_water():
         r = scf.rks(S.cpu().numpy(), H.cpu().numpy(), scf.gpu_fock(fb, prec), 5, enuc)
         out[prec] = {"energy": r["energy"], "iterations": r["iterations"], "converged": r["converged"],
                      "ms_per_iteration": 1e3 * float(np.median(r["seconds_per_iteration"]))}
+    # the same SCF with everything on the device (scf.rks_device), and with
+    # the Fock builds replayed from a CUDA graph (nkx_plan_set_graph)
+    for prec in ("fp64", "mixed"):
+        for graph in (False, True):
+            fb.set_graph(graph)
+            r = scf.rks_device(S, H, fb, 5, enuc, precision=prec)
+            key = f"device_{prec}" + ("_graph" if graph else "")
+            out[key] = {"energy": r["energy"], "iterations": r["iterations"], "converged": r["converged"],
+                        "ms_per_iteration": 1e3 * float(np.median(r["seconds_per_iteration"]))}
+    out["graph_replays"] = fb.info()["graph_replays"]
+    fb.set_graph(False)
     fb.close()
     pts, w, _ = O.make_flat_grid(c, Z, 75, 29, weight_threshold=1e-15, scheme="ta")
     ob, oa = O.make_manual_basis(funcs), O.make_manual_basis(aux)

@@ -115,6 +115,7 @@ typedef struct {
   long npairs;             /* significant (batch, function block) pairs */
   int nchunks;             /* batch chunks streamed per pass */
   double metric_min_diag;  /* smallest diagonal of the Cholesky factor of (A|B) */
+  long graph_replays;      /* builds replayed from a CUDA graph so far (nkx_plan_set_graph) */
 } nkx_plan_info;
 
 /* Timing of the last nkx_fock_build, per stage, in milliseconds (CUDA events). */
@@ -367,6 +368,20 @@ NKX_API nkx_status nkx_plan_set_functional(nkx_plan *plan, int nfunc, const int 
  * compute_coulomb_sparse / _tiled take half_inverse_X
  * (nukexc/coulomb.hpp:117-121, :383-387). */
 NKX_API nkx_status nkx_plan_set_half_inverse(nkx_plan *plan, int K, const double *X, int mem);
+
+/* CUDA-graph replay of the Fock build (no counterpart in the reference; the
+ * reference's driver launches every kernel of every build from the host).
+ * With enable != 0, builds with device buffers (NKX_MEM_DEVICE, phase 0) of
+ * one kind -- precision, spin count, orbital count, J mode -- are recorded
+ * into a CUDA graph on their second call and replayed from then on: the
+ * orbitals are copied into the graph's own buffers and V / J out of them
+ * around one graph launch, so the caller may pass other buffers each time,
+ * as an SCF loop on the device does.  Any other build, or any change of the
+ * plan (functional, metric, half inverse, wait limit, tuning, chunking),
+ * drops the graphs; a kind that cannot be recorded keeps running ordinary
+ * builds.  Replays record no stage times (nkx_get_last_timing gives the
+ * total); nkx_plan_info.graph_replays counts them. */
+NKX_API nkx_status nkx_plan_set_graph(nkx_plan *plan, int enable);
 
 /* Limit, in nanoseconds, of the device-side waits of the plan's tensor-core
  * kernels that may be abandoned (0 restores the default of 2 s).  When such a

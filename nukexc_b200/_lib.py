@@ -28,6 +28,7 @@ EXPORTS = [
     "nkx_morton_order", "nkx_neighbor_list", "nkx_aux_metric", "nkx_exchange_dense", "nkx_plan_set_wait_limit",
     "nkx_fock_build_phase1", "nkx_fock_build_phase2", "nkx_plan_set_metric",
     "nkx_plan_autotune", "nkx_plan_get_tuning", "nkx_plan_set_tuning", "nkx_plan_core_hamiltonian",
+    "nkx_plan_set_graph",
 ]
 
 
@@ -55,7 +56,7 @@ class PlanOptions(C.Structure):
 class PlanInfo(C.Structure):
     _fields_ = [("npoints", C.c_long), ("nbatches", C.c_long), ("nbf", C.c_int), ("naux", C.c_int),
                 ("nblocks", C.c_int), ("npairs", C.c_long), ("nchunks", C.c_int),
-                ("metric_min_diag", C.c_double)]
+                ("metric_min_diag", C.c_double), ("graph_replays", C.c_long)]
 
 
 class BuildTiming(C.Structure):
@@ -108,6 +109,7 @@ def lib():
             "nkx_plan_autotune": [vp, i, i, vp, vp, i, C.c_char_p, vp, vp],
             "nkx_plan_get_tuning": [vp, vp],
             "nkx_plan_core_hamiltonian": [vp, vp, vp, vp, vp, i, vp],
+            "nkx_plan_set_graph": [vp, i],
             "nkx_plan_set_tuning": [vp, vp],
             "nkx_xc_gradient": [vp, i, i, vp, vp, i, d, vp, vp],
             "nkx_get_last_timing": [vp, vp],

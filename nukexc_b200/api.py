@@ -503,6 +503,10 @@ class FockBuilder:
                                                 L.MEM_HOST, None))
         return tuple(M.reshape(self.nbf, self.nbf) for M in (S, T, V))
 
+    def set_graph(self, enable=True):
+        """Replay device-buffer builds from a CUDA graph (nkx_plan_set_graph)."""
+        check(L.lib().nkx_plan_set_graph(self._h, 1 if enable else 0))
+
     def set_metric(self, S):
         """Replace the plan's Coulomb metric (A|B) (naux x naux) and factor it
         again (nkx_plan_set_metric); for a sharded grid, the sum over ranks of

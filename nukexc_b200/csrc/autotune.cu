@@ -65,6 +65,7 @@ void apply(Plan &P, const nkx_tuning &t) {
   NKX_REQUIRE((t.v_n == 64 || t.v_n == 128) && (t.dens_n == 64 || t.dens_n == 128) && t.ypath >= -1 &&
                   t.ypath <= 1,
               NKX_ERR_ARG, "tuning: v_n and dens_n must be 64 or 128, ypath -1, 0 or 1");
+  P.drop_graphs();
   P.tune.v_n = t.v_n;
   P.tune.dens_n = t.dens_n;
   P.tune.ypath = t.ypath;

@@ -601,7 +601,7 @@ __global__ void aux_rtab_kernel(const AuxShell *__restrict__ shells, int nshell,
 // TAB: C R from the mixed build's table (no distance powers or radial
 // factors evaluated here)
 template <int L, bool TAB>
-__global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const AuxShell *__restrict__ shells,
+__global__ void __launch_bounds__(256, TAB ? 2 : 1) aux_y_group_kernel(const AuxGroup *__restrict__ groups, const AuxShell *__restrict__ shells,
                                    const double *__restrict__ px, const double *__restrict__ py,
                                    const double *__restrict__ pz, const double *__restrict__ w,
                                    const double *__restrict__ rho, int nspin, long npad, long slice,
@@ -614,7 +614,34 @@ __global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const Au
   for (int q = 0; q < QM; ++q)
 #pragma unroll
     for (int m = 0; m < NM; ++m) acc[q][m] = 0.0;
-  const float *tab = TAB ? rtab + (size_t)G.first * npad : nullptr;
+  if constexpr (TAB) {
+    // two points per thread and iteration, every table load of both issued
+    // before use (fixed-count shell loop, loads predicated on the group's
+    // size): the loop is load-latency bound otherwise
+    const float *tab = rtab + (size_t)G.first * npad;
+    for (long ga = g0 + threadIdx.x; ga < g1; ga += 2 * blockDim.x) {
+      const long gb = ga + blockDim.x;
+      const bool hb = gb < g1;
+      double wr[2], S[2][NM];
+      float t[2][QM];
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const long g = k ? (hb ? gb : ga) : ga;
+        double r = rho[g];
+        if (nspin == 2) r += rho[npad + g];
+        wr[k] = (k == 0 || hb) ? w[g] * r : 0.0;
+#pragma unroll
+        for (int q = 0; q < QM; ++q) t[k][q] = q < G.n ? tab[(size_t)q * npad + g] : 0.0f;
+        solid_harmonics_all<L>(px[g] - G.cx, py[g] - G.cy, pz[g] - G.cz, S[k]);
+      }
+#pragma unroll
+      for (int q = 0; q < QM; ++q) {
+        const double wa = wr[0] * (double)t[0][q], wb = wr[1] * (double)t[1][q];
+#pragma unroll
+        for (int m = 0; m < NM; ++m) acc[q][m] = fma(wb, S[1][m], fma(wa, S[0][m], acc[q][m]));
+      }
+    }
+  } else {
   for (long g = g0 + threadIdx.x; g < g1; g += blockDim.x) {
     double r = rho[g];
     if (nspin == 2) r += rho[npad + g];
@@ -623,15 +650,7 @@ __global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const Au
     const double dx = px[g] - G.cx, dy = py[g] - G.cy, dz = pz[g] - G.cz;
     double S[NM];
     solid_harmonics_all<L>(dx, dy, dz, S);
-    if constexpr (TAB) {
-#pragma unroll
-      for (int q = 0; q < QM; ++q) {
-        if (q >= G.n) break;
-        const double wI = wr * (double)tab[(size_t)q * npad + g];
-#pragma unroll
-        for (int m = 0; m < NM; ++m) acc[q][m] = fma(wI, S[m], acc[q][m]);
-      }
-    } else {
+    {
       const double rr = sqrt(dx * dx + dy * dy + dz * dz);
       const double r2l1inv = rr < 1e-12 ? 0.0 : ipow_c<2 * L + 1>(1.0 / rr);
 #pragma unroll
@@ -643,6 +662,7 @@ __global__ void aux_y_group_kernel(const AuxGroup *__restrict__ groups, const Au
         for (int m = 0; m < NM; ++m) acc[q][m] = fma(wI, S[m], acc[q][m]);
       }
     }
+  }
   }
   __shared__ double red[32];
 #pragma unroll
@@ -697,6 +717,65 @@ __device__ __forceinline__ double aux_group_v(const AuxGroup &G, const AuxShell 
 
 // v_g = w_g sum_a c_a V_a(g) over the groups, then the loose shells
 // (coulomb.hpp:90-95)
+// v of two points (ga, gb) from one group with the C R table: the group's
+// data and the fit coefficients are loaded once for both
+template <int L>
+__device__ __forceinline__ void aux_group_v2_tab(const AuxGroup &G, const AuxShell *__restrict__ shells,
+                                                 const double *__restrict__ c, const double (&x)[2],
+                                                 const double (&y)[2], const double (&z)[2],
+                                                 const float *__restrict__ rtab, long npad, long ga, long gb,
+                                                 double (&s)[2]) {
+  constexpr int NM = 2 * L + 1;
+  double S[2][NM];
+  solid_harmonics_all<L>(x[0] - G.cx, y[0] - G.cy, z[0] - G.cz, S[0]);
+  solid_harmonics_all<L>(x[1] - G.cx, y[1] - G.cy, z[1] - G.cz, S[1]);
+  for (int q = 0; q < G.n; ++q) {
+    const int f0 = shells[G.first + q].first;
+    const float *row = rtab + (size_t)(G.first + q) * npad;
+    const double ra = (double)row[ga], rb = (double)row[gb];
+    double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+      const double cm = c[f0 + m];
+      a0 = fma(cm, S[0][m], a0);
+      a1 = fma(cm, S[1][m], a1);
+    }
+    s[0] = fma(a0, ra, s[0]);
+    s[1] = fma(a1, rb, s[1]);
+  }
+}
+
+// the table form of aux_v_group_kernel: two points per thread
+__global__ void aux_v_group_tab_kernel(const AuxGroup *__restrict__ groups, int4 goff,
+                                       const AuxShell *__restrict__ shells, const int *__restrict__ loose, int nloose,
+                                       const double *__restrict__ c, const double *__restrict__ px,
+                                       const double *__restrict__ py, const double *__restrict__ pz,
+                                       const double *__restrict__ w, long npad, const float *__restrict__ rtab,
+                                       double *__restrict__ v) {
+  const long ga = blockIdx.x * 2L * blockDim.x + threadIdx.x;
+  if (ga >= npad) return;
+  const long gb = min(ga + (long)blockDim.x, npad - 1);  // a duplicate of the last point when past the end
+  const double x[2] = {px[ga], px[gb]}, y[2] = {py[ga], py[gb]}, z[2] = {pz[ga], pz[gb]};
+  double s[2] = {0.0, 0.0};
+  for (int k = 0; k < goff.x; ++k) aux_group_v2_tab<0>(groups[k], shells, c, x, y, z, rtab, npad, ga, gb, s);
+  for (int k = goff.x; k < goff.y; ++k) aux_group_v2_tab<1>(groups[k], shells, c, x, y, z, rtab, npad, ga, gb, s);
+  for (int k = goff.y; k < goff.z; ++k) aux_group_v2_tab<2>(groups[k], shells, c, x, y, z, rtab, npad, ga, gb, s);
+  for (int k = goff.z; k < goff.w; ++k) aux_group_v2_tab<3>(groups[k], shells, c, x, y, z, rtab, npad, ga, gb, s);
+  for (int k = 0; k < nloose; ++k) {
+    const AuxShell &sh = shells[loose[k]];
+    const AuxFunc &f = sh.f;
+    const float *row = rtab + (size_t)loose[k] * npad;
+    for (int e = 0; e < 2; ++e) {
+      double a = 0.0;
+      for (int m = 0; m < sh.nm; ++m)
+        a += c[sh.first + m] * solid_harmonic(f.l, f.m + m, x[e] - f.cx, y[e] - f.cy, z[e] - f.cz);
+      s[e] += a * (double)row[e ? gb : ga];
+    }
+  }
+  v[ga] = s[0] * w[ga];
+  if (ga + (long)blockDim.x < npad) v[gb] = s[1] * w[gb];
+}
+
 template <bool TAB>
 __global__ void aux_v_group_kernel(const AuxGroup *__restrict__ groups, int4 goff,
                                    const AuxShell *__restrict__ shells, const int *__restrict__ loose, int nloose,
@@ -838,6 +917,8 @@ static void morton_order(long n, const double *xyz, std::vector<long> &perm) {
 void destroy_mixed_state(void *p);
 
 Plan::~Plan() {
+  for (BuildGraph &g : graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   if (mx_state) destroy_mixed_state(mx_state);
   if (grad_state) destroy_grad_state(grad_state);
   for (void *p : allocs) cudaFree(p);
@@ -941,6 +1022,7 @@ constexpr size_t kDefaultWorkspace = (size_t)24 << 30;
 // and the chunk-sized staging: the FP64 planes now; the FP64 build's Z
 // planes and the mixed build's digits when a build first needs them.
 void plan_chunks(Plan &P, long maxp) {
+  P.drop_graphs();
   P.chunks.clear();
   P.max_chunk_pairs = 0;
   long b = 0;
@@ -1464,9 +1546,9 @@ void coulomb_solve(Plan &P, cudaStream_t s, bool mixed) {
     }
     const int4 goff = make_int4(P.h_group_off[1], P.h_group_off[2], P.h_group_off[3], P.h_group_off[4]);
     if (rtab)
-      aux_v_group_kernel<true><<<nblk(P.npad, 128), 128, 0, s>>>(P.d_agroup, goff, P.d_ashell, P.d_loose, P.nloose,
-                                                                 P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, rtab,
-                                                                 P.d_vj);
+      aux_v_group_tab_kernel<<<nblk(P.npad, 256), 128, 0, s>>>(P.d_agroup, goff, P.d_ashell, P.d_loose, P.nloose,
+                                                               P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, rtab,
+                                                               P.d_vj);
     else
       aux_v_group_kernel<false><<<nblk(P.npad, 128), 128, 0, s>>>(P.d_agroup, goff, P.d_ashell, P.d_loose, P.nloose,
                                                                   P.d_c, P.d_px, P.d_py, P.d_pz, P.d_w, P.npad, rtab,
@@ -1606,8 +1688,12 @@ void upload_orbitals(Plan &P, int nspin, int nocc, const double *C, const double
 // summed y (same memory kind) and finishes the build (fit, functional, V and
 // J on this plan's points).  Phase 2 needs a phase 1 of the same
 // precision, spin count and orbitals on this plan immediately before it.
-void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, const double *occ, int mem, int fuse_j,
-                double *E, double *V, double *J, cudaStream_t user, int phase, double *y) {
+// One build on the stream.  capture_only (device buffers, phase 0): only the
+// device work is issued -- no events, host copies, synchronisation or status
+// check -- so that it can be recorded into a CUDA graph.
+static void fock_build_once(Plan &P, int precision, int nspin, int nocc, const double *C, const double *occ, int mem,
+                            int fuse_j, double *E, double *V, double *J, cudaStream_t user, int phase, double *y,
+                            bool capture_only) {
   if (phase == 2) {
     NKX_REQUIRE(P.phase1_done, NKX_ERR_ARG, "phase 2 of a sharded build needs phase 1 on this plan first");
     precision = P.phase1_precision;
@@ -1630,10 +1716,13 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
   cudaStream_t s = user ? user : P.stream;
   P.launches = 0;
   StageTimer T;
-  cudaEvent_t t0, t1;
-  NKX_CUDA(cudaEventCreate(&t0));
-  NKX_CUDA(cudaEventCreate(&t1));
-  NKX_CUDA(cudaEventRecord(t0, s));
+  T.on = !capture_only;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (!capture_only) {
+    NKX_CUDA(cudaEventCreate(&t0));
+    NKX_CUDA(cudaEventCreate(&t1));
+    NKX_CUDA(cudaEventRecord(t0, s));
+  }
   P.phase1_done = false;
   if (phase == 2) {
     NKX_CUDA(cudaMemcpyAsync(P.d_y, y, sizeof(double) * P.naux,
@@ -1687,6 +1776,7 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
     ++P.launches;
   }
   NKX_LAUNCH_CHECK();
+  if (capture_only) return;
   if (mem == NKX_MEM_HOST) {
     if (V) NKX_CUDA(cudaMemcpyAsync(V, dst, sizeof(double) * nspin * nn, cudaMemcpyDeviceToHost, s));
     if (separateJ) NKX_CUDA(cudaMemcpyAsync(J, dst + nspin * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
@@ -1713,6 +1803,123 @@ void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, co
               "a tensor-core kernel wait gave up (wait code " + std::to_string(status[0]) + "); outputs are invalid");
   NKX_REQUIRE(status[1] == 0 && std::isfinite(*E), NKX_ERR_NUMERIC,
               "non-finite value in the orbitals, occupations, grid or an operand of the build; outputs are invalid");
+}
+
+void Plan::drop_graphs() {
+  for (BuildGraph &g : graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    release(g.C);
+    release(g.occ);
+    release(g.V);
+    release(g.J);
+  }
+  graphs.clear();
+}
+
+// A build replayed from a CUDA graph (graph mode, device buffers, phase 0).
+// The second build of a kind (precision, spins, orbitals, outputs) records the
+// device work of a build that reads the orbitals from, and writes V and J to,
+// buffers of the graph's own; every build of that kind then copies the
+// caller's orbitals in, launches the graph and copies the results out.  A
+// build of another kind, or any change of the plan, drops the graphs first
+// (their launch arguments and buffers are baked in).  If recording fails the
+// kind keeps running ordinary builds.
+static void fock_build_graph(Plan &P, int precision, int nspin, int nocc, const double *C, const double *occ,
+                             int fuse_j, double *E, double *V, double *J, cudaStream_t user) {
+  BuildGraph *g = nullptr;
+  for (BuildGraph &x : P.graphs)
+    if (x.precision == precision && x.nspin == nspin && x.nocc == nocc && x.fuse == fuse_j && x.hasV == (V != nullptr) &&
+        x.hasJ == (J != nullptr))
+      g = &x;
+  if (!g || g->failed || !g->exec) {
+    const bool record = g && !g->failed;
+    if (!record) {
+      // first build of this kind: an ordinary build (it may grow buffers the
+      // recorded builds of other kinds use), then remember the kind
+      P.drop_graphs();
+      fock_build_once(P, precision, nspin, nocc, C, occ, NKX_MEM_DEVICE, fuse_j, E, V, J, user, 0, nullptr, false);
+      BuildGraph n;
+      n.precision = precision;
+      n.nspin = nspin;
+      n.nocc = nocc;
+      n.fuse = fuse_j;
+      n.hasV = V != nullptr;
+      n.hasJ = J != nullptr;
+      if (!g) P.graphs.push_back(n);
+      return;
+    }
+    // second build of this kind: record it
+    const size_t nn = (size_t)P.nbf * P.nbf;
+    g->C = P.alloc<double>((size_t)nspin * nocc * P.nbf);
+    g->occ = P.alloc<double>((size_t)nspin * nocc);
+    g->V = V ? P.alloc<double>(nspin * nn) : nullptr;
+    g->J = J ? P.alloc<double>(nn) : nullptr;
+    cudaStream_t s = user ? user : P.stream;
+    cudaGraph_t graph = nullptr;
+    double e_unused = 0.0;
+    NKX_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      fock_build_once(P, precision, nspin, nocc, g->C, g->occ, NKX_MEM_DEVICE, fuse_j, &e_unused, g->V, g->J, s, 0,
+                      nullptr, true);
+    } catch (...) {
+      cudaStreamEndCapture(s, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      g->failed = true;
+      fock_build_once(P, precision, nspin, nocc, C, occ, NKX_MEM_DEVICE, fuse_j, E, V, J, user, 0, nullptr, false);
+      return;
+    }
+    NKX_CUDA(cudaStreamEndCapture(s, &graph));
+    const cudaError_t ie = cudaGraphInstantiate(&g->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+      cudaGetLastError();
+      g->exec = nullptr;
+      g->failed = true;
+      fock_build_once(P, precision, nspin, nocc, C, occ, NKX_MEM_DEVICE, fuse_j, E, V, J, user, 0, nullptr, false);
+      return;
+    }
+    g->launches = P.launches;
+  }
+  // replay
+  cudaStream_t s = user ? user : P.stream;
+  const size_t nn = (size_t)P.nbf * P.nbf;
+  cudaEvent_t t0, t1;
+  NKX_CUDA(cudaEventCreate(&t0));
+  NKX_CUDA(cudaEventCreate(&t1));
+  NKX_CUDA(cudaEventRecord(t0, s));
+  NKX_CUDA(cudaMemcpyAsync(g->C, C, sizeof(double) * nspin * nocc * P.nbf, cudaMemcpyDeviceToDevice, s));
+  NKX_CUDA(cudaMemcpyAsync(g->occ, occ, sizeof(double) * nspin * nocc, cudaMemcpyDeviceToDevice, s));
+  NKX_CUDA(cudaGraphLaunch(g->exec, s));
+  if (V) NKX_CUDA(cudaMemcpyAsync(V, g->V, sizeof(double) * nspin * nn, cudaMemcpyDeviceToDevice, s));
+  if (J) NKX_CUDA(cudaMemcpyAsync(J, g->J, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
+  NKX_CUDA(cudaMemcpyAsync(E, P.d_E, sizeof(double), cudaMemcpyDeviceToHost, s));
+  int status[2] = {0, 0};
+  NKX_CUDA(cudaMemcpyAsync(status, P.d_status, sizeof(status), cudaMemcpyDeviceToHost, s));
+  NKX_CUDA(cudaEventRecord(t1, s));
+  NKX_CUDA(cudaStreamSynchronize(s));
+  P.last = nkx_build_timing{};
+  cudaEventElapsedTime(&P.last.total_ms, t0, t1);
+  P.last.launches = g->launches;
+  P.last_nspin = nspin;
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  ++P.graph_replays;
+  NKX_REQUIRE(status[0] == 0, NKX_ERR_TIMEOUT, "a tensor-core kernel wait gave up; outputs are invalid");
+  NKX_REQUIRE(status[1] == 0 && std::isfinite(*E), NKX_ERR_NUMERIC,
+              "non-finite value in the orbitals, occupations, grid or an operand of the build; outputs are invalid");
+}
+
+void fock_build(Plan &P, int precision, int nspin, int nocc, const double *C, const double *occ, int mem, int fuse_j,
+                double *E, double *V, double *J, cudaStream_t user, int phase, double *y) {
+  if (P.graph_mode && phase == 0 && mem == NKX_MEM_DEVICE) {
+    NKX_REQUIRE(nspin == 1 || nspin == 2, NKX_ERR_ARG, "nspin must be 1 or 2");
+    NKX_REQUIRE(nocc > 0 && C && occ && E && (V || J), NKX_ERR_ARG, "invalid arguments");
+    fock_build_graph(P, precision, nspin, nocc, C, occ, fuse_j, E, V, J, user);
+    return;
+  }
+  if (!P.graphs.empty()) P.drop_graphs();  // an ordinary build may grow buffers a graph uses
+  fock_build_once(P, precision, nspin, nocc, C, occ, mem, fuse_j, E, V, J, user, phase, y, false);
 }
 
 }  // namespace nkx
@@ -1747,6 +1954,7 @@ NKX_API nkx_status nkx_plan_get_info(const nkx_plan *plan, nkx_plan_info *info) 
     info->npairs = P.npairs;
     info->nchunks = (int)P.chunks.size();
     info->metric_min_diag = P.metric_min_diag;
+    info->graph_replays = P.graph_replays;
   });
 }
 
@@ -1782,6 +1990,7 @@ NKX_API nkx_status nkx_plan_set_metric(nkx_plan *plan, const double *S, int mem)
   return run_guarded("nkx_plan_set_metric", [&] {
     NKX_REQUIRE(plan && S, NKX_ERR_ARG, "invalid arguments");
     Plan &P = *reinterpret_cast<Plan *>(plan);
+    P.drop_graphs();
     NKX_REQUIRE(P.naux > 0, NKX_ERR_ARG, "the plan has no aux basis");
     NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
     const size_t NA = P.naux;
@@ -1834,6 +2043,7 @@ NKX_API nkx_status nkx_plan_set_functional(nkx_plan *plan, int nfunc, const int 
   return run_guarded("nkx_plan_set_functional", [&] {
     NKX_REQUIRE(plan && func_ids, NKX_ERR_ARG, "invalid arguments");
     Plan &P = *reinterpret_cast<Plan *>(plan);
+    P.drop_graphs();
     nkx_plan_options o{};
     o.nfunc = nfunc;
     for (int i = 0; i < 4 && i < nfunc; ++i) o.func_ids[i] = func_ids[i];
@@ -1848,6 +2058,7 @@ NKX_API nkx_status nkx_plan_set_half_inverse(nkx_plan *plan, int K, const double
   return run_guarded("nkx_plan_set_half_inverse", [&] {
     NKX_REQUIRE(plan && X, NKX_ERR_ARG, "invalid arguments");
     Plan &P = *reinterpret_cast<Plan *>(plan);
+    P.drop_graphs();
     NKX_REQUIRE(P.naux > 0, NKX_ERR_ARG, "the plan has no aux basis");
     NKX_REQUIRE(K >= 1 && K <= P.naux, NKX_ERR_ARG, "K must be in [1, naux]");
     NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
@@ -1865,8 +2076,18 @@ NKX_API nkx_status nkx_plan_set_wait_limit(nkx_plan *plan, unsigned long long ns
   return run_guarded("nkx_plan_set_wait_limit", [&] {
     NKX_REQUIRE(plan, NKX_ERR_ARG, "plan is NULL");
     Plan &P = *reinterpret_cast<Plan *>(plan);
+    P.drop_graphs();
     P.wait_ns = ns ? ns : 2000000000ull;
     P.stall_test = stall != 0;
+  });
+}
+
+NKX_API nkx_status nkx_plan_set_graph(nkx_plan *plan, int enable) {
+  return run_guarded("nkx_plan_set_graph", [&] {
+    NKX_REQUIRE(plan, NKX_ERR_ARG, "plan is NULL");
+    Plan &P = *reinterpret_cast<Plan *>(plan);
+    P.drop_graphs();
+    P.graph_mode = enable != 0;
   });
 }
 

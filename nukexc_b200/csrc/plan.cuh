@@ -22,6 +22,16 @@ struct Tuning {
   int ypath = -1;  // GGA density gradient through Y = T0 (C occ)^T: -1 from 256 orbitals, 0 off, 1 on
 };
 
+// A Fock build recorded into a CUDA graph (graph mode) with the buffers it
+// reads its orbitals from and writes its results to.
+struct BuildGraph {
+  int precision = 0, nspin = 0, nocc = 0, fuse = 0;
+  bool hasV = false, hasJ = false, failed = false;
+  cudaGraphExec_t exec = nullptr;
+  double *C = nullptr, *occ = nullptr, *V = nullptr, *J = nullptr;
+  int launches = 0;
+};
+
 struct Plan {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -110,6 +120,12 @@ struct Plan {
   bool phase1_done = false;
   int phase1_precision = 0, phase1_nspin = 1, phase1_nocc = 0;
 
+  // CUDA-graph replay of builds with device buffers (nkx_plan_set_graph)
+  bool graph_mode = false;
+  std::vector<BuildGraph> graphs;
+  long graph_replays = 0;
+  void drop_graphs();
+
   nkx_build_timing last{};
   int launches = 0;
   int last_nspin = 1;
@@ -131,6 +147,7 @@ struct StageTimer {
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
   cudaEvent_t begin_ev = nullptr;
   int cur = -1;
+  bool on = true;  // off while a build is recorded into a CUDA graph
   ~StageTimer() {
     for (auto &m : marks) {
       cudaEventDestroy(m.second.first);
@@ -138,6 +155,7 @@ struct StageTimer {
     }
   }
   void begin(int stage, cudaStream_t s) {
+    if (!on) return;
     cudaEvent_t e;
     NKX_CUDA(cudaEventCreate(&e));
     NKX_CUDA(cudaEventRecord(e, s));
@@ -145,6 +163,7 @@ struct StageTimer {
     cur = stage;
   }
   void end(cudaStream_t s) {
+    if (!on) return;
     cudaEvent_t e;
     NKX_CUDA(cudaEventCreate(&e));
     NKX_CUDA(cudaEventRecord(e, s));

@@ -346,7 +346,13 @@ def test_core_hamiltonian_screened_plan_matches_dense():
     # screened out) it equals the dense quadrature up to what the 1e-10
     # cutoff drops (the reference asks 1e-6 of its screened variants,
     # tests/test_integration.cxx:83-311)
-    c, Z, funcs, g = water_case(4, seed=3, nrad=30, order=11)
+    # four waters 50 bohr apart on a line: two function blocks, and the
+    # batches at one end are out of reach of the other end's functions
+    c1, Z1 = M.water()
+    c = np.concatenate([np.asarray(c1, float) + [0.0, 0.0, 50.0 * k] for k in range(4)])
+    Z = np.concatenate([Z1] * 4)
+    funcs = M.sto_basis(c, Z)
+    g = A.make_flat_grid(c, Z, 30, 11, weight_threshold=1e-15, radial="ta")
     b, ob = basis_pair(funcs)
     fb = A.FockBuilder(c, Z, b, g, func_ids=("LDA_X",))
     assert fb.info()["npairs"] < fb.info()["nbatches"] * fb.info()["nblocks"]  # screening active
