@@ -10,9 +10,11 @@ functional, V_xc = Phi Z^T) over the whole synthetic (H2O)_n grid
 batches, screening 1e-10), with the orbital coefficients already resident in
 HBM.  `e2e` is the same build through the public API with host buffers
 (C copied in, V and E copied out inside the timed region).  One JSON line is
-printed by rank 0.  With N > 1 the grid is split by atoms across ranks (one
-process per GPU) and the partial V_xc and E_xc are summed with an NCCL
-all-reduce inside the timed region (strong scaling).
+printed by rank 0.  With N > 1 the grid is split into Morton-contiguous,
+cost-balanced batch ranges (one process per GPU, shard.balanced_split) and
+the partial V_xc and E_xc are summed with an NCCL all-reduce inside the
+timed region (strong scaling; with --aux the J fit vector is all-reduced
+between the two phases of the build).
 
 Beside the headline, `xc_plus_j` reports the mixed vs FP64 XC + fused DF-J
 build of (H2O)_32 with the aux basis zeta_k = 0.3*1.8^k up to l = 3
@@ -66,6 +68,10 @@ def parse():
     ap.add_argument("--no-scf", action="store_true",
                     help="skip the water SCF (Slater + VWN5, SCF to 1e-8 Eh) reported beside the headline")
     ap.add_argument("--no-autotune", action="store_true", help="keep the plan's default kernel choices")
+    ap.add_argument("--tune-cache", default=None,
+                    help="autotuner cache file: choices found there for this device and problem shape are "
+                         "applied without timing, new ones are appended (a profiled run then replays the "
+                         "choices of a plain run)")
     ap.add_argument("--aggregate-gate", type=int, default=1500,
                     help="also time and gate the mixed vs FP64 build of the C/H/N/O aggregate of this many atoms "
                          "beside the headline (0: skip)")
@@ -373,7 +379,7 @@ def xc_gradient_check(n, stream, ngeom=10, ncomp=1, h=1e-4):
             "fd": "Richardson-extrapolated central differences, h = 1e-4 and 5e-5 bohr, FP64 GPU E_xc"}
 
 
-def aggregate_gate(natoms, stream):
+def aggregate_gate(natoms, stream, int8_peak=None):
     """Survey configuration 5: the seeded C/H/N/O aggregate (3:5:1:1, random
     packing in a sphere, d_min 1.0 A, ~12000 STO functions, ~3e7 points),
     PBE, nocc = electrons / 2: one warm-up and one timed mixed build, one
@@ -408,6 +414,7 @@ def aggregate_gate(natoms, stream):
     Ed, Vd, ms_d, td = timed("fp64")
     out.update({"mixed_ms_per_build": ms_m, "mixed_points_per_s": info["npoints"] / (ms_m * 1e-3),
                 "mixed_stage_ms": {k: v for k, v in tm.items() if k.endswith("_ms")},
+                "v_roofline": v_roofline(fb, tm["vgemm_ms"], int8_peak),
                 "launches_per_mixed_build": tm["launches"], "nchunks": int(fb.info()["nchunks"]),
                 "fp64_ms_per_build": ms_d, "fp64_stage_ms": {k: v for k, v in td.items() if k.endswith("_ms")},
                 "mixed_speedup": ms_d / ms_m,
@@ -476,6 +483,13 @@ def scf_water():
 
 
 # ---------------------------------------------------------------- nkx ----
+def v_roofline(fb, vgemm_ms, peak):
+    """The V contraction of one mixed build against the int8 peak: ten int8
+    MMAs per FP64-equivalent product of sum_b 2 n_b^2 256."""
+    ach = 10.0 * vgemm_flops(fb.batch_blocks()) / (vgemm_ms * 1e-3) / 1e12
+    return {"achieved": ach, "unit": "TOP/s (int8)", "peak": peak, "frac": (ach / peak) if peak else None}
+
+
 def vgemm_flops(info_pairs_per_batch, nz=1):
     """Algorithmic FLOPs of the V = Phi Z^T contraction: sum_b 2 n_b^2 256."""
     nb = np.asarray(info_pairs_per_batch, dtype=np.float64) * 128.0
@@ -534,7 +548,7 @@ def run_nkx(args):
         # the plan's autotuner picks the MMA widths, the Y path and the chunk
         # size by timing whole builds (untimed setup)
         t0 = time.perf_counter()
-        tuning = fb.autotune([Cd], [od], stream=stream.cuda_stream)
+        tuning = fb.autotune([Cd], [od], cache_path=args.tune_cache, stream=stream.cuda_stream)
         tuning["seconds"] = time.perf_counter() - t0
         info = fb.info()
 
@@ -715,7 +729,7 @@ def run_nkx(args):
         if world == 1 and not args.no_scf:
             line["scf_water"] = scf_water()
         if world == 1 and args.aggregate_gate > 0 and not args.aggregate:
-            line["aggregate_gate"] = aggregate_gate(args.aggregate_gate, stream)
+            line["aggregate_gate"] = aggregate_gate(args.aggregate_gate, stream, peak if prec == "mixed" else None)
         print(json.dumps(line), flush=True)
     fb.close()
     if dist is not None:

@@ -312,6 +312,7 @@ typedef struct {
   int v_n;            /* tcgen05 MMA width N of the V contraction: 128 or 64 */
   int dens_n;         /* MMA width of the density contraction: 64 or 128 */
   int ypath;          /* GGA density gradient through Y = T0 (C occ)^T: -1 auto (from 256 orbitals), 0, 1 */
+  int v_warps;        /* epilogue warps of the N = 128 V contraction: 16 (32 columns each) or 8 (64 each) */
   long chunk_pairs;   /* (batch, block) pairs per streamed chunk */
   int from_cache;     /* out: 1 when the choices came from the cache file */
   int trials;         /* out: builds timed */
@@ -323,7 +324,7 @@ typedef struct {
  * its kernels take fixed launch shapes).  With the caller's orbitals (as
  * nkx_fock_build, XC only), it times whole builds (CUDA events) and keeps, one
  * knob at a time with the others at their best so far: the Y path (GGA), the
- * density MMA width, the V MMA width, and the chunk size (x1, x2, x4 of the
+ * density MMA width, the V MMA width and epilogue warps, and the chunk size (x1, x2, x4 of the
  * current one while device memory allows).  With cache_path != NULL a file of
  * earlier results keyed by the device and the problem's shape (functions,
  * blocks, pairs, points, orbitals, spins, GGA) is read first -- a hit applies

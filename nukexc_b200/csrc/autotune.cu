@@ -3,13 +3,14 @@
 // fastest of
 //   the Y path of the GGA density gradient (off / on),
 //   the tcgen05 MMA width of the density contraction (N = 64 / 128),
-//   the MMA width of the V contraction (N = 128 / 64),
+//   the MMA width of the V contraction (N = 128 / 64) and, for N = 128, its
+//   epilogue warps (16 of 32 columns / 8 of 64),
 //   the chunk size (x1, x2, x4 of the current pair limit, memory permitting),
 // each knob tried with the others at their best so far.  Every new
 // configuration gets one untimed build first (allocations, first touch), then
 // one timed build (CUDA events around the whole build).  Results can be kept
 // in a text cache file, one line per problem:
-//   <device name>|<SMs>|nbf|nblk|npairs|npts|nocc|nspin|gga  v_n dens_n ypath chunk_pairs best_ms
+//   <device name>|<SMs>|nbf|nblk|npairs|npts|nocc|nspin|gga  v_n dens_n ypath v_warps chunk_pairs best_ms
 #include <algorithm>
 #include <cstdio>
 #include <fstream>
@@ -46,7 +47,7 @@ bool cache_lookup(const char *path, const std::string &sig, nkx_tuning &t) {
     std::istringstream in(line);
     std::string key;
     nkx_tuning r{};
-    if (in >> key >> r.v_n >> r.dens_n >> r.ypath >> r.chunk_pairs >> r.best_ms && key == sig) {
+    if (in >> key >> r.v_n >> r.dens_n >> r.ypath >> r.v_warps >> r.chunk_pairs >> r.best_ms && key == sig) {
       t = r;
       hit = true;
     }
@@ -58,17 +59,19 @@ void cache_store(const char *path, const std::string &sig, const nkx_tuning &t) 
   if (!path) return;
   std::ofstream f(path, std::ios::app);
   NKX_REQUIRE(f.good(), NKX_ERR_ARG, std::string("cannot append to the tuning cache ") + path);
-  f << sig << " " << t.v_n << " " << t.dens_n << " " << t.ypath << " " << t.chunk_pairs << " " << t.best_ms << "\n";
+  f << sig << " " << t.v_n << " " << t.dens_n << " " << t.ypath << " " << t.v_warps << " " << t.chunk_pairs << " "
+    << t.best_ms << "\n";
 }
 
 void apply(Plan &P, const nkx_tuning &t) {
   NKX_REQUIRE((t.v_n == 64 || t.v_n == 128) && (t.dens_n == 64 || t.dens_n == 128) && t.ypath >= -1 &&
-                  t.ypath <= 1,
-              NKX_ERR_ARG, "tuning: v_n and dens_n must be 64 or 128, ypath -1, 0 or 1");
+                  t.ypath <= 1 && (t.v_warps == 8 || t.v_warps == 16),
+              NKX_ERR_ARG, "tuning: v_n and dens_n must be 64 or 128, ypath -1, 0 or 1, v_warps 8 or 16");
   P.drop_graphs();
   P.tune.v_n = t.v_n;
   P.tune.dens_n = t.dens_n;
   P.tune.ypath = t.ypath;
+  P.tune.v_warps = t.v_warps;
   if (t.chunk_pairs > 0 && t.chunk_pairs != P.chunk_pair_limit) plan_chunks(P, t.chunk_pairs);
 }
 
@@ -77,6 +80,7 @@ nkx_tuning current(const Plan &P) {
   t.v_n = P.tune.v_n;
   t.dens_n = P.tune.dens_n;
   t.ypath = P.tune.ypath;
+  t.v_warps = P.tune.v_warps;
   t.chunk_pairs = P.chunk_pair_limit;
   return t;
 }
@@ -143,6 +147,11 @@ static void autotune(Plan &P, int nspin, int nocc, const double *C, const double
     {
       nkx_tuning c = best;
       c.v_n = best.v_n == 128 ? 64 : 128;
+      consider(c);
+    }
+    if (best.v_n == 128) {
+      nkx_tuning c = best;
+      c.v_warps = best.v_warps == 16 ? 8 : 16;
       consider(c);
     }
     for (int mult : {2, 4}) {

@@ -20,6 +20,7 @@ struct Tuning {
   int v_n = 128;   // tcgen05 MMA width N of the V contraction (128 or 64)
   int dens_n = 64; // MMA width of the density contraction (64 or 128)
   int ypath = -1;  // GGA density gradient through Y = T0 (C occ)^T: -1 from 256 orbitals, 0 off, 1 on
+  int v_warps = 16; // epilogue warps of the N = 128 V contraction (16 of 32 columns, or 8 of 64)
 };
 
 // A Fock build recorded into a CUDA graph (graph mode) with the buffers it

@@ -35,6 +35,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "plan.cuh"
@@ -48,7 +49,7 @@ constexpr int kABytes = 4 * 128 * 64;  // four digit planes, 128 rows x 64 B
 constexpr double kTwoM36 = 0x1p-36;
 
 // TC_MODE_GRAD: Y(g, mu) = sum_i T0(g, i) (C occ)(mu, i) over the orbitals
-// (grad rho = 2 sum_mu grad phi_mu Y_mu, ygrad_kernel)
+// (grad rho = 2 sum_mu grad phi_mu Y_mu, summed in the Y pass's epilogue)
 enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1, TC_MODE_GRAD = 2 };
 
 // Shape by the MMA width N.  N = 128: one TMEM buffer of 4 levels x 128
@@ -59,14 +60,22 @@ enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1, TC_MODE_GRAD = 2 };
 // the density unit an N-orbital tile); the Y pass runs N = 64.  The plan's
 // tuning (nkx_plan_autotune) picks the shape per contraction; the defaults
 // are N = 128 for V and N = 64 for the density.
-template <int N_>
+//
+// EW epilogue warps (default N / 8): warp w reads TMEM lanes 32 (w % 4) ..,
+// and CW = 4 N / EW columns of each level.  The V contraction can also run
+// N = 128 with 8 epilogue warps of 64 columns each (320 threads, 200
+// registers a thread: the FP64 accumulators of 64 columns fit without
+// spilling), chosen by the tuning.
+template <int N_, int EW_ = N_ / 8>
 struct TcShape {
   static constexpr int N = N_;
+  static constexpr int EW = EW_;
+  static constexpr int CW = 4 * N / EW;  // columns of an epilogue warp
   static constexpr int NBUF = N == 128 ? 1 : 2;
   static constexpr int kStages = N == 128 ? 3 : 4;
   static constexpr int kBBytes = 4 * N * 64;
   static constexpr int kStageBytes = kABytes + kBBytes;
-  static constexpr int kEpiThreads = 32 * 4 * (N / 32);
+  static constexpr int kEpiThreads = 32 * EW;
   static constexpr int kThreads = 64 + kEpiThreads;
   static constexpr uint32_t kIdesc = idesc_i8(128, N);
   static constexpr int kSmem = kStages * kStageBytes + 1024;
@@ -88,9 +97,13 @@ struct TcArgs {
   int nspin, ncomp, ncs, ntile_i, nocc_pad;
   double *T;
   // grad mode: sA = st0[(bl, s, h)][128] (T0 row scales), sB = sco[s][mu]
-  // (C occ row scales); output Y[pair][spin][g][mu] (FP64)
+  // (C occ row scales); grad phi from the pass-A digits qphT[pair][comp][digit][g][f]
+  // and scales sphT[pair][comp][g] (ncs components); output the partial sums
+  // Gp[pair][spin][t][cq][c][256] of 2 grad phi_c . Y over 32 functions
   const int *pair_batch;
-  double *Y;
+  const uint8_t *qphT;
+  const double *sphT;
+  double *Gp;
   long nunits;
   // err[0]: code of the first wait that gave up (0: none); waits that can
   // be abandoned give up after wait_ns, the drain waits after kDrainLimitNs
@@ -100,6 +113,8 @@ struct TcArgs {
   // barrier that nothing completes, so the kernel gives up after wait_ns
   int stall;
   int nt;  // MMA width N of the launched kernel (V: 128 / nt units per output tile)
+  int ew;  // epilogue warps of the launched kernel (N = 128 V: 16 or 8)
+  int vrow;  // V: row blocks per super-row of the unit order (1: row-major)
 };
 
 // S = 2^24 L0 + 2^16 L1 + 2^8 L2 + L3 of four int32 accumulator levels,
@@ -128,9 +143,13 @@ struct UnitIter {
       u %= n3;
       zi = (int)(u / n2);
       u %= n2;
-      I = (int)(u / ((long)a.nblk * nh));
-      J = (int)((u / nh) % a.nblk);
+      // super-row r holds row blocks r vrow .. + hr - 1, column-major inside
       hc = (int)(u % nh);
+      const long v = u / nh, srow = (long)a.vrow * a.nblk;
+      const int r = (int)(v / srow), w = (int)(v - r * srow);
+      const int hr = min(a.vrow, a.nblk - r * a.vrow);
+      J = w / hr;
+      I = r * a.vrow + w % hr;
     } else if (a.mode == TC_MODE_GRAD) {
       t = (int)(u % 2);  // 64-function half of the block
       h = (int)((u / 2) % 2);
@@ -237,15 +256,18 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
   }
 }
 
-template <int MODE, int NW>
-__global__ void __launch_bounds__(TcShape<NW>::kThreads, 1)
+template <int MODE, int NW, int EW = NW / 8>
+__global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
     tc_i8_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs a) {
-  using Sh = TcShape<NW>;
-  constexpr int N = Sh::N, NBUF = Sh::NBUF, kStages = Sh::kStages, kStageBytes = Sh::kStageBytes;
+  using Sh = TcShape<NW, EW>;
+  constexpr int N = Sh::N, NBUF = Sh::NBUF, kStages = Sh::kStages, kStageBytes = Sh::kStageBytes, CW = Sh::CW;
+  static_assert(MODE == TC_MODE_V || CW == 32, "the density and Y epilogues take 32 columns a warp");
   extern __shared__ __align__(1024) uint8_t dsmem[];
   __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar[NBUF], tempty_bar[NBUF], drain_bar, stall_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_flag;
+  // V: the column scales of each epilogue warp's current group
+  __shared__ __align__(16) double colscale[MODE == TC_MODE_V ? Sh::EW * CW : 2];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dsmem) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -359,36 +381,160 @@ __global__ void __launch_bounds__(TcShape<NW>::kThreads, 1)
     uint32_t grp = 0;
     for (long u = blockIdx.x; u < a.nunits && !abort_flag; u += gridDim.x) {
       UnitIter it(a, u, kBlockF / N);
-      double acc[32];
+      double acc[CW];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+      for (int j = 0; j < CW; ++j) acc[j] = 0.0;
       bool any = false;
       for_each_group(a, it, [&](const Group &g, auto) {
         if (abort_flag) return;
         const uint32_t buf = grp % NBUF, use = grp / NBUF;
+        if constexpr (MODE == TC_MODE_GRAD) {
+          // Y(g, mu) of the thread's point and 32 functions stays in
+          // registers: the thread adds grad phi_c(g, mu) Y(g, mu) over them
+          // (c = x, y, z), grad phi from the pass-A digits, and writes three
+          // partial sums that ygrad_sum_kernel adds up per point.  The digit
+          // words of the next slice of 8 functions load while the current
+          // one is combined; those of the first load before the wait for
+          // the accumulators.
+          const int gpt = 128 * it.h + row;
+          constexpr size_t kPlane = (size_t)kBatch * kBlockF;  // one digit plane of a pair, bytes
+          const uint8_t *dg = a.qphT + ((size_t)it.q * a.ncs + 1) * 4 * kPlane + (size_t)gpt * kBlockF + 64 * it.t + 32 * cq;
+          uint2 da[3][4], db[3][4];
+          auto load_digits = [&](int h, uint2(&w)[3][4]) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+              for (int d = 0; d < 4; ++d) w[c][d] = __ldg(reinterpret_cast<const uint2 *>(dg + (4 * c + d) * kPlane + 8 * h));
+          };
+          load_digits(0, da);
+          const double sa = a.sA[((it.bl * a.nspin + it.s) * 2 + it.h) * 128 + row] * kTwoM36;
+          const double sbl = a.sB[(size_t)it.s * a.nbf_pad + 128 * g.blk + 64 * it.t + 32 * cq + lane];
+          if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag, a.wait_ns)) return;
+          tc_fence_after();
+          __syncwarp();
+          double gs[3] = {0.0, 0.0, 0.0};
+          auto slice = [&](int h, const uint2(&w)[3][4]) {
+            uint32_t v0[8], v1[8], v2[8], v3[8];
+            const uint32_t ta = tmem + lane_addr + buf * 4 * N + 32 * cq + 8 * h;
+            tmem_ld8u_async(ta, v0);
+            tmem_ld8u_async(ta + N, v1);
+            tmem_ld8u_async(ta + 2 * N, v2);
+            tmem_ld8u_async(ta + 3 * N, v3);
+            tmem_wait8(v0);
+            tmem_wait8(v1);
+            tmem_wait8(v2);
+            tmem_wait8(v3);
+            if (h == 3) {
+              tc_fence_before();
+              mbar_arrive(&tempty_bar[buf]);
+            }
+            double y[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              y[j] = level_sum(v0[j], v1[j], v2[j], v3[j]) * (sa * __shfl_sync(0xffffffffu, sbl, 8 * h + j));
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+              for (int half = 0; half < 2; ++half) {
+                uint32_t wd[4], bw[4];
+#pragma unroll
+                for (int d = 0; d < 4; ++d) wd[3 - d] = half ? w[c][d].y : w[c][d].x;
+                transpose4(wd, bw);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) gs[c] = fma(int_to_double(digits_value(bw[k])), y[4 * half + k], gs[c]);
+              }
+          };
+          load_digits(1, db);
+          slice(0, da);
+          load_digits(2, da);
+          slice(1, db);
+          load_digits(3, db);
+          slice(2, da);
+          slice(3, db);
+          double *out = a.Gp + ((((size_t)it.q * a.nspin + it.s) * 2 + it.t) * 2 + cq) * 3 * kBatch + gpt;
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            out[c * kBatch] = gs[c] * (a.sphT[((size_t)it.q * a.ncs + 1 + c) * kBatch + gpt] * 0x1p-29);
+          ++grp;
+          return;
+        }
         if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag, a.wait_ns)) return;
         tc_fence_after();
         __syncwarp();
         const bool live = g.nsteps > 0;
+        // exact combine of the four levels, S = sum_L 2^(8 (3 - L)) Acc_L:
+        // |Acc_L| < 2^24 for K <= 256, so |S| < 2^49 (level_sum); the product
+        // is s_a s_b 2^-36 S (one rounding per group and element)
+        if constexpr (MODE == TC_MODE_V) {
+          // s_a is the thread's row scale; the warp's CW column scales are
+          // staged in shared memory once per group and read back as
+          // broadcasts, two per 16-byte load (instead of two shuffles per
+          // element).  Slices of four columns are software-pipelined: the
+          // loads of slice h + 1 are in flight while slice h is combined, and
+          // TMEM is released as soon as the last slice has arrived in
+          // registers.
+          if (live) {
+            const double sa = a.sA[g.qa * 128 + row] * kTwoM36;
+            double *cs = colscale + (warp - 2) * CW;
+            const double *sbp = a.sB + (g.qb * a.nz + it.zi) * 128 + N * it.hc + CW * cq;
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < CW / 32; ++k) cs[32 * k + lane] = sbp[32 * k + lane];
+            __syncwarp();
+            const uint32_t tb = tmem + lane_addr + buf * 4 * N + CW * cq;
+            constexpr int NS = CW / 4;
+            uint32_t p0[4], p1[4], p2[4], p3[4], r0[4], r1[4], r2[4], r3[4];
+            auto issue = [&](int h, uint32_t(&x0)[4], uint32_t(&x1)[4], uint32_t(&x2)[4], uint32_t(&x3)[4]) {
+              const uint32_t ta = tb + 4 * h;
+              tmem_ld4u_async(ta, x0);
+              tmem_ld4u_async(ta + N, x1);
+              tmem_ld4u_async(ta + 2 * N, x2);
+              tmem_ld4u_async(ta + 3 * N, x3);
+            };
+            auto combine = [&](int h, const uint32_t(&x0)[4], const uint32_t(&x1)[4], const uint32_t(&x2)[4],
+                               const uint32_t(&x3)[4]) {
+              const double2 c01 = *reinterpret_cast<const double2 *>(cs + 4 * h);
+              const double2 c23 = *reinterpret_cast<const double2 *>(cs + 4 * h + 2);
+              const double sc[4] = {c01.x, c01.y, c23.x, c23.y};
+#pragma unroll
+              for (int j = 0; j < 4; ++j)
+                acc[4 * h + j] = fma(level_sum(x0[j], x1[j], x2[j], x3[j]), sa * sc[j], acc[4 * h + j]);
+            };
+            issue(0, p0, p1, p2, p3);
+#pragma unroll
+            for (int h = 0; h < NS; ++h) {
+              if ((h & 1) == 0) {
+                tmem_wait4x4(p0, p1, p2, p3);
+                if (h + 1 < NS) issue(h + 1, r0, r1, r2, r3);
+              } else {
+                tmem_wait4x4(r0, r1, r2, r3);
+                if (h + 1 < NS) issue(h + 1, p0, p1, p2, p3);
+              }
+              if (h + 1 == NS) {
+                tc_fence_before();
+                mbar_arrive(&tempty_bar[buf]);
+              }
+              if ((h & 1) == 0)
+                combine(h, p0, p1, p2, p3);
+              else
+                combine(h, r0, r1, r2, r3);
+            }
+          } else {
+            tc_fence_before();
+            mbar_arrive(&tempty_bar[buf]);
+          }
+          ++grp;
+          any = any || live;
+          return;
+        }
         double sa = 0.0;
         const double *sb = nullptr;
         size_t sbs = 1;
         if (live) {
-          if (a.mode == TC_MODE_V) {
-            sa = a.sA[g.qa * 128 + row] * kTwoM36;
-            sb = a.sB + (g.qb * a.nz + it.zi) * 128 + N * it.hc + 32 * cq;
-          } else if (a.mode == TC_MODE_GRAD) {
-            sa = a.sA[((it.bl * a.nspin + it.s) * 2 + it.h) * 128 + row] * kTwoM36;
-            sb = a.sB + (size_t)it.s * a.nbf_pad + 128 * g.blk + 64 * it.t + 32 * cq;
-          } else {
-            sa = a.sA[(g.qa * a.ncs + it.c) * 256 + 128 * it.h + row] * kTwoM36;
-            sb = a.sB + ((size_t)it.s * a.nocc_pad + N * it.t + 32 * cq) * a.nblk + g.blk;
-            sbs = a.nblk;
-          }
+          sa = a.sA[(g.qa * a.ncs + it.c) * 256 + 128 * it.h + row] * kTwoM36;
+          sb = a.sB + ((size_t)it.s * a.nocc_pad + N * it.t + 32 * cq) * a.nblk + g.blk;
+          sbs = a.nblk;
         }
-        // exact combine of the four levels, S = sum_L 2^(8 (3 - L)) Acc_L:
-        // |Acc_L| < 2^24 for K <= 256, so |S| < 2^49 (level_sum); the product
-        // is s_a s_b 2^-36 S (one rounding per group and element)
         // the warp's 32 column scales, one per lane, handed out by shuffles
         const double sbl = live ? sb[lane * sbs] : 0.0;
         // slices of SL columns: 8 for the 320-thread shape, 4 for the
@@ -417,15 +563,7 @@ __global__ void __launch_bounds__(TcShape<NW>::kThreads, 1)
             tmem_wait4(v2);
             tmem_wait4(v3);
           }
-          if constexpr (MODE == TC_MODE_GRAD) {
-            // Y(g, mu) of the slice's SL functions
-            double *Yp = a.Y + ((it.q * a.nspin + it.s) * 256 + 128 * it.h + row) * 128 + 64 * it.t + 32 * cq + SL * hh;
-#pragma unroll
-            for (int j = 0; j < SL; ++j) {
-              const double S = level_sum(v0[j], v1[j], v2[j], v3[j]);
-              Yp[j] = S * (sa * __shfl_sync(0xffffffffu, sbl, SL * hh + j));
-            }
-          } else if (live) {
+          if (live) {
 #pragma unroll
             for (int j = 0; j < SL; ++j) {
               const double S = level_sum(v0[j], v1[j], v2[j], v3[j]);
@@ -438,21 +576,21 @@ __global__ void __launch_bounds__(TcShape<NW>::kThreads, 1)
         ++grp;
         any = any || live;
       });
-      if (a.mode == TC_MODE_V) {
+      if constexpr (MODE == TC_MODE_V) {
         if (any) {
           double *Vz = a.V + (size_t)it.zi * a.nbf_pad * a.nbf_pad;
           const size_t r = (size_t)it.I * 128 + row;
+          const size_t c0 = (size_t)it.J * 128 + N * it.hc + CW * cq;
           if (a.nsplit > 1) {
 #pragma unroll
-            for (int j = 0; j < 32; ++j)
-              atomicAdd(&Vz[r + ((size_t)it.J * 128 + N * it.hc + 32 * cq + j) * a.nbf_pad], acc[j]);
+            for (int j = 0; j < CW; ++j) atomicAdd(&Vz[r + (c0 + j) * a.nbf_pad], acc[j]);
           } else {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) Vz[r + ((size_t)it.J * 128 + N * it.hc + 32 * cq + j) * a.nbf_pad] += acc[j];
+            for (int j = 0; j < CW; ++j) Vz[r + (c0 + j) * a.nbf_pad] += acc[j];
           }
         }
-      } else if (a.mode == TC_MODE_GRAD) {
-        // Y is written slice by slice above
+      } else if constexpr (MODE == TC_MODE_GRAD) {
+        // the partial sums are written per group above
       } else {
         const long plane = (it.bl * a.nspin + it.s) * a.ncomp + it.c;
         double *Tp = a.T + plane * (long)a.nocc_pad * 256 + 128 * it.h + row;
@@ -586,47 +724,27 @@ __global__ void __launch_bounds__(128) quant_cocc_kernel(const double *__restric
                  sc + (size_t)s * nbf_pad + 128 * I);
 }
 
-// grad rho(g) = 2 sum_mu grad phi(g, mu) Y(g, mu) for one quarter (block z,
-// 64 points) of one batch (block x of the chunk) and spin (block y), summed
-// over the batch's pairs; grad phi comes back from the pass-A digits
-// (components 1..3).  Warp w takes the points 64 z + w + 8k, lane l the
-// functions 4l .. 4l+3 of each block.
-__global__ void __launch_bounds__(256) ygrad_kernel(const double *__restrict__ Y, const uint8_t *__restrict__ qphT,
-                                                    const double *__restrict__ sphT,
-                                                    const int *__restrict__ pair_off, long b0, long p0, int nspin,
-                                                    long npad, double *__restrict__ grad) {
+// grad rho(g) of one batch (block x of the chunk) and spin (block y), one
+// thread per point: the sum over the batch's pairs, function halves and
+// column groups of the partial sums 2 sum_mu grad phi_c(g, mu) Y(g, mu) that
+// the fused Y pass wrote, Gp[pair][spin][t][cq][c][g] (a fixed order, so the
+// result does not depend on scheduling).
+__global__ void __launch_bounds__(256) ygrad_sum_kernel(const double *__restrict__ Gp, const int *__restrict__ pair_off,
+                                                        long b0, long p0, int nspin, long npad,
+                                                        double *__restrict__ grad) {
   const long b = b0 + blockIdx.x;
-  const int s = blockIdx.y;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int s = blockIdx.y, g = threadIdx.x;
   const int q0 = pair_off[b], q1 = pair_off[b + 1];
-  for (int g = 64 * blockIdx.z + warp; g < 64 * (blockIdx.z + 1); g += 8) {
-    double gs[3] = {0.0, 0.0, 0.0};
-    for (int q = q0; q < q1; ++q) {
-      const long qr = q - p0;
-      const double2 *yp = reinterpret_cast<const double2 *>(Y + ((qr * nspin + s) * 256 + g) * 128 + 4 * lane);
-      const double2 ya = yp[0], yb = yp[1];
-      const double y[4] = {ya.x, ya.y, yb.x, yb.y};
+  double gs[3] = {0.0, 0.0, 0.0};
+  for (int q = q0; q < q1; ++q) {
+    const double *p = Gp + ((size_t)(q - p0) * nspin + s) * 12 * kBatch + g;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const long pc = qr * 4 + 1 + c;
-        uint32_t wd[4], bw[4];
+    for (int k = 0; k < 4; ++k)
 #pragma unroll
-        for (int d = 0; d < 4; ++d)
-          wd[3 - d] = reinterpret_cast<const uint32_t *>(qphT + ((pc * 4 + d) * 256 + g) * 128)[lane];
-        transpose4(wd, bw);
-        const double sc = sphT[pc * 256 + g] * 0x1p-30;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) gs[c] = fma(int_to_double(digits_value(bw[k])) * sc, y[k], gs[c]);
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double v = gs[c];
-#pragma unroll
-      for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if (lane == 0) grad[((size_t)s * 3 + c) * npad + b * kBatch + g] = 2.0 * v;
-    }
+      for (int c = 0; c < 3; ++c) gs[c] += p[(3 * k + c) * kBatch];
   }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) grad[((size_t)s * 3 + c) * npad + b * kBatch + g] = gs[c];
 }
 
 // Pass A, fused: collocation of one (batch, block) pair straight into the
@@ -680,6 +798,26 @@ __global__ void __launch_bounds__(256) colloc_quantT_kernel(const StoFunc *__res
       for (int d = 0; d < 4; ++d) reinterpret_cast<uint32_t *>(q + ((pc * 4 + d) * 256 + g) * 128)[lane] = w[d];
       if (lane == 0) sc[pc * 256 + g] = s;
     }
+  }
+}
+
+// Row scales of a pair's V operands from the per-warp maxima red[w][o][f]
+// (256-thread blocks, o = 0 phi, o >= 1 the Z planes): one power-of-two scale
+// per function row, sph[pair][f] and szs[pair][z][f].  (One scale for a whole
+// Z block would let the V epilogue skip the per-column scales, but rows far
+// below the block maximum then lose digits: max|dV| grew from about 1e-9 to
+// 1.3e-7 on an open-shell water cluster, over the 1e-7 target.)
+__device__ void store_operand_scales(double (*red)[4][128], int nop, int nz, long qrel, double *sph, double *szs) {
+  for (int e = threadIdx.x; e < nop * 128; e += blockDim.x) {
+    const int o = e / 128, ff = e % 128;
+    double mm = 0.0;
+    for (int w = 0; w < 8; ++w) mm = fmax(mm, red[w][o][ff]);
+    double sc;
+    inv_pow2_scale(mm, sc);
+    if (o == 0)
+      sph[qrel * 128 + ff] = sc;
+    else
+      szs[(qrel * nz + (o - 1)) * 128 + ff] = sc;
   }
 }
 
@@ -773,17 +911,7 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
 #pragma unroll
     for (int c = 0; c < 4; ++c) red[warp][o][4 * lane + c] = m[o][c];
   __syncthreads();
-  for (int e = threadIdx.x; e < nop * 128; e += 256) {
-    const int o = e / 128, ff = e % 128;
-    double mm = 0.0;
-    for (int w = 0; w < 8; ++w) mm = fmax(mm, red[w][o][ff]);
-    double s;
-    inv_pow2_scale(mm, s);
-    if (o == 0)
-      sph[qrel * 128 + ff] = s;
-    else
-      szs[(qrel * nz + (o - 1)) * 128 + ff] = s;
-  }
+  store_operand_scales(red, nop, nz, qrel, sph, szs);
 }
 
 // Pass B, part 1 for builds without J: the same operands as colloc_z_kernel,
@@ -870,17 +998,7 @@ __global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__
 #pragma unroll
     for (int c = 0; c < 4; ++c) red[warp][o][4 * lane + c] = m[o][c];
   __syncthreads();
-  for (int e = threadIdx.x; e < nop * 128; e += 256) {
-    const int o = e / 128, ff = e % 128;
-    double mm = 0.0;
-    for (int w = 0; w < 8; ++w) mm = fmax(mm, red[w][o][ff]);
-    double sc;
-    inv_pow2_scale(mm, sc);
-    if (o == 0)
-      sph[qrel * 128 + ff] = sc;
-    else
-      szs[(qrel * nz + (o - 1)) * 128 + ff] = sc;
-  }
+  store_operand_scales(red, nop, nz, qrel, sph, szs);
 }
 
 // Pass B, part 2: digits of the V operands, transposed to
@@ -1107,6 +1225,8 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     NKX_CUDA(cudaDeviceGetAttribute(&M->nsm, cudaDevAttrMultiProcessorCount, dev));
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_V, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   TcShape<128>::kSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_V, 128, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TcShape<128, 8>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_V, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   TcShape<64>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_DENSITY, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1135,10 +1255,10 @@ static MixedState &mixed_state(Plan &P, int nocc) {
   return M;
 }
 
-template <int MODE, int NW>
+template <int MODE, int NW, int EW = NW / 8>
 static void launch_i8_shape(const CUtensorMap &mA, const CUtensorMap &mB, const TcArgs &a, unsigned grid,
                             cudaStream_t s) {
-  tc_i8_kernel<MODE, NW><<<grid, TcShape<NW>::kThreads, TcShape<NW>::kSmem, s>>>(mA, mB, a);
+  tc_i8_kernel<MODE, NW, EW><<<grid, TcShape<NW, EW>::kThreads, TcShape<NW, EW>::kSmem, s>>>(mA, mB, a);
 }
 
 // one persistent CTA per SM (or per unit when there are fewer)
@@ -1147,8 +1267,16 @@ static void launch_i8(MixedState &M, const CUtensorMap &mA, const CUtensorMap &m
   const unsigned grid = (unsigned)std::min<long>(a.nunits, M.nsm);
   NKX_REQUIRE(a.nt == 64 || a.nt == 128, NKX_ERR_ARG, "tensor-core width must be 64 or 128");
   NKX_REQUIRE(a.mode != TC_MODE_GRAD || a.nt == 64, NKX_ERR_ARG, "the Y pass runs N = 64");
-  if (a.mode == TC_MODE_V)
-    a.nt == 128 ? launch_i8_shape<TC_MODE_V, 128>(mA, mB, a, grid, s) : launch_i8_shape<TC_MODE_V, 64>(mA, mB, a, grid, s);
+  NKX_REQUIRE(a.ew == a.nt / 8 || (a.mode == TC_MODE_V && a.nt == 128 && a.ew == 8), NKX_ERR_ARG,
+              "epilogue warps: N / 8, or 8 for the N = 128 V contraction");
+  if (a.mode == TC_MODE_V) {
+    if (a.nt == 64)
+      launch_i8_shape<TC_MODE_V, 64>(mA, mB, a, grid, s);
+    else if (a.ew == 8)
+      launch_i8_shape<TC_MODE_V, 128, 8>(mA, mB, a, grid, s);
+    else
+      launch_i8_shape<TC_MODE_V, 128>(mA, mB, a, grid, s);
+  }
   else if (a.mode == TC_MODE_GRAD)
     launch_i8_shape<TC_MODE_GRAD, 64>(mA, mB, a, grid, s);
   else
@@ -1249,6 +1377,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.ncs = nc;
     a.ncomp = grad_mode ? 1 : nc;
     a.nt = P.tune.dens_n;
+    a.ew = a.nt / 8;
     a.ntile_i = (nocc + a.nt - 1) / a.nt;
     a.nocc_pad = M.nocc_pad;
     a.T = M.T;
@@ -1284,16 +1413,19 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       g.nspin = nspin;
       g.ncs = nc;
       g.nocc_pad = M.nocc_pad;
-      g.Y = P.ws_phi;  // free during pass A: the FP64 staging of pass B
+      g.qphT = M.qphT;
+      g.sphT = M.sphT;
+      g.Gp = P.ws_phi;  // free during pass A: the FP64 staging of pass B
       g.err = P.d_status;
       g.wait_ns = P.wait_ns;
       g.stall = P.stall_test;
       g.nunits = np * nspin * 4;
       g.nt = 64;
+      g.ew = 8;
       launch_i8(M, M.m_t0, M.m_co, g, s);
       ++P.launches;
-      ygrad_kernel<<<dim3((unsigned)nb, nspin, 4), 256, 0, s>>>(P.ws_phi, M.qphT, M.sphT, P.d_pair_off, c.b0, c.p0,
-                                                               nspin, P.npad, P.d_grad);
+      ygrad_sum_kernel<<<dim3((unsigned)nb, nspin), 256, 0, s>>>(P.ws_phi, P.d_pair_off, c.b0, c.p0, nspin, P.npad,
+                                                                P.d_grad);
       NKX_LAUNCH_CHECK();
       ++P.launches;
     }
@@ -1332,10 +1464,16 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     // too few output tiles for the SMs: split the chunk's batches
     const long tiles = (long)nzs * P.nblk * P.nblk;
     a.nt = P.tune.v_n;
+    a.ew = a.nt == 128 ? P.tune.v_warps : 8;
     const long parts = tiles * (kBlockF / a.nt);
     a.nsplit = parts >= M.nsm ? 1 : (int)std::min<long>({(M.nsm + parts - 1) / parts, c.b1 - c.b0, 16L});
     a.nsplit = std::max(1, a.nsplit);
     a.nunits = parts * a.nsplit;
+    // output tiles in super-rows of vrow row blocks, so the units running at
+    // once (one per SM) form a near-square patch of tiles and share both
+    // their phi and their Z tiles in L2
+    const double wave = (double)std::min<long>(a.nunits, M.nsm) / (kBlockF / a.nt);
+    a.vrow = std::max(1, std::min(P.nblk, (int)std::lround(std::sqrt(wave))));
     launch_i8(M, M.m_ph, a.nt == 128 ? M.m_z : M.m_z64, a, s);
     ++P.launches;
     Tm.end(s);

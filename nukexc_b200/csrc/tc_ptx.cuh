@@ -152,6 +152,16 @@ __device__ __forceinline__ void tmem_wait4(uint32_t (&r)[4]) {
                : "memory");
 }
 
+// waits for every TMEM load of the thread; the four arrays (one slice of the
+// four accumulator levels) are valid afterwards
+__device__ __forceinline__ void tmem_wait4x4(uint32_t (&a)[4], uint32_t (&b)[4], uint32_t (&c)[4], uint32_t (&d)[4]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(b[0]), "+r"(b[1]), "+r"(b[2]), "+r"(b[3]),
+                 "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3]), "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+               :
+               : "memory");
+}
+
 // 32 lanes x 8 columns of 32-bit words from TMEM, without waiting; the
 // registers are valid only after tmem_wait8 on the same array
 __device__ __forceinline__ void tmem_ld8u_async(uint32_t taddr, uint32_t (&r)[8]) {

@@ -39,13 +39,14 @@ def test_widths_and_y_path_give_the_same_build(case):
     fb = A.FockBuilder(c, Z, A.make_manual_basis(funcs), g, func_ids=XC)
     E64, V64, _ = fb.build([Cm], [occ], precision="fp64")
     ref = {}
-    for v_n, d_n, yp in itertools.product((128, 64), (64, 128), (0, 1)):
-        fb.set_tuning(v_n=v_n, dens_n=d_n, ypath=yp)
+    # V shapes: N = 128 with 16 or 8 epilogue warps, N = 64
+    for (v_n, v_w), d_n, yp in itertools.product(((128, 16), (128, 8), (64, 16)), (64, 128), (0, 1)):
+        fb.set_tuning(v_n=v_n, dens_n=d_n, ypath=yp, v_warps=v_w)
         E, V, _ = fb.build([Cm], [occ], precision="mixed")
-        assert abs(E - E64) <= 1e-6 and np.abs(V[0] - V64[0]).max() <= 1e-7, (v_n, d_n, yp)
+        assert abs(E - E64) <= 1e-6 and np.abs(V[0] - V64[0]).max() <= 1e-7, (v_n, v_w, d_n, yp)
         if yp in ref:
             Er, Vr = ref[yp]
-            assert abs(E - Er) <= 1e-12 * abs(Er) and np.abs(V[0] - Vr).max() <= 1e-12, (v_n, d_n, yp)
+            assert abs(E - Er) <= 1e-12 * abs(Er) and np.abs(V[0] - Vr).max() <= 1e-12, (v_n, v_w, d_n, yp)
         else:
             ref[yp] = (E, V[0])
     fb.close()
@@ -72,6 +73,7 @@ def test_autotune_chooses_applies_and_caches(case, tmp_path):
     t = fb.autotune([Cm], [occ], cache_path=cache)
     assert t["from_cache"] == 0 and t["trials"] >= 4
     assert t["v_n"] in (64, 128) and t["dens_n"] in (64, 128) and t["ypath"] in (-1, 0, 1)
+    assert t["v_warps"] in (8, 16)
     assert 0 < t["best_ms"] <= t["default_ms"] * 1.0001
     assert fb.tuning()["v_n"] == t["v_n"] and fb.tuning()["chunk_pairs"] == t["chunk_pairs"]
     E, V, _ = fb.build([Cm], [occ], precision="mixed")
@@ -81,6 +83,6 @@ def test_autotune_chooses_applies_and_caches(case, tmp_path):
     fb2 = A.FockBuilder(c, Z, A.make_manual_basis(funcs), g, func_ids=XC)
     t2 = fb2.autotune([Cm], [occ], cache_path=cache)
     assert t2["from_cache"] == 1
-    assert (t2["v_n"], t2["dens_n"], t2["ypath"], t2["chunk_pairs"]) == (t["v_n"], t["dens_n"], t["ypath"],
-                                                                         t["chunk_pairs"])
+    keys = ("v_n", "dens_n", "ypath", "v_warps", "chunk_pairs")
+    assert tuple(t2[k] for k in keys) == tuple(t[k] for k in keys)
     fb2.close()
