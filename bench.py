@@ -722,6 +722,11 @@ def run_nkx(args):
             fp64["roofline"] = {"kernel": "vgemm_fp64_kernel (V = Phi Z^T, FP64 CUDA cores)", "achieved": v64,
                                 "peak": pd, "unit": "TFLOP/s", "frac": v64 / pd,
                                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (torch.matmul f64)"}
+        # the measurements below build plans of their own: the headline plan's
+        # device memory (its chunk workspace can hold ~100 GB) is freed first
+        fb.close()
+        fb = None
+        torch.cuda.empty_cache()
         if world == 1 and args.j_waters > 0 and not args.aux:
             line["xc_plus_j"] = xc_plus_j(args.j_waters, max(1, min(args.steps, 3)), args.warmup, stream)
         if world == 1 and args.grad_waters > 0:
@@ -731,7 +736,8 @@ def run_nkx(args):
         if world == 1 and args.aggregate_gate > 0 and not args.aggregate:
             line["aggregate_gate"] = aggregate_gate(args.aggregate_gate, stream, peak if prec == "mixed" else None)
         print(json.dumps(line), flush=True)
-    fb.close()
+    if fb is not None:
+        fb.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -1037,6 +1037,47 @@ void plan_chunks(Plan &P, long maxp) {
     P.chunks.push_back(c);
   }
   P.chunk_pair_limit = maxp;
+  // V output tiles of each chunk.  A unit of the V contraction is one
+  // (I, J) tile walking the chunk's batches where both blocks are
+  // significant; tiles with no such batch get no unit, and the rest are
+  // ordered heaviest first (round-robin over the SMs then spreads the heavy
+  // tiles evenly).  Ties keep a square-patch order (row blocks in super-rows
+  // of about sqrt(SMs)), so that the units running at once share their phi
+  // and Z tiles in L2; on a dense problem every tile costs the same and the
+  // whole order is the patch order.
+  {
+    int nsm = 148;
+    NKX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P.device));
+    const int nb = P.nblk, vrow = std::max(1, std::min(nb, (int)std::lround(std::sqrt((double)nsm))));
+    NKX_REQUIRE(nb < (1 << 15), NKX_ERR_UNSUPPORTED, "more than 32767 function blocks");
+    std::vector<int> patch;
+    patch.reserve((size_t)nb * nb);
+    for (int r0 = 0; r0 < nb; r0 += vrow)
+      for (int J = 0; J < nb; ++J)
+        for (int I = r0; I < std::min(nb, r0 + vrow); ++I) patch.push_back(I * nb + J);
+    std::vector<int> cnt((size_t)nb * nb), blk, tiles, all;
+    for (Chunk &c : P.chunks) {
+      std::fill(cnt.begin(), cnt.end(), 0);
+      for (long b = c.b0; b < c.b1; ++b) {
+        blk.clear();
+        for (int w = 0; w < P.mask_words; ++w)
+          for (uint32_t m = P.h_mask[b * P.mask_words + w]; m; m &= m - 1) blk.push_back(32 * w + __builtin_ctz(m));
+        for (int I : blk)
+          for (int J : blk) ++cnt[(size_t)I * nb + J];
+      }
+      tiles.clear();
+      for (int t : patch)
+        if (cnt[t]) tiles.push_back(t);
+      std::stable_sort(tiles.begin(), tiles.end(), [&](int x, int y) { return cnt[x] > cnt[y]; });
+      c.t0 = (long)all.size();
+      for (int t : tiles) all.push_back(((t / nb) << 16) | (t % nb));
+      c.t1 = (long)all.size();
+    }
+    P.release(P.d_vtiles);
+    P.d_vtiles = P.alloc<int>(std::max<size_t>(1, all.size()));
+    if (!all.empty())
+      NKX_CUDA(cudaMemcpy(P.d_vtiles, all.data(), sizeof(int) * all.size(), cudaMemcpyHostToDevice));
+  }
   const size_t tile = (size_t)kBatch * kBlockF;
   P.release(P.ws_phi);
   P.release(P.ws_z);

@@ -12,6 +12,7 @@ namespace nkx {
 struct Chunk {
   long b0 = 0, b1 = 0;  // batch range
   long p0 = 0, p1 = 0;  // (batch, block) pair range
+  long t0 = 0, t1 = 0;  // range of the chunk's V output tiles in d_vtiles
 };
 
 // Choices of the mixed-precision build that the autotuner (nkx_plan_autotune)
@@ -80,6 +81,9 @@ struct Plan {
 
   std::vector<Chunk> chunks;
   long max_chunk_pairs = 0, chunk_pair_limit = 0;
+  // V output tiles (I << 16 | J) of each chunk that have at least one batch
+  // with both blocks significant, heaviest first (plan_chunks)
+  int *d_vtiles = nullptr;
   Tuning tune;
   double *ws_phi = nullptr;  // PhiT tiles of a chunk: [pair][comp][g][f]
   double *ws_z = nullptr;    // Z^T tiles of a chunk:  [pair][z][g][f]

@@ -114,7 +114,8 @@ struct TcArgs {
   int stall;
   int nt;  // MMA width N of the launched kernel (V: 128 / nt units per output tile)
   int ew;  // epilogue warps of the launched kernel (N = 128 V: 16 or 8)
-  int vrow;  // V: row blocks per super-row of the unit order (1: row-major)
+  const int *vtiles;  // V: the chunk's output tiles (I << 16 | J), ntiles of them
+  long ntiles;
 };
 
 // S = 2^24 L0 + 2^16 L1 + 2^8 L2 + L3 of four int32 accumulator levels,
@@ -138,18 +139,15 @@ struct UnitIter {
   // compile-time constant at the kernel's call sites)
   __device__ UnitIter(const TcArgs &a, long u, int nh) {
     if (a.mode == TC_MODE_V) {
-      const long n2 = (long)a.nblk * a.nblk * nh, n3 = n2 * a.nz;
+      const long n2 = a.ntiles * nh, n3 = n2 * a.nz;
       sp = (int)(u / n3);
       u %= n3;
       zi = (int)(u / n2);
       u %= n2;
-      // super-row r holds row blocks r vrow .. + hr - 1, column-major inside
       hc = (int)(u % nh);
-      const long v = u / nh, srow = (long)a.vrow * a.nblk;
-      const int r = (int)(v / srow), w = (int)(v - r * srow);
-      const int hr = min(a.vrow, a.nblk - r * a.vrow);
-      J = w / hr;
-      I = r * a.vrow + w % hr;
+      const int t = a.vtiles[u / nh];
+      I = t >> 16;
+      J = t & 0xffff;
     } else if (a.mode == TC_MODE_GRAD) {
       t = (int)(u % 2);  // 64-function half of the block
       h = (int)((u / 2) % 2);
@@ -392,28 +390,28 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
           // Y(g, mu) of the thread's point and 32 functions stays in
           // registers: the thread adds grad phi_c(g, mu) Y(g, mu) over them
           // (c = x, y, z), grad phi from the pass-A digits, and writes three
-          // partial sums that ygrad_sum_kernel adds up per point.  The digit
-          // words of the next slice of 8 functions load while the current
-          // one is combined; those of the first load before the wait for
-          // the accumulators.
+          // partial sums that ygrad_sum_kernel adds up per point.  Each digit
+          // plane of a component is one 32-byte load per thread (the 32
+          // functions' bytes of its point); the loads of component c + 1 are
+          // in flight while component c is combined, those of the first
+          // before the wait for the accumulators.
           const int gpt = 128 * it.h + row;
           constexpr size_t kPlane = (size_t)kBatch * kBlockF;  // one digit plane of a pair, bytes
           const uint8_t *dg = a.qphT + ((size_t)it.q * a.ncs + 1) * 4 * kPlane + (size_t)gpt * kBlockF + 64 * it.t + 32 * cq;
-          uint2 da[3][4], db[3][4];
-          auto load_digits = [&](int h, uint2(&w)[3][4]) {
+          uint32_t w0[4][8], w1[4][8];
+          auto load_comp = [&](int c, uint32_t(&w)[4][8]) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
-#pragma unroll
-              for (int d = 0; d < 4; ++d) w[c][d] = __ldg(reinterpret_cast<const uint2 *>(dg + (4 * c + d) * kPlane + 8 * h));
+            for (int d = 0; d < 4; ++d) ldg256(dg + (4 * c + d) * kPlane, w[d]);
           };
-          load_digits(0, da);
+          load_comp(0, w0);
           const double sa = a.sA[((it.bl * a.nspin + it.s) * 2 + it.h) * 128 + row] * kTwoM36;
           const double sbl = a.sB[(size_t)it.s * a.nbf_pad + 128 * g.blk + 64 * it.t + 32 * cq + lane];
           if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag, a.wait_ns)) return;
           tc_fence_after();
           __syncwarp();
-          double gs[3] = {0.0, 0.0, 0.0};
-          auto slice = [&](int h, const uint2(&w)[3][4]) {
+          double y[32];
+#pragma unroll
+          for (int h = 0; h < 4; ++h) {
             uint32_t v0[8], v1[8], v2[8], v3[8];
             const uint32_t ta = tmem + lane_addr + buf * 4 * N + 32 * cq + 8 * h;
             tmem_ld8u_async(ta, v0);
@@ -428,29 +426,29 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
               tc_fence_before();
               mbar_arrive(&tempty_bar[buf]);
             }
-            double y[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j)
-              y[j] = level_sum(v0[j], v1[j], v2[j], v3[j]) * (sa * __shfl_sync(0xffffffffu, sbl, 8 * h + j));
+              y[8 * h + j] = level_sum(v0[j], v1[j], v2[j], v3[j]) * (sa * __shfl_sync(0xffffffffu, sbl, 8 * h + j));
+          }
+          // word k of plane d holds digit d of functions 4k .. 4k + 3
+          auto combine = [&](const uint32_t(&w)[4][8]) {
+            double gsum = 0.0;
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 8; ++k) {
+              const uint32_t wd[4] = {w[3][k], w[2][k], w[1][k], w[0][k]};
+              uint32_t bw[4];
+              transpose4(wd, bw);
 #pragma unroll
-              for (int half = 0; half < 2; ++half) {
-                uint32_t wd[4], bw[4];
-#pragma unroll
-                for (int d = 0; d < 4; ++d) wd[3 - d] = half ? w[c][d].y : w[c][d].x;
-                transpose4(wd, bw);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) gs[c] = fma(int_to_double(digits_value(bw[k])), y[4 * half + k], gs[c]);
-              }
+              for (int e = 0; e < 4; ++e) gsum = fma(int_to_double(digits_value(bw[e])), y[4 * k + e], gsum);
+            }
+            return gsum;
           };
-          load_digits(1, db);
-          slice(0, da);
-          load_digits(2, da);
-          slice(1, db);
-          load_digits(3, db);
-          slice(2, da);
-          slice(3, db);
+          load_comp(1, w1);
+          const double g0 = combine(w0);
+          load_comp(2, w0);
+          const double g1 = combine(w1);
+          const double g2 = combine(w0);
+          const double gs[3] = {g0, g1, g2};
           double *out = a.Gp + ((((size_t)it.q * a.nspin + it.s) * 2 + it.t) * 2 + cq) * 3 * kBatch + gpt;
 #pragma unroll
           for (int c = 0; c < 3; ++c)
@@ -1461,19 +1459,17 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.err = P.d_status;
     a.wait_ns = P.wait_ns;
     a.stall = P.stall_test;
-    // too few output tiles for the SMs: split the chunk's batches
-    const long tiles = (long)nzs * P.nblk * P.nblk;
+    // the chunk's nonempty output tiles, heaviest first; too few units for
+    // the SMs: split the chunk's batches
+    a.vtiles = P.d_vtiles + c.t0;
+    a.ntiles = c.t1 - c.t0;
+    const long tiles = (long)nzs * a.ntiles;
     a.nt = P.tune.v_n;
     a.ew = a.nt == 128 ? P.tune.v_warps : 8;
     const long parts = tiles * (kBlockF / a.nt);
-    a.nsplit = parts >= M.nsm ? 1 : (int)std::min<long>({(M.nsm + parts - 1) / parts, c.b1 - c.b0, 16L});
+    a.nsplit = (parts == 0 || parts >= M.nsm) ? 1 : (int)std::min<long>({(M.nsm + parts - 1) / parts, c.b1 - c.b0, 16L});
     a.nsplit = std::max(1, a.nsplit);
     a.nunits = parts * a.nsplit;
-    // output tiles in super-rows of vrow row blocks, so the units running at
-    // once (one per SM) form a near-square patch of tiles and share both
-    // their phi and their Z tiles in L2
-    const double wave = (double)std::min<long>(a.nunits, M.nsm) / (kBlockF / a.nt);
-    a.vrow = std::max(1, std::min(P.nblk, (int)std::lround(std::sqrt(wave))));
     launch_i8(M, M.m_ph, a.nt == 128 ? M.m_z : M.m_z64, a, s);
     ++P.launches;
     Tm.end(s);

@@ -162,6 +162,13 @@ __device__ __forceinline__ void tmem_wait4x4(uint32_t (&a)[4], uint32_t (&b)[4],
                : "memory");
 }
 
+// 32 bytes from global memory in one read-only load (32-byte aligned address)
+__device__ __forceinline__ void ldg256(const void *p, uint32_t (&r)[8]) {
+  asm volatile("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "l"(p));
+}
+
 // 32 lanes x 8 columns of 32-bit words from TMEM, without waiting; the
 // registers are valid only after tmem_wait8 on the same array
 __device__ __forceinline__ void tmem_ld8u_async(uint32_t taddr, uint32_t (&r)[8]) {

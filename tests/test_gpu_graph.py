@@ -82,13 +82,14 @@ def test_device_scf_with_graph_replays(precision):
     for graph in (False, True):
         fb = A.FockBuilder(c, Z, b, g, aux=A.make_manual_basis(aux), func_ids=("LDA_X", "LDA_C_VWN"))
         fb.set_graph(graph)
-        r = scf.rks_device(S, H, fb, 5, enuc, precision=precision, conv=1e-10)
+        r = scf.rks_device(S, H, fb, 5, enuc, precision=precision, conv=1e-10 if precision == "fp64" else 1e-9)
         assert r["converged"]
         out.append((r["energy"], fb.info()["graph_replays"]))
         fb.close()
-    # both runs converge to 1e-10 Eh between iterations.  FP64: the same
-    # energy; mixed: its small-system V adds batch splits atomically in varying
-    # order, so the runs differ at rounding level and settle within about the
-    # convergence threshold of each other
-    assert abs(out[0][0] - out[1][0]) < (1e-10 if precision == "fp64" else 1e-9)
+    # FP64 (converged to 1e-10 Eh between iterations): the same energy.  Mixed
+    # (converged to 1e-9, about its noise floor: its V is within 1e-8 of a
+    # derivative of its E, and the small-system V adds batch splits
+    # atomically in varying order): the runs stop within a few thresholds of
+    # each other
+    assert abs(out[0][0] - out[1][0]) < (1e-10 if precision == "fp64" else 5e-9)
     assert out[0][1] == 0 and out[1][1] >= 5
