@@ -82,14 +82,14 @@ def test_device_scf_with_graph_replays(precision):
     for graph in (False, True):
         fb = A.FockBuilder(c, Z, b, g, aux=A.make_manual_basis(aux), func_ids=("LDA_X", "LDA_C_VWN"))
         fb.set_graph(graph)
-        r = scf.rks_device(S, H, fb, 5, enuc, precision=precision, conv=1e-10 if precision == "fp64" else 1e-9)
+        r = scf.rks_device(S, H, fb, 5, enuc, precision=precision, conv=1e-10 if precision == "fp64" else 1e-8)
         assert r["converged"]
         out.append((r["energy"], fb.info()["graph_replays"]))
         fb.close()
     # FP64 (converged to 1e-10 Eh between iterations): the same energy.  Mixed
-    # (converged to 1e-9, about its noise floor: its V is within 1e-8 of a
-    # derivative of its E, and the small-system V adds batch splits
-    # atomically in varying order): the runs stop within a few thresholds of
-    # each other
-    assert abs(out[0][0] - out[1][0]) < (1e-10 if precision == "fp64" else 5e-9)
+    # (converged to 1e-8, its practical floor: the orbitals' int8 digits round
+    # differently from one iteration to the next, which moves E by about
+    # 1e-9, and the small-system V adds batch splits atomically in varying
+    # order): the two runs stop within about two thresholds of each other
+    assert abs(out[0][0] - out[1][0]) < (1e-10 if precision == "fp64" else 3e-8)
     assert out[0][1] == 0 and out[1][1] >= 5
