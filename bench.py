@@ -328,11 +328,12 @@ def xc_plus_j(n, steps, warmup, stream):
 
 
 def xc_gradient_check(n, stream, ngeom=10, ncomp=1, h=1e-4):
-    """XC nuclear gradient (FP64) of (H2O)_n PBE at seeded perturbed geometries
-    (each atom + N(0, 0.05 bohr)): time per gradient and the largest deviation
+    """XC nuclear gradient of (H2O)_n PBE at seeded perturbed geometries (each
+    atom + N(0, 0.05 bohr)): FP64 time per gradient and its largest deviation
     from Richardson-extrapolated central differences of the FP64 E_xc of the
     GPU build on a few seeded components (grid rebuilt at each displaced
-    geometry, no weight-threshold compaction)."""
+    geometry, no weight-threshold compaction); the mixed-precision gradient's
+    time and its largest deviation from the FP64 gradient."""
     import torch
     from nukexc_b200 import api as A
     from nukexc_b200 import molecules as M
@@ -352,7 +353,7 @@ def xc_gradient_check(n, stream, ngeom=10, ncomp=1, h=1e-4):
         fb.close()
         return E
 
-    times, worst, comps = [], 0.0, []
+    times, times_m, worst, worst_m, comps = [], [], 0.0, 0.0, []
     for k in range(ngeom):
         c = np.asarray(c0, float) + rng.normal(0.0, 0.05, size=np.shape(c0))
         fb = builder(c)
@@ -361,6 +362,12 @@ def xc_gradient_check(n, stream, ngeom=10, ncomp=1, h=1e-4):
         t0 = time.perf_counter()
         G = fb.xc_gradient([Cm], [occ])
         times.append((time.perf_counter() - t0) * 1e3)
+        fb.xc_gradient([Cm], [occ], precision="mixed")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Gm = fb.xc_gradient([Cm], [occ], precision="mixed")
+        times_m.append((time.perf_counter() - t0) * 1e3)
+        worst_m = max(worst_m, float(np.abs(Gm - G).max()))
         fb.close()
         for _ in range(ncomp):
             a, j = int(rng.integers(len(Z))), int(rng.integers(3))
@@ -373,10 +380,13 @@ def xc_gradient_check(n, stream, ngeom=10, ncomp=1, h=1e-4):
             fd = (4.0 * central(h / 2) - central(h)) / 3.0
             worst = max(worst, abs(G[a, j] - fd))
             comps.append([k, a, j])
-    return {"workload": f"(H2O)_{n} PBE XC nuclear gradient, FP64", "geometries": ngeom,
+    return {"workload": f"(H2O)_{n} PBE XC nuclear gradient", "geometries": ngeom,
             "ms_per_gradient": float(np.median(times)), "fd_components": comps,
             "max_abs_error_vs_fd": worst, "gate": "<= 1e-5 Eh/bohr",
-            "fd": "Richardson-extrapolated central differences, h = 1e-4 and 5e-5 bohr, FP64 GPU E_xc"}
+            "fd": "Richardson-extrapolated central differences, h = 1e-4 and 5e-5 bohr, FP64 GPU E_xc",
+            "mixed": {"ms_per_gradient": float(np.median(times_m)), "max_abs_diff_vs_fp64_gradient": worst_m,
+                      "note": "orbital values and density from the int8-digit tensor-core contraction, "
+                              "pair terms, STO Hessians and Becke term in FP64"}}
 
 
 def aggregate_gate(natoms, stream, int8_peak=None):

@@ -337,16 +337,20 @@ NKX_API nkx_status nkx_plan_get_tuning(const nkx_plan *plan, nkx_tuning *out);
 /* Apply choices (for example a stored autotune result); chunk_pairs <= 0 keeps the chunking. */
 NKX_API nkx_status nkx_plan_set_tuning(nkx_plan *plan, const nkx_tuning *t);
 
-/* XC nuclear gradient at fixed orbitals, FP64 (no counterpart in the
- * reference): grad[3*natoms] (host, Eh/bohr) = dE_xc/dR of
+/* XC nuclear gradient at fixed orbitals (no counterpart in the reference):
+ * grad[3*natoms] (host, Eh/bohr) = dE_xc/dR of
  * E_xc = sum_g w_g f(rho(r_g)) with every grid point moving with its owner
  * atom and the Becke weights differentiated (becke_clamp as in
  * nkx_becke_partition; the plan's weights must be radial x angular weights
  * times that Becke partition).  The plan must have been created with the
  * molecule and the point owners, with every basis function centred on an
- * atom.  C / occ as in nkx_fock_build (mem selects host or device). */
-NKX_API nkx_status nkx_xc_gradient(nkx_plan *plan, int nspin, int nocc, const double *C, const double *occ,
-                                   int mem, double becke_clamp, double *grad, void *stream);
+ * atom.  C / occ as in nkx_fock_build (mem selects host or device).
+ * precision: NKX_PREC_FP64 (everything in FP64), or NKX_PREC_MIXED (B200:
+ * the orbital values T = C^T Phi and grad Phi, and with them the density,
+ * come from the int8-digit tensor-core contraction of the mixed Fock build;
+ * the pair terms, STO Hessians and the Becke term stay FP64). */
+NKX_API nkx_status nkx_xc_gradient(nkx_plan *plan, int precision, int nspin, int nocc, const double *C,
+                                   const double *occ, int mem, double becke_clamp, double *grad, void *stream);
 
 NKX_API nkx_status nkx_get_last_timing(const nkx_plan *plan, nkx_build_timing *t);
 

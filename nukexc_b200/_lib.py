@@ -112,7 +112,7 @@ def lib():
             "nkx_plan_core_hamiltonian": [vp, vp, vp, vp, vp, i, vp],
             "nkx_plan_set_graph": [vp, i],
             "nkx_plan_set_tuning": [vp, vp],
-            "nkx_xc_gradient": [vp, i, i, vp, vp, i, d, vp, vp],
+            "nkx_xc_gradient": [vp, i, i, i, vp, vp, i, d, vp, vp],
             "nkx_get_last_timing": [vp, vp],
             "nkx_plan_last_density": [vp, vp, vp],
             "nkx_plan_batch_blocks": [vp, vp],

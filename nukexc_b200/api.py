@@ -399,10 +399,12 @@ class FockBuilder:
             Jm = J.view(self.nbf, self.nbf).t() if J is not None else None
         return E.value, Vs, Jm
 
-    def xc_gradient(self, C_list, occ_list, becke_clamp=5.0, stream=None):
-        """dE_xc/dR (natoms x 3, Eh/bohr) at fixed orbitals, FP64, with the grid
+    def xc_gradient(self, C_list, occ_list, becke_clamp=5.0, stream=None, precision="fp64"):
+        """dE_xc/dR (natoms x 3, Eh/bohr) at fixed orbitals, with the grid
         points moving with their owner atoms and the Becke weights
-        differentiated (nkx_xc_gradient)."""
+        differentiated (nkx_xc_gradient).  precision "mixed" takes the
+        orbital values and the density from the int8-digit tensor-core
+        contraction; the rest is FP64."""
         nspin = len(C_list)
         nocc = C_list[0].shape[1]
         Cc = np.concatenate([np.ascontiguousarray(np.asarray(c, np.float64).T).reshape(-1) for c in C_list])
@@ -410,7 +412,8 @@ class FockBuilder:
         natoms = len(self._mk[0]) // 3
         g = np.zeros(3 * natoms)
         s = C.c_void_p(stream) if stream else None
-        check(L.lib().nkx_xc_gradient(self._h, nspin, nocc, Cc.ctypes.data_as(C.c_void_p),
+        prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
+        check(L.lib().nkx_xc_gradient(self._h, prec, nspin, nocc, Cc.ctypes.data_as(C.c_void_p),
                                       oc.ctypes.data_as(C.c_void_p), L.MEM_HOST, becke_clamp,
                                       g.ctypes.data_as(C.c_void_p), s))
         return g.reshape(natoms, 3)

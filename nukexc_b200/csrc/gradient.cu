@@ -424,7 +424,7 @@ void destroy_grad_state(void *p) { delete static_cast<GradState *>(p); }
 // orbital-value tiles of at most this many bytes per sub-range of batches
 constexpr size_t kGradTBytes = (size_t)2 << 30;
 
-static GradState &grad_state(Plan &P, int nspin, int nocc) {
+static GradState &grad_state(Plan &P, int nspin, int nocc, bool need_T) {
   if (!P.grad_state) {
     GradState *G = new GradState();
     P.grad_state = G;
@@ -432,6 +432,7 @@ static GradState &grad_state(Plan &P, int nspin, int nocc) {
     G->F = G->alloc(3 * (size_t)P.natoms);
   }
   GradState &G = *static_cast<GradState *>(P.grad_state);
+  if (!need_T) return G;
   const int NC = P.gga ? 4 : 1;
   const int nocc_pad = ((nocc + 63) / 64) * 64;
   long maxb = 1;
@@ -447,21 +448,10 @@ static GradState &grad_state(Plan &P, int nspin, int nocc) {
   return G;
 }
 
-static void xc_gradient(Plan &P, int nspin, int nocc, const double *C, const double *occ, int mem, double clamp,
-                        double *grad, cudaStream_t s) {
-  NKX_REQUIRE(nspin == 1 || nspin == 2, NKX_ERR_ARG, "nspin must be 1 or 2");
-  NKX_REQUIRE(nocc > 0 && C && occ && grad, NKX_ERR_ARG, "invalid arguments");
-  NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
-  NKX_REQUIRE(P.natoms > 0 && P.d_owner, NKX_ERR_ARG, "the gradient needs a plan created with atoms and point owners");
-  NKX_REQUIRE(P.all_funcs_on_atoms, NKX_ERR_ARG, "the gradient needs every basis function centred on an atom");
-  P.launches = 0;
-  StageTimer Tm;
-  NKX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int) * 2, s));
-  upload_orbitals(P, nspin, nocc, C, occ, mem, s);
+// FP64 part of the gradient: the density of the FP64 build, the functional,
+// then per chunk the FP64 collocation, the orbital values T and the pair terms.
+static void fp64_gradient_chunks(Plan &P, GradState &G, int nspin, int nocc, cudaStream_t s, StageTimer &Tm) {
   fp64_density_pass(P, nspin, nocc, s, Tm);
-  GradState &G = grad_state(P, nspin, nocc);
-  NKX_CUDA(cudaMemsetAsync(P.d_E, 0, sizeof(double), s));
-  NKX_CUDA(cudaMemsetAsync(G.F, 0, sizeof(double) * 3 * P.natoms, s));
   functional_kernel<<<gblk(P.npad, 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, P.npad, P.d_w, P.d_rho, P.d_grad, nullptr,
                                                      P.d_coef, P.d_E, G.edens);
   NKX_LAUNCH_CHECK();
@@ -493,6 +483,53 @@ static void xc_gradient(Plan &P, int nspin, int nocc, const double *C, const dou
       P.launches += 2;
     }
   }
+}
+
+static void xc_gradient(Plan &P, int precision, int nspin, int nocc, const double *C, const double *occ, int mem,
+                        double clamp, double *grad, cudaStream_t s) {
+  NKX_REQUIRE(precision == NKX_PREC_FP64 || precision == NKX_PREC_MIXED, NKX_ERR_ARG,
+              "precision must be NKX_PREC_FP64 or NKX_PREC_MIXED");
+  NKX_REQUIRE(precision == NKX_PREC_FP64 || mixed_available(P), NKX_ERR_UNSUPPORTED,
+              "the mixed-precision gradient needs an sm_100 device");
+  NKX_REQUIRE(nspin == 1 || nspin == 2, NKX_ERR_ARG, "nspin must be 1 or 2");
+  NKX_REQUIRE(nocc > 0 && C && occ && grad, NKX_ERR_ARG, "invalid arguments");
+  NKX_REQUIRE(mem == NKX_MEM_DEVICE || mem == NKX_MEM_HOST, NKX_ERR_ARG, "mem must be NKX_MEM_DEVICE or NKX_MEM_HOST");
+  NKX_REQUIRE(P.natoms > 0 && P.d_owner, NKX_ERR_ARG, "the gradient needs a plan created with atoms and point owners");
+  NKX_REQUIRE(P.all_funcs_on_atoms, NKX_ERR_ARG, "the gradient needs every basis function centred on an atom");
+  P.launches = 0;
+  StageTimer Tm;
+  NKX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int) * 2, s));
+  upload_orbitals(P, nspin, nocc, C, occ, mem, s);
+  const bool mixed = precision == NKX_PREC_MIXED;
+  GradState &G = grad_state(P, nspin, nocc, !mixed);
+  NKX_CUDA(cudaMemsetAsync(P.d_E, 0, sizeof(double), s));
+  NKX_CUDA(cudaMemsetAsync(G.F, 0, sizeof(double) * 3 * P.natoms, s));
+  if (mixed) {
+    // Mixed precision: per chunk, the orbital values T_c come from the int8
+    // digit contraction on the tensor cores, which also gives rho, grad rho
+    // and the functional of the chunk's points; the rest of the gradient
+    // (X = C (occ T) and its gradient, the STO Hessians, the Becke term) is
+    // the FP64 code below.
+    mixed_gradient_begin(P, nspin, nocc, s);
+    for (const Chunk &c : P.chunks) {
+      int npadT = 0;
+      const double *T = mixed_gradient_chunk(P, c, nspin, nocc, G.edens, s, &npadT);
+      const long q0 = c.p0, q1 = c.p1;
+      if (q1 <= q0) continue;
+      if (P.gga)
+        grad_pair_kernel<true><<<(unsigned)(q1 - q0), 256, 0, s>>>(
+            P.d_sto, P.d_fatom, P.d_px, P.d_py, P.d_pz, P.d_owner, P.d_pair_batch, P.d_pair_blk, q0, c.b0, P.d_Ct,
+            P.d_occ, nocc, npadT, P.nbf_pad, nspin, T, P.d_coef, P.npad, G.F);
+      else
+        grad_pair_kernel<false><<<(unsigned)(q1 - q0), 256, 0, s>>>(
+            P.d_sto, P.d_fatom, P.d_px, P.d_py, P.d_pz, P.d_owner, P.d_pair_batch, P.d_pair_blk, q0, c.b0, P.d_Ct,
+            P.d_occ, nocc, npadT, P.nbf_pad, nspin, T, P.d_coef, P.npad, G.F);
+      NKX_LAUNCH_CHECK();
+      ++P.launches;
+    }
+  } else {
+    fp64_gradient_chunks(P, G, nspin, nocc, s, Tm);
+  }
   const size_t fs_bytes = sizeof(double) * 3 * (size_t)P.natoms;
   const bool smem = fs_bytes <= 48 * 1024;
   becke_grad_kernel<<<gblk(P.npad, 128), 128, smem ? fs_bytes : 0, s>>>(P.d_centers, P.natoms, P.d_px, P.d_py,
@@ -504,17 +541,19 @@ static void xc_gradient(Plan &P, int nspin, int nocc, const double *C, const dou
   int status[2] = {0, 0};
   NKX_CUDA(cudaMemcpyAsync(status, P.d_status, sizeof(status), cudaMemcpyDeviceToHost, s));
   NKX_CUDA(cudaStreamSynchronize(s));
+  NKX_REQUIRE(status[0] == 0, NKX_ERR_TIMEOUT, "a tensor-core kernel wait gave up; the gradient is invalid");
   NKX_REQUIRE(status[1] == 0, NKX_ERR_NUMERIC, "non-finite value in the orbitals or occupations");
 }
 
 }  // namespace nkx
 
-extern "C" NKX_API nkx_status nkx_xc_gradient(nkx_plan *plan, int nspin, int nocc, const double *C, const double *occ,
-                                              int mem, double becke_clamp, double *grad, void *stream) {
+extern "C" NKX_API nkx_status nkx_xc_gradient(nkx_plan *plan, int precision, int nspin, int nocc, const double *C,
+                                               const double *occ, int mem, double becke_clamp, double *grad,
+                                               void *stream) {
   return nkx::run_guarded("nkx_xc_gradient", [&] {
     NKX_REQUIRE(plan, NKX_ERR_ARG, "plan is NULL");
     nkx::Plan &P = *reinterpret_cast<nkx::Plan *>(plan);
-    nkx::xc_gradient(P, nspin, nocc, C, occ, mem, becke_clamp, grad,
+    nkx::xc_gradient(P, precision, nspin, nocc, C, occ, mem, becke_clamp, grad,
                      stream ? (cudaStream_t)stream : P.stream);
   });
 }

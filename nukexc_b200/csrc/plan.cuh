@@ -195,6 +195,9 @@ __global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, long
                                   const double *__restrict__ rho, const double *__restrict__ grad,
                                   const double *__restrict__ vj, double *__restrict__ coef, double *Eacc,
                                   double *__restrict__ edens);
+void mixed_gradient_begin(Plan &P, int nspin, int nocc, cudaStream_t s);
+const double *mixed_gradient_chunk(Plan &P, const Chunk &c, int nspin, int nocc, double *edens, cudaStream_t s,
+                                   int *nocc_pad);
 void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
                       StageTimer &T, int phase);
 // mixed: read the aux radial factors from the plan's FP32 table (made on first use)

@@ -1306,6 +1306,86 @@ static void launch_colloc_z(Plan &P, MixedState &M, const Chunk &c, int nzs, int
     launch_colloc_z_g<false>(P, M, c, nzs, nspin, s);
 }
 
+// The mixed-precision XC gradient's per-build set-up: the orbital digits.
+void mixed_gradient_begin(Plan &P, int nspin, int nocc, cudaStream_t s) {
+  MixedState &M = mixed_state(P, nocc);
+  const int nc = P.gga ? 4 : 1;
+  M.ensure_T((size_t)M.nbatch_chunk * nspin * nc * M.nocc_pad * 256);
+  const long rows = (long)nspin * M.nocc_pad * P.nblk;
+  quant_ct_kernel<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(P.d_Ct, nocc, M.nocc_pad, nspin, P.nbf_pad,
+                                                                       P.nblk, M.qct, M.sct, P.d_status + 1);
+  NKX_LAUNCH_CHECK();
+  ++P.launches;
+}
+
+// One chunk of the mixed-precision XC gradient: pass-A digits of the chunk's
+// pairs, the orbital values T_c(g, i) = sum_f Phi_c(g, f) C(f, i) for the
+// value and (GGA) the three gradient components on the tensor cores (the
+// density contraction with all components), rho and grad rho of the chunk's
+// points from them, and the functional there (Z coefficients, energy, energy
+// density edens).  Returns T[(bl, s, c)][i][g] (bl from the chunk's first
+// batch, i padded to *nocc_pad), resident until the next chunk.
+const double *mixed_gradient_chunk(Plan &P, const Chunk &c, int nspin, int nocc, double *edens, cudaStream_t s,
+                                   int *nocc_pad) {
+  MixedState &M = mixed_state(P, nocc);
+  const int nc = P.gga ? 4 : 1;
+  const long np = c.p1 - c.p0, nb = c.b1 - c.b0;
+  if (np > 0) {
+    if (P.gga)
+      colloc_quantT_kernel<true><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_fshell, P.d_bshell, P.d_bnshell, P.d_px,
+                                                              P.d_py, P.d_pz, P.d_pair_batch, P.d_pair_blk, c.p0,
+                                                              M.qphT, M.sphT, P.d_status + 1);
+    else
+      colloc_quantT_kernel<false><<<(unsigned)np, 256, 0, s>>>(P.d_sto, P.d_fshell, P.d_bshell, P.d_bnshell, P.d_px,
+                                                               P.d_py, P.d_pz, P.d_pair_batch, P.d_pair_blk, c.p0,
+                                                               M.qphT, M.sphT, P.d_status + 1);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+  }
+  TcArgs a{};
+  a.mode = TC_MODE_DENSITY;
+  a.b0 = c.b0;
+  a.b1 = c.b1;
+  a.p0 = c.p0;
+  a.pair_off = P.d_pair_off;
+  a.pair_blk = P.d_pair_blk;
+  a.mask = P.d_mask;
+  a.mask_words = P.mask_words;
+  a.nblk = P.nblk;
+  a.sA = M.sphT;
+  a.sB = M.sct;
+  a.nspin = nspin;
+  a.ncs = nc;
+  a.ncomp = nc;
+  a.nt = P.tune.dens_n;
+  a.ew = a.nt / 8;
+  a.ntile_i = (nocc + a.nt - 1) / a.nt;
+  a.nocc_pad = M.nocc_pad;
+  a.T = M.T;
+  a.err = P.d_status;
+  a.wait_ns = P.wait_ns;
+  a.stall = P.stall_test;
+  a.nunits = nb * nspin * 2 * a.ncomp * a.ntile_i;
+  launch_i8(M, M.m_phT, a.nt == 128 ? M.m_ct128 : M.m_ct, a, s);
+  ++P.launches;
+  if (P.gga)
+    density_contract_kernel<true><<<dim3((unsigned)nb, nspin), 256, 0, s>>>(M.T, P.d_occ, nocc, M.nocc_pad, nspin,
+                                                                            c.b0, P.d_rho, P.d_grad, P.npad);
+  else
+    density_contract_kernel<false><<<dim3((unsigned)nb, nspin), 256, 0, s>>>(M.T, P.d_occ, nocc, M.nocc_pad, nspin,
+                                                                             c.b0, P.d_rho, P.d_grad, P.npad);
+  NKX_LAUNCH_CHECK();
+  ++P.launches;
+  const long g0 = c.b0 * kBatch, n = nb * kBatch;
+  functional_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P.xc, P.gga, nspin, P.npad, n, P.d_w + g0,
+                                                                P.d_rho + g0, P.d_grad + g0, nullptr, P.d_coef + g0,
+                                                                P.d_E, edens + g0);
+  NKX_LAUNCH_CHECK();
+  ++P.launches;
+  *nocc_pad = M.nocc_pad;
+  return M.T;
+}
+
 void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
                       StageTimer &Tm, int phase) {
   MixedState &M = mixed_state(P, nocc);

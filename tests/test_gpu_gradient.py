@@ -1,4 +1,4 @@
-"""The XC nuclear gradient (nkx_xc_gradient, FP64) against central finite
+"""The XC nuclear gradient (nkx_xc_gradient, FP64 and mixed) against central finite
 differences of E_xc at fixed orbitals, with the grid rebuilt at each displaced
 geometry (points move with their owner atom, Becke weights recomputed, no
 weight-threshold compaction).  The finite-difference oracle is the CPU
@@ -171,3 +171,23 @@ def test_screened_becke_gradient_short_clamp_cluster():
             return (energy(cp) - energy(cm)) / (2 * h)
         fd = (4.0 * central(H / 2) - central(H)) / 3.0
         assert abs(G[a, k] - fd) < 1e-8, (a, k, G[a, k], fd)
+
+
+@pytest.mark.parametrize("xc", [("LDA_X", "LDA_C_VWN"), ("GGA_X_PBE", "GGA_C_PBE")])
+def test_mixed_gradient_matches_fp64(xc):
+    # the mixed-precision gradient (orbital values and density from the int8
+    # digit contraction) against the FP64 one on (H2O)4, closed and open
+    # shell: well inside the 1e-5 Eh/bohr force target, translation invariant
+    c, Z = M.water_cluster(4, seed=12)
+    c = np.asarray(c, float)
+    nbf = len(funcs_at(c, Z))
+    g = A.make_flat_grid(c, Z, NRAD, ORDER, weight_threshold=-1.0, radial="ta")
+    fb = A.FockBuilder(c, Z, A.make_manual_basis(funcs_at(c, Z)), g, func_ids=xc)
+    Ca, Cb = M.random_orbitals(nbf, 20, seed=13), M.random_orbitals(nbf, 20, seed=14)
+    for C_list, occ_list in (([Ca], [2.0 * np.ones(20)]), ([Ca, Cb], [np.ones(20), np.r_[np.ones(17), np.zeros(3)]])):
+        G64 = fb.xc_gradient(C_list, occ_list)
+        for _ in range(2):
+            Gm = fb.xc_gradient(C_list, occ_list, precision="mixed")
+            assert np.abs(Gm - G64).max() < 1e-6, np.abs(Gm - G64).max()
+            assert np.abs(Gm.sum(0)).max() < 1e-8
+    fb.close()
