@@ -456,10 +456,24 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
           ++grp;
           return;
         }
+        const bool live = g.nsteps > 0;
+        // the group's row and column scales are loaded before the wait for
+        // its accumulators, so their latency hides behind the MMAs
+        double sa_g = 0.0, sb_g[MODE == TC_MODE_V ? CW / 32 : 1];
+        if (live) {
+          if constexpr (MODE == TC_MODE_V) {
+            sa_g = a.sA[g.qa * 128 + row];
+            const double *sbp = a.sB + (g.qb * a.nz + it.zi) * 128 + N * it.hc + CW * cq;
+#pragma unroll
+            for (int k = 0; k < CW / 32; ++k) sb_g[k] = sbp[32 * k + lane];
+          } else {
+            sa_g = a.sA[(g.qa * a.ncs + it.c) * 256 + 128 * it.h + row];
+            sb_g[0] = a.sB[((size_t)it.s * a.nocc_pad + N * it.t + 32 * cq + lane) * a.nblk + g.blk];
+          }
+        }
         if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag, a.wait_ns)) return;
         tc_fence_after();
         __syncwarp();
-        const bool live = g.nsteps > 0;
         // exact combine of the four levels, S = sum_L 2^(8 (3 - L)) Acc_L:
         // |Acc_L| < 2^24 for K <= 256, so |S| < 2^49 (level_sum); the product
         // is s_a s_b 2^-36 S (one rounding per group and element)
@@ -472,12 +486,10 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
           // TMEM is released as soon as the last slice has arrived in
           // registers.
           if (live) {
-            const double sa = a.sA[g.qa * 128 + row] * kTwoM36;
+            const double sa = sa_g * kTwoM36;
             double *cs = colscale + (warp - 2) * CW;
-            const double *sbp = a.sB + (g.qb * a.nz + it.zi) * 128 + N * it.hc + CW * cq;
-            __syncwarp();
 #pragma unroll
-            for (int k = 0; k < CW / 32; ++k) cs[32 * k + lane] = sbp[32 * k + lane];
+            for (int k = 0; k < CW / 32; ++k) cs[32 * k + lane] = sb_g[k];
             __syncwarp();
             const uint32_t tb = tmem + lane_addr + buf * 4 * N + CW * cq;
             constexpr int NS = CW / 4;
@@ -525,16 +537,9 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
           any = any || live;
           return;
         }
-        double sa = 0.0;
-        const double *sb = nullptr;
-        size_t sbs = 1;
-        if (live) {
-          sa = a.sA[(g.qa * a.ncs + it.c) * 256 + 128 * it.h + row] * kTwoM36;
-          sb = a.sB + ((size_t)it.s * a.nocc_pad + N * it.t + 32 * cq) * a.nblk + g.blk;
-          sbs = a.nblk;
-        }
+        const double sa = sa_g * kTwoM36;
         // the warp's 32 column scales, one per lane, handed out by shuffles
-        const double sbl = live ? sb[lane * sbs] : 0.0;
+        const double sbl = sb_g[0];
         // slices of SL columns: 8 for the 320-thread shape, 4 for the
         // 576-thread one (96 registers a thread)
         constexpr int SL = N == 128 ? 4 : 8;
