@@ -491,7 +491,7 @@ class FockBuilder:
         return {k: getattr(t, k) for k, _ in L.Tuning._fields_
                 if k in ("v_n", "dens_n", "ypath", "v_warps", "chunk_pairs")}
 
-    def set_tuning(self, v_n=128, dens_n=64, ypath=-1, chunk_pairs=0, v_warps=16):
+    def set_tuning(self, v_n=128, dens_n=0, ypath=-1, chunk_pairs=0, v_warps=16):
         t = L.Tuning(v_n=v_n, dens_n=dens_n, ypath=ypath, v_warps=v_warps, chunk_pairs=chunk_pairs)
         check(L.lib().nkx_plan_set_tuning(self._h, C.byref(t)))
 

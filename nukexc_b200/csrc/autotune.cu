@@ -2,7 +2,8 @@
 // whole builds on the caller's orbitals and keeps, one knob at a time, the
 // fastest of
 //   the Y path of the GGA density gradient (off / on),
-//   the tcgen05 MMA width of the density contraction (N = 64 / 128),
+//   the tcgen05 MMA width of the density contraction (N = 64 / 128; by
+//   default 128 from 1024 orbitals on),
 //   the MMA width of the V contraction (N = 128 / 64) and, for N = 128, its
 //   epilogue warps (16 of 32 columns / 8 of 64),
 //   the chunk size (x1, x2, x4 of the current pair limit, memory permitting),
@@ -64,9 +65,9 @@ void cache_store(const char *path, const std::string &sig, const nkx_tuning &t) 
 }
 
 void apply(Plan &P, const nkx_tuning &t) {
-  NKX_REQUIRE((t.v_n == 64 || t.v_n == 128) && (t.dens_n == 64 || t.dens_n == 128) && t.ypath >= -1 &&
+  NKX_REQUIRE((t.v_n == 64 || t.v_n == 128) && (t.dens_n == 0 || t.dens_n == 64 || t.dens_n == 128) && t.ypath >= -1 &&
                   t.ypath <= 1 && (t.v_warps == 8 || t.v_warps == 16),
-              NKX_ERR_ARG, "tuning: v_n and dens_n must be 64 or 128, ypath -1, 0 or 1, v_warps 8 or 16");
+              NKX_ERR_ARG, "tuning: v_n must be 64 or 128, dens_n 0, 64 or 128, ypath -1, 0 or 1, v_warps 8 or 16");
   P.drop_graphs();
   P.tune.v_n = t.v_n;
   P.tune.dens_n = t.dens_n;
@@ -100,6 +101,7 @@ static void autotune(Plan &P, int nspin, int nocc, const double *C, const double
     if (out) *out = best;
     return;
   }
+  if (best.dens_n == 0) best.dens_n = density_width(P, nocc);  // the width the default picks
   const size_t nn = (size_t)P.nbf * P.nbf;
   double *V = nullptr;
   NKX_CUDA(cudaMalloc(&V, sizeof(double) * nspin * nn));

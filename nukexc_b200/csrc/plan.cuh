@@ -19,7 +19,7 @@ struct Chunk {
 // measures; the defaults are what it found best on (H2O)_64.
 struct Tuning {
   int v_n = 128;   // tcgen05 MMA width N of the V contraction (128 or 64)
-  int dens_n = 64; // MMA width of the density contraction (64 or 128)
+  int dens_n = 0;  // MMA width of the density contraction (64, 128, or 0: by orbital count, density_width)
   int ypath = -1;  // GGA density gradient through Y = T0 (C occ)^T: -1 from 256 orbitals, 0 off, 1 on
   int v_warps = 16; // epilogue warps of the N = 128 V contraction (16 of 32 columns, or 8 of 64)
 };
@@ -195,6 +195,14 @@ __global__ void functional_kernel(XcSpec s, bool gga, int nspin, long npad, long
                                   const double *__restrict__ rho, const double *__restrict__ grad,
                                   const double *__restrict__ vj, double *__restrict__ coef, double *Eacc,
                                   double *__restrict__ edens);
+// MMA width of the density contraction: the tuning's, or by default 128 from
+// 1024 (padded) orbitals on -- half as many orbital tiles re-read each
+// Phi tile (1500-atom aggregate, 2850 orbitals: 11.0 vs 12.0 s) -- else 64
+// (two TMEM buffers; ahead for short orbital ranges)
+inline int density_width(const Plan &P, int nocc) {
+  if (P.tune.dens_n) return P.tune.dens_n;
+  return ((nocc + 127) / 128) * 128 >= 1024 ? 128 : 64;
+}
 void mixed_gradient_begin(Plan &P, int nspin, int nocc, cudaStream_t s);
 const double *mixed_gradient_chunk(Plan &P, const Chunk &c, int nspin, int nocc, double *edens, cudaStream_t s,
                                    int *nocc_pad);

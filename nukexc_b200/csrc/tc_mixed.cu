@@ -264,8 +264,8 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
   __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar[NBUF], tempty_bar[NBUF], drain_bar, stall_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_flag;
-  // V: the column scales of each epilogue warp's current group
-  __shared__ __align__(16) double colscale[MODE == TC_MODE_V ? Sh::EW * CW : 2];
+  // V and density: the column scales of each epilogue warp's current group
+  __shared__ __align__(16) double colscale[MODE != TC_MODE_GRAD ? Sh::EW * CW : 2];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dsmem) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
         // exact combine of the four levels, S = sum_L 2^(8 (3 - L)) Acc_L:
         // |Acc_L| < 2^24 for K <= 256, so |S| < 2^49 (level_sum); the product
         // is s_a s_b 2^-36 S (one rounding per group and element)
-        if constexpr (MODE == TC_MODE_V) {
+        if constexpr (MODE == TC_MODE_V || MODE == TC_MODE_DENSITY) {
           // s_a is the thread's row scale; the warp's CW column scales are
           // staged in shared memory once per group and read back as
           // broadcasts, two per 16-byte load (instead of two shuffles per
@@ -537,47 +537,6 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
           any = any || live;
           return;
         }
-        const double sa = sa_g * kTwoM36;
-        // the warp's 32 column scales, one per lane, handed out by shuffles
-        const double sbl = sb_g[0];
-        // slices of SL columns: 8 for the 320-thread shape, 4 for the
-        // 576-thread one (96 registers a thread)
-        constexpr int SL = N == 128 ? 4 : 8;
-#pragma unroll
-        for (int hh = 0; hh < 32 / SL; ++hh) {
-          uint32_t v0[SL], v1[SL], v2[SL], v3[SL];
-          const uint32_t ta = tmem + lane_addr + buf * 4 * N + 32 * cq + SL * hh;
-          if constexpr (SL == 8) {
-            tmem_ld8u_async(ta, v0);
-            tmem_ld8u_async(ta + N, v1);
-            tmem_ld8u_async(ta + 2 * N, v2);
-            tmem_ld8u_async(ta + 3 * N, v3);
-            tmem_wait8(v0);
-            tmem_wait8(v1);
-            tmem_wait8(v2);
-            tmem_wait8(v3);
-          } else {
-            tmem_ld4u_async(ta, v0);
-            tmem_ld4u_async(ta + N, v1);
-            tmem_ld4u_async(ta + 2 * N, v2);
-            tmem_ld4u_async(ta + 3 * N, v3);
-            tmem_wait4(v0);
-            tmem_wait4(v1);
-            tmem_wait4(v2);
-            tmem_wait4(v3);
-          }
-          if (live) {
-#pragma unroll
-            for (int j = 0; j < SL; ++j) {
-              const double S = level_sum(v0[j], v1[j], v2[j], v3[j]);
-              acc[SL * hh + j] = fma(S, sa * __shfl_sync(0xffffffffu, sbl, SL * hh + j), acc[SL * hh + j]);
-            }
-          }
-        }
-        tc_fence_before();
-        mbar_arrive(&tempty_bar[buf]);
-        ++grp;
-        any = any || live;
       });
       if constexpr (MODE == TC_MODE_V) {
         if (any) {
@@ -1362,7 +1321,7 @@ const double *mixed_gradient_chunk(Plan &P, const Chunk &c, int nspin, int nocc,
   a.nspin = nspin;
   a.ncs = nc;
   a.ncomp = nc;
-  a.nt = P.tune.dens_n;
+  a.nt = density_width(P, nocc);
   a.ew = a.nt / 8;
   a.ntile_i = (nocc + a.nt - 1) / a.nt;
   a.nocc_pad = M.nocc_pad;
@@ -1459,7 +1418,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.nspin = nspin;
     a.ncs = nc;
     a.ncomp = grad_mode ? 1 : nc;
-    a.nt = P.tune.dens_n;
+    a.nt = density_width(P, nocc);
     a.ew = a.nt / 8;
     a.ntile_i = (nocc + a.nt - 1) / a.nt;
     a.nocc_pad = M.nocc_pad;
