@@ -104,16 +104,18 @@ __global__ void __launch_bounds__(256) orbital_values_kernel(const double *__res
 // Basis-centre and point-motion terms of one (batch, block) pair.  Thread
 // (ty, tx) owns functions 4 ty .. 4 ty + 3 of the block and, per 16-point
 // subtile, points 2 tx, 2 tx + 1.  X and grad X come from a small FP64 GEMM
-// of C (block rows) with occ * T staged in shared memory.  Contributions are
-// summed per owner atom (points) and per function atom in shared memory and
-// leave the block as a few global atomics.
-template <bool GRAD>
+// of C (block rows) with occ * T staged in shared memory, or (XIN) are read
+// from X[pair][spin][comp][g][mu] made by the tensor cores.  Contributions
+// are summed per owner atom (points) and per function atom in shared memory
+// and leave the block as a few global atomics.
+template <bool GRAD, bool XIN = false>
 __global__ void __launch_bounds__(256) grad_pair_kernel(
     const StoFunc *__restrict__ sto, const int *__restrict__ fatom, const double *__restrict__ px,
     const double *__restrict__ py, const double *__restrict__ pz, const int *__restrict__ owner,
     const int *__restrict__ pair_batch, const int *__restrict__ pair_blk, long pstart, long sb0,
     const double *__restrict__ Ct, const double *__restrict__ occ, int nocc, int nocc_pad, int nbf_pad, int nspin,
-    const double *__restrict__ T, const double *__restrict__ coef, long npad, double *__restrict__ F) {
+    const double *__restrict__ T, const double *__restrict__ coef, long npad, double *__restrict__ F,
+    const double *__restrict__ Xin = nullptr) {
   constexpr int NC = GRAD ? 4 : 1;
   __shared__ double Cs[16][kBlockF];
   __shared__ double Ts[16][NC][16];
@@ -171,7 +173,22 @@ __global__ void __launch_bounds__(256) grad_pair_kernel(
         for (int q = 0; q < 2; ++q)
 #pragma unroll
           for (int c = 0; c < NC; ++c) acc[a][q][c] = 0.0;
-      for (int i0 = 0; i0 < nocc; i0 += 16) {
+      if (XIN) {
+        const double *Xs = Xin + ((size_t)blockIdx.x * nspin + s) * NC * kBatch * kBlockF;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            const double2 *xp =
+                reinterpret_cast<const double2 *>(Xs + ((size_t)c * kBatch + st * 16 + 2 * tx + q) * kBlockF + 4 * ty);
+            const double2 u = xp[0], v = xp[1];
+            acc[0][q][c] = u.x;
+            acc[1][q][c] = u.y;
+            acc[2][q][c] = v.x;
+            acc[3][q][c] = v.y;
+          }
+      }
+      for (int i0 = 0; !XIN && i0 < nocc; i0 += 16) {
         for (int e = tid; e < 16 * kBlockF; e += 256) {
           const int k = e >> 7, m = e & 127, i = i0 + k;
           Cs[k][m] = i < nocc ? C[(size_t)i * nbf_pad + I * kBlockF + m] : 0.0;
@@ -507,23 +524,24 @@ static void xc_gradient(Plan &P, int precision, int nspin, int nocc, const doubl
   if (mixed) {
     // Mixed precision: per chunk, the orbital values T_c come from the int8
     // digit contraction on the tensor cores, which also gives rho, grad rho
-    // and the functional of the chunk's points; the rest of the gradient
-    // (X = C (occ T) and its gradient, the STO Hessians, the Becke term) is
-    // the FP64 code below.
+    // and the functional of the chunk's points, and so do X = C (occ T) and
+    // its gradient; the pair terms with the STO Hessians and the Becke term
+    // are FP64.
     mixed_gradient_begin(P, nspin, nocc, s);
     for (const Chunk &c : P.chunks) {
       int npadT = 0;
-      const double *T = mixed_gradient_chunk(P, c, nspin, nocc, G.edens, s, &npadT);
+      const double *X = nullptr;
+      const double *T = mixed_gradient_chunk(P, c, nspin, nocc, G.edens, s, &npadT, &X);
       const long q0 = c.p0, q1 = c.p1;
       if (q1 <= q0) continue;
       if (P.gga)
-        grad_pair_kernel<true><<<(unsigned)(q1 - q0), 256, 0, s>>>(
+        grad_pair_kernel<true, true><<<(unsigned)(q1 - q0), 256, 0, s>>>(
             P.d_sto, P.d_fatom, P.d_px, P.d_py, P.d_pz, P.d_owner, P.d_pair_batch, P.d_pair_blk, q0, c.b0, P.d_Ct,
-            P.d_occ, nocc, npadT, P.nbf_pad, nspin, T, P.d_coef, P.npad, G.F);
+            P.d_occ, nocc, npadT, P.nbf_pad, nspin, T, P.d_coef, P.npad, G.F, X);
       else
-        grad_pair_kernel<false><<<(unsigned)(q1 - q0), 256, 0, s>>>(
+        grad_pair_kernel<false, true><<<(unsigned)(q1 - q0), 256, 0, s>>>(
             P.d_sto, P.d_fatom, P.d_px, P.d_py, P.d_pz, P.d_owner, P.d_pair_batch, P.d_pair_blk, q0, c.b0, P.d_Ct,
-            P.d_occ, nocc, npadT, P.nbf_pad, nspin, T, P.d_coef, P.npad, G.F);
+            P.d_occ, nocc, npadT, P.nbf_pad, nspin, T, P.d_coef, P.npad, G.F, X);
       NKX_LAUNCH_CHECK();
       ++P.launches;
     }

@@ -205,7 +205,7 @@ inline int density_width(const Plan &P, int nocc) {
 }
 void mixed_gradient_begin(Plan &P, int nspin, int nocc, cudaStream_t s);
 const double *mixed_gradient_chunk(Plan &P, const Chunk &c, int nspin, int nocc, double *edens, cudaStream_t s,
-                                   int *nocc_pad);
+                                   int *nocc_pad, const double **X);
 void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool separateJ, cudaStream_t s,
                       StageTimer &T, int phase);
 // mixed: read the aux radial factors from the plan's FP32 table (made on first use)

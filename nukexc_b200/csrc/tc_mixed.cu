@@ -50,7 +50,9 @@ constexpr double kTwoM36 = 0x1p-36;
 
 // TC_MODE_GRAD: Y(g, mu) = sum_i T0(g, i) (C occ)(mu, i) over the orbitals
 // (grad rho = 2 sum_mu grad phi_mu Y_mu, summed in the Y pass's epilogue)
-enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1, TC_MODE_GRAD = 2 };
+// TC_MODE_X (mixed XC gradient): X_c(g, mu) = sum_i T_c(g, i) (C occ)(mu, i)
+// for the value and the three gradient components, written in FP64
+enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1, TC_MODE_GRAD = 2, TC_MODE_X = 3 };
 
 // Shape by the MMA width N.  N = 128: one TMEM buffer of 4 levels x 128
 // columns, 16 epilogue warps, 3 stages of 64 KB.  N = 64: two buffers of
@@ -104,6 +106,9 @@ struct TcArgs {
   const uint8_t *qphT;
   const double *sphT;
   double *Gp;
+  // X mode (same operands as grad mode, ncomp components of T): output
+  // X[pair][spin][comp][g][mu] in FP64
+  double *X;
   long nunits;
   // err[0]: code of the first wait that gave up (0: none); waits that can
   // be abandoned give up after wait_ns, the drain waits after kDrainLimitNs
@@ -148,11 +153,13 @@ struct UnitIter {
       const int t = a.vtiles[u / nh];
       I = t >> 16;
       J = t & 0xffff;
-    } else if (a.mode == TC_MODE_GRAD) {
+    } else if (a.mode == TC_MODE_GRAD || a.mode == TC_MODE_X) {
       t = (int)(u % 2);  // 64-function half of the block
       h = (int)((u / 2) % 2);
-      s = (int)((u / 4) % a.nspin);
-      q = u / (4 * a.nspin);
+      const int nc = a.mode == TC_MODE_X ? a.ncomp : 1;
+      c = (int)((u / 4) % nc);
+      s = (int)((u / (4 * nc)) % a.nspin);
+      q = u / (4 * nc * a.nspin);
       bl = a.pair_batch[a.p0 + q] - a.b0;
     } else {
       long r = u;
@@ -207,15 +214,17 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
         zB = zb;
       });
     }
-  } else if (a.mode == TC_MODE_GRAD) {
-    // one run over all orbitals: A = T0 digits of (batch, spin, half),
-    // B = (C occ) digits of the pair's block
+  } else if (a.mode == TC_MODE_GRAD || a.mode == TC_MODE_X) {
+    // one run over all orbitals: A = T_c digits of (batch, spin, comp, half)
+    // (the Y pass: c = 0 only), B = (C occ) digits of the pair's block
     Group g;
     g.nsteps = a.nocc_pad / 64;
     g.qa = it.q;
     g.qb = 0;
     g.blk = a.pair_blk[a.p0 + it.q];
-    const int za = (int)(((it.bl * a.nspin + it.s) * 2 + it.h) * 4), yb = 128 * g.blk + 64 * it.t, zb = it.s * 4;
+    const int nc = a.mode == TC_MODE_X ? a.ncomp : 1;
+    const int za = (int)((((it.bl * a.nspin + it.s) * nc + it.c) * 2 + it.h) * 4), yb = 128 * g.blk + 64 * it.t,
+              zb = it.s * 4;
     fn(g, [=](int k, int &xa, int &ya, int &zA, int &xb, int &yB, int &zB) {
       xa = 64 * k;
       ya = 0;
@@ -259,13 +268,13 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
     tc_i8_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs a) {
   using Sh = TcShape<NW, EW>;
   constexpr int N = Sh::N, NBUF = Sh::NBUF, kStages = Sh::kStages, kStageBytes = Sh::kStageBytes, CW = Sh::CW;
-  static_assert(MODE == TC_MODE_V || CW == 32, "the density and Y epilogues take 32 columns a warp");
+  static_assert(MODE == TC_MODE_V || CW == 32, "the density, Y and X epilogues take 32 columns a warp");
   extern __shared__ __align__(1024) uint8_t dsmem[];
   __shared__ uint64_t full_bar[kStages], empty_bar[kStages], tfull_bar[NBUF], tempty_bar[NBUF], drain_bar, stall_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_flag;
   // V and density: the column scales of each epilogue warp's current group
-  __shared__ __align__(16) double colscale[MODE != TC_MODE_GRAD ? Sh::EW * CW : 2];
+  __shared__ __align__(16) double colscale[MODE == TC_MODE_V || MODE == TC_MODE_DENSITY ? Sh::EW * CW : 2];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dsmem) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -386,6 +395,44 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
       for_each_group(a, it, [&](const Group &g, auto) {
         if (abort_flag) return;
         const uint32_t buf = grp % NBUF, use = grp / NBUF;
+        if constexpr (MODE == TC_MODE_X) {
+          // X_c(g, mu) of the thread's point and 32 functions, written in
+          // FP64 slice by slice (8 consecutive doubles a slice)
+          const int gpt = 128 * it.h + row;
+          const double sa =
+              a.sA[((((it.bl * a.nspin + it.s) * a.ncomp + it.c) * 2 + it.h)) * 128 + row] * kTwoM36;
+          const double sbl = a.sB[(size_t)it.s * a.nbf_pad + 128 * g.blk + 64 * it.t + 32 * cq + lane];
+          if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag, a.wait_ns)) return;
+          tc_fence_after();
+          __syncwarp();
+          double *Xp = a.X + ((((size_t)it.q * a.nspin + it.s) * a.ncomp + it.c) * kBatch + gpt) * kBlockF +
+                       64 * it.t + 32 * cq;
+#pragma unroll
+          for (int h = 0; h < 4; ++h) {
+            uint32_t v0[8], v1[8], v2[8], v3[8];
+            const uint32_t ta = tmem + lane_addr + buf * 4 * N + 32 * cq + 8 * h;
+            tmem_ld8u_async(ta, v0);
+            tmem_ld8u_async(ta + N, v1);
+            tmem_ld8u_async(ta + 2 * N, v2);
+            tmem_ld8u_async(ta + 3 * N, v3);
+            tmem_wait8(v0);
+            tmem_wait8(v1);
+            tmem_wait8(v2);
+            tmem_wait8(v3);
+            if (h == 3) {
+              tc_fence_before();
+              mbar_arrive(&tempty_bar[buf]);
+            }
+            double x[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              x[j] = level_sum(v0[j], v1[j], v2[j], v3[j]) * (sa * __shfl_sync(0xffffffffu, sbl, 8 * h + j));
+#pragma unroll
+            for (int j = 0; j < 8; j += 2) reinterpret_cast<double2 *>(Xp + 8 * h + j)[0] = make_double2(x[j], x[j + 1]);
+          }
+          ++grp;
+          return;
+        }
         if constexpr (MODE == TC_MODE_GRAD) {
           // Y(g, mu) of the thread's point and 32 functions stays in
           // registers: the thread adds grad phi_c(g, mu) Y(g, mu) over them
@@ -551,8 +598,8 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
             for (int j = 0; j < CW; ++j) Vz[r + (c0 + j) * a.nbf_pad] += acc[j];
           }
         }
-      } else if constexpr (MODE == TC_MODE_GRAD) {
-        // the partial sums are written per group above
+      } else if constexpr (MODE == TC_MODE_GRAD || MODE == TC_MODE_X) {
+        // the partial sums (grad) or X (x) are written per group above
       } else {
         const long plane = (it.bl * a.nspin + it.s) * a.ncomp + it.c;
         double *Tp = a.T + plane * (long)a.nocc_pad * 256 + 128 * it.h + row;
@@ -1117,6 +1164,20 @@ struct MixedState {
     for (void *p : bufs) cudaFree(p);
     cudaFree(T);
     cudaFree(qt0);
+    cudaFree(X);
+  }
+  double *X = nullptr;  // the mixed gradient's X[pair][spin][comp][g][mu]
+  size_t X_cap = 0;
+  void ensure_X(size_t doubles) {
+    if (doubles <= X_cap) return;
+    cudaFree(X);
+    X = nullptr;
+    X_cap = 0;
+    if (cudaMalloc(&X, doubles * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error{NKX_ERR_ALLOC, "gradient X allocation of " + std::to_string(doubles * 8) + " bytes failed"};
+    }
+    X_cap = doubles;
   }
   // T: the chunk's FP64 density tiles, nbatch x nspin x ncomp planes of
   // nocc_pad x 256 (one component on the Y path); qt0: their T0 digits
@@ -1197,6 +1258,8 @@ static MixedState &mixed_state(Plan &P, int nocc) {
                                   TcShape<128>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_GRAD, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   TcShape<64>::kSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_X, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TcShape<64>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(zquant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 68));
   }
   MixedState &M = *static_cast<MixedState *>(P.mx_state);
@@ -1209,7 +1272,7 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     M.T_cap = M.qt0_cap = 0;  // regrown for the new orbital padding
     M.m_ct = make_map3(M.qct, P.nbf_pad, nocc_pad, 8, 64);
     M.m_ct128 = make_map3(M.qct, P.nbf_pad, nocc_pad, 8, 128);
-    M.st0 = M.alloc<double>((size_t)M.nbatch_chunk * 2 * 2 * 128);
+    M.st0 = M.alloc<double>((size_t)M.nbatch_chunk * 2 * 4 * 2 * 128);  // up to 2 spins x 4 comps x 2 halves
     M.qco = M.alloc<uint8_t>((size_t)2 * 4 * P.nbf_pad * nocc_pad);
     M.sco = M.alloc<double>((size_t)2 * P.nbf_pad);
     M.m_co = make_map3(M.qco, nocc_pad, P.nbf_pad, 2 * 4, 64);
@@ -1228,7 +1291,8 @@ static void launch_i8(MixedState &M, const CUtensorMap &mA, const CUtensorMap &m
   if (a.nunits <= 0) return;
   const unsigned grid = (unsigned)std::min<long>(a.nunits, M.nsm);
   NKX_REQUIRE(a.nt == 64 || a.nt == 128, NKX_ERR_ARG, "tensor-core width must be 64 or 128");
-  NKX_REQUIRE(a.mode != TC_MODE_GRAD || a.nt == 64, NKX_ERR_ARG, "the Y pass runs N = 64");
+  NKX_REQUIRE((a.mode != TC_MODE_GRAD && a.mode != TC_MODE_X) || a.nt == 64, NKX_ERR_ARG,
+              "the Y and X passes run N = 64");
   NKX_REQUIRE(a.ew == a.nt / 8 || (a.mode == TC_MODE_V && a.nt == 128 && a.ew == 8), NKX_ERR_ARG,
               "epilogue warps: N / 8, or 8 for the N = 128 V contraction");
   if (a.mode == TC_MODE_V) {
@@ -1241,6 +1305,8 @@ static void launch_i8(MixedState &M, const CUtensorMap &mA, const CUtensorMap &m
   }
   else if (a.mode == TC_MODE_GRAD)
     launch_i8_shape<TC_MODE_GRAD, 64>(mA, mB, a, grid, s);
+  else if (a.mode == TC_MODE_X)
+    launch_i8_shape<TC_MODE_X, 64>(mA, mB, a, grid, s);
   else
     a.nt == 128 ? launch_i8_shape<TC_MODE_DENSITY, 128>(mA, mB, a, grid, s)
                 : launch_i8_shape<TC_MODE_DENSITY, 64>(mA, mB, a, grid, s);
@@ -1275,11 +1341,17 @@ void mixed_gradient_begin(Plan &P, int nspin, int nocc, cudaStream_t s) {
   MixedState &M = mixed_state(P, nocc);
   const int nc = P.gga ? 4 : 1;
   M.ensure_T((size_t)M.nbatch_chunk * nspin * nc * M.nocc_pad * 256);
+  M.ensure_qt0((size_t)M.nbatch_chunk * nspin * nc * 2 * 4 * 128 * M.nocc_pad,
+               (long)M.nbatch_chunk * nspin * nc * 2 * 4, M.nocc_pad);
+  M.ensure_X((size_t)M.cap * nspin * nc * kBatch * kBlockF);
   const long rows = (long)nspin * M.nocc_pad * P.nblk;
   quant_ct_kernel<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(P.d_Ct, nocc, M.nocc_pad, nspin, P.nbf_pad,
                                                                        P.nblk, M.qct, M.sct, P.d_status + 1);
   NKX_LAUNCH_CHECK();
-  ++P.launches;
+  quant_cocc_kernel<<<dim3((unsigned)P.nblk, nspin), 128, 0, s>>>(P.d_Ct, P.d_occ, nocc, M.nocc_pad, P.nbf_pad,
+                                                                  M.qco, M.sco);
+  NKX_LAUNCH_CHECK();
+  P.launches += 2;
 }
 
 // One chunk of the mixed-precision XC gradient: pass-A digits of the chunk's
@@ -1290,7 +1362,7 @@ void mixed_gradient_begin(Plan &P, int nspin, int nocc, cudaStream_t s) {
 // density edens).  Returns T[(bl, s, c)][i][g] (bl from the chunk's first
 // batch, i padded to *nocc_pad), resident until the next chunk.
 const double *mixed_gradient_chunk(Plan &P, const Chunk &c, int nspin, int nocc, double *edens, cudaStream_t s,
-                                   int *nocc_pad) {
+                                   int *nocc_pad, const double **X) {
   MixedState &M = mixed_state(P, nocc);
   const int nc = P.gga ? 4 : 1;
   const long np = c.p1 - c.p0, nb = c.b1 - c.b0;
@@ -1346,7 +1418,40 @@ const double *mixed_gradient_chunk(Plan &P, const Chunk &c, int nspin, int nocc,
                                                                 P.d_E, edens + g0);
   NKX_LAUNCH_CHECK();
   ++P.launches;
+  // X_c(g, mu) = sum_i T_c(g, i) occ_i C(mu, i) of every pair on the tensor
+  // cores: T_c as digit rows over the orbitals, then the Y-pass contraction
+  // with all components, written in FP64
+  if (np > 0) {
+    quant_t0_kernel<<<(unsigned)(nb * nspin * nc * 2), 128, 0, s>>>(M.T, nocc, M.nocc_pad, M.qt0, M.st0);
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+    TcArgs x{};
+    x.mode = TC_MODE_X;
+    x.b0 = c.b0;
+    x.b1 = c.b1;
+    x.p0 = c.p0;
+    x.pair_blk = P.d_pair_blk;
+    x.pair_batch = P.d_pair_batch;
+    x.nblk = P.nblk;
+    x.nbf_pad = P.nbf_pad;
+    x.sA = M.st0;
+    x.sB = M.sco;
+    x.nspin = nspin;
+    x.ncs = nc;
+    x.ncomp = nc;
+    x.nocc_pad = M.nocc_pad;
+    x.X = M.X;
+    x.err = P.d_status;
+    x.wait_ns = P.wait_ns;
+    x.stall = P.stall_test;
+    x.nunits = np * nspin * nc * 4;
+    x.nt = 64;
+    x.ew = 8;
+    launch_i8(M, M.m_t0, M.m_co, x, s);
+    ++P.launches;
+  }
   *nocc_pad = M.nocc_pad;
+  *X = M.X;
   return M.T;
 }
 
