@@ -310,6 +310,84 @@ __device__ __forceinline__ void becke_s_ds(double mu, double &s, double &ds) {
 // close, the loops run over all atoms.
 constexpr int kGradList = 192;
 
+// The Becke-weight term of one point over its candidate list (n <= kGradList
+// atoms): the distances to the listed atoms once, every cell function once,
+// then the pair terms.  Of the three atoms a pair term (i, j) moves, the
+// owner's and i's shares are summed in registers and added once per point
+// and per i; only j's share goes to shared memory per pair.
+__device__ void becke_grad_listed(const double *__restrict__ C, const double r[3], int o, const int *list, int n,
+                                  double rmin, double clamp, double wg, double eg, double *Fa) {
+  double rd[kGradList], Pl[kGradList];
+  for (int k = 0; k < n; ++k) {
+    const int a = list[k];
+    const double dx = r[0] - C[3 * a], dy = r[1] - C[3 * a + 1], dz = r[2] - C[3 * a + 2];
+    rd[k] = sqrt(dx * dx + dy * dy + dz * dz);
+  }
+  double Z = 0.0, Po = 0.0;
+  for (int k = 0; k < n; ++k) {
+    const int i = list[k];
+    double P = 0.0;
+    if (rd[k] < rmin + clamp) {  // else P_i = 0 exactly (Laqua clamp)
+      P = 1.0;
+      for (int c = 0; c < n && P != 0.0; ++c) {
+        if (c == k) continue;
+        const int j = list[c];
+        const double dx = C[3 * i] - C[3 * j], dy = C[3 * i + 1] - C[3 * j + 1], dz = C[3 * i + 2] - C[3 * j + 2];
+        const double Rij = fmin(sqrt(dx * dx + dy * dy + dz * dz), clamp);
+        double mu = (rd[k] - rd[c]) / Rij;
+        mu = mu > 1.0 ? 1.0 : (mu < -1.0 ? -1.0 : mu);
+        double sv, dsv;
+        becke_s_ds(mu, sv, dsv);
+        P *= sv;
+      }
+    }
+    Pl[k] = P;
+    Z += P;
+    if (i == o) Po = P;
+  }
+  if (!(Po > 0.0 && Z > 0.0)) return;
+  const double Q = Po / Z, fa = eg * (wg / Q);
+  double Fo[3] = {0.0, 0.0, 0.0};
+  for (int ci = 0; ci < n; ++ci) {
+    const int i = list[ci];
+    const double kappa = Q * ((i == o ? 1.0 : 0.0) - Pl[ci] / Z);
+    if (kappa == 0.0 || !(rd[ci] > 0.0)) continue;
+    const double ri = rd[ci];
+    const double ui[3] = {(r[0] - C[3 * i]) / ri, (r[1] - C[3 * i + 1]) / ri, (r[2] - C[3 * i + 2]) / ri};
+    double Fi[3] = {0.0, 0.0, 0.0};
+    for (int cj = 0; cj < n; ++cj) {
+      if (cj == ci) continue;
+      const int j = list[cj];
+      const double rj = rd[cj];
+      if (!(rj > 0.0)) continue;
+      const double e[3] = {C[3 * i] - C[3 * j], C[3 * i + 1] - C[3 * j + 1], C[3 * i + 2] - C[3 * j + 2]};
+      const double dij = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+      const bool clamped = dij >= clamp;
+      const double Rij = clamped ? clamp : dij;
+      const double mu = (ri - rj) / Rij;
+      if (!(mu > -1.0 && mu < 1.0)) continue;  // clamped: s' = 0
+      double sv, ds;
+      becke_s_ds(mu, sv, ds);
+      if (!(sv > 0.0)) continue;
+      const double lam = fa * kappa * ds / sv / Rij;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const double uj = (r[k] - C[3 * j + k]) / rj;
+        const double ek = clamped ? 0.0 : mu * e[k] / dij;
+        Fo[k] += lam * (ui[k] - uj);
+        Fi[k] -= lam * (ui[k] + ek);
+        atomicAdd(&Fa[3 * j + k], lam * (uj + ek));
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if (Fi[k] != 0.0) atomicAdd(&Fa[3 * i + k], Fi[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    if (Fo[k] != 0.0) atomicAdd(&Fa[3 * o + k], Fo[k]);
+}
+
 __global__ void becke_grad_kernel(const double *__restrict__ C, int natoms, const double *__restrict__ px,
                                   const double *__restrict__ py, const double *__restrict__ pz,
                                   const double *__restrict__ w, const int *__restrict__ owner,
@@ -344,71 +422,76 @@ __global__ void becke_grad_kernel(const double *__restrict__ C, int natoms, cons
           list[nl++] = a;
         }
     }
-    const int n = full ? natoms : nl;
-    auto atom = [&](int k) { return full ? k : list[k]; };
-    // P_i over the candidate set (factors of the other atoms are exactly 1)
-    auto cellP = [&](int i) {
-      const double ri = dist(i);
-      if (!full && ri >= rmin + clamp) return 0.0;
-      double P = 1.0;
-      for (int c = 0; c < n && P != 0.0; ++c) {
-        const int j = atom(c);
-        if (j == i) continue;
-        const double dx = C[3 * i] - C[3 * j], dy = C[3 * i + 1] - C[3 * j + 1], dz = C[3 * i + 2] - C[3 * j + 2];
-        double Rij = sqrt(dx * dx + dy * dy + dz * dz);
-        if (clamp > 0.0) Rij = fmin(Rij, clamp);
-        double mu = (ri - dist(j)) / Rij;
-        mu = mu > 1.0 ? 1.0 : (mu < -1.0 ? -1.0 : mu);
-        double sv, dsv;
-        becke_s_ds(mu, sv, dsv);
-        P *= sv;
-      }
-      return P;
-    };
-    double Z = 0.0, Po = 0.0;
-    for (int c = 0; c < n; ++c) {
-      const int i = atom(c);
-      const double P = cellP(i);
-      Z += P;
-      if (i == o) Po = P;
-    }
-    if (Po > 0.0 && Z > 0.0) {
-      const double Q = Po / Z, a = w[g] / Q, fa = edens[g] * a;
-      for (int ci = 0; ci < n; ++ci) {
-        const int i = atom(ci);
-        const double Pi = (i == o) ? Po : cellP(i);
-        const double kappa = Q * ((i == o ? 1.0 : 0.0) - Pi / Z);
-        if (kappa == 0.0) continue;
-        double ui[3] = {r[0] - C[3 * i], r[1] - C[3 * i + 1], r[2] - C[3 * i + 2]};
-        const double ri = sqrt(ui[0] * ui[0] + ui[1] * ui[1] + ui[2] * ui[2]);
-        if (!(ri > 0.0)) continue;
-        for (int k = 0; k < 3; ++k) ui[k] /= ri;
-        for (int cj = 0; cj < n; ++cj) {
-          const int j = atom(cj);
+    if (!full) {
+      becke_grad_listed(C, r, o, list, nl, rmin, clamp, w[g], edens[g], Fa);
+    } else {
+      // without the clamp, or with more than kGradList candidates: every atom
+      const int n = natoms;
+      auto atom = [&](int k) { return k; };
+      // P_i over the candidate set (factors of the other atoms are exactly 1)
+      auto cellP = [&](int i) {
+        const double ri = dist(i);
+        if (!full && ri >= rmin + clamp) return 0.0;
+        double P = 1.0;
+        for (int c = 0; c < n && P != 0.0; ++c) {
+          const int j = atom(c);
           if (j == i) continue;
-          double e[3] = {C[3 * i] - C[3 * j], C[3 * i + 1] - C[3 * j + 1], C[3 * i + 2] - C[3 * j + 2]};
-          const double dij = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
-          const bool clamped = clamp > 0.0 && dij >= clamp;
-          const double Rij = clamped ? clamp : dij;
-          double uj[3] = {r[0] - C[3 * j], r[1] - C[3 * j + 1], r[2] - C[3 * j + 2]};
-          const double rj = sqrt(uj[0] * uj[0] + uj[1] * uj[1] + uj[2] * uj[2]);
-          if (!(rj > 0.0)) continue;
-          const double mu = (ri - rj) / Rij;
-          if (!(mu > -1.0 && mu < 1.0)) continue;  // clamped: s' = 0
-          double sv, ds;
-          becke_s_ds(mu, sv, ds);
-          if (!(sv > 0.0)) continue;
-          const double lam = fa * kappa * ds / sv / Rij;
-          for (int k = 0; k < 3; ++k) {
-            uj[k] /= rj;
-            const double ek = clamped ? 0.0 : mu * e[k] / dij;
-            atomicAdd(&Fa[3 * o + k], lam * (ui[k] - uj[k]));
-            atomicAdd(&Fa[3 * i + k], -lam * (ui[k] + ek));
-            atomicAdd(&Fa[3 * j + k], lam * (uj[k] + ek));
+          const double dx = C[3 * i] - C[3 * j], dy = C[3 * i + 1] - C[3 * j + 1], dz = C[3 * i + 2] - C[3 * j + 2];
+          double Rij = sqrt(dx * dx + dy * dy + dz * dz);
+          if (clamp > 0.0) Rij = fmin(Rij, clamp);
+          double mu = (ri - dist(j)) / Rij;
+          mu = mu > 1.0 ? 1.0 : (mu < -1.0 ? -1.0 : mu);
+          double sv, dsv;
+          becke_s_ds(mu, sv, dsv);
+          P *= sv;
+        }
+        return P;
+      };
+      double Z = 0.0, Po = 0.0;
+      for (int c = 0; c < n; ++c) {
+        const int i = atom(c);
+        const double P = cellP(i);
+        Z += P;
+        if (i == o) Po = P;
+      }
+      if (Po > 0.0 && Z > 0.0) {
+        const double Q = Po / Z, a = w[g] / Q, fa = edens[g] * a;
+        for (int ci = 0; ci < n; ++ci) {
+          const int i = atom(ci);
+          const double Pi = (i == o) ? Po : cellP(i);
+          const double kappa = Q * ((i == o ? 1.0 : 0.0) - Pi / Z);
+          if (kappa == 0.0) continue;
+          double ui[3] = {r[0] - C[3 * i], r[1] - C[3 * i + 1], r[2] - C[3 * i + 2]};
+          const double ri = sqrt(ui[0] * ui[0] + ui[1] * ui[1] + ui[2] * ui[2]);
+          if (!(ri > 0.0)) continue;
+          for (int k = 0; k < 3; ++k) ui[k] /= ri;
+          for (int cj = 0; cj < n; ++cj) {
+            const int j = atom(cj);
+            if (j == i) continue;
+            double e[3] = {C[3 * i] - C[3 * j], C[3 * i + 1] - C[3 * j + 1], C[3 * i + 2] - C[3 * j + 2]};
+            const double dij = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+            const bool clamped = clamp > 0.0 && dij >= clamp;
+            const double Rij = clamped ? clamp : dij;
+            double uj[3] = {r[0] - C[3 * j], r[1] - C[3 * j + 1], r[2] - C[3 * j + 2]};
+            const double rj = sqrt(uj[0] * uj[0] + uj[1] * uj[1] + uj[2] * uj[2]);
+            if (!(rj > 0.0)) continue;
+            const double mu = (ri - rj) / Rij;
+            if (!(mu > -1.0 && mu < 1.0)) continue;  // clamped: s' = 0
+            double sv, ds;
+            becke_s_ds(mu, sv, ds);
+            if (!(sv > 0.0)) continue;
+            const double lam = fa * kappa * ds / sv / Rij;
+            for (int k = 0; k < 3; ++k) {
+              uj[k] /= rj;
+              const double ek = clamped ? 0.0 : mu * e[k] / dij;
+              atomicAdd(&Fa[3 * o + k], lam * (ui[k] - uj[k]));
+              atomicAdd(&Fa[3 * i + k], -lam * (ui[k] + ek));
+              atomicAdd(&Fa[3 * j + k], lam * (uj[k] + ek));
+            }
           }
         }
       }
-    }
+    }  // every atom
   }
   if (smem) {
     __syncthreads();
