@@ -245,14 +245,21 @@ def int8_gemm_peak(torch):
         return None
 
 
-def measured_traffic(workload):
+def measured_traffic(workload, pairs_per_launch=None):
     """DRAM bytes per launch of the dominant kernel from the committed ncu capture
-    of this workload (profiles/roofline_traffic.json), or None."""
+    of this workload (profiles/roofline_traffic.json), scaled by the pairs a
+    launch covers in this run when the chunking differs from the capture's
+    (the traffic of a V launch grows in proportion to its chunk), or None."""
     p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if not os.path.exists(p):
         return None
     d = json.load(open(p))
-    return d["dram_bytes_per_launch"] if d.get("workload") == workload else None
+    if d.get("workload") != workload:
+        return None
+    t = d["dram_bytes_per_launch"]
+    if pairs_per_launch and d.get("pairs_per_launch"):
+        t *= pairs_per_launch / d["pairs_per_launch"]
+    return t
 
 
 def measured_peaks():
@@ -711,8 +718,10 @@ def run_nkx(args):
             "stage_ms_per_step": {k: v / args.steps for k, v in stage.items() if k.endswith("_ms")},
             "roofline": {"bound": "tensor", "kernel": "vgemm (V = Phi Z^T)", "achieved": ach, "peak": peak,
                          "unit": unit, "frac": ach / peak,
-                         "traffic": measured_traffic(config(args)["workload"]) if prec == "mixed" else None,
-                         "traffic_unit": "DRAM bytes per V launch (ncu, profiles/roofline_traffic.json)",
+                         "traffic": (measured_traffic(config(args)["workload"], info["npairs"] / max(1, info["nchunks"]))
+                                     if prec == "mixed" else None),
+                         "traffic_unit": "DRAM bytes per V launch (ncu, profiles/roofline_traffic.json, scaled to "
+                                         "this run's pairs per chunk)",
                          "peak_source": peak_note,
                          "algorithmic_flops_per_step": flops,
                          "fp64_equivalent_tflops": flops / (vg_ms * 1e-3) / 1e12},
