@@ -45,7 +45,10 @@ def test_replayed_builds_equal_ordinary_builds(precision, jmode):
         assert abs(E - Eo) <= 1e-12 * abs(Eo)
         assert float((V[0] - Vo[0]).abs().max()) <= 1e-12 * float(Vo[0].abs().max())
         if jmode == "separate":
-            assert float((J - Jo).abs().max()) <= 1e-12 * float(Jo.abs().max())
+            # the fit vector y is summed with atomic FP64 adds in varying order
+            # and the solve with the grid metric (condition number about 1e5 for
+            # this aux set) magnifies that rounding in J
+            assert float((J - Jo).abs().max()) <= 1e-10 * float(Jo.abs().max())
     assert fb.info()["graph_replays"] >= 2
     ref.close()
     fb.close()
