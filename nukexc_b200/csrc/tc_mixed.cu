@@ -1012,12 +1012,13 @@ __global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__
 
 // Pass B, part 2: digits of the V operands, transposed to
 // qph[pair][digit][f][g] and qz[pair][z][digit][f][g] through a shared
-// tile in slabs of 64 points (rows padded to 68 bytes: conflict-free).
+// tile in slabs of 32 points (rows padded to 36 bytes: conflict-free; 37 KB
+// for one Z plane, so four blocks share an SM).
 __global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ ws, const double *__restrict__ sph,
                                                      const double *__restrict__ szs, int nz, uint8_t *__restrict__ qph,
                                                      uint8_t *__restrict__ qz, const uint8_t *__restrict__ qphT,
                                                      const double *__restrict__ sphT, int ncs) {
-  extern __shared__ __align__(16) uint8_t tile[];  // [(1 + nz)][4][128][68]
+  extern __shared__ __align__(16) uint8_t tile[];  // [(1 + nz)][4][128][36]
   const long q = blockIdx.x;
   const size_t T = (size_t)kBatch * kBlockF;
   const int f = threadIdx.x & 127, gs = threadIdx.x >> 7;
@@ -1030,11 +1031,11 @@ __global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ 
     inv[o] = 1.0 / s;  // exact: s is a power of two
   }
   const double *src = ws + q * 4 * T;
-  for (int g0 = 0; g0 < kBatch; g0 += 64) {
+  for (int g0 = 0; g0 < kBatch; g0 += 32) {
     // thread (f, gs) quantises points 4 gq .. 4 gq + 3 of the slab, gq = gs + 2 kq:
     // all loads of a step are issued before use, and the four digit bytes of
     // four consecutive points go to shared memory as one word
-    for (int kq = 0; kq < 8; ++kq) {
+    for (int kq = 0; kq < 4; ++kq) {
       const int gq = gs + 2 * kq;
       double v[4][4];
 #pragma unroll
@@ -1062,17 +1063,17 @@ __global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ 
         if (o >= nop) break;
         uint32_t w[4];
         quant4(v[o], inv[o], w);
-        uint32_t *t = reinterpret_cast<uint32_t *>(tile + ((size_t)o * 4 * 128 + f) * 68) + gq;
+        uint32_t *t = reinterpret_cast<uint32_t *>(tile + ((size_t)o * 4 * 128 + f) * 36) + gq;
 #pragma unroll
-        for (int dd = 0; dd < 4; ++dd) t[dd * 128 * 17] = w[dd];
+        for (int dd = 0; dd < 4; ++dd) t[dd * 128 * 9] = w[dd];
       }
     }
     __syncthreads();
     const int nrow = nop * 4 * 128;
-    for (int e = threadIdx.x; e < nrow * 16; e += 256) {
-      const int rw = e >> 4, part = e & 15;
+    for (int e = threadIdx.x; e < nrow * 8; e += 256) {
+      const int rw = e >> 3, part = e & 7;
       const int o = rw / 512, d = (rw / 128) & 3, ff = rw & 127;
-      const uint32_t val = *reinterpret_cast<const uint32_t *>(tile + (size_t)rw * 68 + 4 * part);
+      const uint32_t val = *reinterpret_cast<const uint32_t *>(tile + (size_t)rw * 36 + 4 * part);
       uint8_t *dst = (o == 0) ? qph + ((q * 4 + d) * 128 + ff) * 256
                               : qz + (((q * nz + (o - 1)) * 4 + d) * 128 + ff) * 256;
       *reinterpret_cast<uint32_t *>(dst + g0 + 4 * part) = val;
@@ -1260,7 +1261,7 @@ static MixedState &mixed_state(Plan &P, int nocc) {
                                   TcShape<64>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_X, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   TcShape<64>::kSmem));
-    NKX_CUDA(cudaFuncSetAttribute(zquant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 68));
+    NKX_CUDA(cudaFuncSetAttribute(zquant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 36));
   }
   MixedState &M = *static_cast<MixedState *>(P.mx_state);
   // orbitals pad to 128 so that either density tile width divides them
@@ -1584,7 +1585,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
   auto pass_b = [&](const Chunk &c, bool phi_digits) {
     const long np = c.p1 - c.p0;
     Tm.begin(ST_ZBUILD, s);
-    zquant_kernel<<<(unsigned)np, 256, (size_t)(1 + nzs) * 4 * 128 * 68, s>>>(
+    zquant_kernel<<<(unsigned)np, 256, (size_t)(1 + nzs) * 4 * 128 * 36, s>>>(
         P.ws_phi, M.sph, M.sz, nzs, M.qph, M.qz, phi_digits ? M.qphT : nullptr, M.sphT, nc);
     NKX_LAUNCH_CHECK();
     ++P.launches;
