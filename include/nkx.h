@@ -310,7 +310,7 @@ NKX_API nkx_status nkx_plan_set_metric(nkx_plan *plan, const double *S, int mem)
 /* Choices of the mixed-precision build that nkx_plan_autotune measures. */
 typedef struct {
   int v_n;            /* tcgen05 MMA width N of the V contraction: 128 or 64 */
-  int dens_n;         /* MMA width of the density contraction: 64, 128, or 0 (128 from 1024 orbitals on) */
+  int dens_n;         /* MMA width of the density contractions (T0 and the GGA Y pass): 64, 128, or 0 (128 from 1024 orbitals on) */
   int ypath;          /* GGA density gradient through Y = T0 (C occ)^T: -1 auto (from 256 orbitals), 0, 1 */
   int v_warps;        /* epilogue warps of the N = 128 V contraction: 16 (32 columns each) or 8 (64 each) */
   long chunk_pairs;   /* (batch, block) pairs per streamed chunk */

@@ -24,14 +24,13 @@
 // (64-byte swizzle); warp 1 lane 0 issues the MMAs (M = 128, N, K = 32) and
 // owns TMEM (all 512 columns: NBUF buffers x 4 levels x N); warps 2.. are
 // the epilogue (warp w reads TMEM lanes 32 (w % 4) .. + 31, columns
-// 32 ((w - 2) / 4) .. + 31 of each level, in slices of 8) with FP64
-// accumulators in registers.  The V contraction uses N = 128 (576 threads,
-// one TMEM buffer): M = 128 x N = 64 int8 MMAs are limited by shared-memory
-// operand bandwidth to about two thirds of the tensor rate.  The density
-// contraction keeps N = 64 (320 threads, two TMEM buffers): its groups are
-// two K steps long, so overlapping the epilogue matters more there, and its
-// orbital dimension pads to 64; the Y pass uses the same shape over
-// 64-function halves of a block.  All waits are bounded (tc_ptx.cuh).
+// 32 ((w - 2) / 4) .. + 31 of each level, in slices) with FP64 accumulators
+// in registers.  The V contraction uses N = 128 (576 threads, one TMEM
+// buffer): M = 128 x N = 64 int8 MMAs are limited by shared-memory operand
+// bandwidth to about two thirds of the tensor rate.  The density
+// contractions (T0 and the Y pass) run N = 64 (320 threads, two TMEM
+// buffers; their groups are short, so overlapping the epilogue matters) or,
+// from 1024 orbitals on, N = 128.  All waits are bounded (tc_ptx.cuh).
 #include <cuda.h>
 
 #include <algorithm>
@@ -59,9 +58,10 @@ enum { TC_MODE_V = 0, TC_MODE_DENSITY = 1, TC_MODE_GRAD = 2, TC_MODE_X = 3 };
 // 4 levels x 64 columns, so the epilogue of one group overlaps the MMAs of
 // the next, 8 epilogue warps, 4 stages of 48 KB.  Any contraction can run
 // either shape (the V unit then covers a 128 x N part of its output tile,
-// the density unit an N-orbital tile); the Y pass runs N = 64.  The plan's
-// tuning (nkx_plan_autotune) picks the shape per contraction; the defaults
-// are N = 128 for V and N = 64 for the density.
+// the density unit an N-orbital tile, the Y-pass unit N functions).  The
+// plan's tuning (nkx_plan_autotune) picks the shape per contraction; the
+// defaults are N = 128 for V and, for T0 and the Y pass, N = 64 below 1024
+// orbitals and N = 128 from there on.
 //
 // EW epilogue warps (default N / 8): warp w reads TMEM lanes 32 (w % 4) ..,
 // and CW = 4 N / EW columns of each level.  The V contraction can also run
@@ -154,12 +154,13 @@ struct UnitIter {
       I = t >> 16;
       J = t & 0xffff;
     } else if (a.mode == TC_MODE_GRAD || a.mode == TC_MODE_X) {
-      t = (int)(u % 2);  // 64-function half of the block
-      h = (int)((u / 2) % 2);
+      const int nt = 128 / a.nt;  // column parts of the block (N = 64: two halves)
+      t = (int)(u % nt);
+      h = (int)((u / nt) % 2);
       const int nc = a.mode == TC_MODE_X ? a.ncomp : 1;
-      c = (int)((u / 4) % nc);
-      s = (int)((u / (4 * nc)) % a.nspin);
-      q = u / (4 * nc * a.nspin);
+      c = (int)((u / (2 * nt)) % nc);
+      s = (int)((u / (2 * nt * nc)) % a.nspin);
+      q = u / (2 * nt * nc * a.nspin);
       bl = a.pair_batch[a.p0 + q] - a.b0;
     } else {
       long r = u;
@@ -223,7 +224,7 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
     g.qb = 0;
     g.blk = a.pair_blk[a.p0 + it.q];
     const int nc = a.mode == TC_MODE_X ? a.ncomp : 1;
-    const int za = (int)((((it.bl * a.nspin + it.s) * nc + it.c) * 2 + it.h) * 4), yb = 128 * g.blk + 64 * it.t,
+    const int za = (int)((((it.bl * a.nspin + it.s) * nc + it.c) * 2 + it.h) * 4), yb = 128 * g.blk + a.nt * it.t,
               zb = it.s * 4;
     fn(g, [=](int k, int &xa, int &ya, int &zA, int &xb, int &yB, int &zB) {
       xa = 64 * k;
@@ -437,51 +438,41 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
           // Y(g, mu) of the thread's point and 32 functions stays in
           // registers: the thread adds grad phi_c(g, mu) Y(g, mu) over them
           // (c = x, y, z), grad phi from the pass-A digits, and writes three
-          // partial sums that ygrad_sum_kernel adds up per point.  Each digit
-          // plane of a component is one 32-byte load per thread (the 32
-          // functions' bytes of its point); the loads of component c + 1 are
-          // in flight while component c is combined, those of the first
-          // before the wait for the accumulators.
+          // partial sums that ygrad_sum_kernel adds up per point.  The 32
+          // columns go in NH parts (two of 16 in the 96-register N = 128
+          // shape); each digit plane of a component and part is one load per
+          // thread (the part's function bytes of its point), and the loads of
+          // the next (part, component) are in flight while the current one is
+          // combined, those of the first before the wait for the accumulators.
+          constexpr int NH = N == 128 ? 2 : 1, CWH = 32 / NH, WPP = CWH / 4;
           const int gpt = 128 * it.h + row;
+          const int f0 = N * it.t + 32 * cq;  // the warp's first function in the block
           constexpr size_t kPlane = (size_t)kBatch * kBlockF;  // one digit plane of a pair, bytes
-          const uint8_t *dg = a.qphT + ((size_t)it.q * a.ncs + 1) * 4 * kPlane + (size_t)gpt * kBlockF + 64 * it.t + 32 * cq;
-          uint32_t w0[4][8], w1[4][8];
-          auto load_comp = [&](int c, uint32_t(&w)[4][8]) {
+          const uint8_t *dg = a.qphT + ((size_t)it.q * a.ncs + 1) * 4 * kPlane + (size_t)gpt * kBlockF + f0;
+          uint32_t w0[4][WPP], w1[4][WPP];
+          auto load = [&](int idx, uint32_t(&w)[4][WPP]) {  // idx = 3 part + component
+            const int hf = idx / 3, c = idx % 3;
 #pragma unroll
-            for (int d = 0; d < 4; ++d) ldg256(dg + (4 * c + d) * kPlane, w[d]);
+            for (int d = 0; d < 4; ++d) {
+              const uint8_t *p = dg + (4 * c + d) * kPlane + CWH * hf;
+              if constexpr (WPP == 8)
+                ldg256(p, w[d]);
+              else
+                ldg128(p, w[d]);
+            }
           };
-          load_comp(0, w0);
+          load(0, w0);
           const double sa = a.sA[((it.bl * a.nspin + it.s) * 2 + it.h) * 128 + row] * kTwoM36;
-          const double sbl = a.sB[(size_t)it.s * a.nbf_pad + 128 * g.blk + 64 * it.t + 32 * cq + lane];
+          const double sbl = a.sB[(size_t)it.s * a.nbf_pad + 128 * g.blk + f0 + lane];
           if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag, a.wait_ns)) return;
           tc_fence_after();
           __syncwarp();
-          double y[32];
-#pragma unroll
-          for (int h = 0; h < 4; ++h) {
-            uint32_t v0[8], v1[8], v2[8], v3[8];
-            const uint32_t ta = tmem + lane_addr + buf * 4 * N + 32 * cq + 8 * h;
-            tmem_ld8u_async(ta, v0);
-            tmem_ld8u_async(ta + N, v1);
-            tmem_ld8u_async(ta + 2 * N, v2);
-            tmem_ld8u_async(ta + 3 * N, v3);
-            tmem_wait8(v0);
-            tmem_wait8(v1);
-            tmem_wait8(v2);
-            tmem_wait8(v3);
-            if (h == 3) {
-              tc_fence_before();
-              mbar_arrive(&tempty_bar[buf]);
-            }
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-              y[8 * h + j] = level_sum(v0[j], v1[j], v2[j], v3[j]) * (sa * __shfl_sync(0xffffffffu, sbl, 8 * h + j));
-          }
-          // word k of plane d holds digit d of functions 4k .. 4k + 3
-          auto combine = [&](const uint32_t(&w)[4][8]) {
+          double gs[3] = {0.0, 0.0, 0.0};
+          // word k of plane d holds digit d of functions 4k .. 4k + 3 of the part
+          auto combine = [&](const uint32_t(&w)[4][WPP], const double(&y)[CWH]) {
             double gsum = 0.0;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
+            for (int k = 0; k < WPP; ++k) {
               const uint32_t wd[4] = {w[3][k], w[2][k], w[1][k], w[0][k]};
               uint32_t bw[4];
               transpose4(wd, bw);
@@ -490,13 +481,55 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
             }
             return gsum;
           };
-          load_comp(1, w1);
-          const double g0 = combine(w0);
-          load_comp(2, w0);
-          const double g1 = combine(w1);
-          const double g2 = combine(w0);
-          const double gs[3] = {g0, g1, g2};
-          double *out = a.Gp + ((((size_t)it.q * a.nspin + it.s) * 2 + it.t) * 2 + cq) * 3 * kBatch + gpt;
+#pragma unroll
+          for (int hf = 0; hf < NH; ++hf) {
+            double y[CWH];
+            // slices of SLW columns (4 in the 96-register shape)
+            constexpr int SLW = NH == 2 ? 4 : 8;
+#pragma unroll
+            for (int h = 0; h < CWH / SLW; ++h) {
+              uint32_t v0[SLW], v1[SLW], v2[SLW], v3[SLW];
+              const uint32_t ta = tmem + lane_addr + buf * 4 * N + 32 * cq + CWH * hf + SLW * h;
+              if constexpr (SLW == 8) {
+                tmem_ld8u_async(ta, v0);
+                tmem_ld8u_async(ta + N, v1);
+                tmem_ld8u_async(ta + 2 * N, v2);
+                tmem_ld8u_async(ta + 3 * N, v3);
+                tmem_wait8(v0);
+                tmem_wait8(v1);
+                tmem_wait8(v2);
+                tmem_wait8(v3);
+              } else {
+                tmem_ld4u_async(ta, v0);
+                tmem_ld4u_async(ta + N, v1);
+                tmem_ld4u_async(ta + 2 * N, v2);
+                tmem_ld4u_async(ta + 3 * N, v3);
+                tmem_wait4x4(v0, v1, v2, v3);
+              }
+              if (hf == NH - 1 && h == CWH / SLW - 1) {
+                tc_fence_before();
+                mbar_arrive(&tempty_bar[buf]);
+              }
+#pragma unroll
+              for (int j = 0; j < SLW; ++j)
+                y[SLW * h + j] = level_sum(v0[j], v1[j], v2[j], v3[j]) *
+                                 (sa * __shfl_sync(0xffffffffu, sbl, CWH * hf + SLW * h + j));
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const int idx = 3 * hf + c;
+              if ((idx & 1) == 0) {
+                if (idx + 1 < 3 * NH) load(idx + 1, w1);
+                gs[c] += combine(w0, y);
+              } else {
+                if (idx + 1 < 3 * NH) load(idx + 1, w0);
+                gs[c] += combine(w1, y);
+              }
+            }
+          }
+          // partial sum p = (column part, warp column group) of 4 per (pair, spin)
+          const int p = it.t * (N / 32) + cq;
+          double *out = a.Gp + (((size_t)it.q * a.nspin + it.s) * 4 + p) * 3 * kBatch + gpt;
 #pragma unroll
           for (int c = 0; c < 3; ++c)
             out[c * kBatch] = gs[c] * (a.sphT[((size_t)it.q * a.ncs + 1 + c) * kBatch + gpt] * 0x1p-29);
@@ -1158,7 +1191,7 @@ struct MixedState {
   double *st0 = nullptr, *sco = nullptr;
   // B operand maps by box width: Z with 128- and 64-row boxes (V at N = 128 / 64),
   // Ct with 64- and 128-row boxes (density at N = 64 / 128)
-  CUtensorMap m_phT, m_ph, m_z, m_z64, m_ct, m_ct128, m_t0, m_co;
+  CUtensorMap m_phT, m_ph, m_z, m_z64, m_ct, m_ct128, m_t0, m_co, m_co128;
   std::vector<void *> bufs;
   size_t T_cap = 0, qt0_cap = 0;  // doubles of T, bytes of qt0 (grown on demand)
   ~MixedState() {
@@ -1261,6 +1294,8 @@ static MixedState &mixed_state(Plan &P, int nocc) {
                                   TcShape<64>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_X, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   TcShape<64>::kSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_GRAD, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TcShape<128>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(zquant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 36));
   }
   MixedState &M = *static_cast<MixedState *>(P.mx_state);
@@ -1277,6 +1312,7 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     M.qco = M.alloc<uint8_t>((size_t)2 * 4 * P.nbf_pad * nocc_pad);
     M.sco = M.alloc<double>((size_t)2 * P.nbf_pad);
     M.m_co = make_map3(M.qco, nocc_pad, P.nbf_pad, 2 * 4, 64);
+    M.m_co128 = make_map3(M.qco, nocc_pad, P.nbf_pad, 2 * 4, 128);
   }
   return M;
 }
@@ -1292,8 +1328,7 @@ static void launch_i8(MixedState &M, const CUtensorMap &mA, const CUtensorMap &m
   if (a.nunits <= 0) return;
   const unsigned grid = (unsigned)std::min<long>(a.nunits, M.nsm);
   NKX_REQUIRE(a.nt == 64 || a.nt == 128, NKX_ERR_ARG, "tensor-core width must be 64 or 128");
-  NKX_REQUIRE((a.mode != TC_MODE_GRAD && a.mode != TC_MODE_X) || a.nt == 64, NKX_ERR_ARG,
-              "the Y and X passes run N = 64");
+  NKX_REQUIRE(a.mode != TC_MODE_X || a.nt == 64, NKX_ERR_ARG, "the X pass runs N = 64");
   NKX_REQUIRE(a.ew == a.nt / 8 || (a.mode == TC_MODE_V && a.nt == 128 && a.ew == 8), NKX_ERR_ARG,
               "epilogue warps: N / 8, or 8 for the N = 128 V contraction");
   if (a.mode == TC_MODE_V) {
@@ -1305,7 +1340,8 @@ static void launch_i8(MixedState &M, const CUtensorMap &mA, const CUtensorMap &m
       launch_i8_shape<TC_MODE_V, 128>(mA, mB, a, grid, s);
   }
   else if (a.mode == TC_MODE_GRAD)
-    launch_i8_shape<TC_MODE_GRAD, 64>(mA, mB, a, grid, s);
+    a.nt == 128 ? launch_i8_shape<TC_MODE_GRAD, 128>(mA, mB, a, grid, s)
+                : launch_i8_shape<TC_MODE_GRAD, 64>(mA, mB, a, grid, s);
   else if (a.mode == TC_MODE_X)
     launch_i8_shape<TC_MODE_X, 64>(mA, mB, a, grid, s);
   else
@@ -1567,10 +1603,14 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       g.err = P.d_status;
       g.wait_ns = P.wait_ns;
       g.stall = P.stall_test;
-      g.nunits = np * nspin * 4;
-      g.nt = 64;
-      g.ew = 8;
-      launch_i8(M, M.m_t0, M.m_co, g, s);
+      // the density contractions' MMA width: N = 128 covers a whole block
+      // per unit (shared-memory operand traffic per MMA halved), N = 64 a
+      // half with two TMEM buffers (read-back overlapped; better for short
+      // orbital runs)
+      g.nt = density_width(P, nocc);
+      g.ew = g.nt / 8;
+      g.nunits = np * nspin * 2 * (128 / g.nt);
+      launch_i8(M, M.m_t0, g.nt == 128 ? M.m_co128 : M.m_co, g, s);
       ++P.launches;
       ygrad_sum_kernel<<<dim3((unsigned)nb, nspin), 256, 0, s>>>(P.ws_phi, P.d_pair_off, c.b0, c.p0, nspin, P.npad,
                                                                 P.d_grad);

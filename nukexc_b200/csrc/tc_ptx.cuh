@@ -162,6 +162,11 @@ __device__ __forceinline__ void tmem_wait4x4(uint32_t (&a)[4], uint32_t (&b)[4],
                : "memory");
 }
 
+// 16 bytes from global memory in one read-only load (16-byte aligned address)
+__device__ __forceinline__ void ldg128(const void *p, uint32_t (&r)[4]) {
+  asm volatile("ld.global.nc.v4.b32 {%0, %1, %2, %3}, [%4];" : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "l"(p));
+}
+
 // 32 bytes from global memory in one read-only load (32-byte aligned address)
 __device__ __forceinline__ void ldg256(const void *p, uint32_t (&r)[8]) {
   asm volatile("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
