@@ -392,8 +392,8 @@ def xc_gradient_check(n, stream, ngeom=10, ncomp=1, h=1e-4):
             "max_abs_error_vs_fd": worst, "gate": "<= 1e-5 Eh/bohr",
             "fd": "Richardson-extrapolated central differences, h = 1e-4 and 5e-5 bohr, FP64 GPU E_xc",
             "mixed": {"ms_per_gradient": float(np.median(times_m)), "max_abs_diff_vs_fp64_gradient": worst_m,
-                      "note": "orbital values and density from the int8-digit tensor-core contraction, "
-                              "pair terms, STO Hessians and Becke term in FP64"}}
+                      "note": "orbital values, density and X = C (occ T) from the int8-digit tensor-core "
+                              "contractions; pair terms, STO Hessians (e^x to 1e-14) and Becke term in FP64"}}
 
 
 def aggregate_gate(natoms, stream, int8_peak=None):

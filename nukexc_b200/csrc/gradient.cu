@@ -227,6 +227,7 @@ __global__ void __launch_bounds__(256) grad_pair_kernel(
           ck[2] = cs[3 * npad + gg];
         }
         double tq[3] = {0.0, 0.0, 0.0};
+        HessRadialCache rc;  // the thread's four functions at this point
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
           const StoFunc &fn = sfn[4 * ty + a];
@@ -234,7 +235,8 @@ __global__ void __launch_bounds__(256) grad_pair_kernel(
           double t[3];
           if (GRAD) {
             double v, gr[3], h[6];
-            sto_value_grad_hess(fn, x, y, z, v, gr, h);
+            // the mixed gradient (XIN) takes e^x from exp_neg
+            sto_value_grad_hess_cached<XIN>(fn, x, y, z, rc, v, gr, h);
             const double H[3][3] = {{h[0], h[1], h[2]}, {h[1], h[3], h[4]}, {h[2], h[4], h[5]}};
             const double dX[3] = {acc[a][q][NC > 1 ? 1 : 0], acc[a][q][NC > 2 ? 2 : 0], acc[a][q][NC > 3 ? 3 : 0]};
 #pragma unroll

@@ -199,6 +199,60 @@ __device__ __forceinline__ double exp_neg(double x) {
   return p * __hiloint2double(((int)n + 1023) << 20, 0);
 }
 
+// Radial factor cache of sto_value_grad_hess for consecutive functions of
+// one thread at one point: functions of a shell share r, 1/r, r^k e^(-zeta r)
+// and k/r - zeta (the function's norm scales them).
+struct HessRadialCache {
+  double cx = 1e300, cy = 0, cz = 0, zeta = -1;
+  int k = -1;
+  double r = 0, ir = 0, Rn = 0, a = 0;
+};
+
+// sto_value_grad_hess with the radial factor shared over a shell's functions
+// (rc) and, with FAST, e^x by exp_neg (about 1e-14 relative; the
+// mixed-precision gradient); the same formulas, so the results differ from
+// sto_value_grad_hess by rounding only.
+template <bool FAST>
+__device__ __forceinline__ void sto_value_grad_hess_cached(const StoFunc &f, double px, double py, double pz,
+                                                           HessRadialCache &rc, double &v, double g[3],
+                                                           double h[6]) {
+  const double d[3] = {px - f.cx, py - f.cy, pz - f.cz};
+  if (!(f.cx == rc.cx && f.cy == rc.cy && f.cz == rc.cz && f.zeta == rc.zeta && f.k == rc.k)) {
+    rc.cx = f.cx;
+    rc.cy = f.cy;
+    rc.cz = f.cz;
+    rc.zeta = f.zeta;
+    rc.k = f.k;
+    rc.r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    rc.ir = rc.r > 0.0 ? 1.0 / rc.r : 0.0;
+    rc.Rn = ipow(rc.r, f.k) * (FAST ? exp_neg(-f.zeta * rc.r) : exp(-f.zeta * rc.r));
+    rc.a = f.k * rc.ir - f.zeta;
+  }
+  const double R = f.norm * rc.Rn;
+  double s, sg[3], sh[6];
+  solid_harmonic_grad(f.l, f.m, d[0], d[1], d[2], s, sg[0], sg[1], sg[2]);
+  solid_harmonic_hess(f.l, f.m, d[0], d[1], d[2], sh[0], sh[1], sh[2], sh[3], sh[4], sh[5]);
+  double cR = 0.0, dd = 0.0;
+  if (rc.r > 0.0) {
+    cR = rc.a * R * rc.ir;
+    dd = ((rc.a * rc.a - f.k * rc.ir * rc.ir) * R - cR) * (rc.ir * rc.ir);
+  }
+  v = R * s;
+  double dR[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    dR[j] = cR * d[j];
+    g[j] = dR[j] * s + R * sg[j];
+  }
+  const int ij[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+#pragma unroll
+  for (int e = 0; e < 6; ++e) {
+    const int j = ij[e][0], k = ij[e][1];
+    const double d2R = (j == k ? cR : 0.0) + dd * d[j] * d[k];
+    h[e] = d2R * s + dR[j] * sg[k] + dR[k] * sg[j] + R * sh[e];
+  }
+}
+
 // radial factors of every shell of the block at one point, shared by the
 // warp: R[s] = r^k e^(-zeta r) and, with GRAD, C[s] = (k/r - zeta)/r (0 at r = 0),
 // from 1/r = rsqrt(r^2) (1 ulp) and exp_neg
