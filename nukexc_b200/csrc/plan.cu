@@ -1443,11 +1443,11 @@ __global__ void core_vne_kernel(const double *__restrict__ px, const double *__r
 }
 
 // Z planes of the core Hamiltonian for the pairs of one chunk, Z^T[pair][3][g][f]
-// from PhiT[pair][4][g][f]: round 0: plane 0 = 1/2 w phi (S), plane 1 =
-// -1/2 w v_n phi (V_n); round 1: plane k = 1/4 w d_k phi (T, k = x, y, z), so
+// from PhiT[pair][4][g][f]: pass 0: plane 0 = 1/2 w phi (S), plane 1 =
+// -1/2 w v_n phi (V_n); pass 1: plane k = 1/4 w d_k phi (T, k = x, y, z), so
 // that Vbar + Vbar^T of each contraction is the matrix itself.
 __global__ void core_z_kernel(const double *__restrict__ phiT, const double *__restrict__ w,
-                              const double *__restrict__ wv, const int *__restrict__ pair_batch, long p0, int round,
+                              const double *__restrict__ wv, const int *__restrict__ pair_batch, long p0, int pass,
                               double *__restrict__ zT) {
   const size_t tile = (size_t)kBatch * kBlockF;
   const long q = blockIdx.x;
@@ -1456,7 +1456,7 @@ __global__ void core_z_kernel(const double *__restrict__ phiT, const double *__r
   double *Z = zT + (size_t)q * 3 * tile;
   for (int e = threadIdx.x; e < (int)tile; e += blockDim.x) {
     const long g = b * kBatch + e / kBlockF;
-    if (round == 0) {
+    if (pass == 0) {
       Z[e] = 0.5 * w[g] * P[e];
       Z[tile + e] = -0.5 * wv[g] * P[e];
     } else {
