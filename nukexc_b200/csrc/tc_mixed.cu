@@ -35,6 +35,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "plan.cuh"
@@ -141,9 +142,11 @@ struct UnitIter {
   long q = 0;                      // grad: chunk-relative pair
   int h = 0, c = 0, s = 0, t = 0;  // density: point half, comp, spin, 128-orbital tile
   // nh: column parts of a 128-function block in a V unit (128 / N, a
-  // compile-time constant at the kernel's call sites)
-  __device__ UnitIter(const TcArgs &a, long u, int nh) {
-    if (a.mode == TC_MODE_V) {
+  // compile-time constant at the kernel's call sites); MODE = a.mode, so
+  // each kernel carries only its own mode's decoding
+  template <int MODE>
+  __device__ UnitIter(std::integral_constant<int, MODE>, const TcArgs &a, long u, int nh) {
+    if constexpr (MODE == TC_MODE_V) {
       const long n2 = a.ntiles * nh, n3 = n2 * a.nz;
       sp = (int)(u / n3);
       u %= n3;
@@ -153,11 +156,11 @@ struct UnitIter {
       const int t = a.vtiles[u / nh];
       I = t >> 16;
       J = t & 0xffff;
-    } else if (a.mode == TC_MODE_GRAD || a.mode == TC_MODE_X) {
+    } else if constexpr (MODE == TC_MODE_GRAD || MODE == TC_MODE_X) {
       const int nt = 128 / a.nt;  // column parts of the block (N = 64: two halves)
       t = (int)(u % nt);
       h = (int)((u / nt) % 2);
-      const int nc = a.mode == TC_MODE_X ? a.ncomp : 1;
+      const int nc = MODE == TC_MODE_X ? a.ncomp : 1;
       c = (int)((u / (2 * nt)) % nc);
       s = (int)((u / (2 * nt * nc)) % a.nspin);
       q = u / (2 * nt * nc * a.nspin);
@@ -192,9 +195,9 @@ __device__ __forceinline__ bool blk_has(const uint32_t *m, int I) { return (m[I 
 // Calls fn(group, coords) for each accumulation group of a unit; the three
 // roles run the same iteration so their barrier phases stay in step.
 // coords(k, xa, ya, za, xb, yb, zb) gives the 3-D TMA box origins of step k.
-template <class Fn>
+template <int MODE, class Fn>
 __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &it, Fn &&fn) {
-  if (a.mode == TC_MODE_V) {
+  if constexpr (MODE == TC_MODE_V) {
     const int Jb = it.J;
     for (long b = a.b0 + it.sp; b < a.b1; b += a.nsplit) {
       const uint32_t *m = a.mask + b * a.mask_words;
@@ -215,7 +218,7 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
         zB = zb;
       });
     }
-  } else if (a.mode == TC_MODE_GRAD || a.mode == TC_MODE_X) {
+  } else if constexpr (MODE == TC_MODE_GRAD || MODE == TC_MODE_X) {
     // one run over all orbitals: A = T_c digits of (batch, spin, comp, half)
     // (the Y pass: c = 0 only), B = (C occ) digits of the pair's block
     Group g;
@@ -223,7 +226,7 @@ __device__ __forceinline__ void for_each_group(const TcArgs &a, const UnitIter &
     g.qa = it.q;
     g.qb = 0;
     g.blk = a.pair_blk[a.p0 + it.q];
-    const int nc = a.mode == TC_MODE_X ? a.ncomp : 1;
+    const int nc = MODE == TC_MODE_X ? a.ncomp : 1;
     const int za = (int)((((it.bl * a.nspin + it.s) * nc + it.c) * 2 + it.h) * 4), yb = 128 * g.blk + a.nt * it.t,
               zb = it.s * 4;
     fn(g, [=](int k, int &xa, int &ya, int &zA, int &xb, int &yB, int &zB) {
@@ -309,8 +312,8 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
     if (lane == 0) {
       uint32_t step = 0;
       for (long u = blockIdx.x; u < a.nunits && !abort_flag; u += gridDim.x) {
-        UnitIter it(a, u, kBlockF / N);
-        for_each_group(a, it, [&](const Group &g, auto coords) {
+        const UnitIter it(std::integral_constant<int, MODE>{}, a, u, kBlockF / N);
+        for_each_group<MODE>(a, it, [&](const Group &g, auto coords) {
           for (int k = 0; k < g.nsteps && !abort_flag; ++k, ++step) {
             const int st = step % kStages;
             if (!mbar_wait(&empty_bar[st], ((step / kStages) & 1) ^ 1, a.err, 1, &abort_flag, a.wait_ns)) return;
@@ -333,8 +336,8 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
       uint32_t step = 0, grp = 0;
       if (a.stall) mbar_wait(&stall_bar, 0, a.err, 7, &abort_flag, a.wait_ns);
       for (long u = blockIdx.x; u < a.nunits && !abort_flag; u += gridDim.x) {
-        UnitIter it(a, u, kBlockF / N);
-        for_each_group(a, it, [&](const Group &g, auto) {
+        const UnitIter it(std::integral_constant<int, MODE>{}, a, u, kBlockF / N);
+        for_each_group<MODE>(a, it, [&](const Group &g, auto) {
           if (abort_flag) return;
           // TMEM buffer grp % NBUF: wait until the epilogue has read the group
           // that used it last
@@ -388,12 +391,12 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
     const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
     uint32_t grp = 0;
     for (long u = blockIdx.x; u < a.nunits && !abort_flag; u += gridDim.x) {
-      UnitIter it(a, u, kBlockF / N);
+      const UnitIter it(std::integral_constant<int, MODE>{}, a, u, kBlockF / N);
       double acc[CW];
 #pragma unroll
       for (int j = 0; j < CW; ++j) acc[j] = 0.0;
       bool any = false;
-      for_each_group(a, it, [&](const Group &g, auto) {
+      for_each_group<MODE>(a, it, [&](const Group &g, auto) {
         if (abort_flag) return;
         const uint32_t buf = grp % NBUF, use = grp / NBUF;
         if constexpr (MODE == TC_MODE_X) {
