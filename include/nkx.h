@@ -312,7 +312,10 @@ typedef struct {
   int v_n;            /* tcgen05 MMA width N of the V contraction: 128 or 64 */
   int dens_n;         /* MMA width of the density contractions (T0 and the GGA Y pass): 64, 128, or 0 (128 from 1024 orbitals on) */
   int ypath;          /* GGA density gradient through Y = T0 (C occ)^T: -1 auto (from 256 orbitals), 0, 1 */
-  int v_warps;        /* epilogue warps of the N = 128 V contraction: 16 (32 columns each) or 8 (64 each) */
+  int v_warps;        /* epilogue warps a CTA of the V contraction: 16 or 8 (N = 128 on one CTA: 32 or 64 columns
+                         each; CTA pairs: 16 or 32) */
+  int v_pair;         /* 1: V on clusters of two CTAs (tcgen05 cta_group::2, M = 256 x N = 64, double-buffered
+                         accumulators; v_n unused), 0: one CTA per output tile */
   long chunk_pairs;   /* (batch, block) pairs per streamed chunk */
   int from_cache;     /* out: 1 when the choices came from the cache file */
   int trials;         /* out: builds timed */

@@ -67,7 +67,7 @@ class BuildTiming(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("v_n", C.c_int), ("dens_n", C.c_int), ("ypath", C.c_int), ("v_warps", C.c_int),
-                ("chunk_pairs", C.c_long),
+                ("v_pair", C.c_int), ("chunk_pairs", C.c_long),
                 ("from_cache", C.c_int), ("trials", C.c_int), ("default_ms", C.c_float), ("best_ms", C.c_float)]
 
 

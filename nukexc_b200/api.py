@@ -489,10 +489,10 @@ class FockBuilder:
         t = L.Tuning()
         check(L.lib().nkx_plan_get_tuning(self._h, C.byref(t)))
         return {k: getattr(t, k) for k, _ in L.Tuning._fields_
-                if k in ("v_n", "dens_n", "ypath", "v_warps", "chunk_pairs")}
+                if k in ("v_n", "dens_n", "ypath", "v_warps", "v_pair", "chunk_pairs")}
 
-    def set_tuning(self, v_n=128, dens_n=0, ypath=-1, chunk_pairs=0, v_warps=16):
-        t = L.Tuning(v_n=v_n, dens_n=dens_n, ypath=ypath, v_warps=v_warps, chunk_pairs=chunk_pairs)
+    def set_tuning(self, v_n=128, dens_n=0, ypath=-1, chunk_pairs=0, v_warps=16, v_pair=0):
+        t = L.Tuning(v_n=v_n, dens_n=dens_n, ypath=ypath, v_warps=v_warps, v_pair=v_pair, chunk_pairs=chunk_pairs)
         check(L.lib().nkx_plan_set_tuning(self._h, C.byref(t)))
 
     def core_hamiltonian(self, centers, Z):

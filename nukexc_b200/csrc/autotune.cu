@@ -4,14 +4,15 @@
 //   the Y path of the GGA density gradient (off / on),
 //   the tcgen05 MMA width of the density contraction (N = 64 / 128; by
 //   default 128 from 1024 orbitals on),
-//   the MMA width of the V contraction (N = 128 / 64) and, for N = 128, its
-//   epilogue warps (16 of 32 columns / 8 of 64),
+//   the V contraction's shape: CTA pairs (M = 256 x N = 64, double-buffered
+//   accumulators) or one CTA per tile, and then its MMA width (N = 128 / 64)
+//   and its epilogue warps (16 / 8; CTA pairs, or one CTA at N = 128),
 //   the chunk size (x1, x2, x4 of the current pair limit, memory permitting),
 // each knob tried with the others at their best so far.  Every new
 // configuration gets one untimed build first (allocations, first touch), then
 // one timed build (CUDA events around the whole build).  Results can be kept
 // in a text cache file, one line per problem:
-//   <device name>|<SMs>|nbf|nblk|npairs|npts|nocc|nspin|gga  v_n dens_n ypath v_warps chunk_pairs best_ms
+//   <device name>|<SMs>|nbf|nblk|npairs|npts|nocc|nspin|gga|v2  v_n dens_n ypath v_warps v_pair chunk_pairs best_ms
 #include <algorithm>
 #include <cstdio>
 #include <fstream>
@@ -35,7 +36,7 @@ std::string signature(const Plan &P, int nspin, int nocc) {
   std::replace(name.begin(), name.end(), ' ', '_');
   std::ostringstream o;
   o << name << "|" << prop.multiProcessorCount << "|" << P.nbf << "|" << P.nblk << "|" << P.npairs << "|" << P.npts
-    << "|" << nocc << "|" << nspin << "|" << (P.gga ? 1 : 0);
+    << "|" << nocc << "|" << nspin << "|" << (P.gga ? 1 : 0) << "|v2";
   return o.str();
 }
 
@@ -48,7 +49,8 @@ bool cache_lookup(const char *path, const std::string &sig, nkx_tuning &t) {
     std::istringstream in(line);
     std::string key;
     nkx_tuning r{};
-    if (in >> key >> r.v_n >> r.dens_n >> r.ypath >> r.v_warps >> r.chunk_pairs >> r.best_ms && key == sig) {
+    if (in >> key >> r.v_n >> r.dens_n >> r.ypath >> r.v_warps >> r.v_pair >> r.chunk_pairs >> r.best_ms &&
+        key == sig) {
       t = r;
       hit = true;
     }
@@ -60,19 +62,21 @@ void cache_store(const char *path, const std::string &sig, const nkx_tuning &t) 
   if (!path) return;
   std::ofstream f(path, std::ios::app);
   NKX_REQUIRE(f.good(), NKX_ERR_ARG, std::string("cannot append to the tuning cache ") + path);
-  f << sig << " " << t.v_n << " " << t.dens_n << " " << t.ypath << " " << t.v_warps << " " << t.chunk_pairs << " "
-    << t.best_ms << "\n";
+  f << sig << " " << t.v_n << " " << t.dens_n << " " << t.ypath << " " << t.v_warps << " " << t.v_pair << " "
+    << t.chunk_pairs << " " << t.best_ms << "\n";
 }
 
 void apply(Plan &P, const nkx_tuning &t) {
   NKX_REQUIRE((t.v_n == 64 || t.v_n == 128) && (t.dens_n == 0 || t.dens_n == 64 || t.dens_n == 128) && t.ypath >= -1 &&
-                  t.ypath <= 1 && (t.v_warps == 8 || t.v_warps == 16),
-              NKX_ERR_ARG, "tuning: v_n must be 64 or 128, dens_n 0, 64 or 128, ypath -1, 0 or 1, v_warps 8 or 16");
+                  t.ypath <= 1 && (t.v_warps == 8 || t.v_warps == 16) && (t.v_pair == 0 || t.v_pair == 1),
+              NKX_ERR_ARG,
+              "tuning: v_n must be 64 or 128, dens_n 0, 64 or 128, ypath -1, 0 or 1, v_warps 8 or 16, v_pair 0 or 1");
   P.drop_graphs();
   P.tune.v_n = t.v_n;
   P.tune.dens_n = t.dens_n;
   P.tune.ypath = t.ypath;
   P.tune.v_warps = t.v_warps;
+  P.tune.v_pair = t.v_pair;
   if (t.chunk_pairs > 0 && t.chunk_pairs != P.chunk_pair_limit) plan_chunks(P, t.chunk_pairs);
 }
 
@@ -82,6 +86,7 @@ nkx_tuning current(const Plan &P) {
   t.dens_n = P.tune.dens_n;
   t.ypath = P.tune.ypath;
   t.v_warps = P.tune.v_warps;
+  t.v_pair = P.tune.v_pair;
   t.chunk_pairs = P.chunk_pair_limit;
   return t;
 }
@@ -148,10 +153,15 @@ static void autotune(Plan &P, int nspin, int nocc, const double *C, const double
     }
     {
       nkx_tuning c = best;
+      c.v_pair = 1 - best.v_pair;
+      consider(c);
+    }
+    if (!best.v_pair) {
+      nkx_tuning c = best;
       c.v_n = best.v_n == 128 ? 64 : 128;
       consider(c);
     }
-    if (best.v_n == 128) {
+    if (best.v_pair || best.v_n == 128) {
       nkx_tuning c = best;
       c.v_warps = best.v_warps == 16 ? 8 : 16;
       consider(c);

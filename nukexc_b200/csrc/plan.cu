@@ -1055,15 +1055,31 @@ void plan_chunks(Plan &P, long maxp) {
     for (int r0 = 0; r0 < nb; r0 += vrow)
       for (int J = 0; J < nb; ++J)
         for (int I = r0; I < std::min(nb, r0 + vrow); ++I) patch.push_back(I * nb + J);
-    std::vector<int> cnt((size_t)nb * nb), blk, tiles, all;
+    // pair tiles (R, J) of the CTA-pair V contraction: row blocks 2R and
+    // 2R + 1 together, costed by the batches where J and either row block
+    // are significant, in the same patch order over about sqrt(SMs / 2) row
+    // pairs
+    const int nr = (nb + 1) / 2, vrow2 = std::max(1, std::min(nr, (int)std::lround(std::sqrt(nsm / 2.0))));
+    std::vector<int> patch2;
+    patch2.reserve((size_t)nr * nb);
+    for (int r0 = 0; r0 < nr; r0 += vrow2)
+      for (int J = 0; J < nb; ++J)
+        for (int R = r0; R < std::min(nr, r0 + vrow2); ++R) patch2.push_back(R * nb + J);
+    std::vector<int> cnt((size_t)nb * nb), cnt2((size_t)nr * nb), blk, rows, tiles, all, all2;
     for (Chunk &c : P.chunks) {
       std::fill(cnt.begin(), cnt.end(), 0);
+      std::fill(cnt2.begin(), cnt2.end(), 0);
       for (long b = c.b0; b < c.b1; ++b) {
         blk.clear();
+        rows.clear();
         for (int w = 0; w < P.mask_words; ++w)
           for (uint32_t m = P.h_mask[b * P.mask_words + w]; m; m &= m - 1) blk.push_back(32 * w + __builtin_ctz(m));
         for (int I : blk)
+          if (rows.empty() || rows.back() != I / 2) rows.push_back(I / 2);  // blk is ascending
+        for (int I : blk)
           for (int J : blk) ++cnt[(size_t)I * nb + J];
+        for (int R : rows)
+          for (int J : blk) ++cnt2[(size_t)R * nb + J];
       }
       tiles.clear();
       for (int t : patch)
@@ -1072,11 +1088,22 @@ void plan_chunks(Plan &P, long maxp) {
       c.t0 = (long)all.size();
       for (int t : tiles) all.push_back(((t / nb) << 16) | (t % nb));
       c.t1 = (long)all.size();
+      tiles.clear();
+      for (int t : patch2)
+        if (cnt2[t]) tiles.push_back(t);
+      std::stable_sort(tiles.begin(), tiles.end(), [&](int x, int y) { return cnt2[x] > cnt2[y]; });
+      c.u0 = (long)all2.size();
+      for (int t : tiles) all2.push_back(((t / nb) << 16) | (t % nb));
+      c.u1 = (long)all2.size();
     }
     P.release(P.d_vtiles);
     P.d_vtiles = P.alloc<int>(std::max<size_t>(1, all.size()));
     if (!all.empty())
       NKX_CUDA(cudaMemcpy(P.d_vtiles, all.data(), sizeof(int) * all.size(), cudaMemcpyHostToDevice));
+    P.release(P.d_vtiles2);
+    P.d_vtiles2 = P.alloc<int>(std::max<size_t>(1, all2.size()));
+    if (!all2.empty())
+      NKX_CUDA(cudaMemcpy(P.d_vtiles2, all2.data(), sizeof(int) * all2.size(), cudaMemcpyHostToDevice));
   }
   const size_t tile = (size_t)kBatch * kBlockF;
   P.release(P.ws_phi);

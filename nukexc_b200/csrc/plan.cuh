@@ -13,6 +13,7 @@ struct Chunk {
   long b0 = 0, b1 = 0;  // batch range
   long p0 = 0, p1 = 0;  // (batch, block) pair range
   long t0 = 0, t1 = 0;  // range of the chunk's V output tiles in d_vtiles
+  long u0 = 0, u1 = 0;  // range of its V pair tiles (row blocks 2R, 2R + 1) in d_vtiles2
 };
 
 // Choices of the mixed-precision build that the autotuner (nkx_plan_autotune)
@@ -22,6 +23,9 @@ struct Tuning {
   int dens_n = 0;  // MMA width of the density contraction (64, 128, or 0: by orbital count, density_width)
   int ypath = -1;  // GGA density gradient through Y = T0 (C occ)^T: -1 from 256 orbitals, 0 off, 1 on
   int v_warps = 16; // epilogue warps of the N = 128 V contraction (16 of 32 columns, or 8 of 64)
+  // V on CTA pairs (M = 256 x N = 64, double-buffered TMEM, v_warps
+  // epilogue warps a CTA) instead of one CTA per tile
+  int v_pair = 0;
 };
 
 // A Fock build recorded into a CUDA graph (graph mode) with the buffers it
@@ -84,6 +88,7 @@ struct Plan {
   // V output tiles (I << 16 | J) of each chunk that have at least one batch
   // with both blocks significant, heaviest first (plan_chunks)
   int *d_vtiles = nullptr;
+  int *d_vtiles2 = nullptr;  // V pair tiles (R << 16 | J), by chunk
   Tuning tune;
   double *ws_phi = nullptr;  // PhiT tiles of a chunk: [pair][comp][g][f]
   double *ws_z = nullptr;    // Z^T tiles of a chunk:  [pair][z][g][f]

@@ -653,6 +653,301 @@ __global__ void __launch_bounds__(TcShape<NW, EW>::kThreads, 1)
   }
 }
 
+// ------------------------------------------------ V on CTA pairs ----
+//
+// The V contraction on clusters of two CTAs (tcgen05 cta_group::2): one
+// M = 256 x N = 64 MMA covers the rows of two function blocks (I0 = 2R on
+// rank 0, I1 = 2R + 1 on rank 1) against 64 columns of block J.  Per K step
+// each CTA stages its own block's Phi digits (4 planes x 128 rows) and half
+// of the 64 Z columns (4 planes x 32 rows), 40 KB, in a 5-stage ring.
+// Rank 0 issues the MMAs; its full barriers count the bytes of both CTAs'
+// loads, and its commits arrive on the empty and TMEM-full barriers of both
+// CTAs.  Four int32 levels of N = 64 fill half of TMEM, so the accumulators
+// are double-buffered: the epilogue of one batch (each CTA reads its own
+// 128 rows) overlaps the MMAs of the next, and both CTAs' epilogue warps
+// report a drained buffer on rank 0's TMEM-empty barrier.  A batch where
+// only one of the two row blocks is significant still runs the pair's MMAs:
+// the CTA without its block loads the other block's digits and discards
+// its accumulators.  Per SM an MMA reads 4 KB of A (kept in the collector
+// across its run of B planes) and 1 KB of B from shared memory for
+// 128 x 64 x 32 products, so the tensor pipe, not shared memory, bounds it.
+constexpr int kPairStages = 5;
+constexpr int kPairABytes = 4 * 128 * 64;  // four digit planes, 128 rows x 64 B
+constexpr int kPairBBytes = 4 * 32 * 64;   // four digit planes, 32 rows x 64 B
+constexpr int kPairStageBytes = kPairABytes + kPairBBytes;
+constexpr int kPairSmem = kPairStages * kPairStageBytes + 1024;
+constexpr uint32_t kPairIdesc = idesc_i8(256, 64);
+
+struct PairGroup {
+  long qa;    // chunk-relative pair whose Phi digits this CTA loads
+  long qb;    // chunk-relative pair of block J
+  bool live;  // this CTA's row block is significant in the batch
+};
+
+// The batches of a pair unit (row blocks 2R, 2R + 1, column block J): those
+// where J and at least one of the row blocks are significant.
+template <class Fn>
+__device__ __forceinline__ void for_each_pair_group(const TcArgs &a, int R, int J, int sp, uint32_t rank, Fn &&fn) {
+  const int I0 = 2 * R, I1 = 2 * R + 1;
+  for (long b = a.b0 + sp; b < a.b1; b += a.nsplit) {
+    const uint32_t *m = a.mask + b * a.mask_words;
+    if (!blk_has(m, J)) continue;
+    const bool h0 = blk_has(m, I0), h1 = I1 < a.nblk && blk_has(m, I1);
+    if (!h0 && !h1) continue;
+    const bool own = rank == 0 ? h0 : h1;
+    const int Ia = (rank == 0) == own ? I0 : I1;
+    const long qb0 = a.pair_off[b] - a.p0;
+    PairGroup g;
+    g.qa = qb0 + blk_pos(m, Ia);
+    g.qb = qb0 + blk_pos(m, J);
+    g.live = own;
+    fn(g);
+  }
+}
+
+// EW epilogue warps a CTA (8: 32 columns each, 16: 16 columns each)
+template <int EW>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(64 + 32 * EW, 1)
+    tc_v_pair_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs a) {
+  constexpr int N = 64, CW = 4 * N / EW, S = kPairStages;
+  static_assert(CW == 16 || CW == 32, "16 or 32 columns an epilogue warp");
+  extern __shared__ __align__(1024) uint8_t dsmem[];
+  __shared__ uint64_t full_bar[S], empty_bar[S], tfull_bar[2], tempty_bar[2], drain_bar, stall_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ volatile int abort_flag;
+  __shared__ __align__(16) double colscale[EW * CW];
+  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(dsmem) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    for (int i = 0; i < S; ++i) {
+      mbar_init(&full_bar[i], 1);
+      mbar_init(&empty_bar[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&tfull_bar[i], 1);
+      mbar_init(&tempty_bar[i], 2 * EW);  // one arrival per epilogue warp of either CTA
+    }
+    mbar_init(&drain_bar, 1);
+    mbar_init(&stall_bar, 1);
+    fence_mbar_init();
+    prefetch_tmap(&mapA);
+    prefetch_tmap(&mapB);
+  }
+  if (warp == 1) {
+    tmem_alloc_pair(&tmem_base_sh, 512);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  cluster_sync();  // both CTAs' barriers initialised before any remote arrival
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  // a wait that gave up stops the other CTA of the pair as well
+  const uint32_t peer_abort = map_to_rank((const void *)&abort_flag, rank ^ 1u);
+  auto give_up = [&]() { st_cluster_u32(peer_abort, 1u); };
+  const long cid = cluster_id_x(), ncl = cluster_count_x();
+  auto unit = [&](long u, int &R, int &J, int &zi, int &hc, int &sp) {
+    const long n2 = a.ntiles * 2, n3 = n2 * a.nz;
+    sp = (int)(u / n3);
+    u %= n3;
+    zi = (int)(u / n2);
+    u %= n2;
+    hc = (int)(u % 2);
+    const int t = a.vtiles[u / 2];
+    R = t >> 16;
+    J = t & 0xffff;
+  };
+
+  if (warp == 0) {
+    // ------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      uint32_t step = 0;
+      for (long u = cid; u < a.nunits && !abort_flag; u += ncl) {
+        int R, J, zi, hc, sp;
+        unit(u, R, J, zi, hc, sp);
+        for_each_pair_group(a, R, J, sp, rank, [&](const PairGroup &g) {
+          const int za = (int)(g.qa * 4), zb = (int)((g.qb * a.nz + zi) * 4), yb = 64 * hc + 32 * (int)rank;
+          for (int k = 0; k < 4 && !abort_flag; ++k, ++step) {
+            const int st = step % S;
+            if (!mbar_wait(&empty_bar[st], ((step / S) & 1) ^ 1, a.err, 1, &abort_flag, a.wait_ns)) {
+              give_up();
+              return;
+            }
+            uint8_t *base = smem + st * kPairStageBytes;
+            if (rank == 0) mbar_arrive_expect_tx(&full_bar[st], 2 * kPairStageBytes);
+            const uint32_t fb = map_to_rank(&full_bar[st], 0);
+            tma_load_3d_pair(base, &mapA, 64 * k, 0, za, fb);
+            tma_load_3d_pair(base + kPairABytes, &mapB, 64 * k, yb, zb, fb);
+          }
+        });
+      }
+      if (rank == 0) {
+        // the last stages' loads of both CTAs have landed
+        volatile int keep_waiting = 0;
+        for (uint32_t k = (step > S ? step - S : 0); k < step; ++k)
+          mbar_wait(&full_bar[k % S], (k / S) & 1, a.err, 2, &keep_waiting, kDrainLimitNs);
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------ MMA issuer (rank 0)
+    if (lane == 0 && rank == 0) {
+      uint32_t step = 0, grp = 0;
+      if (a.stall && !mbar_wait(&stall_bar, 0, a.err, 7, &abort_flag, a.wait_ns)) give_up();
+      for (long u = cid; u < a.nunits && !abort_flag; u += ncl) {
+        int R, J, zi, hc, sp;
+        unit(u, R, J, zi, hc, sp);
+        for_each_pair_group(a, R, J, sp, rank, [&](const PairGroup &) {
+          if (abort_flag) return;
+          const uint32_t buf = grp & 1, use = grp >> 1;
+          if (!mbar_wait(&tempty_bar[buf], (use & 1) ^ 1, a.err, 3, &abort_flag, a.wait_ns)) {
+            give_up();
+            return;
+          }
+          tc_fence_after();
+          const uint32_t d = tmem + buf * 4 * N;
+          for (int k = 0; k < 4; ++k, ++step) {
+            const int st = step % S;
+            if (!mbar_wait(&full_bar[st], (step / S) & 1, a.err, 4, &abort_flag, a.wait_ns)) {
+              give_up();
+              return;
+            }
+            tc_fence_after();
+            const uint32_t base = smem_u32(smem + st * kPairStageBytes);
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk)
+#pragma unroll
+              for (int i = 0; i < 4; ++i) {
+                const uint64_t ad = smem_desc_k64(base + i * (128 * 64) + kk * 32);
+#pragma unroll
+                for (int j = 0; j <= 3 - i; ++j) {
+                  const uint64_t bd = smem_desc_k64(base + kPairABytes + j * (32 * 64) + kk * 32);
+                  const uint32_t dt = d + (i + j) * N;
+                  const uint32_t acc = (k == 0 && kk == 0 && i == 0) ? 0u : 1u;
+                  if (i == 3)
+                    mma_i8_pair<CollectorDiscard>(dt, ad, bd, kPairIdesc, acc);
+                  else if (j == 0)
+                    mma_i8_pair<CollectorFill>(dt, ad, bd, kPairIdesc, acc);
+                  else if (j == 3 - i)
+                    mma_i8_pair<CollectorLastUse>(dt, ad, bd, kPairIdesc, acc);
+                  else
+                    mma_i8_pair<CollectorUse>(dt, ad, bd, kPairIdesc, acc);
+                }
+              }
+            mma_commit_pair(&empty_bar[st], 3);
+          }
+          mma_commit_pair(&tfull_bar[buf], 3);
+          ++grp;
+        });
+      }
+      volatile int keep_waiting = 0;
+      mma_commit_pair(&drain_bar, 1);
+      mbar_wait(&drain_bar, 0, a.err, 5, &keep_waiting, kDrainLimitNs);
+    }
+  } else {
+    // ------------------------------------------------------ epilogue
+    const int q = warp & 3, cq = (warp - 2) >> 2;
+    const int row = 32 * q + lane;
+    const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
+    const uint32_t tempty_r0[2] = {map_to_rank(&tempty_bar[0], 0), map_to_rank(&tempty_bar[1], 0)};
+    double *cs = colscale + (warp - 2) * CW;
+    uint32_t grp = 0;
+    for (long u = cid; u < a.nunits && !abort_flag; u += ncl) {
+      int R, J, zi, hc, sp;
+      unit(u, R, J, zi, hc, sp);
+      double acc[CW];
+#pragma unroll
+      for (int j = 0; j < CW; ++j) acc[j] = 0.0;
+      bool any = false;
+      for_each_pair_group(a, R, J, sp, rank, [&](const PairGroup &g) {
+        if (abort_flag) return;
+        const uint32_t buf = grp & 1, use = grp >> 1;
+        auto release = [&]() {
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive_cluster(tempty_r0[buf]);
+        };
+        double sa = 0.0, sb = 0.0;
+        if (g.live) {
+          sa = a.sA[g.qa * 128 + row] * kTwoM36;
+          if (lane < CW) sb = a.sB[(g.qb * a.nz + zi) * 128 + 64 * hc + CW * cq + lane];
+        }
+        if (!mbar_wait(&tfull_bar[buf], use & 1, a.err, 6, &abort_flag, a.wait_ns)) {
+          give_up();
+          return;
+        }
+        tc_fence_after();
+        __syncwarp();
+        if (g.live) {
+          if (lane < CW) cs[lane] = sb;
+          __syncwarp();
+          const uint32_t tb = tmem + lane_addr + buf * 4 * N + CW * cq;
+          constexpr int NS = CW / 4;
+          uint32_t p0[4], p1[4], p2[4], p3[4], r0[4], r1[4], r2[4], r3[4];
+          auto issue = [&](int h, uint32_t(&x0)[4], uint32_t(&x1)[4], uint32_t(&x2)[4], uint32_t(&x3)[4]) {
+            const uint32_t ta = tb + 4 * h;
+            tmem_ld4u_async(ta, x0);
+            tmem_ld4u_async(ta + N, x1);
+            tmem_ld4u_async(ta + 2 * N, x2);
+            tmem_ld4u_async(ta + 3 * N, x3);
+          };
+          auto combine = [&](int h, const uint32_t(&x0)[4], const uint32_t(&x1)[4], const uint32_t(&x2)[4],
+                             const uint32_t(&x3)[4]) {
+            const double2 c01 = *reinterpret_cast<const double2 *>(cs + 4 * h);
+            const double2 c23 = *reinterpret_cast<const double2 *>(cs + 4 * h + 2);
+            const double sc[4] = {c01.x, c01.y, c23.x, c23.y};
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              acc[4 * h + j] = fma(level_sum(x0[j], x1[j], x2[j], x3[j]), sa * sc[j], acc[4 * h + j]);
+          };
+          issue(0, p0, p1, p2, p3);
+#pragma unroll
+          for (int h = 0; h < NS; ++h) {
+            if ((h & 1) == 0) {
+              tmem_wait4x4(p0, p1, p2, p3);
+              if (h + 1 < NS) issue(h + 1, r0, r1, r2, r3);
+            } else {
+              tmem_wait4x4(r0, r1, r2, r3);
+              if (h + 1 < NS) issue(h + 1, p0, p1, p2, p3);
+            }
+            if (h + 1 == NS) release();
+            if ((h & 1) == 0)
+              combine(h, p0, p1, p2, p3);
+            else
+              combine(h, r0, r1, r2, r3);
+          }
+          __syncwarp();  // the column scales are read before the next group overwrites them
+        } else {
+          release();
+        }
+        ++grp;
+        any = any || g.live;
+      });
+      const int I = 2 * R + (int)rank;
+      if (any && I < a.nblk) {
+        double *Vz = a.V + (size_t)zi * a.nbf_pad * a.nbf_pad;
+        const size_t r = (size_t)I * 128 + row;
+        const size_t c0 = (size_t)J * 128 + 64 * hc + CW * cq;
+        if (a.nsplit > 1) {
+#pragma unroll
+          for (int j = 0; j < CW; ++j) atomicAdd(&Vz[r + (c0 + j) * a.nbf_pad], acc[j]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < CW; ++j) Vz[r + (c0 + j) * a.nbf_pad] += acc[j];
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  cluster_sync();  // neither CTA leaves while the other's MMAs or loads may touch its memory
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc_pair(tmem, 512);
+  }
+}
+
 // ----------------------------------------------------- quantisation ----
 
 __device__ __forceinline__ double warp_max(double v) {
@@ -1193,8 +1488,10 @@ struct MixedState {
   uint8_t *qt0 = nullptr, *qco = nullptr;
   double *st0 = nullptr, *sco = nullptr;
   // B operand maps by box width: Z with 128- and 64-row boxes (V at N = 128 / 64),
-  // Ct with 64- and 128-row boxes (density at N = 64 / 128)
-  CUtensorMap m_phT, m_ph, m_z, m_z64, m_ct, m_ct128, m_t0, m_co, m_co128;
+  // Ct with 64- and 128-row boxes (density at N = 64 / 128); Z with 32-row
+  // boxes for the CTA-pair V contraction (each CTA's half of 64 columns)
+  CUtensorMap m_phT, m_ph, m_z, m_z64, m_z32, m_ct, m_ct128, m_t0, m_co, m_co128;
+  int pair_clusters = 0;  // CTA pairs of the V contraction that fit on the device at once
   std::vector<void *> bufs;
   size_t T_cap = 0, qt0_cap = 0;  // doubles of T, bytes of qt0 (grown on demand)
   ~MixedState() {
@@ -1280,11 +1577,24 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     M->m_ph = make_map3(M->qph, 256, 128, M->cap * 4, 128);
     M->m_z = make_map3(M->qz, 256, 128, M->cap * 3 * 4, 128);
     M->m_z64 = make_map3(M->qz, 256, 128, M->cap * 3 * 4, 64);
+    M->m_z32 = make_map3(M->qz, 256, 128, M->cap * 3 * 4, 32);
     int dev = 0;
     NKX_CUDA(cudaGetDevice(&dev));
     NKX_CUDA(cudaDeviceGetAttribute(&M->nsm, cudaDevAttrMultiProcessorCount, dev));
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_V, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   TcShape<128>::kSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_v_pair_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairSmem));
+    NKX_CUDA(cudaFuncSetAttribute(tc_v_pair_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairSmem));
+    {
+      // clusters of two that are resident at once (the persistent grid)
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(2 * M->nsm);
+      cfg.blockDim = dim3(64 + 32 * 8);
+      cfg.dynamicSmemBytes = kPairSmem;
+      int ncl = 0;
+      NKX_CUDA(cudaOccupancyMaxActiveClusters(&ncl, tc_v_pair_kernel<8>, &cfg));
+      M->pair_clusters = std::max(1, ncl);
+    }
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_V, 128, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   TcShape<128, 8>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_V, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1324,6 +1634,19 @@ template <int MODE, int NW, int EW = NW / 8>
 static void launch_i8_shape(const CUtensorMap &mA, const CUtensorMap &mB, const TcArgs &a, unsigned grid,
                             cudaStream_t s) {
   tc_i8_kernel<MODE, NW, EW><<<grid, TcShape<NW, EW>::kThreads, TcShape<NW, EW>::kSmem, s>>>(mA, mB, a);
+}
+
+// The CTA-pair V contraction: one persistent cluster of two per pair of
+// SMs that fits at once (or per unit when there are fewer).
+static void launch_v_pair(MixedState &M, const TcArgs &a, int ew, cudaStream_t s) {
+  if (a.nunits <= 0) return;
+  const unsigned grid = 2u * (unsigned)std::min<long>(a.nunits, M.pair_clusters);
+  NKX_REQUIRE(ew == 8 || ew == 16, NKX_ERR_ARG, "CTA-pair V epilogue warps must be 8 or 16");
+  if (ew == 8)
+    tc_v_pair_kernel<8><<<grid, 64 + 32 * 8, kPairSmem, s>>>(M.m_ph, M.m_z32, a);
+  else
+    tc_v_pair_kernel<16><<<grid, 64 + 32 * 16, kPairSmem, s>>>(M.m_ph, M.m_z32, a);
+  NKX_LAUNCH_CHECK();
 }
 
 // one persistent CTA per SM (or per unit when there are fewer)
@@ -1654,6 +1977,23 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     a.stall = P.stall_test;
     // the chunk's nonempty output tiles, heaviest first; too few units for
     // the SMs: split the chunk's batches
+    if (P.tune.v_pair) {
+      // pair tiles (row blocks 2R, 2R + 1; column block J) in two column
+      // halves; too few units for the CTA pairs: split the chunk's batches
+      a.vtiles = P.d_vtiles2 + c.u0;
+      a.ntiles = c.u1 - c.u0;
+      a.nt = 64;
+      const long parts = (long)nzs * a.ntiles * 2;
+      a.nsplit = (parts == 0 || parts >= M.pair_clusters)
+                     ? 1
+                     : (int)std::min<long>({(M.pair_clusters + parts - 1) / parts, c.b1 - c.b0, 16L});
+      a.nsplit = std::max(1, a.nsplit);
+      a.nunits = parts * a.nsplit;
+      launch_v_pair(M, a, P.tune.v_warps, s);
+      ++P.launches;
+      Tm.end(s);
+      return;
+    }
     a.vtiles = P.d_vtiles + c.t0;
     a.ntiles = c.t1 - c.t0;
     const long tiles = (long)nzs * a.ntiles;

@@ -1,5 +1,6 @@
 // Thin inline-PTX layer for the sm_100a tensor-core kernels: mbarriers,
-// TMA tile loads into the CTA's own shared memory, tcgen05 MMA / TMEM.  Every wait is
+// TMA tile loads into the CTA's own shared memory (never multicast), tcgen05
+// MMA / TMEM, on one CTA or a cluster of two (cta_group::2).  Every wait is
 // bounded: after its limit of global time it raises an error flag and
 // returns false, so no kernel can spin forever.
 #pragma once
@@ -160,6 +161,95 @@ __device__ __forceinline__ void tmem_wait4x4(uint32_t (&a)[4], uint32_t (&b)[4],
                  "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3]), "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
                :
                : "memory");
+}
+
+// ------------------------------------------------------ CTA pairs --
+// A cluster of two CTAs on two SMs runs one M = 256 MMA (cta_group::2): each
+// CTA holds half of A (128 rows) and half of B (N / 2 rows) in its own
+// shared memory at the same offsets and receives its 128 rows x N of D in
+// its own TMEM.  Rank 0 issues the MMAs.
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_id_x() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_count_x() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+  return r;
+}
+// shared::cluster address of the same shared-memory location in CTA `rank`
+__device__ __forceinline__ uint32_t map_to_rank(const void *p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+// all threads of both CTAs (the non-.aligned form: callers may come from
+// diverged warps)
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+__device__ __forceinline__ void st_cluster_u32(uint32_t cluster_addr, uint32_t v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(cluster_addr), "r"(v) : "memory");
+}
+// 3-D TMA box load into this CTA's shared memory whose completion is
+// counted on an mbarrier of either CTA of the pair (a shared::cluster
+// address); no multicast
+__device__ __forceinline__ void tma_load_3d_pair(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                                 uint32_t bar_cluster_addr) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+      "%4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar_cluster_addr)
+      : "memory");
+}
+// TMEM of a CTA pair: the same warp of both CTAs allocates (and frees) the
+// same columns in both SMs
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t *dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+               "r"(ncols));
+}
+__device__ __forceinline__ void tmem_relinquish_pair() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::);
+}
+__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+// M = 256 kind::i8 MMA of the pair (collector usage as mma_i8_a)
+template <int U>
+__device__ __forceinline__ void mma_i8_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            uint32_t accumulate) {
+#define NKX_MMA_I8_PAIR(Q)                                                                                 \
+  asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"                                          \
+               "tcgen05.mma.cta_group::2.kind::i8" Q " [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem), "l"(a_desc), \
+               "l"(b_desc), "r"(idesc), "r"(accumulate)                                                    \
+               : "memory")
+  if constexpr (U == CollectorFill)
+    NKX_MMA_I8_PAIR(".collector::a::fill");
+  else if constexpr (U == CollectorUse)
+    NKX_MMA_I8_PAIR(".collector::a::use");
+  else if constexpr (U == CollectorLastUse)
+    NKX_MMA_I8_PAIR(".collector::a::lastuse");
+  else
+    NKX_MMA_I8_PAIR("");
+#undef NKX_MMA_I8_PAIR
+}
+// Arrive once on the mbarrier at `bar`'s offset in every CTA of cta_mask
+// when all earlier MMAs of this thread complete
+__device__ __forceinline__ void mma_commit_pair(uint64_t *bar, uint16_t cta_mask) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "h"(cta_mask)
+      : "memory");
 }
 
 // 16 bytes from global memory in one read-only load (16-byte aligned address)

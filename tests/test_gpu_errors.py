@@ -76,8 +76,12 @@ def test_nonfinite_orbitals_in_density_and_gradient(water):
     assert np.isfinite(fb.density([Cm], [occ])).all()
 
 
-def test_stalled_wait_reports_timeout_and_plan_recovers(water):
+@pytest.mark.parametrize("v_pair", [0, 1])
+def test_stalled_wait_reports_timeout_and_plan_recovers(water, v_pair):
+    """v_pair = 1: the V contraction on CTA pairs, whose waits give up in
+    one CTA and stop the other through the cluster's shared memory."""
     fb, Cm, occ = water
+    fb.set_tuning(v_pair=v_pair, v_warps=8 if v_pair else 16)
     E0, V0, _ = fb.build([Cm], [occ], precision="mixed")
     try:
         fb.set_wait_limit(ns=2_000_000, stall=True)  # 2 ms
@@ -90,6 +94,7 @@ def test_stalled_wait_reports_timeout_and_plan_recovers(water):
         E1, V1, _ = fb.build([Cm], [occ], precision="mixed")
         assert abs(E1 - E0) <= 1e-12 * abs(E0)
         assert np.abs(V1[0] - V0[0]).max() <= 1e-12 * np.abs(V0[0]).max()
+    fb.set_tuning()
 
 
 def test_short_wait_limit_without_stall_still_builds(water):

@@ -1,7 +1,8 @@
 """The mixed build's tunable choices and the autotuner (nkx_plan_autotune).
 
-Every combination of the tcgen05 MMA widths (V: N = 128 / 64, density:
-N = 64 / 128) and of the Y path of the GGA density gradient must give the
+Every combination of the V contraction's shape (one CTA per tile at
+N = 128 / 64, or CTA pairs at M = 256 x N = 64), the density MMA width
+(N = 64 / 128) and the Y path of the GGA density gradient must give the
 same build: bit-for-bit up to the order of FP64 additions for the same
 algorithm (1e-12), and within the mixed scheme's gate of the FP64 build
 (|dE| <= 1e-6 Eh, max|dV| <= 1e-7) across the Y-path switch.  Re-chunking
@@ -39,14 +40,16 @@ def test_widths_and_y_path_give_the_same_build(case):
     fb = A.FockBuilder(c, Z, A.make_manual_basis(funcs), g, func_ids=XC)
     E64, V64, _ = fb.build([Cm], [occ], precision="fp64")
     ref = {}
-    # V shapes: N = 128 with 16 or 8 epilogue warps, N = 64
-    for (v_n, v_w), d_n, yp in itertools.product(((128, 16), (128, 8), (64, 16)), (64, 128), (0, 1)):
-        fb.set_tuning(v_n=v_n, dens_n=d_n, ypath=yp, v_warps=v_w)
+    # V shapes: one CTA at N = 128 with 16 or 8 epilogue warps, one CTA at
+    # N = 64, CTA pairs with 8 or 16 epilogue warps a CTA
+    shapes = ((128, 16, 0), (128, 8, 0), (64, 16, 0), (64, 8, 1), (64, 16, 1))
+    for (v_n, v_w, v_p), d_n, yp in itertools.product(shapes, (64, 128), (0, 1)):
+        fb.set_tuning(v_n=v_n, dens_n=d_n, ypath=yp, v_warps=v_w, v_pair=v_p)
         E, V, _ = fb.build([Cm], [occ], precision="mixed")
-        assert abs(E - E64) <= 1e-6 and np.abs(V[0] - V64[0]).max() <= 1e-7, (v_n, v_w, d_n, yp)
+        assert abs(E - E64) <= 1e-6 and np.abs(V[0] - V64[0]).max() <= 1e-7, (v_n, v_w, v_p, d_n, yp)
         if yp in ref:
             Er, Vr = ref[yp]
-            assert abs(E - Er) <= 1e-12 * abs(Er) and np.abs(V[0] - Vr).max() <= 1e-12, (v_n, v_w, d_n, yp)
+            assert abs(E - Er) <= 1e-12 * abs(Er) and np.abs(V[0] - Vr).max() <= 1e-12, (v_n, v_w, v_p, d_n, yp)
         else:
             ref[yp] = (E, V[0])
     fb.close()
@@ -73,7 +76,7 @@ def test_autotune_chooses_applies_and_caches(case, tmp_path):
     t = fb.autotune([Cm], [occ], cache_path=cache)
     assert t["from_cache"] == 0 and t["trials"] >= 4
     assert t["v_n"] in (64, 128) and t["dens_n"] in (64, 128) and t["ypath"] in (-1, 0, 1)
-    assert t["v_warps"] in (8, 16)
+    assert t["v_warps"] in (8, 16) and t["v_pair"] in (0, 1)
     assert 0 < t["best_ms"] <= t["default_ms"] * 1.0001
     assert fb.tuning()["v_n"] == t["v_n"] and fb.tuning()["chunk_pairs"] == t["chunk_pairs"]
     E, V, _ = fb.build([Cm], [occ], precision="mixed")
@@ -83,6 +86,6 @@ def test_autotune_chooses_applies_and_caches(case, tmp_path):
     fb2 = A.FockBuilder(c, Z, A.make_manual_basis(funcs), g, func_ids=XC)
     t2 = fb2.autotune([Cm], [occ], cache_path=cache)
     assert t2["from_cache"] == 1
-    keys = ("v_n", "dens_n", "ypath", "v_warps", "chunk_pairs")
+    keys = ("v_n", "dens_n", "ypath", "v_warps", "v_pair", "chunk_pairs")
     assert tuple(t2[k] for k in keys) == tuple(t[k] for k in keys)
     fb2.close()
