@@ -1254,58 +1254,80 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
   store_operand_scales(red, nop, nz, qrel, sph, szs);
 }
 
-// Pass B, part 1 for builds without J: the same operands as colloc_z_kernel,
-// but phi and grad phi come back from the pass-A digits of the pair instead
-// of a second STO evaluation.  Only the Z planes are staged: the phi plane
-// (o = 0) is left unwritten, so this kernel must be followed by
-// zquant_kernel with the pass-A digits given (pass_b(c, true)), which takes
-// phi from those digits.  qphT[pair][comp][digit][g][f] holds
-// X = d0 2^24 + d1 2^16 + d2 2^8 + d3 with x = X s_g 2^-30 (s_g the
-// power-of-two scale of point g over the block), so the recovered values
-// differ from the collocation by less than 2^-31 s_g.
+// Pass B of a build without J in one kernel: the V operands of one
+// (batch, block) pair on a cluster of four CTAs, 64 points each.  Phi and
+// grad Phi come back exactly from the pair's pass-A digits; the Z planes
+// (Z_s = c0 phi + c . grad phi, s < nz) go to shared memory in FP64, phi as
+// its packed pass-A digits and point scales, and each (plane, function)
+// row's largest exponent field is reduced over the CTA's warps and then,
+// through the cluster's shared memory, over the four CTAs: the row scale is
+// 2^(E - 1022) for the largest field E, the power-of-two scale of the row
+// maximum.  Each CTA then writes the digits of its 64 points from shared
+// memory as 16-byte pieces of the rows of qph[pair][digit][f][g] and
+// qz[pair][z][digit][f][g]; rank 0 writes the scales sph[pair][f] and
+// szs[pair][z][f].  Against the staging of Z in HBM by a separate kernel
+// this moves about half the bytes (the pass-A digits in, the V digits
+// out).  (Clusters of eight CTAs of 32 points, phi staged in FP64, ran
+// 111 ms per (H2O)64 build against 97.)  A row field of 0x7fd or more
+// (values of 2^1022 and up, Inf, NaN) is reported in *nonfinite.
+constexpr int kZdRanks = 4;
+constexpr size_t zdigits_smem(int nz) {
+  return ((size_t)nz * 8 + 4) * (kBatch / kZdRanks) * kBlockF + 8 * (kBatch / kZdRanks);
+}
 template <bool GRAD, int NZ>
-__global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__restrict__ qphT,
-                                                              const double *__restrict__ sphT,
-                                                              const int *__restrict__ pair_batch, long p0,
-                                                              const double *__restrict__ coef, long npad,
-                                                              double *__restrict__ ws, double *__restrict__ sph,
-                                                              double *__restrict__ szs, int *nonfinite) {
-  constexpr int NC = GRAD ? 4 : 1;
-  constexpr int nz = NZ, nop = 1 + NZ;
-  __shared__ double red[8][4][128];
-  const long qrel = blockIdx.x;
-  const int b = pair_batch[p0 + qrel];
+__global__ void __cluster_dims__(kZdRanks, 1, 1) __launch_bounds__(256, 2)
+    zdigits_kernel(const uint8_t *__restrict__ qphT, const double *__restrict__ sphT,
+                   const int *__restrict__ pair_batch, long p0, const double *__restrict__ coef, long npad,
+                   uint8_t *__restrict__ qph, double *__restrict__ sph, uint8_t *__restrict__ qz,
+                   double *__restrict__ szs, int *nonfinite) {
+  constexpr int NC = GRAD ? 4 : 1, nop = 1 + NZ, kPts = kBatch / kZdRanks;
+  constexpr size_t kPlane = (size_t)kBatch * kBlockF;  // one digit plane of a pair, bytes
+  // dynamic shared memory: Z_s [NZ][kPts][128] FP64, then phi as packed
+  // pass-A digits [kPts][128] and its point scales s_g 2^-30 [kPts]
+  extern __shared__ __align__(16) double zst[];
+  uint32_t(*phid)[128] = reinterpret_cast<uint32_t(*)[128]>(zst + (size_t)NZ * kPts * kBlockF);
+  double *phis = reinterpret_cast<double *>(phid + kPts);
+  __shared__ uint32_t red[8][nop][128];
+  __shared__ uint32_t part[nop][128];
+  __shared__ double inv_s[nop][128];
+  const uint32_t rank = cluster_rank();
+  const long q = cluster_id_x();
+  const int b = pair_batch[p0 + q];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const size_t T = (size_t)kBatch * kBlockF;
-  double m[nop][4];
+  const int gbase = kPts * (int)rank;
+  const int ncs = NC;
+  uint32_t e[nop][4];
 #pragma unroll
   for (int o = 0; o < nop; ++o)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) m[o][c] = 0.0;
-  double *out = ws + qrel * 4 * T;
-  unsigned efield = 0;  // largest exponent field of the Z values (0x7ff: non-finite)
-  for (int g = warp; g < kBatch; g += 8) {
+    for (int k = 0; k < 4; ++k) e[o][k] = 0u;
+  // ---- phase 1: warp w takes points gbase + w + 8 j, lane l functions 4 l .. 4 l + 3
+#pragma unroll 2
+  for (int j = 0; j < kPts / 8; ++j) {
+    const int gl = warp + 8 * j, g = gbase + gl;
     const long gg = (long)b * kBatch + g;
     double v[NC][4];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      const long pc = qrel * NC + c;
-      const double sc = sphT[pc * 256 + g] * 0x1p-30;
-      // plane words (leading digit first) -> one packed digit word per value
+      const long pc = q * ncs + c;
+      const double sc = sphT[pc * kBatch + g] * 0x1p-30;
       uint32_t wd[4], bw[4];
 #pragma unroll
       for (int d = 0; d < 4; ++d)
-        wd[3 - d] = reinterpret_cast<const uint32_t *>(qphT + ((pc * 4 + d) * 256 + g) * 128)[lane];
+        wd[3 - d] = reinterpret_cast<const uint32_t *>(qphT + (pc * 4 + d) * kPlane + (size_t)g * kBlockF)[lane];
       transpose4(wd, bw);
 #pragma unroll
       for (int k = 0; k < 4; ++k) v[c][k] = int_to_double(digits_value(bw[k])) * sc;
+      if (c == 0) {
+        *reinterpret_cast<uint4 *>(&phid[gl][4 * lane]) = make_uint4(bw[0], bw[1], bw[2], bw[3]);
+        if (lane == 0) phis[gl] = sc;
+      }
     }
-    double z[nop][4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) z[0][k] = v[0][k];
+    for (int k = 0; k < 4; ++k) e[0][k] = max(e[0][k], exp_field(v[0][k]));
 #pragma unroll
-    for (int sp = 0; sp < nz; ++sp) {
-      const double *cs = coef + (size_t)sp * 4 * npad;
+    for (int s = 0; s < NZ; ++s) {
+      const double *cs = coef + (size_t)s * 4 * npad;
       const double c0 = cs[gg];
       double c1 = 0.0, c2 = 0.0, c3 = 0.0;
       if (GRAD) {
@@ -1313,32 +1335,89 @@ __global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__
         c2 = cs[2 * npad + gg];
         c3 = cs[3 * npad + gg];
       }
+      double z[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        z[1 + sp][k] = c0 * v[0][k];
-        if (GRAD) z[1 + sp][k] += c1 * v[NC > 1 ? 1 : 0][k] + c2 * v[NC > 2 ? 2 : 0][k] + c3 * v[NC > 3 ? 3 : 0][k];
+        z[k] = c0 * v[0][k];
+        if (GRAD) z[k] += c1 * v[NC > 1 ? 1 : 0][k] + c2 * v[NC > 2 ? 2 : 0][k] + c3 * v[NC > 3 ? 3 : 0][k];
+        e[1 + s][k] = max(e[1 + s][k], exp_field(z[k]));
       }
-    }
-#pragma unroll
-    for (int o = 0; o < nop; ++o) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        m[o][c] = fmax(m[o][c], fabs(z[o][c]));
-        efield = max(efield, exp_field(z[o][c]));
-      }
-      if (o == 0) continue;  // zquant takes phi from the digits again
-      double2 *dst = reinterpret_cast<double2 *>(out + o * T + (size_t)g * kBlockF + 4 * lane);
-      dst[0] = make_double2(z[o][0], z[o][1]);
-      dst[1] = make_double2(z[o][2], z[o][3]);
+      double2 *dst = reinterpret_cast<double2 *>(zst + ((size_t)s * kPts + gl) * kBlockF + 4 * lane);
+      dst[0] = make_double2(z[0], z[1]);
+      dst[1] = make_double2(z[2], z[3]);
     }
   }
-  report_nonfinite(efield == 0x7ffu, nonfinite);
+  unsigned ez = 0;
+#pragma unroll
+  for (int o = 1; o < nop; ++o)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ez = max(ez, e[o][k]);
+  report_nonfinite(ez >= 0x7fdu, nonfinite);
 #pragma unroll
   for (int o = 0; o < nop; ++o)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) red[warp][o][4 * lane + c] = m[o][c];
+    for (int k = 0; k < 4; ++k) red[warp][o][4 * lane + k] = e[o][k];
   __syncthreads();
-  store_operand_scales(red, nop, nz, qrel, sph, szs);
+  for (int t = threadIdx.x; t < nop * 128; t += blockDim.x) {
+    uint32_t m = 0u;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) m = max(m, red[w][t / 128][t % 128]);
+    part[t / 128][t % 128] = m;
+  }
+  cluster_sync();  // every CTA's row fields are in place
+  for (int t = threadIdx.x; t < nop * 128; t += blockDim.x) {
+    const int o = t / 128, f = t % 128;
+    uint32_t E = 0u;
+#pragma unroll
+    for (uint32_t rr = 0; rr < kZdRanks; ++rr) E = max(E, ld_cluster_u32(map_to_rank(&part[o][f], rr)));
+    double sc = 1.0, inv = 1.0;  // an all-zero row keeps scale 1
+    if (E > 0u && E < 0x7fdu) {
+      sc = __hiloint2double((int)((E + 1u) << 20), 0);
+      inv = __hiloint2double((int)((2045u - E) << 20), 0);
+    }
+    inv_s[o][f] = inv;
+    if (rank == 0) {
+      if (o == 0)
+        sph[q * 128 + f] = sc;
+      else
+        szs[(q * NZ + (o - 1)) * 128 + f] = sc;
+    }
+  }
+  __syncthreads();
+  // ---- phase 2: thread (f, gh) writes points gbase + 32 gh .. + 31 of row f
+  static_assert(kPts == 64, "two threads a row, 32 points each");
+  {
+    const int f = threadIdx.x & 127, gh = threadIdx.x >> 7;
+#pragma unroll
+    for (int o = 0; o < nop; ++o) {
+      const double inv = inv_s[o][f];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        uint32_t w[4][4];  // [digit plane][group of four points]
+#pragma unroll
+        for (int k4 = 0; k4 < 4; ++k4) {
+          const int gl = 32 * gh + 16 * h + 4 * k4;
+          double v[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            v[i] = (o == 0) ? int_to_double(digits_value(phid[gl + i][f])) * phis[gl + i]
+                            : zst[((size_t)(o - 1) * kPts + gl + i) * kBlockF + f];
+          uint32_t ww[4];
+          quant4(v, inv, ww);
+#pragma unroll
+          for (int d = 0; d < 4; ++d) w[d][k4] = ww[d];
+        }
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+          uint8_t *row = (o == 0) ? qph + ((q * 4 + d) * 128 + f) * (size_t)kBatch
+                                  : qz + (((q * NZ + (o - 1)) * 4 + d) * 128 + f) * (size_t)kBatch;
+          *reinterpret_cast<uint4 *>(row + gbase + 32 * gh + 16 * h) =
+              make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
+        }
+      }
+    }
+  }
+  cluster_sync();  // no CTA leaves while another may still read its row fields
 }
 
 // Pass B, part 2: digits of the V operands, transposed to
@@ -1347,8 +1426,7 @@ __global__ void __launch_bounds__(256, 2) z_from_digits_kernel(const uint8_t *__
 // for one Z plane, so four blocks share an SM).
 __global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ ws, const double *__restrict__ sph,
                                                      const double *__restrict__ szs, int nz, uint8_t *__restrict__ qph,
-                                                     uint8_t *__restrict__ qz, const uint8_t *__restrict__ qphT,
-                                                     const double *__restrict__ sphT, int ncs) {
+                                                     uint8_t *__restrict__ qz) {
   extern __shared__ __align__(16) uint8_t tile[];  // [(1 + nz)][4][128][36]
   const long q = blockIdx.x;
   const size_t T = (size_t)kBatch * kBlockF;
@@ -1372,20 +1450,6 @@ __global__ void __launch_bounds__(256) zquant_kernel(const double *__restrict__ 
 #pragma unroll
       for (int o = 0; o < 4; ++o) {
         if (o >= nop) break;
-        if (o == 0 && qphT) {
-          // phi straight from the pass-A digits of the pair (value component):
-          // X from the four digit bytes, x = X s_g 2^-30
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            const int g = g0 + 4 * gq + r;
-            int X = 0;
-#pragma unroll
-            for (int d = 0; d < 4; ++d)
-              X = X * 256 + (int)(int8_t)qphT[(((size_t)q * ncs * 4 + d) * 256 + g) * 128 + f];
-            v[0][r] = int_to_double(X) * (sphT[(size_t)q * ncs * 256 + g] * 0x1p-30);
-          }
-          continue;
-        }
 #pragma unroll
         for (int r = 0; r < 4; ++r) v[o][r] = src[o * T + (size_t)(g0 + 4 * gq + r) * kBlockF + f];
       }
@@ -1610,6 +1674,10 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     NKX_CUDA(cudaFuncSetAttribute(tc_i8_kernel<TC_MODE_GRAD, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   TcShape<128>::kSmem));
     NKX_CUDA(cudaFuncSetAttribute(zquant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 4 * 128 * 36));
+    NKX_CUDA(cudaFuncSetAttribute(zdigits_kernel<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zdigits_smem(1)));
+    NKX_CUDA(cudaFuncSetAttribute(zdigits_kernel<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zdigits_smem(2)));
+    NKX_CUDA(cudaFuncSetAttribute(zdigits_kernel<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zdigits_smem(1)));
+    NKX_CUDA(cudaFuncSetAttribute(zdigits_kernel<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zdigits_smem(2)));
   }
   MixedState &M = *static_cast<MixedState *>(P.mx_state);
   // orbitals pad to 128 so that either density tile width divides them
@@ -1945,17 +2013,18 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     }
     Tm.end(s);
   };
-  // pass B of one chunk after its Phi / Z staging is written: digits, int8 V
-  // (phi_digits: pass B of the streamed build, whose Phi comes back from the
-  // pass-A digits instead of the FP64 staging)
-  auto pass_b = [&](const Chunk &c, bool phi_digits) {
+  // pass B of one chunk: the digits of the V operands from their FP64
+  // staging (quantise; the streamed build writes them directly), int8 V
+  auto pass_b = [&](const Chunk &c, bool quantise) {
     const long np = c.p1 - c.p0;
-    Tm.begin(ST_ZBUILD, s);
-    zquant_kernel<<<(unsigned)np, 256, (size_t)(1 + nzs) * 4 * 128 * 36, s>>>(
-        P.ws_phi, M.sph, M.sz, nzs, M.qph, M.qz, phi_digits ? M.qphT : nullptr, M.sphT, nc);
-    NKX_LAUNCH_CHECK();
-    ++P.launches;
-    Tm.end(s);
+    if (quantise) {
+      Tm.begin(ST_ZBUILD, s);
+      zquant_kernel<<<(unsigned)np, 256, (size_t)(1 + nzs) * 4 * 128 * 36, s>>>(P.ws_phi, M.sph, M.sz, nzs, M.qph,
+                                                                                M.qz);
+      NKX_LAUNCH_CHECK();
+      ++P.launches;
+      Tm.end(s);
+    }
     Tm.begin(ST_VGEMM, s);
     TcArgs a{};
     a.mode = TC_MODE_V;
@@ -2027,9 +2096,11 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       const long np = c.p1 - c.p0;
       if (np <= 0) continue;
       Tm.begin(ST_ZBUILD, s);
-#define NKX_ZD(G, NZ)                                                                                               \
-  z_from_digits_kernel<G, NZ><<<(unsigned)np, 256, 0, s>>>(M.qphT, M.sphT, P.d_pair_batch, c.p0, P.d_coef, P.npad, \
-                                                           P.ws_phi, M.sph, M.sz, P.d_status + 1)
+      // the V operands' digits straight from the pass-A digits (one cluster
+      // of four CTAs per pair)
+#define NKX_ZD(G, NZ)                                                                                            \
+  zdigits_kernel<G, NZ><<<(unsigned)np * kZdRanks, 256, zdigits_smem(NZ), s>>>(                               \
+      M.qphT, M.sphT, P.d_pair_batch, c.p0, P.d_coef, P.npad, M.qph, M.sph, M.qz, M.sz, P.d_status + 1)
       if (P.gga) {
         if (nspin == 1)
           NKX_ZD(true, 1);
@@ -2045,7 +2116,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       NKX_LAUNCH_CHECK();
       ++P.launches;
       Tm.end(s);
-      pass_b(c, true);
+      pass_b(c, false);
     }
   } else {
     if (phase != 2) {
@@ -2076,7 +2147,7 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       NKX_LAUNCH_CHECK();
       ++P.launches;
       Tm.end(s);
-      pass_b(c, false);
+      pass_b(c, true);
     }
   }
 }
