@@ -1296,67 +1296,89 @@ __global__ void __cluster_dims__(kZdRanks, 1, 1) __launch_bounds__(256, 2)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gbase = kPts * (int)rank;
   const int ncs = NC;
-  uint32_t e[nop][4];
+  uint32_t e[nop][8];
 #pragma unroll
   for (int o = 0; o < nop; ++o)
 #pragma unroll
-    for (int k = 0; k < 4; ++k) e[o][k] = 0u;
-  // ---- phase 1: warp w takes points gbase + w + 8 j, lane l functions 4 l .. 4 l + 3
+    for (int k = 0; k < 8; ++k) e[o][k] = 0u;
+  // ---- phase 1: lanes 16 h .. 16 h + 15 of warp w take point
+  // gl = 2 (w + 8 j) + h, lane l functions 8 (l % 16) .. + 7 (one 8-byte
+  // load per digit plane and component)
+  const int hp = lane >> 4, f8 = 8 * (lane & 15);
 #pragma unroll 2
-  for (int j = 0; j < kPts / 8; ++j) {
-    const int gl = warp + 8 * j, g = gbase + gl;
+  for (int j = 0; j < kPts / 16; ++j) {
+    const int gl = 2 * (warp + 8 * j) + hp, g = gbase + gl;
     const long gg = (long)b * kBatch + g;
-    double v[NC][4];
+    double z[NZ][8], t[NZ][8];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       const long pc = q * ncs + c;
       const double sc = sphT[pc * kBatch + g] * 0x1p-30;
-      uint32_t wd[4], bw[4];
+      uint2 wv[4];
 #pragma unroll
       for (int d = 0; d < 4; ++d)
-        wd[3 - d] = reinterpret_cast<const uint32_t *>(qphT + (pc * 4 + d) * kPlane + (size_t)g * kBlockF)[lane];
-      transpose4(wd, bw);
+        wv[d] = *reinterpret_cast<const uint2 *>(qphT + (pc * 4 + d) * kPlane + (size_t)g * kBlockF + f8);
+      uint32_t bw[8];
+      {
+        const uint32_t lo[4] = {wv[3].x, wv[2].x, wv[1].x, wv[0].x}, hi[4] = {wv[3].y, wv[2].y, wv[1].y, wv[0].y};
+        transpose4(lo, bw);
+        transpose4(hi, bw + 4);
+      }
+      double v[8];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) v[c][k] = int_to_double(digits_value(bw[k])) * sc;
+      for (int k = 0; k < 8; ++k) v[k] = int_to_double(digits_value(bw[k])) * sc;
       if (c == 0) {
-        *reinterpret_cast<uint4 *>(&phid[gl][4 * lane]) = make_uint4(bw[0], bw[1], bw[2], bw[3]);
-        if (lane == 0) phis[gl] = sc;
+        uint4 *pd = reinterpret_cast<uint4 *>(&phid[gl][f8]);
+        pd[0] = make_uint4(bw[0], bw[1], bw[2], bw[3]);
+        pd[1] = make_uint4(bw[4], bw[5], bw[6], bw[7]);
+        if ((lane & 15) == 0) phis[gl] = sc;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) e[0][k] = max(e[0][k], exp_field(v[k]));
+      }
+#pragma unroll
+      for (int s = 0; s < NZ; ++s) {
+        const double cc = coef[((size_t)s * 4 + c) * npad + gg];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          // Z = c0 phi + ((c1 dx phi + c2 dy phi) + c3 dz phi)
+          if (c == 0)
+            z[s][k] = cc * v[k];
+          else if (c == 1)
+            t[s][k] = cc * v[k];
+          else
+            t[s][k] += cc * v[k];
+        }
       }
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) e[0][k] = max(e[0][k], exp_field(v[0][k]));
-#pragma unroll
     for (int s = 0; s < NZ; ++s) {
-      const double *cs = coef + (size_t)s * 4 * npad;
-      const double c0 = cs[gg];
-      double c1 = 0.0, c2 = 0.0, c3 = 0.0;
-      if (GRAD) {
-        c1 = cs[npad + gg];
-        c2 = cs[2 * npad + gg];
-        c3 = cs[3 * npad + gg];
-      }
-      double z[4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        z[k] = c0 * v[0][k];
-        if (GRAD) z[k] += c1 * v[NC > 1 ? 1 : 0][k] + c2 * v[NC > 2 ? 2 : 0][k] + c3 * v[NC > 3 ? 3 : 0][k];
-        e[1 + s][k] = max(e[1 + s][k], exp_field(z[k]));
+      for (int k = 0; k < 8; ++k) {
+        if (GRAD) z[s][k] += t[s][k];
+        e[1 + s][k] = max(e[1 + s][k], exp_field(z[s][k]));
       }
-      double2 *dst = reinterpret_cast<double2 *>(zst + ((size_t)s * kPts + gl) * kBlockF + 4 * lane);
-      dst[0] = make_double2(z[0], z[1]);
-      dst[1] = make_double2(z[2], z[3]);
+      double2 *dst = reinterpret_cast<double2 *>(zst + ((size_t)s * kPts + gl) * kBlockF + f8);
+#pragma unroll
+      for (int k = 0; k < 8; k += 2) dst[k / 2] = make_double2(z[s][k], z[s][k + 1]);
     }
   }
   unsigned ez = 0;
 #pragma unroll
   for (int o = 1; o < nop; ++o)
 #pragma unroll
-    for (int k = 0; k < 4; ++k) ez = max(ez, e[o][k]);
+    for (int k = 0; k < 8; ++k) ez = max(ez, e[o][k]);
   report_nonfinite(ez >= 0x7fdu, nonfinite);
+  // the two points of a warp step, then the warps
 #pragma unroll
   for (int o = 0; o < nop; ++o)
 #pragma unroll
-    for (int k = 0; k < 4; ++k) red[warp][o][4 * lane + k] = e[o][k];
+    for (int k = 0; k < 8; ++k) e[o][k] = max(e[o][k], __shfl_xor_sync(0xffffffffu, e[o][k], 16));
+  if (hp == 0) {
+#pragma unroll
+    for (int o = 0; o < nop; ++o)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) red[warp][o][f8 + k] = e[o][k];
+  }
   __syncthreads();
   for (int t = threadIdx.x; t < nop * 128; t += blockDim.x) {
     uint32_t m = 0u;
