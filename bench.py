@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--no-scf", action="store_true",
                     help="skip the water SCF (Slater + VWN5, SCF to 1e-8 Eh) reported beside the headline")
     ap.add_argument("--no-autotune", action="store_true", help="keep the plan's default kernel choices")
+    ap.add_argument("--tuning", default=None,
+                    help="fixed kernel choices instead of the autotuner, as FockBuilder.set_tuning keywords, "
+                         "e.g. v_pair=1,v_warps=8 (the V contraction on CTA pairs)")
     ap.add_argument("--tune-cache", default=None,
                     help="autotuner cache file: choices found there for this device and problem shape are "
                          "applied without timing, new ones are appended (a profiled run then replays the "
@@ -561,7 +564,11 @@ def run_nkx(args):
         except Exception:
             prec = "fp64"
     tuning = None
-    if prec == "mixed" and not args.no_autotune:
+    if prec == "mixed" and args.tuning:
+        kw = {k: int(v) for k, v in (item.split("=") for item in args.tuning.split(","))}
+        fb.set_tuning(**kw)
+        tuning = dict(fb.tuning(), fixed=True)
+    elif prec == "mixed" and not args.no_autotune:
         # the plan's autotuner picks the MMA widths, the Y path and the chunk
         # size by timing whole builds (untimed setup)
         t0 = time.perf_counter()
