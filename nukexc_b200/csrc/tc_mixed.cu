@@ -1260,7 +1260,7 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
 // (Z_s = c0 phi + c . grad phi, s < nz) go to shared memory in FP64, phi as
 // its packed pass-A digits and point scales, and each (plane, function)
 // row's largest exponent field is reduced over the CTA's warps and then,
-// through the cluster's shared memory, over the four CTAs: the row scale is
+// pushed into every CTA's shared memory, over the four CTAs: the row scale is
 // 2^(E - 1022) for the largest field E, the power-of-two scale of the row
 // maximum.  Each CTA then writes the digits of its 64 points from shared
 // memory as 16-byte pieces of the rows of qph[pair][digit][f][g] and
@@ -1288,13 +1288,16 @@ __global__ void __cluster_dims__(kZdRanks, 1, 1) __launch_bounds__(256, 2)
   uint32_t(*phid)[128] = reinterpret_cast<uint32_t(*)[128]>(zst + (size_t)NZ * kPts * kBlockF);
   double *phis = reinterpret_cast<double *>(phid + kPts);
   __shared__ uint32_t red[8][nop][128];
-  __shared__ uint32_t part[nop][128];
+  __shared__ uint32_t part[kZdRanks][nop][128];  // every CTA's row fields, pushed by their owners
   __shared__ double inv_s[nop][128];
   const uint32_t rank = cluster_rank();
   const long q = cluster_id_x();
   const int b = pair_batch[p0 + q];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gbase = kPts * (int)rank;
+  // first half of a barrier whose wait, before the first store into another
+  // CTA's shared memory, shows that every CTA of the cluster has started
+  cluster_arrive_relaxed();
   const int ncs = NC;
   uint32_t e[nop][8];
 #pragma unroll
@@ -1380,18 +1383,23 @@ __global__ void __cluster_dims__(kZdRanks, 1, 1) __launch_bounds__(256, 2)
       for (int k = 0; k < 8; ++k) red[warp][o][f8 + k] = e[o][k];
   }
   __syncthreads();
+  cluster_wait();
+  // this CTA's row fields go to slot `rank` of every CTA's part[]: every
+  // access to another CTA's shared memory comes before the cluster barrier
+  // below, so none can meet a CTA that has finished
   for (int t = threadIdx.x; t < nop * 128; t += blockDim.x) {
     uint32_t m = 0u;
 #pragma unroll
     for (int w = 0; w < 8; ++w) m = max(m, red[w][t / 128][t % 128]);
-    part[t / 128][t % 128] = m;
+#pragma unroll
+    for (uint32_t rr = 0; rr < kZdRanks; ++rr) st_cluster_u32(map_to_rank(&part[rank][t / 128][t % 128], rr), m);
   }
-  cluster_sync();  // every CTA's row fields are in place
+  cluster_sync();  // every CTA's row fields are in place in every CTA
   for (int t = threadIdx.x; t < nop * 128; t += blockDim.x) {
     const int o = t / 128, f = t % 128;
     uint32_t E = 0u;
 #pragma unroll
-    for (uint32_t rr = 0; rr < kZdRanks; ++rr) E = max(E, ld_cluster_u32(map_to_rank(&part[o][f], rr)));
+    for (int rr = 0; rr < kZdRanks; ++rr) E = max(E, part[rr][o][f]);
     double sc = 1.0, inv = 1.0;  // an all-zero row keeps scale 1
     if (E > 0u && E < 0x7fdu) {
       sc = __hiloint2double((int)((E + 1u) << 20), 0);
@@ -1439,7 +1447,6 @@ __global__ void __cluster_dims__(kZdRanks, 1, 1) __launch_bounds__(256, 2)
       }
     }
   }
-  cluster_sync();  // no CTA leaves while another may still read its row fields
 }
 
 // Pass B, part 2: digits of the V operands, transposed to
