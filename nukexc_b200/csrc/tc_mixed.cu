@@ -1268,7 +1268,8 @@ __global__ void __launch_bounds__(256, 2) colloc_z_kernel(const StoFunc *__restr
 // szs[pair][z][f].  Against the staging of Z in HBM by a separate kernel
 // this moves about half the bytes (the pass-A digits in, the V digits
 // out).  (Clusters of eight CTAs of 32 points, phi staged in FP64, ran
-// 111 ms per (H2O)64 build against 97.)  A row field of 0x7fd or more
+// 111 ms per (H2O)64 build against 97.)  Planes s >= nspin (a J build's
+// separate Coulomb plane) are Z = 1/2 vJ phi.  A row field of 0x7fd or more
 // (values of 2^1022 and up, Inf, NaN) is reported in *nonfinite.
 constexpr int kZdRanks = 4;
 constexpr size_t zdigits_smem(int nz) {
@@ -1277,9 +1278,9 @@ constexpr size_t zdigits_smem(int nz) {
 template <bool GRAD, int NZ>
 __global__ void __cluster_dims__(kZdRanks, 1, 1) __launch_bounds__(256, 2)
     zdigits_kernel(const uint8_t *__restrict__ qphT, const double *__restrict__ sphT,
-                   const int *__restrict__ pair_batch, long p0, const double *__restrict__ coef, long npad,
-                   uint8_t *__restrict__ qph, double *__restrict__ sph, uint8_t *__restrict__ qz,
-                   double *__restrict__ szs, int *nonfinite) {
+                   const int *__restrict__ pair_batch, long p0, const double *__restrict__ coef,
+                   const double *__restrict__ vj, int nspin, long npad, uint8_t *__restrict__ qph,
+                   double *__restrict__ sph, uint8_t *__restrict__ qz, double *__restrict__ szs, int *nonfinite) {
   constexpr int NC = GRAD ? 4 : 1, nop = 1 + NZ, kPts = kBatch / kZdRanks;
   constexpr size_t kPlane = (size_t)kBatch * kBlockF;  // one digit plane of a pair, bytes
   // dynamic shared memory: Z_s [NZ][kPts][128] FP64, then phi as packed
@@ -1340,7 +1341,7 @@ __global__ void __cluster_dims__(kZdRanks, 1, 1) __launch_bounds__(256, 2)
       }
 #pragma unroll
       for (int s = 0; s < NZ; ++s) {
-        const double cc = coef[((size_t)s * 4 + c) * npad + gg];
+        const double cc = s < nspin ? coef[((size_t)s * 4 + c) * npad + gg] : (c == 0 ? 0.5 * vj[gg] : 0.0);
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
           // Z = c0 phi + ((c1 dx phi + c2 dy phi) + c3 dz phi)
@@ -1592,6 +1593,52 @@ struct MixedState {
     cudaFree(T);
     cudaFree(qt0);
     cudaFree(X);
+    cudaFree(qphT_res);
+    cudaFree(sphT_res);
+  }
+  // J builds: every chunk's pass-A digits and scales, kept until pass B when
+  // they fit in half of the free device memory (qphT / sphT / m_phT then
+  // address the current chunk's slice of them; the chunk buffers are
+  // restored after the build)
+  uint8_t *qphT_res = nullptr, *qphT_chunk = nullptr;
+  double *sphT_res = nullptr, *sphT_chunk = nullptr;
+  CUtensorMap m_phT_chunk;
+  long res_pairs = 0;
+  bool ensure_resident(long npairs) {
+    const size_t tile = (size_t)kBatch * kBlockF;
+    if (qphT_res && res_pairs >= npairs) return true;
+    cudaFree(qphT_res);
+    cudaFree(sphT_res);
+    qphT_res = nullptr;
+    sphT_res = nullptr;
+    res_pairs = 0;
+    const size_t bytes = (size_t)npairs * 4 * 4 * tile, sbytes = (size_t)npairs * 4 * 256 * sizeof(double);
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess || bytes + sbytes > fr / 2) {
+      cudaGetLastError();
+      return false;
+    }
+    if (cudaMalloc(&qphT_res, bytes) != cudaSuccess || cudaMalloc(&sphT_res, sbytes) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(qphT_res);
+      cudaFree(sphT_res);
+      qphT_res = nullptr;
+      sphT_res = nullptr;
+      return false;
+    }
+    res_pairs = npairs;
+    return true;
+  }
+  void use_resident_slice(const Chunk &c) {
+    const size_t tile = (size_t)kBatch * kBlockF;
+    qphT = qphT_res + (size_t)c.p0 * 4 * 4 * tile;
+    sphT = sphT_res + (size_t)c.p0 * 4 * 256;
+    m_phT = make_map3(qphT, 128, 256, std::max<long>(1, c.p1 - c.p0) * 4 * 4, 128);
+  }
+  void use_chunk_buffers() {
+    qphT = qphT_chunk;
+    sphT = sphT_chunk;
+    m_phT = m_phT_chunk;
   }
   double *X = nullptr;  // the mixed gradient's X[pair][spin][comp][g][mu]
   size_t X_cap = 0;
@@ -1667,6 +1714,9 @@ static MixedState &mixed_state(Plan &P, int nocc) {
     M->qz = M->alloc<uint8_t>(M->cap * 3 * 4 * tile);
     M->sz = M->alloc<double>(M->cap * 3 * 128);
     M->m_phT = make_map3(M->qphT, 128, 256, M->cap * 4 * 4, 128);
+    M->qphT_chunk = M->qphT;
+    M->sphT_chunk = M->sphT;
+    M->m_phT_chunk = M->m_phT;
     M->m_ph = make_map3(M->qph, 256, 128, M->cap * 4, 128);
     M->m_z = make_map3(M->qz, 256, 128, M->cap * 3 * 4, 128);
     M->m_z64 = make_map3(M->qz, 256, 128, M->cap * 3 * 4, 64);
@@ -2105,6 +2155,29 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     ++P.launches;
     Tm.end(s);
   };
+  // the V operands' digits of one chunk straight from its pass-A digits
+  // (one cluster of four CTAs per pair); nzs <= 2
+  auto launch_zdigits = [&](const Chunk &c) {
+    const long np = c.p1 - c.p0;
+#define NKX_ZD(G, NZ)                                                                                            \
+  zdigits_kernel<G, NZ><<<(unsigned)np * kZdRanks, 256, zdigits_smem(NZ), s>>>(                               \
+      M.qphT, M.sphT, P.d_pair_batch, c.p0, P.d_coef, P.d_vj, nspin, P.npad, M.qph, M.sph, M.qz, M.sz,         \
+      P.d_status + 1)
+    if (P.gga) {
+      if (nzs == 1)
+        NKX_ZD(true, 1);
+      else
+        NKX_ZD(true, 2);
+    } else {
+      if (nzs == 1)
+        NKX_ZD(false, 1);
+      else
+        NKX_ZD(false, 2);
+    }
+#undef NKX_ZD
+    NKX_LAUNCH_CHECK();
+    ++P.launches;
+  };
   NKX_CUDA(cudaMemsetAsync(P.d_E, 0, sizeof(double), s));
   NKX_CUDA(cudaMemsetAsync(P.d_V, 0, sizeof(double) * nzs * P.nbf_pad * P.nbf_pad, s));
   if (!needJ) {
@@ -2127,29 +2200,27 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
       Tm.begin(ST_ZBUILD, s);
       // the V operands' digits straight from the pass-A digits (one cluster
       // of four CTAs per pair)
-#define NKX_ZD(G, NZ)                                                                                            \
-  zdigits_kernel<G, NZ><<<(unsigned)np * kZdRanks, 256, zdigits_smem(NZ), s>>>(                               \
-      M.qphT, M.sphT, P.d_pair_batch, c.p0, P.d_coef, P.npad, M.qph, M.sph, M.qz, M.sz, P.d_status + 1)
-      if (P.gga) {
-        if (nspin == 1)
-          NKX_ZD(true, 1);
-        else
-          NKX_ZD(true, 2);
-      } else {
-        if (nspin == 1)
-          NKX_ZD(false, 1);
-        else
-          NKX_ZD(false, 2);
-      }
-#undef NKX_ZD
-      NKX_LAUNCH_CHECK();
-      ++P.launches;
+      launch_zdigits(c);
       Tm.end(s);
       pass_b(c, false);
     }
   } else {
+    // J needs every point's density before any Z.  When every chunk's pass-A
+    // digits fit in half of the free device memory (at (H2O)32, 47 GB) they
+    // stay there until pass B, which takes Phi and grad Phi back from them
+    // (zdigits_kernel); otherwise pass B evaluates the STOs again
+    // (colloc_z_kernel) and quantises their FP64 staging.  Only whole builds
+    // (a two-phase build may run other builds between its phases).
+    const bool resident = phase == 0 && nzs <= 2 && M.ensure_resident(P.npairs);
+    struct Restore {
+      MixedState &M;
+      ~Restore() { M.use_chunk_buffers(); }
+    } restore{M};
     if (phase != 2) {
-      for (const Chunk &c : P.chunks) pass_a(c);
+      for (const Chunk &c : P.chunks) {
+        if (resident) M.use_resident_slice(c);
+        pass_a(c);
+      }
       // this plan's share of the J fit vector
       Tm.begin(ST_COULOMB, s);
       coulomb_y(P, nspin, s, true);
@@ -2167,10 +2238,18 @@ void fock_build_mixed(Plan &P, int nspin, int nocc, bool needJ, bool fuse, bool 
     NKX_LAUNCH_CHECK();
     ++P.launches;
     Tm.end(s);
-    // ---- pass B: Phi and Z from a second collocation (J needs every point's
-    // density before any Z), digits, int8 V contraction
+    // ---- pass B: Phi and Z from the resident pass-A digits or from a second
+    // collocation, digits, int8 V contraction
     for (const Chunk &c : P.chunks) {
       if (c.p1 - c.p0 <= 0) continue;
+      if (resident) {
+        M.use_resident_slice(c);
+        Tm.begin(ST_ZBUILD, s);
+        launch_zdigits(c);
+        Tm.end(s);
+        pass_b(c, false);
+        continue;
+      }
       Tm.begin(ST_COLLOC, s);
       launch_colloc_z(P, M, c, nzs, nspin, s);
       NKX_LAUNCH_CHECK();
