@@ -1,7 +1,8 @@
 """CUDA-graph replay of the Fock build (nkx_plan_set_graph): builds with
 device buffers are recorded into a graph on the second call of a kind and
 replayed from then on.  Replayed builds must equal ordinary ones (up to the
-order of atomic FP64 additions, 1e-12), with the caller passing new buffers
+order of atomic FP64 additions: 1e-12, and 1e-10 for what carries the
+Coulomb fit), with the caller passing new buffers
 each time; a change of kind (precision, J mode) or of the plan re-records;
 the water SCF on the device converges to the same energy with replays."""
 import numpy as np
@@ -43,7 +44,10 @@ def test_replayed_builds_equal_ordinary_builds(precision, jmode):
         E, V, J = fb.build([C2], [occ], precision=precision, **kw)
         Eo, Vo, Jo = ref.build([C2], [occ], precision=precision, **kw)
         assert abs(E - Eo) <= 1e-12 * abs(Eo)
-        assert float((V[0] - Vo[0]).abs().max()) <= 1e-12 * float(Vo[0].abs().max())
+        # with J fused, V holds the Coulomb potential, whose fit vector varies
+        # at rounding level from build to build (below)
+        vtol = 1e-10 if jmode == "fused" else 1e-12
+        assert float((V[0] - Vo[0]).abs().max()) <= vtol * float(Vo[0].abs().max())
         if jmode == "separate":
             # the fit vector y is summed with atomic FP64 adds in varying order
             # and the solve with the grid metric (condition number about 1e5 for
