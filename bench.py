@@ -8,8 +8,8 @@ A step is one Fock build (one SCF iteration's XC work: collocation, density,
 functional, V_xc = Phi Z^T) over the whole synthetic (H2O)_n grid
 (Treutler-Ahlrichs 75 radial x Lebedev 302 per atom, Becke, 256-point
 batches, screening 1e-10), with the orbital coefficients already resident in
-HBM.  `e2e` is the same build through the public API with host buffers
-(C copied in, V and E copied out inside the timed region).  One JSON line is
+HBM.  `e2e` is the same build through the public API with page-locked host
+buffers (C and occ copied in, V and E copied out inside the timed region).  One JSON line is
 printed by rank 0.  With N > 1 the grid is split into Morton-contiguous,
 cost-balanced batch ranges (one process per GPU, shard.balanced_split) and
 the partial V_xc and E_xc are summed with an NCCL all-reduce inside the
@@ -576,6 +576,19 @@ def run_nkx(args):
         tuning["seconds"] = time.perf_counter() - t0
         info = fb.info()
 
+    # page-locked host buffers of the end-to-end step: C (column-major, as the
+    # C-ABI takes it) and occ copied in, V copied out, every step
+    pinned = {}
+
+    def host_buffers():
+        if not pinned:
+            Cp = torch.empty((Cm.shape[1], nbf), dtype=torch.float64, pin_memory=True)
+            Cp.copy_(torch.from_numpy(np.ascontiguousarray(Cm.T)))
+            op = torch.empty(occ.shape[0], dtype=torch.float64, pin_memory=True)
+            op.copy_(torch.from_numpy(occ))
+            pinned.update(C=Cp.t(), occ=op, V=torch.empty(nbf * nbf, dtype=torch.float64, pin_memory=True))
+        return pinned
+
     def step(host=False):
         if fuse and dist is not None:
             # J on a sharded grid: density, all-reduce of the fit vector y,
@@ -585,7 +598,9 @@ def run_nkx(args):
                                       stream=stream.cuda_stream)
             return E
         if host:
-            E, V, _ = fb.build([Cm], [occ], precision=prec, fuse_j=fuse, stream=stream.cuda_stream)
+            hb = host_buffers()
+            E, V, _ = fb.build([hb["C"]], [hb["occ"]], precision=prec, fuse_j=fuse, stream=stream.cuda_stream,
+                               out_V=hb["V"])
             # the all-reduce of several ranks needs V back on the device
             V = torch.as_tensor(V[0], device="cuda") if dist is not None else V[0]
         else:

@@ -358,19 +358,42 @@ class FockBuilder:
         check(L.lib().nkx_get_last_timing(self._h, C.byref(t)))
         return {k: getattr(t, k) for k, _ in L.BuildTiming._fields_}
 
-    def build(self, C_list, occ_list, precision="fp64", want_J=False, fuse_j=False, stream=None, want_V=True):
+    def build(self, C_list, occ_list, precision="fp64", want_J=False, fuse_j=False, stream=None, want_V=True,
+              out_V=None):
         """One Fock build.  C_list/occ_list: one (nbf x nocc, nocc) per spin,
-        numpy (host: copied inside the call) or CUDA tensors (device).
-        Returns (E_xc, [V per spin], J or None); with fuse_j, V includes J.
-        want_V=False (with want_J) returns J alone: (E_xc, None, J)."""
+        numpy or CPU tensors (host: copied inside the call) or CUDA tensors
+        (device).  Returns (E_xc, [V per spin], J or None); with fuse_j, V
+        includes J.  want_V=False (with want_J) returns J alone: (E_xc, None, J).
+        Host builds with page-locked buffers copy at full PCIe / C2C speed: a
+        single spin's C as a pinned CPU tensor stored column-major (C.t()
+        contiguous) and occ as a pinned CPU tensor are passed as they are, and
+        out_V, a pinned CPU tensor of nspin * nbf^2 doubles, receives V (the
+        returned matrices are views of it)."""
         if not want_V and not (want_J and not fuse_j):
             raise ValueError("want_V=False needs want_J=True and fuse_j=False")
         nspin = len(C_list)
-        host = not isinstance(C_list[0], torch.Tensor)
+        host = not (isinstance(C_list[0], torch.Tensor) and C_list[0].is_cuda)
         nocc = C_list[0].shape[1]
         prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
         nn = self.nbf * self.nbf
-        if host:
+        if host and isinstance(C_list[0], torch.Tensor):
+            # CPU tensors: used in place when already in the C-ABI's layout
+            if nspin == 1 and C_list[0].dtype == torch.float64 and C_list[0].t().is_contiguous():
+                Cc = C_list[0]
+            else:
+                Cc = torch.cat([c.to(torch.float64).t().contiguous().reshape(-1) for c in C_list])
+            oc = occ_list[0] if nspin == 1 and occ_list[0].dtype == torch.float64 and occ_list[0].is_contiguous() \
+                else torch.cat([o.to(torch.float64).reshape(-1) for o in occ_list])
+            if out_V is not None and want_V:
+                if out_V.dtype != torch.float64 or out_V.numel() != nspin * nn or not out_V.is_contiguous():
+                    raise ValueError("out_V must be a contiguous float64 CPU tensor of nspin * nbf^2 elements")
+                V = out_V.reshape(-1).numpy()
+            else:
+                V = np.empty(nspin * nn) if want_V else None
+            J = np.empty(nn) if want_J and not fuse_j else None
+            pC, po = C.c_void_p(Cc.data_ptr()), C.c_void_p(oc.data_ptr())
+            pV, pJ = (a.ctypes.data_as(C.c_void_p) if a is not None else None for a in (V, J))
+        elif host:
             Cc = np.concatenate([np.ascontiguousarray(np.asarray(c, np.float64).T).reshape(-1) for c in C_list])
             oc = np.concatenate([_np(o, np.float64) for o in occ_list])
             V = np.empty(nspin * nn) if want_V else None

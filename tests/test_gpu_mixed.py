@@ -110,3 +110,32 @@ def test_mixed_gga_many_orbitals_gradient_path():
     assert abs(Em - E64) < E_TOL
     for s in range(2):
         assert np.abs(Vm[s] - V64[s]).max() < V_TOL
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_pinned_host_buffers_match_device_build(precision):
+    """Host builds from page-locked CPU tensors (C column-major and occ passed
+    as they are, V written into the caller's pinned out_V) equal the build
+    from device tensors and the one from numpy arrays, twice in a row."""
+    c, Z, funcs, g = case(2, seed=7)
+    fb = A.FockBuilder(c, Z, A.make_manual_basis(funcs), g, func_ids=("GGA_X_PBE", "GGA_C_PBE"))
+    nbf = len(funcs)
+    Cm = M.random_orbitals(nbf, 9, seed=8)
+    occ = np.linspace(2.0, 1.0, 9)
+    Ed, Vd, _ = fb.build([torch.as_tensor(Cm, device="cuda")], [torch.as_tensor(occ, device="cuda")],
+                         precision=precision)
+    En, Vn, _ = fb.build([Cm], [occ], precision=precision)
+    Cp = torch.empty((9, nbf), dtype=torch.float64, pin_memory=True)
+    Cp.copy_(torch.from_numpy(np.ascontiguousarray(Cm.T)))
+    op = torch.empty(9, dtype=torch.float64, pin_memory=True)
+    op.copy_(torch.from_numpy(occ))
+    Vp = torch.empty(nbf * nbf, dtype=torch.float64, pin_memory=True)
+    for _ in range(2):
+        Vp.fill_(float("nan"))
+        Ep, Vs, _ = fb.build([Cp.t()], [op], precision=precision, out_V=Vp)
+        assert np.shares_memory(Vs[0], Vp.numpy())
+        scale = float(Vd[0].abs().max())
+        for E, V in ((Ed, Vd[0].cpu().numpy()), (En, Vn[0])):
+            assert abs(Ep - E) <= 1e-12 * abs(E)
+            assert np.abs(Vs[0] - V).max() <= 1e-12 * scale
+    fb.close()
