@@ -400,7 +400,7 @@ def xc_gradient_check(n, stream, ngeom=10, ncomp=1, h=1e-4):
 
 
 def aggregate_gate(natoms, stream, int8_peak=None):
-    """Survey configuration 5: the seeded C/H/N/O aggregate (3:5:1:1, random
+    """The 1500-atom workload: the seeded C/H/N/O aggregate (3:5:1:1, random
     packing in a sphere, d_min 1.0 A, ~12000 STO functions, ~3e7 points),
     PBE, nocc = electrons / 2: one warm-up and one timed mixed build, one
     timed FP64 build of the same plan, and the accuracy gate of the mixed

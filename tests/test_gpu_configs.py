@@ -1,11 +1,10 @@
-"""Parity with the CPU oracle on the configurations' own grid: Treutler-
+"""Parity with the CPU oracle on the benchmark workloads' own grid: Treutler-
 Ahlrichs M4 75 radial x Lebedev 302 per atom, Becke with the Laqua clamp,
-w > 1e-15 (the benchmark's grid), instead of the reduced grids of the other
-parity tests.
+w > 1e-15, instead of the reduced grids of the other parity tests.
 
-* configuration 1: water, Slater + VWN5, closed and open shell;
-* configuration 2 at n = 8: (H2O)_8 PBE (543,600 points before compaction,
-  384 functions, 40 orbitals);
+* the water case: Slater + VWN5, closed and open shell;
+* the water-cluster case at n = 8: (H2O)_8 PBE (543,600 points before
+  compaction, 384 functions, 40 orbitals);
 * the grid itself, and the grid DF-J of water on it.
 
 Tolerances: FP64 build vs oracle 1e-10 relative on E_xc and 1e-10 absolute on

@@ -1,4 +1,4 @@
-"""Survey configuration 1: water, Slater + VWN5, TA-M4 75 x Lebedev 302,
+"""The water case: Slater + VWN5, TA-M4 75 x Lebedev 302,
 plain closed-shell SCF to 1e-8 Eh with the stand-in driver
 (nukexc_b200/scf.py) -- on the GPU (core Hamiltonian by quadrature through
 nkx_core_hamiltonian_dense, XC and grid DF-J through nkx_fock_build) and on
